@@ -1,0 +1,289 @@
+#!/usr/bin/env python
+"""k-mer counting throughput (Gbp/s) of the B200 counter, with the reference
+CPU path timed beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step counts every k-mer of one batch of synthetic reads end to end: reads
+-> superkmers -> canonical 31-mers -> counts -> threshold >= 2.  The default
+workload is the 100 Mbp bacterial-to-small-eukaryote genome (GC 41%, 10%
+repeat families at 2% divergence) read as 20M x 150 bp reads at 30x (3 Gbp,
+0.3% substitutions), k=31, m=11, canonical; it is generated here from a fixed
+seed (no public dataset is available).  Its 3 GB of reads exceed L2, so no L2
+flush is needed between steps.
+
+Reported (one JSON line on rank 0):
+  value      Gbp/s with the reads already in device memory (whole job, all ranks)
+  e2e        Gbp/s through the C ABI from pinned host reads to host (k-mer,
+             count) arrays, copies inside the timed region
+  roofline   the dominant kernel class: algorithmic DRAM bytes per launch /
+             CUDA-event launch time, against the measured HBM copy bandwidth
+  cpu_baseline  the reference's own CPU path (oracle/_ref, compiled from its
+             sources) on a bounded sample of the same workload, all host cores
+With --gpus N > 1 (under torchrun) each rank counts its own read set of the
+same size drawn from the same genome (weak scaling, no collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "k-mer counting Gbp/s at k=31 on 1 B200, learned vs default order, bit-exact"
+WORKLOAD_DESC = {
+    "bacterial_100m": "100 Mbp genome GC 41%, 10% repeats (200 families 1-5 kb, 2% div); 20M x 150 bp reads, "
+                      "30x, 0.3% subst., both strands",
+    "uniform_5m": "5 Mbp uniform genome; 1M x 150 bp reads, 30x, 0.5% subst., both strands",
+    "skewed_200m": "200 Mbp genome GC 38%, 8% low-complexity, 15% repeats; 40M x 150 bp reads, 30x, 0.3% subst.",
+    "mixed_100m": "100 Mbp genome; 80% bases from 150 bp reads (0.3%), 20% log-normal long reads (5%)",
+}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(", ") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        mx = float(rows[0][2])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(args, threads):
+    """The reference's CPU path (oracle/_ref) on a bounded sample of the workload."""
+    from oracle.oracle import RefOracle
+    from rapidgkc_b200 import synth
+    ref = RefOracle()
+    reads, offs = synth.make_workload(args.workload, read_fraction=args.cpu_fraction, threads=threads)
+    t0 = time.perf_counter()
+    d, t1, t2 = ref.run(reads, offs, args.k, args.p, args.partitions, threads)
+    wall = time.perf_counter() - t0
+    bases = int(offs[-1])
+    return {"value": bases / wall / 1e9, "unit": "Gbp/s", "cores": threads, "kind": "reference",
+            "sample": f"{len(offs) - 1} reads ({bases / 1e6:.0f} Mbp, {args.cpu_fraction:.1%} of the workload's "
+                      f"reads, same genome); reference cpu_funcs.cpp phase 1 + KmerCountingCPU per partition, "
+                      f"in-tree MSD radix sort (RADULS not in the reference build); wall {wall:.1f} s "
+                      f"(phase1 {t1:.1f} s, phase2 {t2:.1f} s); {d} distinct"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    vals = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(args, threads)
+        if i >= args.warmup:
+            vals.append(b["value"])
+            base = b
+    v = statistics.mean(vals)
+    base["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Gbp/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": args.workload, "k": args.k, "p": args.p, "partitions": args.partitions,
+                       "threshold": ">=2", "sample_fraction": args.cpu_fraction},
+            "cpu_baseline": base,
+            "e2e": {"value": v, "unit": "Gbp/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="bacterial_100m")
+    ap.add_argument("--counter", default="hash", choices=["hash", "sort"])
+    ap.add_argument("--k", type=int, default=31)
+    ap.add_argument("--p", type=int, default=11)
+    ap.add_argument("--partitions", type=int, default=512)
+    ap.add_argument("--cmin", type=int, default=2)
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--cpu-fraction", type=float, default=0.01)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    from rapidgkc_b200 import KmerCounter, synth
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    threads = max(1, (os.cpu_count() or 1) // max(1, world))
+    t_gen = time.perf_counter()
+    reads, offs = synth.make_workload(args.workload, scale=args.scale, pinned=True, threads=threads,
+                                      read_seed=rank)
+    t_gen = time.perf_counter() - t_gen
+    bases = int(offs[-1])
+    d_reads = torch.from_numpy(reads).cuda()
+    d_offs = torch.from_numpy(offs.view(np.int64)).cuda()
+    stream = torch.cuda.Stream()
+    c = KmerCounter(k=args.k, p=args.p, partitions=args.partitions, counter=args.counter, device=local)
+    c.set_stream(stream)
+
+    def step_device():
+        return c.count_reads(d_reads, d_offs, args.cmin)
+
+    # ---- device-resident throughput ----
+    for _ in range(args.warmup):
+        n_out, n_dist = step_device()
+    torch.cuda.synchronize()
+    barrier()
+    c.set_profiling(True)
+    c.kernel_stats(reset=True)
+    launches0 = c.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            n_out, n_dist = step_device()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    launches = (c.kernel_launches() - launches0) // args.steps
+    kstats = c.kernel_stats(reset=True)
+    c.set_profiling(False)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = bases * world / (ms / 1e3) / 1e9
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        cap = int(n_out * 1.05) + 1024
+        hk = torch.empty(cap, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+        hc = torch.empty(cap, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        for _ in range(max(1, args.warmup // 2)):
+            c.count_reads(reads, offs, args.cmin, out_kmers=hk, out_counts=hc)
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            no, _ = c.count_reads(reads, offs, args.cmin, out_kmers=hk, out_counts=hc)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": bases * world / (ems / 1e3) / 1e9, "unit": "Gbp/s",
+               "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)), "d2h_bytes_per_step": int(12 * no),
+               "ms_per_step": ems}
+
+    # ---- roofline of the dominant kernel class ----
+    hbm, src = peaks()
+    dom = max(kstats, key=lambda k: kstats[k][0])
+    kms, kl, kb = kstats[dom]
+    per_launch_s = kms / 1e3 / max(kl, 1)
+    achieved = kb / max(kl, 1) / per_launch_s / 1e9 if kl else 0.0
+    classes = {k: {"ms_per_step": v[0] / args.steps, "launches_per_step": v[1] // args.steps,
+                   "gbs": (v[2] / (v[0] / 1e3) / 1e9) if v[0] else 0.0}
+               for k, v in kstats.items() if v[1]}
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": src, "traffic": None,
+                "bytes_per_launch": kb / max(kl, 1), "launch_ms": per_launch_s * 1e3, "classes": classes}
+
+    line = {"metric": METRIC, "value": value, "unit": "Gbp/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": WORKLOAD_DESC.get(args.workload, ""),
+                       "bases_per_rank": bases, "reads_per_rank": len(offs) - 1, "k": args.k, "p": args.p,
+                       "partitions": args.partitions, "counter": args.counter, "order": "default",
+                       "threshold": f">={args.cmin}", "parallelism": f"dp{world} (independent read sets)",
+                       "l2": "inputs (3 GB) larger than L2; no flush", "kmers_kept": n_out,
+                       "distinct": n_dist, "gen_s": round(t_gen, 1)},
+            "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches)}
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(args, os.cpu_count() or 1)
+        except Exception as ex:  # the reference library is test infrastructure; report why it is absent
+            line["cpu_baseline"] = {"value": None, "unavailable": str(ex)}
+    c.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

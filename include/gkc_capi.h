@@ -1,0 +1,155 @@
+/*
+ * gkc_capi.h -- C ABI of the B200 k-mer counter (librapidgkc_b200.so).
+ *
+ * Plain pointers and sizes only.  Every function returns GKC_OK (0) or a
+ * negative GKC_E* code and never exits the process; gkc_last_error() gives
+ * the message.  A context is bound to one CUDA device and is not thread-safe:
+ * use one context per host thread (the reference runs several host workers
+ * per GPU, utilities.hpp:214; each would own a context here).
+ *
+ * The entry points replace the reference's GPU interface
+ * (paths relative to the RapidGKC source tree):
+ *   gkc_create       GPUReset                 gpu_skmgen.h:52, gpu_skmgen.cu:487-497
+ *   gkc_add_reads    GenSuperkmerGPU          gpu_skmgen.h:54-58, gpu_skmgen.cu:504-718
+ *   gkc_store_stats  SKMStoreNoncon counters  skmstore.hpp:85-87
+ *   gkc_store_export SKMStoreNoncon bytes     skmstore.hpp:156-187, 222-236
+ *   gkc_count        kmc_counting_GPU_streams gpu_kmercounting.h:14-17, gpu_kmercounting.cu:343-548
+ *   gkc_result       the kmc_result vectors   gkc_main.cpp:294, gpu_kmercounting.cu:505-508
+ * and add what the reference declares but never does: the count threshold
+ * [min, max] (utilities.hpp:190) and an output of the counted k-mers.
+ */
+#ifndef GKC_CAPI_H
+#define GKC_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    GKC_OK = 0,
+    GKC_EINVAL = -1,    /* bad argument */
+    GKC_ECUDA = -2,     /* CUDA runtime error */
+    GKC_ENOMEM = -3,    /* device or pinned memory exhausted */
+    GKC_ESTATE = -4,    /* call out of order (e.g. result before count) */
+    GKC_EINTERNAL = -5  /* retries exhausted or inconsistent internal state */
+};
+
+enum { GKC_COUNTER_SORT = 0, GKC_COUNTER_HASH = 1 };
+enum { GKC_MEM_HOST = 0, GKC_MEM_DEVICE = 1 };
+
+typedef struct gkc_ctx gkc_ctx;
+
+typedef struct gkc_options {
+    int k;                  /* k-mer length, p <= k <= 32 (reference -k, utilities.hpp:187)      */
+    int p;                  /* minimizer length, 3 <= p <= 16 (reference -p, utilities.hpp:188)   */
+    int partitions;         /* superkmer partitions, 1..4096 (reference -skm, utilities.hpp:189)  */
+    int counter;            /* GKC_COUNTER_SORT or GKC_COUNTER_HASH                               */
+    int radix_bits;         /* LSD digit width of the sort counter, 4..8 (0 = 8)                  */
+    double table_slots;     /* hash slots per k-mer instance of a partition (0 = 0.75)            */
+    uint64_t batch_bases;   /* bases per phase-1 batch for host input (0 = 1 GiB)                 */
+    int spill_host;         /* keep the partition store in pinned host memory (streamed input)    */
+    uint64_t group_keys;    /* max k-mer instances per sort group (0 = from free device memory)   */
+} gkc_options;
+
+/* Fills defaults: k=31, p=11, partitions=512, hash counter. */
+void gkc_default_options(gkc_options *opt);
+
+/* Creates a context on CUDA device `device` (replaces GPUReset; the device
+ * is not reset, other users of it are unaffected). */
+int gkc_create(int device, const gkc_options *opt, gkc_ctx **out);
+int gkc_destroy(gkc_ctx *ctx);
+const char *gkc_last_error(const gkc_ctx *ctx);
+const char *gkc_strerror(int code);
+
+/* Minimizer order: `lut` holds 4^p ranks (uint32) indexed by the 2-bit p-mer
+ * value; the canonical minimizer of a k-mer is the p-mer of least rank over
+ * both strands.  NULL restores the reference's default order (value order
+ * with the "rapidgkc" filter, minimizer_filter.h:20).  `mem` says where lut
+ * lives. */
+int gkc_set_order(gkc_ctx *ctx, const uint32_t *lut, uint64_t n, int mem);
+
+/* Phase 1: splits a CSR batch of ASCII reads (reads[offs[i]..offs[i+1])) into
+ * superkmers and appends them to the context's partition store.  Host input
+ * is copied in batches of opt.batch_bases bases, overlapped with compute
+ * (pinned host memory gives the overlap).  Device input requires offs[0]==0.
+ * Reads shorter than k contribute nothing. */
+int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads, int mem);
+
+/* Per-partition totals of the store: superkmer bytes, superkmers, k-mers
+ * (SKMStoreNoncon::tot_size_bytes / skm_cnt / kmer_cnt).  Arrays of
+ * opt.partitions entries; any may be NULL. */
+int gkc_store_stats(gkc_ctx *ctx, uint64_t *part_bytes, uint64_t *part_skms, uint64_t *part_kmers);
+
+/* Copies partition `part`'s superkmer bytes (the reference's .skm format,
+ * skmstore.hpp:129-141) to host memory `out` of `cap` bytes; *n = bytes. */
+int gkc_store_export(gkc_ctx *ctx, int part, uint8_t *out, uint64_t cap, uint64_t *n);
+
+/* Drops every superkmer in the store. */
+int gkc_store_clear(gkc_ctx *ctx);
+
+/* Phase 2: counts every partition of the store and keeps the k-mers whose
+ * count c satisfies cmin <= c <= cmax.  *n_out = k-mers kept; *n_distinct =
+ * distinct k-mers before the threshold (the reference's return value).  The
+ * store is consumed (the reference deletes its stores, gpu_kmercounting.cu:532).
+ * Output order: partition by partition; ascending k-mer inside a partition
+ * with the sort counter, unordered with the hash counter. */
+int gkc_count(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, uint64_t *n_out, uint64_t *n_distinct);
+
+/* Copies the last gkc_count result: kmers[i] (2-bit, first base in the most
+ * significant position, canonical) and counts[i], i < min(cap, n_out). */
+int gkc_result(gkc_ctx *ctx, uint64_t *kmers, uint32_t *counts, uint64_t cap, int mem);
+
+/* Device pointers to the last result (valid until the next call). */
+int gkc_result_device(gkc_ctx *ctx, const uint64_t **kmers, const uint32_t **counts, uint64_t *n);
+
+/* One call: gkc_store_clear + gkc_add_reads + gkc_count + gkc_result. */
+int gkc_count_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads, int mem,
+                    uint32_t cmin, uint32_t cmax, uint64_t *kmers, uint32_t *counts, uint64_t cap,
+                    int out_mem, uint64_t *n_out, uint64_t *n_distinct);
+
+/* Counts raw 64-bit keys (no superkmers, no canonical step) with the
+ * configured counter; results as gkc_count.  keys must not be 2^64-1. */
+int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint32_t cmin, uint32_t cmax,
+                   uint64_t *n_out, uint64_t *n_distinct);
+
+/* Device milliseconds of the last gkc_add_reads (phase 1) and gkc_count
+ * (phase 2) calls, from CUDA events; times[0..3] = phase 1 total, phase 1
+ * superkmer search, phase 2 total, phase 2 dominant kernel. */
+int gkc_last_timings(gkc_ctx *ctx, double *times, int n);
+
+/* Number of kernels this context launched since creation. */
+uint64_t gkc_kernel_launches(const gkc_ctx *ctx);
+
+/* Runs the context's work on `stream` (a cudaStream_t of the context's
+ * device; NULL restores the context's own stream). */
+int gkc_set_stream(gkc_ctx *ctx, void *stream);
+
+/* Kernel classes of gkc_kernel_stats. */
+enum {
+    GKC_K_FIND_SUPERKMERS = 0,  /* phase 1: minimizers + superkmer records */
+    GKC_K_SCATTER = 1,          /* phase 1: records -> partition bytes     */
+    GKC_K_HASH_INSERT = 2,      /* phase 2 hash: decode + insert           */
+    GKC_K_HASH_COLLECT = 3,     /* phase 2 hash: threshold + clear table   */
+    GKC_K_SORT_EXTRACT = 4,     /* phase 2 sort: decode -> key buffer      */
+    GKC_K_RADIX_HIST = 5,       /* phase 2 sort: tile digit histograms     */
+    GKC_K_RADIX_SCATTER = 6,    /* phase 2 sort: stable scatter            */
+    GKC_K_SCAN = 7,             /* device-wide scans                       */
+    GKC_K_RLE = 8,              /* run-length encoding + threshold         */
+    GKC_K_CLASSES = 9
+};
+
+/* With profiling on, every kernel launch is bracketed by CUDA events on the
+ * launching stream; gkc_kernel_stats then returns, per class, the summed
+ * device milliseconds, the number of launches and the algorithmic DRAM bytes
+ * (compulsory reads + writes of the class's inputs and outputs) since the
+ * last reset.  Arrays of n <= GKC_K_CLASSES entries; any may be NULL. */
+int gkc_set_profiling(gkc_ctx *ctx, int on);
+int gkc_kernel_stats(gkc_ctx *ctx, double *ms, uint64_t *launches, double *bytes, int n, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GKC_CAPI_H */

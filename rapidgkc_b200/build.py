@@ -1,0 +1,89 @@
+"""Builds the native libraries in-tree (they travel with the source tree).
+
+    python -m rapidgkc_b200.build          # everything
+    python -m rapidgkc_b200.build --ptxas  # also print register/spill usage
+
+Outputs (git-ignored):
+    rapidgkc_b200/librapidgkc_b200.so   CUDA kernels + C ABI (sm_100a only)
+    rapidgkc_b200/libgkc_synth.so       seeded synthetic read generator
+    rapidgkc_b200/gkc_main              command-line front end
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _run(cmd):
+    print("+", " ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+
+
+def _stale(out, srcs):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(s) > t for s in srcs)
+
+
+def _csrc(*names):
+    return [os.path.join(CSRC, n) for n in names]
+
+
+def build_cuda(ptxas: bool = False, force: bool = False) -> str:
+    out = os.path.join(PKG, "librapidgkc_b200.so")
+    srcs = _csrc("engine.cu", "skmgen.cu", "count_hash.cu", "count_sort.cu", "gkc_device.cuh")
+    srcs += [os.path.join(ROOT, "include", "gkc_capi.h")]
+    if force or ptxas or _stale(out, srcs):
+        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+               "-Xcompiler", "-fPIC", "-shared", "-o", out, os.path.join(CSRC, "engine.cu")]
+        if ptxas:
+            cmd.insert(1, "-Xptxas=-v")
+        _run(cmd)
+    return out
+
+
+def build_synth(force: bool = False) -> str:
+    out = os.path.join(PKG, "libgkc_synth.so")
+    src = os.path.join(CSRC, "synth.cpp")
+    if force or _stale(out, [src]):
+        _run(["g++", "-std=c++17", "-O3", "-fPIC", "-shared", "-pthread", "-o", out, src])
+    return out
+
+
+def build_cli(force: bool = False) -> str:
+    out = os.path.join(PKG, "gkc_main")
+    src = os.path.join(CSRC, "gkc_main.cpp")
+    lib = build_cuda()
+    if os.path.exists(src) and (force or _stale(out, [src, lib])):
+        _run(["g++", "-std=c++17", "-O2", "-o", out, src, "-I", os.path.join(ROOT, "include"),
+              "-L", PKG, "-lrapidgkc_b200", "-Wl,-rpath,$ORIGIN", "-pthread"])
+    return out
+
+
+def build_oracle() -> None:
+    """The test oracles (oracle/Makefile); the reference part only where the
+    reference tree exists, otherwise the prebuilt library is used as is."""
+    oracle = os.path.join(ROOT, "oracle")
+    _run(["make", "-s", "-C", oracle, "liboracle.so"])
+    ref_tree = os.environ.get("GKC_REFERENCE_TREE", "/root/reference")
+    if os.path.isdir(ref_tree):
+        _run(["make", "-s", "-C", oracle, "ref", f"REF={ref_tree}"])
+
+
+def build_all(ptxas: bool = False, force: bool = False) -> None:
+    build_cuda(ptxas=ptxas, force=force)
+    build_synth(force=force)
+    build_cli(force=force)
+    build_oracle()
+
+
+if __name__ == "__main__":
+    build_all(ptxas="--ptxas" in sys.argv, force="--force" in sys.argv)

@@ -1,0 +1,259 @@
+"""ctypes binding of librapidgkc_b200.so (include/gkc_capi.h).
+
+The Python mirror of the reference's GPU interface:
+
+* ``KmerCounter.add_reads``  <- ``GenSuperkmerGPU`` (gpu_skmgen.h:54-58)
+* ``KmerCounter.count``      <- ``kmc_counting_GPU_streams`` (gpu_kmercounting.h:14-17)
+* ``KmerCounter.store_stats`` / ``store_export`` <- ``SKMStoreNoncon`` counters
+  and bytes (skmstore.hpp:85-87, 222-236)
+
+There is no CPU fallback: constructing a counter without the CUDA library, or
+without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "librapidgkc_b200.so")
+
+GKC_OK, GKC_EINVAL, GKC_ECUDA, GKC_ENOMEM, GKC_ESTATE, GKC_EINTERNAL = 0, -1, -2, -3, -4, -5
+COUNTER_SORT, COUNTER_HASH = 0, 1
+MEM_HOST, MEM_DEVICE = 0, 1
+UINT32_MAX = 0xFFFFFFFF
+
+# Every symbol declared in include/gkc_capi.h.
+EXPORTS = (
+    "gkc_default_options", "gkc_create", "gkc_destroy", "gkc_last_error", "gkc_strerror",
+    "gkc_set_order", "gkc_add_reads", "gkc_store_stats", "gkc_store_export", "gkc_store_clear",
+    "gkc_count", "gkc_result", "gkc_result_device", "gkc_count_reads", "gkc_count_keys",
+    "gkc_last_timings", "gkc_kernel_launches", "gkc_set_stream", "gkc_set_profiling", "gkc_kernel_stats",
+)
+KERNEL_CLASSES = ("find_superkmers", "scatter_superkmers", "hash_insert", "hash_collect", "sort_extract",
+                  "radix_hist", "radix_scatter", "scan", "rle")
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("k", C.c_int),
+        ("p", C.c_int),
+        ("partitions", C.c_int),
+        ("counter", C.c_int),
+        ("radix_bits", C.c_int),
+        ("table_slots", C.c_double),
+        ("batch_bases", C.c_uint64),
+        ("spill_host", C.c_int),
+        ("group_keys", C.c_uint64),
+    ]
+
+
+class GkcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"gkc error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads the CUDA library; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `python -m rapidgkc_b200.build`")
+    L = C.CDLL(path)
+    vp, u64, u32, i32 = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int
+    L.gkc_default_options.argtypes = [C.POINTER(Options)]
+    L.gkc_default_options.restype = None
+    L.gkc_create.argtypes = [i32, C.POINTER(Options), C.POINTER(vp)]
+    L.gkc_destroy.argtypes = [vp]
+    L.gkc_last_error.argtypes = [vp]
+    L.gkc_last_error.restype = C.c_char_p
+    L.gkc_strerror.argtypes = [i32]
+    L.gkc_strerror.restype = C.c_char_p
+    L.gkc_set_order.argtypes = [vp, vp, u64, i32]
+    L.gkc_add_reads.argtypes = [vp, vp, vp, u64, i32]
+    L.gkc_store_stats.argtypes = [vp, vp, vp, vp]
+    L.gkc_store_export.argtypes = [vp, i32, vp, u64, C.POINTER(u64)]
+    L.gkc_store_clear.argtypes = [vp]
+    L.gkc_count.argtypes = [vp, u32, u32, C.POINTER(u64), C.POINTER(u64)]
+    L.gkc_result.argtypes = [vp, vp, vp, u64, i32]
+    L.gkc_result_device.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(u64)]
+    L.gkc_count_reads.argtypes = [vp, vp, vp, u64, i32, u32, u32, vp, vp, u64, i32, C.POINTER(u64),
+                                  C.POINTER(u64)]
+    L.gkc_count_keys.argtypes = [vp, vp, u64, i32, u32, u32, C.POINTER(u64), C.POINTER(u64)]
+    L.gkc_last_timings.argtypes = [vp, C.POINTER(C.c_double), i32]
+    L.gkc_kernel_launches.argtypes = [vp]
+    L.gkc_kernel_launches.restype = u64
+    L.gkc_set_stream.argtypes = [vp, vp]
+    L.gkc_set_profiling.argtypes = [vp, i32]
+    L.gkc_kernel_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(u64), C.POINTER(C.c_double), i32, i32]
+    for name in EXPORTS:
+        if name not in ("gkc_default_options", "gkc_last_error", "gkc_strerror", "gkc_kernel_launches"):
+            getattr(L, name).restype = i32
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    """(pointer, mem) of a numpy array (host) or a CUDA torch tensor (device)."""
+    if a is None:
+        return None, MEM_HOST
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return a.ctypes.data_as(C.c_void_p), MEM_HOST
+    if hasattr(a, "data_ptr") and hasattr(a, "is_cuda"):
+        if not a.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        return C.c_void_p(a.data_ptr()), MEM_DEVICE if a.is_cuda else MEM_HOST
+    raise TypeError(f"unsupported buffer type {type(a)!r}")
+
+
+class KmerCounter:
+    """A counting context on one CUDA device (reference CLI names in brackets):
+    k [-k], p [-p], partitions [-skm], counter 'hash' or 'sort'."""
+
+    def __init__(self, k: int = 31, p: int = 11, partitions: int = 512, counter: str = "hash",
+                 device: int = 0, radix_bits: int = 8, table_slots: float = 0.75,
+                 batch_bases: int = 1 << 30, spill_host: bool = False, group_keys: int = 0):
+        L = load_library()
+        o = Options()
+        L.gkc_default_options(C.byref(o))
+        o.k, o.p, o.partitions = k, p, partitions
+        o.counter = {"hash": COUNTER_HASH, "sort": COUNTER_SORT}[counter]
+        o.radix_bits, o.table_slots, o.batch_bases = radix_bits, table_slots, batch_bases
+        o.spill_host, o.group_keys = int(spill_host), group_keys
+        h = C.c_void_p()
+        rc = L.gkc_create(device, C.byref(o), C.byref(h))
+        if rc != GKC_OK:
+            raise GkcError(rc, L.gkc_strerror(rc).decode())
+        self._L, self._h = L, h
+        self.k, self.p, self.partitions, self.counter = k, p, partitions, counter
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gkc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc):
+        if rc != GKC_OK:
+            raise GkcError(rc, self._L.gkc_last_error(self._h).decode())
+
+    # -- phase 1 -------------------------------------------------------------
+    def set_order(self, lut):
+        """Minimizer order table of 4^p uint32 ranks, or None for the default."""
+        if lut is None:
+            self._check(self._L.gkc_set_order(self._h, None, 0, MEM_HOST))
+            return
+        ptr, mem = _ptr(lut)
+        self._check(self._L.gkc_set_order(self._h, ptr, len(lut), mem))
+
+    def add_reads(self, reads, offs):
+        """Appends the superkmers of a CSR read batch to the partition store."""
+        rp, rm = _ptr(reads)
+        op, om = _ptr(offs)
+        if rm != om:
+            raise ValueError("reads and offsets must live in the same memory")
+        self._check(self._L.gkc_add_reads(self._h, rp, op, len(offs) - 1, rm))
+
+    def store_stats(self):
+        P = self.partitions
+        b, s, k = (np.zeros(P, np.uint64) for _ in range(3))
+        self._check(self._L.gkc_store_stats(self._h, _ptr(b)[0], _ptr(s)[0], _ptr(k)[0]))
+        return b, s, k
+
+    def store_export(self, part: int) -> np.ndarray:
+        n = C.c_uint64(0)
+        self._check(self._L.gkc_store_export(self._h, part, None, 0, C.byref(n)))
+        out = np.zeros(max(1, n.value), np.uint8)
+        self._check(self._L.gkc_store_export(self._h, part, _ptr(out)[0], n.value, C.byref(n)))
+        return out[: n.value]
+
+    def store_clear(self):
+        self._check(self._L.gkc_store_clear(self._h))
+
+    # -- phase 2 -------------------------------------------------------------
+    def count(self, cmin: int = 1, cmax: int = UINT32_MAX):
+        """Counts the store; returns (kept, distinct)."""
+        no, nd = C.c_uint64(0), C.c_uint64(0)
+        self._check(self._L.gkc_count(self._h, cmin, cmax, C.byref(no), C.byref(nd)))
+        return no.value, nd.value
+
+    def result(self, n: int | None = None):
+        """The last count's (kmers uint64, counts uint32) as host arrays."""
+        if n is None:
+            kp, cp, nn = C.c_void_p(), C.c_void_p(), C.c_uint64(0)
+            self._check(self._L.gkc_result_device(self._h, C.byref(kp), C.byref(cp), C.byref(nn)))
+            n = nn.value
+        km = np.zeros(max(1, n), np.uint64)
+        ct = np.zeros(max(1, n), np.uint32)
+        self._check(self._L.gkc_result(self._h, _ptr(km)[0], _ptr(ct)[0], n, MEM_HOST))
+        return km[:n], ct[:n]
+
+    def result_device(self):
+        kp, cp, nn = C.c_void_p(), C.c_void_p(), C.c_uint64(0)
+        self._check(self._L.gkc_result_device(self._h, C.byref(kp), C.byref(cp), C.byref(nn)))
+        return kp.value, cp.value, nn.value
+
+    def count_reads(self, reads, offs, cmin: int = 1, cmax: int = UINT32_MAX, out_kmers=None,
+                    out_counts=None):
+        """reads -> (kept, distinct); fills out_kmers/out_counts when given."""
+        rp, rm = _ptr(reads)
+        op, _ = _ptr(offs)
+        kp, km = _ptr(out_kmers)
+        cp, _ = _ptr(out_counts)
+        cap = 0 if out_kmers is None else len(out_kmers)
+        no, nd = C.c_uint64(0), C.c_uint64(0)
+        self._check(self._L.gkc_count_reads(self._h, rp, op, len(offs) - 1, rm, cmin, cmax, kp, cp, cap,
+                                            km, C.byref(no), C.byref(nd)))
+        return no.value, nd.value
+
+    def count_keys(self, keys, cmin: int = 1, cmax: int = UINT32_MAX):
+        """Counts raw uint64 keys (no canonical step); returns (kept, distinct)."""
+        kp, km = _ptr(keys)
+        no, nd = C.c_uint64(0), C.c_uint64(0)
+        self._check(self._L.gkc_count_keys(self._h, kp, len(keys), km, cmin, cmax, C.byref(no), C.byref(nd)))
+        return no.value, nd.value
+
+    def timings(self):
+        t = (C.c_double * 4)()
+        self._check(self._L.gkc_last_timings(self._h, t, 4))
+        return {"phase1_ms": t[0], "phase1_search_ms": t[1], "phase2_ms": t[2], "phase2_kernel_ms": t[3]}
+
+    def kernel_launches(self) -> int:
+        return int(self._L.gkc_kernel_launches(self._h))
+
+    def set_stream(self, stream):
+        """Runs on a CUDA stream (an int handle or a torch.cuda.Stream); None = own."""
+        h = None
+        if stream is not None:
+            h = C.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+        self._check(self._L.gkc_set_stream(self._h, h))
+
+    def set_profiling(self, on: bool = True):
+        self._check(self._L.gkc_set_profiling(self._h, int(on)))
+
+    def kernel_stats(self, reset: bool = False):
+        """{class: (ms, launches, algorithmic bytes)} since the last reset."""
+        n = len(KERNEL_CLASSES)
+        ms, nl, by = (C.c_double * n)(), (C.c_uint64 * n)(), (C.c_double * n)()
+        self._check(self._L.gkc_kernel_stats(self._h, ms, nl, by, n, int(reset)))
+        return {KERNEL_CLASSES[i]: (ms[i], int(nl[i]), by[i]) for i in range(n)}

@@ -1,0 +1,1186 @@
+// engine.cu -- host orchestration and the C ABI of the B200 k-mer counter.
+//
+// One translation unit: the kernels of skmgen.cu, count_hash.cu and
+// count_sort.cu are compiled here together with the host code that drives
+// them.  The data path is
+//   host/device CSR reads --(H2D, overlapped, batches)--> phase 1 kernels
+//   --> partition store (one chunk per batch: partition-ordered superkmer
+//   bytes + index, on the device or spilled to pinned host memory)
+//   --> phase 2 (hash: one partition at a time through an L2-resident table;
+//   sort: groups of partitions through the segmented radix sort)
+//   --> thresholded (k-mer, count) arrays on the device.
+#include "../../include/gkc_capi.h"
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "count_hash.cu"
+#include "count_sort.cu"
+#include "skmgen.cu"
+
+using namespace gkc;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want; else p = nullptr;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+struct PinBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap && p) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaHostAlloc(&p, std::max<size_t>(bytes, 256), cudaHostAllocDefault);
+        if (e == cudaSuccess) cap = std::max<size_t>(bytes, 256); else p = nullptr;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// One phase-1 batch worth of superkmers, partition-ordered.
+struct StoreChunk {
+    bool on_host = false;
+    uint8_t *bytes = nullptr;  // device or pinned host
+    uint64_t *idx = nullptr;
+    uint64_t nbytes = 0, nskm = 0;
+    std::vector<uint64_t> byte_off, skm_off;  // [P+1]
+    std::vector<uint64_t> kmers;              // [P]
+    DevBuf d_byte_off, d_skm_off;             // device copies of the offsets
+};
+
+uint64_t next_pow2(uint64_t v) {
+    uint64_t r = 1;
+    while (r < v) r <<= 1;
+    return r;
+}
+
+}  // namespace
+
+struct gkc_ctx {
+    int device = 0;
+    gkc_options opt{};
+    int sms = 148;
+    cudaStream_t s = nullptr, cs = nullptr, own_s = nullptr;
+
+    // per-kernel-class profiling (events resolved after each public call)
+    struct Pending {
+        int cls;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    bool prof = false;
+    std::vector<Pending> pend;
+    std::vector<cudaEvent_t> evpool;
+    double kms[GKC_K_CLASSES] = {}, kbytes[GKC_K_CLASSES] = {};
+    uint64_t klaunch[GKC_K_CLASSES] = {};
+    cudaEvent_t take_event() {
+        if (!evpool.empty()) {
+            cudaEvent_t e = evpool.back();
+            evpool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void prof_flush() {
+        for (auto &q : pend) {
+            float ms = 0;
+            if (cudaEventSynchronize(q.b) == cudaSuccess && cudaEventElapsedTime(&ms, q.a, q.b) == cudaSuccess) {
+                kms[q.cls] += ms;
+                klaunch[q.cls]++;
+                kbytes[q.cls] += q.bytes;
+            }
+            evpool.push_back(q.a);
+            evpool.push_back(q.b);
+        }
+        pend.clear();
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+    std::string err;
+    uint64_t launches = 0;
+    double times[4] = {0, 0, 0, 0};
+
+    // phase 1 buffers
+    DevBuf reads[2], offs[2];
+    PinBuf offs_pin[2];
+    cudaEvent_t buf_free[2] = {nullptr, nullptr}, buf_ready[2] = {nullptr, nullptr};
+    DevBuf records, region_count, hist, flags, cursors, part_off;
+    PinBuf h_hist, h_flags;
+    DevBuf lut;
+    bool has_lut = false;
+    std::vector<StoreChunk *> store;
+
+    // phase 2 buffers
+    DevBuf tkeys, tcnts;
+    uint64_t tcap = 0;
+    DevBuf out_k, out_c;
+    uint64_t out_cap = 0, n_out = 0, n_distinct = 0;
+    bool has_result = false;
+    DevBuf keysA, keysB, tiles, counts, offsets, blocksums, heads_pos, heads_key, tilecnt, tileoff;
+    DevBuf segoff, segcur, part_err, scal;
+    DevBuf stage_bytes, stage_idx;
+    PinBuf h_scal;
+
+    ~gkc_ctx() {
+        for (auto *c : store) delete_chunk(c);
+        store.clear();
+        DevBuf *ds[] = {&reads[0], &reads[1], &offs[0], &offs[1], &records, &region_count, &hist, &flags,
+                        &cursors, &part_off, &lut, &tkeys, &tcnts, &out_k, &out_c, &keysA, &keysB, &tiles,
+                        &counts, &offsets, &blocksums, &heads_pos, &heads_key, &tilecnt, &tileoff, &segoff,
+                        &segcur, &part_err, &scal, &stage_bytes, &stage_idx};
+        for (auto *d : ds) d->release();
+        PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal};
+        for (auto *p : ps) p->release();
+        cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_ready[0], buf_ready[1]};
+        for (auto e : evs) if (e) cudaEventDestroy(e);
+        prof_flush();
+        for (auto e : evpool) cudaEventDestroy(e);
+        if (own_s) cudaStreamDestroy(own_s);
+        if (cs) cudaStreamDestroy(cs);
+    }
+    static void delete_chunk(StoreChunk *c) {
+        if (c->on_host) {
+            if (c->bytes) cudaFreeHost(c->bytes);
+            if (c->idx) cudaFreeHost(c->idx);
+        } else {
+            if (c->bytes) cudaFree(c->bytes);
+            if (c->idx) cudaFree(c->idx);
+        }
+        c->d_byte_off.release();
+        c->d_skm_off.release();
+        delete c;
+    }
+    int fail(int code, const char *fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        err = buf;
+        return code;
+    }
+};
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t _e = (call);                                                          \
+        if (_e != cudaSuccess)                                                            \
+            return ctx->fail(_e == cudaErrorMemoryAllocation ? GKC_ENOMEM : GKC_ECUDA,    \
+                             "%s: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, __LINE__); \
+    } while (0)
+
+#define LAUNCHED()                          \
+    do {                                    \
+        ctx->launches++;                    \
+        CK(cudaPeekAtLastError());          \
+    } while (0)
+
+#define RET(call)                \
+    do {                         \
+        int _r = (call);         \
+        if (_r != GKC_OK) return _r; \
+    } while (0)
+
+namespace {
+
+// Brackets one kernel launch with events when profiling is on.
+struct KScope {
+    gkc_ctx *c;
+    int cls;
+    double bytes;
+    cudaEvent_t a = nullptr;
+    KScope(gkc_ctx *ctx, int k, double b) : c(ctx), cls(k), bytes(b) {
+        if (c->prof) {
+            a = c->take_event();
+            cudaEventRecord(a, c->s);
+        }
+    }
+    ~KScope() {
+        if (c->prof && a) {
+            cudaEvent_t b = c->take_event();
+            cudaEventRecord(b, c->s);
+            c->pend.push_back({cls, a, b, bytes});
+        }
+    }
+};
+
+}  // namespace
+
+namespace {
+
+// device-wide exclusive scan u32 -> u64; total (optional) on the device
+int scan_u32(gkc_ctx *ctx, const uint32_t *in, uint64_t n, uint64_t *out, unsigned long long *total) {
+    uint64_t nb = (n + SC_PER_BLOCK - 1) / SC_PER_BLOCK;
+    if (nb == 0) {
+        if (total) CK(cudaMemsetAsync(total, 0, sizeof(unsigned long long), ctx->s));
+        return GKC_OK;
+    }
+    CK(ctx->blocksums.ensure(nb * sizeof(unsigned long long)));
+    auto *bs = ctx->blocksums.as<unsigned long long>();
+    {
+        KScope ks(ctx, GKC_K_SCAN, 4.0 * n + 8.0 * nb);
+        scan_reduce_kernel<<<(unsigned)nb, SC_THREADS, 0, ctx->s>>>(in, n, bs);
+        LAUNCHED();
+    }
+    {
+        KScope ks(ctx, GKC_K_SCAN, 16.0 * nb);
+        scan_blocksums_kernel<<<1, 1024, 0, ctx->s>>>(bs, nb, total);
+        LAUNCHED();
+    }
+    {
+        KScope ks(ctx, GKC_K_SCAN, 12.0 * n + 8.0 * nb);
+        scan_down_kernel<<<(unsigned)nb, SC_THREADS, 0, ctx->s>>>(in, n, bs, out);
+        LAUNCHED();
+    }
+    return GKC_OK;
+}
+
+int ensure_out(gkc_ctx *ctx, uint64_t need) {
+    if (need <= ctx->out_cap && ctx->out_k.p) return GKC_OK;
+    uint64_t cap = std::max<uint64_t>(need, 1024);
+    DevBuf nk, nc;
+    CK(nk.ensure(cap * 8));
+    CK(nc.ensure(cap * 4));
+    if (ctx->n_out && ctx->out_k.p) {
+        CK(cudaMemcpyAsync(nk.p, ctx->out_k.p, ctx->n_out * 8, cudaMemcpyDeviceToDevice, ctx->s));
+        CK(cudaMemcpyAsync(nc.p, ctx->out_c.p, ctx->n_out * 4, cudaMemcpyDeviceToDevice, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+    }
+    ctx->out_k.release();
+    ctx->out_c.release();
+    ctx->out_k = nk;
+    ctx->out_c = nc;
+    nk.p = nullptr;
+    nc.p = nullptr;
+    ctx->out_cap = cap;
+    return GKC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// phase 1 on a device-resident batch (offs[0] == 0)
+int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, uint64_t n_reads,
+                 uint64_t total) {
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    if (total == 0 || n_reads == 0) return GKC_OK;
+    const uint64_t ntiles = (total + P1_TILE - 1) / P1_TILE;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)ctx->sms * 4);
+    const uint64_t tiles_per_cta = (ntiles + grid - 1) / grid;
+    uint64_t cap = tiles_per_cta * P1_TILE / 4 + 4096;
+    const uint64_t cap_max = tiles_per_cta * P1_TILE + 64;
+    CK(ctx->region_count.ensure(grid * sizeof(uint32_t)));
+    CK(ctx->hist.ensure(3ull * P * sizeof(unsigned long long)));
+    CK(ctx->flags.ensure(64));
+    CK(ctx->h_hist.ensure(3ull * P * sizeof(unsigned long long)));
+    CK(ctx->h_flags.ensure(64));
+    auto *hist = ctx->hist.as<unsigned long long>();
+    auto *hh = ctx->h_hist.as<unsigned long long>();
+    size_t dyn = 3ull * P * sizeof(uint32_t);
+    CK(cudaFuncSetAttribute(find_superkmers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    for (int attempt = 0;; attempt++) {
+        if (cap > UINT32_MAX) cap = UINT32_MAX;
+        CK(ctx->records.ensure(cap * grid * sizeof(SkmRecord)));
+        CK(cudaMemsetAsync(hist, 0, 3ull * P * sizeof(unsigned long long), ctx->s));
+        CK(cudaMemsetAsync(ctx->flags.p, 0, 64, ctx->s));
+        P1Params a;
+        a.reads = d_reads;
+        a.offs = d_offs;
+        a.n_reads = (int64_t)n_reads;
+        a.total = total;
+        a.k = ctx->opt.k;
+        a.p = ctx->opt.p;
+        a.P = P;
+        a.lut = ctx->has_lut ? ctx->lut.as<uint32_t>() : nullptr;
+        a.vec_ok = ((uintptr_t)d_reads & 15) == 0;
+        a.records = ctx->records.as<SkmRecord>();
+        a.region_cap = (uint32_t)cap;
+        a.region_count = ctx->region_count.as<uint32_t>();
+        a.part_bytes = hist;
+        a.part_skms = hist + P;
+        a.part_kmers = hist + 2 * P;
+        a.smem_hist = 1;
+        a.err = ctx->flags.as<uint32_t>();
+        CK(cudaEventRecord(ctx->e0, ctx->s));
+        {
+            KScope ks(ctx, GKC_K_FIND_SUPERKMERS, (double)total + 8.0 * (n_reads + 1));
+            find_superkmers_kernel<<<grid, P1_THREADS, dyn, ctx->s>>>(a);
+            LAUNCHED();
+        }
+        CK(cudaEventRecord(ctx->e1, ctx->s));
+        CK(cudaMemcpyAsync(hh, hist, 3ull * P * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(ctx->h_flags.p, ctx->flags.p, 4, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->e0, ctx->e1));
+        ctx->times[1] += ms;
+        uint32_t f = *ctx->h_flags.as<uint32_t>();
+        if (f & ERR_SKM_TOO_LONG) return ctx->fail(GKC_EINVAL, "a superkmer exceeds %u k-mers", IDX_MAX_LEN);
+        if (f & ERR_RECORD_OVERFLOW) {
+            if (cap >= cap_max || attempt >= 3)
+                return ctx->fail(GKC_EINTERNAL, "superkmer record region overflow at capacity %llu",
+                                 (unsigned long long)cap);
+            cap = std::min<uint64_t>(cap * 4, cap_max);
+            continue;
+        }
+        break;
+    }
+    // ---- partition offsets, store chunk ----
+    auto *c = new StoreChunk();
+    c->byte_off.assign(P + 1, 0);
+    c->skm_off.assign(P + 1, 0);
+    c->kmers.assign(P, 0);
+    for (uint32_t i = 0; i < P; i++) {
+        c->byte_off[i + 1] = c->byte_off[i] + hh[i];
+        c->skm_off[i + 1] = c->skm_off[i] + hh[P + i];
+        c->kmers[i] = hh[2 * P + i];
+    }
+    c->nbytes = c->byte_off[P];
+    c->nskm = c->skm_off[P];
+    if (ctx->prof && !ctx->pend.empty()) ctx->pend.back().bytes += 16.0 * c->nskm;  // records written
+    cudaError_t e1 = cudaMalloc((void **)&c->bytes, c->nbytes + 16);
+    cudaError_t e2 = e1 == cudaSuccess ? cudaMalloc((void **)&c->idx, std::max<uint64_t>(c->nskm, 1) * 8) : e1;
+    cudaError_t e3 = e2 == cudaSuccess ? c->d_byte_off.ensure((P + 1) * 8) : e2;
+    cudaError_t e4 = e3 == cudaSuccess ? c->d_skm_off.ensure((P + 1) * 8) : e3;
+    if (e4 != cudaSuccess) {
+        gkc_ctx::delete_chunk(c);
+        return ctx->fail(GKC_ENOMEM, "store chunk allocation (%llu bytes): %s",
+                         (unsigned long long)c->nbytes, cudaGetErrorString(e4));
+    }
+    CK(cudaMemcpyAsync(c->d_byte_off.p, c->byte_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemcpyAsync(c->d_skm_off.p, c->skm_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
+    CK(ctx->cursors.ensure(2ull * P * sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(ctx->cursors.p, 0, 2ull * P * sizeof(unsigned long long), ctx->s));
+    P2Params b;
+    b.reads = d_reads;
+    b.records = ctx->records.as<SkmRecord>();
+    b.region_cap = (uint32_t)cap;
+    b.region_count = ctx->region_count.as<uint32_t>();
+    b.k = ctx->opt.k;
+    b.P = P;
+    b.part_byte_off = c->d_byte_off.as<unsigned long long>();
+    b.part_skm_off = c->d_skm_off.as<unsigned long long>();
+    b.cur_bytes = ctx->cursors.as<unsigned long long>();
+    b.cur_skms = ctx->cursors.as<unsigned long long>() + P;
+    b.bytes = c->bytes;
+    b.idx = c->idx;
+    size_t dyn2 = 2ull * P * sizeof(unsigned long long);
+    CK(cudaFuncSetAttribute(scatter_superkmers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn2));
+    {
+        KScope ks(ctx, GKC_K_SCATTER, 24.0 * c->nskm + (double)total + (double)c->nbytes);
+        scatter_superkmers_kernel<<<grid, P2_THREADS, dyn2, ctx->s>>>(b);
+        LAUNCHED();
+    }
+    if (ctx->opt.spill_host) {
+        uint8_t *hb = nullptr;
+        uint64_t *hi = nullptr;
+        cudaError_t ea = cudaHostAlloc((void **)&hb, c->nbytes + 16, cudaHostAllocDefault);
+        cudaError_t eb = ea == cudaSuccess ? cudaHostAlloc((void **)&hi, std::max<uint64_t>(c->nskm, 1) * 8,
+                                                           cudaHostAllocDefault) : ea;
+        if (eb != cudaSuccess) {
+            if (hb) cudaFreeHost(hb);
+            gkc_ctx::delete_chunk(c);
+            return ctx->fail(GKC_ENOMEM, "pinned spill allocation: %s", cudaGetErrorString(eb));
+        }
+        CK(cudaMemcpyAsync(hb, c->bytes, c->nbytes, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(hi, c->idx, c->nskm * 8, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        cudaFree(c->bytes);
+        cudaFree(c->idx);
+        c->bytes = hb;
+        c->idx = hi;
+        c->on_host = true;
+    }
+    ctx->store.push_back(c);
+    return GKC_OK;
+}
+
+// Device pointers of partition p of chunk c (staging spilled chunks).
+int chunk_part(gkc_ctx *ctx, StoreChunk *c, uint32_t p, const uint8_t **bytes, const uint64_t **idx,
+               uint64_t *nskm) {
+    uint64_t b0 = c->byte_off[p], b1 = c->byte_off[p + 1], s0 = c->skm_off[p], s1 = c->skm_off[p + 1];
+    *nskm = s1 - s0;
+    if (!c->on_host) {
+        *bytes = c->bytes + b0;
+        *idx = c->idx + s0;
+        return GKC_OK;
+    }
+    CK(cudaStreamSynchronize(ctx->s));  // staging buffers are reused
+    CK(ctx->stage_bytes.ensure(b1 - b0 + 16));
+    CK(ctx->stage_idx.ensure((s1 - s0) * 8 + 8));
+    CK(cudaMemcpyAsync(ctx->stage_bytes.p, c->bytes + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemcpyAsync(ctx->stage_idx.p, c->idx + s0, (s1 - s0) * 8, cudaMemcpyHostToDevice, ctx->s));
+    *bytes = ctx->stage_bytes.as<uint8_t>();
+    *idx = ctx->stage_idx.as<uint64_t>();
+    return GKC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// phase 2, hash counter
+int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    std::vector<uint64_t> np(P, 0);
+    uint64_t N = 0;
+    for (auto *c : ctx->store)
+        for (uint32_t p = 0; p < P; p++) np[p] += c->kmers[p];
+    for (uint32_t p = 0; p < P; p++) N += np[p];
+    const double slots = ctx->opt.table_slots > 0 ? ctx->opt.table_slots : 0.75;
+    auto cap_of = [&](uint64_t n, int scale) {
+        return next_pow2(std::max<uint64_t>(1024, (uint64_t)((double)n * slots) * scale));
+    };
+    uint64_t cmax_cap = 1024;
+    for (uint32_t p = 0; p < P; p++) cmax_cap = std::max(cmax_cap, cap_of(np[p], 1));
+    if (cmax_cap > ctx->tcap) {
+        ctx->tkeys.release();
+        ctx->tcnts.release();
+        CK(ctx->tkeys.ensure(cmax_cap * 8));
+        CK(ctx->tcnts.ensure(cmax_cap * 4));
+        CK(cudaMemsetAsync(ctx->tkeys.p, 0xFF, cmax_cap * 8, ctx->s));
+        CK(cudaMemsetAsync(ctx->tcnts.p, 0, cmax_cap * 4, ctx->s));
+        ctx->tcap = cmax_cap;
+    }
+    RET(ensure_out(ctx, N / std::max<uint32_t>(cmin, 1) + 1024));
+    CK(ctx->part_err.ensure(P * 4));
+    CK(ctx->scal.ensure(64));
+    CK(ctx->h_scal.ensure(64));
+    CK(cudaMemsetAsync(ctx->part_err.p, 0, P * 4, ctx->s));
+    CK(cudaMemsetAsync(ctx->scal.p, 0, 64, ctx->s));
+    auto *sc = ctx->scal.as<unsigned long long>();  // [0] cursor [1] distinct [2] err
+    CK(cudaMemcpyAsync(sc, &ctx->n_out, 8, cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    float acc_insert = 0;
+    std::vector<uint32_t> todo;
+    for (uint32_t p = 0; p < P; p++) if (np[p]) todo.push_back(p);
+    std::vector<int> scale(P, 1);
+    for (int round = 0; !todo.empty(); round++) {
+        if (round > 4) return ctx->fail(GKC_EINTERNAL, "hash table retries exhausted");
+        for (uint32_t p : todo) {
+            uint64_t C = cap_of(np[p], scale[p]);
+            if (C > ctx->tcap) {  // a retried partition needs a larger table
+                CK(cudaStreamSynchronize(ctx->s));
+                ctx->tkeys.release();
+                ctx->tcnts.release();
+                CK(ctx->tkeys.ensure(C * 8));
+                CK(ctx->tcnts.ensure(C * 4));
+                CK(cudaMemsetAsync(ctx->tkeys.p, 0xFF, C * 8, ctx->s));
+                CK(cudaMemsetAsync(ctx->tcnts.p, 0, C * 4, ctx->s));
+                ctx->tcap = C;
+            }
+            CK(cudaEventRecord(ctx->e2, ctx->s));
+            for (auto *c : ctx->store) {
+                const uint8_t *pb;
+                const uint64_t *pi;
+                uint64_t ns;
+                RET(chunk_part(ctx, c, p, &pb, &pi, &ns));
+                if (!ns) continue;
+                HInsertParams h;
+                h.bytes = pb;
+                h.idx = pi;
+                h.n_skm = ns;
+                h.k = ctx->opt.k;
+                h.keys = ctx->tkeys.as<unsigned long long>();
+                h.cnts = ctx->tcnts.as<uint32_t>();
+                h.mask = C - 1;
+                h.err = ctx->part_err.as<uint32_t>() + p;
+                uint32_t g = (uint32_t)std::min<uint64_t>((ns + H_THREADS - 1) / H_THREADS, (uint64_t)ctx->sms * 8);
+                KScope ks(ctx, GKC_K_HASH_INSERT,
+                          (double)(c->byte_off[p + 1] - c->byte_off[p]) + 8.0 * ns);
+                hash_insert_kernel<<<g, H_THREADS, 0, ctx->s>>>(h);
+                LAUNCHED();
+            }
+            CK(cudaEventRecord(ctx->e3, ctx->s));
+            HCollectParams q;
+            q.keys = ctx->tkeys.as<unsigned long long>();
+            q.cnts = ctx->tcnts.as<uint32_t>();
+            q.cap = C;
+            q.cmin = cmin;
+            q.cmax = cmax;
+            q.out_k = ctx->out_k.as<uint64_t>();
+            q.out_c = ctx->out_c.as<uint32_t>();
+            q.out_cursor = sc;
+            q.out_cap = ctx->out_cap;
+            q.distinct = sc + 1;
+            q.err = reinterpret_cast<uint32_t *>(sc + 2);
+            q.part_err = ctx->part_err.as<uint32_t>() + p;
+            uint32_t g = (uint32_t)std::min<uint64_t>((C + H_THREADS * HC_ITEMS - 1) / (H_THREADS * HC_ITEMS),
+                                                      (uint64_t)ctx->sms * 8);
+            {
+                KScope ks(ctx, GKC_K_HASH_COLLECT, 24.0 * C);
+                hash_collect_kernel<<<g, H_THREADS, 0, ctx->s>>>(q);
+                LAUNCHED();
+            }
+            if (round == 0 && p == todo.front()) {
+                // time one partition's insert as the dominant-kernel sample
+                CK(cudaEventSynchronize(ctx->e3));
+                float ms = 0;
+                CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
+                acc_insert = ms;
+            }
+        }
+        std::vector<uint32_t> perr(P);
+        CK(cudaMemcpyAsync(perr.data(), ctx->part_err.p, P * 4, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        std::vector<uint32_t> again;
+        for (uint32_t p : todo)
+            if (perr[p] & ERR_TABLE_FULL) { again.push_back(p); scale[p] *= 4; }
+        if (!again.empty()) CK(cudaMemsetAsync(ctx->part_err.p, 0, P * 4, ctx->s));
+        todo.swap(again);
+    }
+    auto *hs = ctx->h_scal.as<unsigned long long>();
+    if ((uint32_t)hs[2] & ERR_OUTPUT_FULL) return ctx->fail(GKC_EINTERNAL, "output capacity exceeded");
+    ctx->n_out = hs[0];
+    ctx->n_distinct += hs[1];
+    ctx->times[3] = acc_insert;
+    return GKC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// phase 2, sort counter: sorts `n` keys already in keysA split into segments
+// segs (sizes), then RLE + threshold, appending to the output.
+template <int RB>
+int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, int nbits, uint32_t cmin,
+                       uint32_t cmax, float *sort_ms) {
+    // tiles
+    std::vector<TileDesc> td;
+    uint64_t start = 0, cnt_base = 0;
+    for (uint64_t sz : segs) {
+        uint32_t nt = (uint32_t)((sz + RS_TILE - 1) / RS_TILE);
+        for (uint32_t t = 0; t < nt; t++) {
+            TileDesc d;
+            d.start = start + (uint64_t)t * RS_TILE;
+            d.cnt_base = cnt_base;
+            d.n = (uint32_t)std::min<uint64_t>(RS_TILE, sz - (uint64_t)t * RS_TILE);
+            d.t = t;
+            d.nt = nt;
+            d.pad = 0;
+            td.push_back(d);
+        }
+        start += sz;
+        cnt_base += (uint64_t)nt << RB;
+    }
+    const uint64_t ntiles = td.size();
+    const uint64_t ncounts = cnt_base;
+    if (ntiles) {
+        CK(ctx->tiles.ensure(ntiles * sizeof(TileDesc)));
+        CK(ctx->counts.ensure(ncounts * 4));
+        CK(ctx->offsets.ensure(ncounts * 8));
+        CK(cudaMemcpyAsync(ctx->tiles.p, td.data(), ntiles * sizeof(TileDesc), cudaMemcpyHostToDevice, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));  // td is host memory about to go out of scope
+    }
+    uint64_t *src = ctx->keysA.as<uint64_t>(), *dst = ctx->keysB.as<uint64_t>();
+    CK(cudaEventRecord(ctx->e2, ctx->s));
+    for (int shift = 0; shift < nbits && ntiles; shift += RB) {
+        {
+            KScope ks(ctx, GKC_K_RADIX_HIST, 8.0 * n + 4.0 * ncounts);
+            radix_hist_kernel<RB><<<(unsigned)ntiles, RS_THREADS, 0, ctx->s>>>(src, ctx->tiles.as<TileDesc>(), shift,
+                                                                                 ctx->counts.as<uint32_t>());
+            LAUNCHED();
+        }
+        RET(scan_u32(ctx, ctx->counts.as<uint32_t>(), ncounts, ctx->offsets.as<uint64_t>(), nullptr));
+        {
+            KScope ks(ctx, GKC_K_RADIX_SCATTER, 16.0 * n + 8.0 * ncounts);
+            radix_scatter_kernel<RB><<<(unsigned)ntiles, RS_THREADS, 0, ctx->s>>>(
+                src, dst, ctx->tiles.as<TileDesc>(), shift, ctx->offsets.as<uint64_t>());
+            LAUNCHED();
+        }
+        std::swap(src, dst);
+    }
+    CK(cudaEventRecord(ctx->e3, ctx->s));
+    // ---- RLE ----
+    const uint64_t rt = (n + RL_TILE - 1) / RL_TILE;
+    CK(ctx->tilecnt.ensure(std::max<uint64_t>(rt, 1) * 4));
+    CK(ctx->tileoff.ensure(std::max<uint64_t>(rt, 1) * 8));
+    CK(ctx->scal.ensure(64));
+    CK(ctx->h_scal.ensure(64));
+    auto *sc = ctx->scal.as<unsigned long long>();
+    uint64_t d = 0;
+    if (rt) {
+        {
+            KScope ks(ctx, GKC_K_RLE, 8.0 * n);
+            rle_count_kernel<<<(unsigned)rt, RL_THREADS, 0, ctx->s>>>(src, n, ctx->tilecnt.as<uint32_t>());
+            LAUNCHED();
+        }
+        RET(scan_u32(ctx, ctx->tilecnt.as<uint32_t>(), rt, ctx->tileoff.as<uint64_t>(), sc));
+        CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 8, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        d = ctx->h_scal.as<unsigned long long>()[0];
+        CK(ctx->heads_pos.ensure(std::max<uint64_t>(d, 1) * 8));
+        CK(ctx->heads_key.ensure(std::max<uint64_t>(d, 1) * 8));
+        KScope ks(ctx, GKC_K_RLE, 8.0 * n + 16.0 * d);
+        rle_write_kernel<<<(unsigned)rt, RL_THREADS, 0, ctx->s>>>(src, n, ctx->tileoff.as<uint64_t>(),
+                                                                   ctx->heads_pos.as<uint64_t>(),
+                                                                   ctx->heads_key.as<uint64_t>());
+        LAUNCHED();
+    }
+    uint64_t kept = 0;
+    const uint64_t kt = (d + RL_TILE - 1) / RL_TILE;
+    if (kt) {
+        CK(ctx->tilecnt.ensure(kt * 4));
+        CK(ctx->tileoff.ensure(kt * 8));
+        {
+            KScope ks(ctx, GKC_K_RLE, 8.0 * d);
+            keep_count_kernel<<<(unsigned)kt, RL_THREADS, 0, ctx->s>>>(ctx->heads_pos.as<uint64_t>(), d, n, cmin,
+                                                                         cmax, ctx->tilecnt.as<uint32_t>());
+            LAUNCHED();
+        }
+        RET(scan_u32(ctx, ctx->tilecnt.as<uint32_t>(), kt, ctx->tileoff.as<uint64_t>(), sc));
+        CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 8, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        kept = ctx->h_scal.as<unsigned long long>()[0];
+        RET(ensure_out(ctx, ctx->n_out + kept));
+        KScope ks(ctx, GKC_K_RLE, 16.0 * d + 12.0 * kept);
+        keep_write_kernel<<<(unsigned)kt, RL_THREADS, 0, ctx->s>>>(
+            ctx->heads_pos.as<uint64_t>(), ctx->heads_key.as<uint64_t>(), d, n, cmin, cmax,
+            ctx->tileoff.as<uint64_t>(), ctx->out_k.as<uint64_t>() + ctx->n_out,
+            ctx->out_c.as<uint32_t>() + ctx->n_out);
+        LAUNCHED();
+    }
+    float ms = 0;
+    CK(cudaEventSynchronize(ctx->e3));
+    CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
+    *sort_ms += ms;
+    ctx->n_out += kept;
+    ctx->n_distinct += d;
+    return GKC_OK;
+}
+
+int sort_and_reduce(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, int nbits, uint32_t cmin,
+                    uint32_t cmax, float *sort_ms) {
+    switch (ctx->opt.radix_bits) {
+        case 4: return sort_and_reduce_rb<4>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        case 5: return sort_and_reduce_rb<5>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        case 6: return sort_and_reduce_rb<6>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        case 7: return sort_and_reduce_rb<7>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        default: return sort_and_reduce_rb<8>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+    }
+}
+
+int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    std::vector<uint64_t> np(P, 0);
+    for (auto *c : ctx->store)
+        for (uint32_t p = 0; p < P; p++) np[p] += c->kmers[p];
+    uint64_t budget = ctx->opt.group_keys;
+    if (!budget) {
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        budget = std::max<uint64_t>(1ull << 20, (uint64_t)(fr * 0.5) / 40);
+    }
+    CK(ctx->segoff.ensure(P * 8));
+    CK(ctx->segcur.ensure(P * 8));
+    float sort_ms = 0;
+    uint32_t p0 = 0;
+    while (p0 < P) {
+        uint32_t p1 = p0;
+        uint64_t n = 0;
+        while (p1 < P && (p1 == p0 || n + np[p1] <= budget)) n += np[p1++];
+        std::vector<uint64_t> segoff(P, 0), segs;
+        uint64_t o = 0;
+        for (uint32_t p = p0; p < p1; p++) { segoff[p] = o; o += np[p]; segs.push_back(np[p]); }
+        if (n) {
+            CK(ctx->keysA.ensure(n * 8));
+            CK(ctx->keysB.ensure(n * 8));
+            CK(cudaMemcpyAsync(ctx->segoff.p, segoff.data(), P * 8, cudaMemcpyHostToDevice, ctx->s));
+            CK(cudaMemsetAsync(ctx->segcur.p, 0, P * 8, ctx->s));
+            for (auto *c : ctx->store) {
+                uint64_t i0 = c->skm_off[p0], i1 = c->skm_off[p1];
+                if (i1 == i0) continue;
+                const uint8_t *bytes = c->bytes;
+                const uint64_t *idx = c->idx;
+                if (c->on_host) {  // stage the group's part of a spilled chunk
+                    uint64_t b0 = c->byte_off[p0], b1 = c->byte_off[p1];
+                    CK(cudaStreamSynchronize(ctx->s));
+                    CK(ctx->stage_bytes.ensure(b1 - b0 + 16));
+                    CK(ctx->stage_idx.ensure((i1 - i0) * 8 + 8));
+                    CK(cudaMemcpyAsync(ctx->stage_bytes.p, c->bytes + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->s));
+                    CK(cudaMemcpyAsync(ctx->stage_idx.p, c->idx + i0, (i1 - i0) * 8, cudaMemcpyHostToDevice, ctx->s));
+                    // kernel indexes bytes by partition offsets: rebase the pointers
+                    bytes = ctx->stage_bytes.as<uint8_t>() - b0;
+                    idx = ctx->stage_idx.as<uint64_t>() - i0;
+                }
+                SExtractParams x;
+                x.bytes = bytes;
+                x.idx = idx;
+                x.n_skm = i1;
+                x.part_skm_off = c->d_skm_off.as<unsigned long long>();
+                x.part_byte_off = c->d_byte_off.as<unsigned long long>();
+                x.P = P;
+                x.k = ctx->opt.k;
+                x.canonical = 1;
+                x.keys = ctx->keysA.as<uint64_t>();
+                x.seg_off = ctx->segoff.as<unsigned long long>();
+                x.seg_cursor = ctx->segcur.as<unsigned long long>();
+                x.i_begin = i0;
+                uint32_t g = (uint32_t)std::min<uint64_t>((i1 - i0 + SX_THREADS - 1) / SX_THREADS, (uint64_t)ctx->sms * 8);
+                uint64_t kx = 0;
+                for (uint32_t p = p0; p < p1; p++) kx += c->kmers[p];
+                KScope ks(ctx, GKC_K_SORT_EXTRACT,
+                          (double)(c->byte_off[p1] - c->byte_off[p0]) + 8.0 * (i1 - i0) + 8.0 * kx);
+                sort_extract_kernel<<<g, SX_THREADS, 0, ctx->s>>>(x);
+                LAUNCHED();
+            }
+            RET(sort_and_reduce(ctx, segs, n, 2 * ctx->opt.k, cmin, cmax, &sort_ms));
+        }
+        p0 = p1;
+    }
+    ctx->times[3] = sort_ms;
+    return GKC_OK;
+}
+
+int upload(gkc_ctx *ctx, DevBuf &buf, const void *src, uint64_t bytes, int mem, const void **dptr) {
+    if (mem == GKC_MEM_DEVICE) {
+        *dptr = src;
+        return GKC_OK;
+    }
+    CK(buf.ensure(bytes + 16));
+    CK(cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, ctx->s));
+    *dptr = buf.p;
+    return GKC_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+extern "C" {
+
+void gkc_default_options(gkc_options *o) {
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->k = 31;
+    o->p = 11;
+    o->partitions = 512;
+    o->counter = GKC_COUNTER_HASH;
+    o->radix_bits = 8;
+    o->table_slots = 0.75;
+    o->batch_bases = 1ull << 30;
+    o->spill_host = 0;
+    o->group_keys = 0;
+}
+
+const char *gkc_strerror(int code) {
+    switch (code) {
+        case GKC_OK: return "ok";
+        case GKC_EINVAL: return "invalid argument";
+        case GKC_ECUDA: return "CUDA error";
+        case GKC_ENOMEM: return "out of memory";
+        case GKC_ESTATE: return "invalid call order";
+        case GKC_EINTERNAL: return "internal error";
+        default: return "unknown error";
+    }
+}
+
+const char *gkc_last_error(const gkc_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+uint64_t gkc_kernel_launches(const gkc_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int gkc_create(int device, const gkc_options *opt, gkc_ctx **out) {
+    if (!out) return GKC_EINVAL;
+    *out = nullptr;
+    gkc_options o;
+    gkc_default_options(&o);
+    if (opt) o = *opt;
+    if (o.p < 3 || o.p > 16 || o.k < o.p || o.k > 32 || o.partitions < 1 || o.partitions > 4096 ||
+        (o.counter != GKC_COUNTER_SORT && o.counter != GKC_COUNTER_HASH) || o.radix_bits < 0 || o.radix_bits > 8 ||
+        (o.radix_bits != 0 && o.radix_bits < 4))
+        return GKC_EINVAL;
+    if (!o.radix_bits) o.radix_bits = 8;
+    if (!o.batch_bases) o.batch_bases = 1ull << 30;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return GKC_ECUDA;
+    auto *ctx = new gkc_ctx();
+    ctx->device = device;
+    ctx->opt = o;
+    auto cleanup = [&](int code) { delete ctx; return code; };
+    if (cudaSetDevice(device) != cudaSuccess) return cleanup(GKC_ECUDA);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return cleanup(GKC_ECUDA);
+    ctx->sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->own_s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->cs, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(GKC_ECUDA);
+    ctx->s = ctx->own_s;
+    cudaEvent_t *evs[] = {&ctx->e0, &ctx->e1, &ctx->e2, &ctx->e3};
+    for (auto *e : evs)
+        if (cudaEventCreate(e) != cudaSuccess) return cleanup(GKC_ECUDA);
+    for (int i = 0; i < 2; i++)
+        if (cudaEventCreateWithFlags(&ctx->buf_free[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->buf_ready[i], cudaEventDisableTiming) != cudaSuccess)
+            return cleanup(GKC_ECUDA);
+    *out = ctx;
+    return GKC_OK;
+}
+
+int gkc_destroy(gkc_ctx *ctx) {
+    if (!ctx) return GKC_EINVAL;
+    cudaSetDevice(ctx->device);
+    if (ctx->s) cudaStreamSynchronize(ctx->s);
+    if (ctx->cs) cudaStreamSynchronize(ctx->cs);
+    delete ctx;
+    return GKC_OK;
+}
+
+int gkc_set_order(gkc_ctx *ctx, const uint32_t *lut, uint64_t n, int mem) {
+    if (!ctx) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    if (!lut) {
+        ctx->has_lut = false;
+        return GKC_OK;
+    }
+    uint64_t need = 1ull << (2 * ctx->opt.p);
+    if (n != need) return ctx->fail(GKC_EINVAL, "order table needs 4^p = %llu entries", (unsigned long long)need);
+    CK(ctx->lut.ensure(n * 4));
+    CK(cudaMemcpyAsync(ctx->lut.p, lut, n * 4, mem == GKC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    ctx->has_lut = true;
+    return GKC_OK;
+}
+
+int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads, int mem) {
+    if (!ctx || (!reads && n_reads) || !offs) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    ctx->times[0] = ctx->times[1] = 0;
+    if (n_reads == 0) return GKC_OK;
+    if (mem == GKC_MEM_DEVICE) {
+        uint64_t first = 0, total = 0;
+        CK(cudaMemcpyAsync(&first, offs, 8, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(&total, offs + n_reads, 8, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        if (first != 0) return ctx->fail(GKC_EINVAL, "device input needs offs[0] == 0");
+        CK(cudaEventRecord(ctx->e2, ctx->s));
+        RET(phase1_batch(ctx, reinterpret_cast<const uint8_t *>(reads), offs, n_reads, total));
+        CK(cudaEventRecord(ctx->e3, ctx->s));
+        CK(cudaEventSynchronize(ctx->e3));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
+        ctx->times[0] = ms;
+        return GKC_OK;
+    }
+    if (offs[0] > offs[n_reads]) return ctx->fail(GKC_EINVAL, "offsets are not ascending");
+    // host input: batches of whole reads of about batch_bases bases, double
+    // buffered so the copy of batch i+1 overlaps phase 1 of batch i
+    struct Batch { uint64_t r0, r1; };
+    std::vector<Batch> batches;
+    uint64_t r = 0;
+    while (r < n_reads) {
+        uint64_t r1 = r + 1;
+        uint64_t lim = offs[r] + ctx->opt.batch_bases;
+        // binary search the last read end within the budget
+        uint64_t lo = r + 1, hi = n_reads;
+        while (lo < hi) {
+            uint64_t mid = (lo + hi + 1) >> 1;
+            if (offs[mid] <= lim) lo = mid; else hi = mid - 1;
+        }
+        r1 = std::max(r1, lo);
+        batches.push_back({r, r1});
+        r = r1;
+    }
+    auto stage = [&](size_t bi) -> int {
+        int slot = (int)(bi & 1);
+        const Batch &b = batches[bi];
+        uint64_t base = offs[b.r0], nb = offs[b.r1] - base, nr = b.r1 - b.r0;
+        CK(cudaStreamWaitEvent(ctx->cs, ctx->buf_free[slot], 0));
+        CK(ctx->reads[slot].ensure(nb + 64));
+        CK(ctx->offs[slot].ensure((nr + 1) * 8));
+        CK(ctx->offs_pin[slot].ensure((nr + 1) * 8));
+        CK(cudaEventSynchronize(ctx->buf_free[slot]));  // pinned offsets buffer reuse
+        uint64_t *po = ctx->offs_pin[slot].as<uint64_t>();
+        for (uint64_t i = 0; i <= nr; i++) po[i] = offs[b.r0 + i] - base;
+        CK(cudaMemcpyAsync(ctx->reads[slot].p, reads + base, nb, cudaMemcpyHostToDevice, ctx->cs));
+        CK(cudaMemcpyAsync(ctx->offs[slot].p, po, (nr + 1) * 8, cudaMemcpyHostToDevice, ctx->cs));
+        CK(cudaEventRecord(ctx->buf_ready[slot], ctx->cs));
+        return GKC_OK;
+    };
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    CK(cudaEventRecord(ctx->buf_free[0], ctx->s));
+    CK(cudaEventRecord(ctx->buf_free[1], ctx->s));
+    CK(cudaEventRecord(t0, ctx->s));
+    int rc = stage(0);
+    for (size_t bi = 0; rc == GKC_OK && bi < batches.size(); bi++) {
+        int slot = (int)(bi & 1);
+        if (bi + 1 < batches.size()) rc = stage(bi + 1);
+        if (rc != GKC_OK) break;
+        CK(cudaStreamWaitEvent(ctx->s, ctx->buf_ready[slot], 0));
+        const Batch &b = batches[bi];
+        rc = phase1_batch(ctx, ctx->reads[slot].as<uint8_t>(), ctx->offs[slot].as<uint64_t>(), b.r1 - b.r0,
+                          offs[b.r1] - offs[b.r0]);
+        CK(cudaEventRecord(ctx->buf_free[slot], ctx->s));
+    }
+    CK(cudaEventRecord(t1, ctx->s));
+    CK(cudaEventSynchronize(t1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, t0, t1);
+    ctx->times[0] = ms;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return rc;
+}
+
+int gkc_store_stats(gkc_ctx *ctx, uint64_t *pb, uint64_t *ps, uint64_t *pk) {
+    if (!ctx) return GKC_EINVAL;
+    const int P = ctx->opt.partitions;
+    for (int p = 0; p < P; p++) {
+        uint64_t b = 0, s = 0, k = 0;
+        for (auto *c : ctx->store) {
+            b += c->byte_off[p + 1] - c->byte_off[p];
+            s += c->skm_off[p + 1] - c->skm_off[p];
+            k += c->kmers[p];
+        }
+        if (pb) pb[p] = b;
+        if (ps) ps[p] = s;
+        if (pk) pk[p] = k;
+    }
+    return GKC_OK;
+}
+
+int gkc_store_export(gkc_ctx *ctx, int part, uint8_t *out, uint64_t cap, uint64_t *n) {
+    if (!ctx || part < 0 || part >= ctx->opt.partitions || !n) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    uint64_t total = 0;
+    for (auto *c : ctx->store) total += c->byte_off[part + 1] - c->byte_off[part];
+    *n = total;
+    if (!out) return GKC_OK;
+    if (cap < total) return ctx->fail(GKC_EINVAL, "export buffer too small (%llu < %llu)",
+                                      (unsigned long long)cap, (unsigned long long)total);
+    uint64_t o = 0;
+    for (auto *c : ctx->store) {
+        uint64_t b0 = c->byte_off[part], b1 = c->byte_off[part + 1];
+        if (b1 > b0)
+            CK(cudaMemcpyAsync(out + o, c->bytes + b0, b1 - b0, c->on_host ? cudaMemcpyHostToHost : cudaMemcpyDeviceToHost,
+                               ctx->s));
+        o += b1 - b0;
+    }
+    CK(cudaStreamSynchronize(ctx->s));
+    return GKC_OK;
+}
+
+int gkc_store_clear(gkc_ctx *ctx) {
+    if (!ctx) return GKC_EINVAL;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->s);
+    for (auto *c : ctx->store) gkc_ctx::delete_chunk(c);
+    ctx->store.clear();
+    return GKC_OK;
+}
+
+int gkc_count(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, uint64_t *n_out, uint64_t *n_distinct) {
+    if (!ctx || cmin > cmax) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    ctx->n_out = 0;
+    ctx->n_distinct = 0;
+    ctx->has_result = false;
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    CK(cudaEventRecord(t0, ctx->s));
+    int rc = ctx->opt.counter == GKC_COUNTER_HASH ? count_hash(ctx, cmin, cmax) : count_sort(ctx, cmin, cmax);
+    cudaEventRecord(t1, ctx->s);
+    cudaEventSynchronize(t1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, t0, t1);
+    ctx->times[2] = ms;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    gkc_store_clear(ctx);
+    if (rc != GKC_OK) return rc;
+    ctx->has_result = true;
+    if (n_out) *n_out = ctx->n_out;
+    if (n_distinct) *n_distinct = ctx->n_distinct;
+    return GKC_OK;
+}
+
+int gkc_result(gkc_ctx *ctx, uint64_t *kmers, uint32_t *counts, uint64_t cap, int mem) {
+    if (!ctx) return GKC_EINVAL;
+    if (!ctx->has_result) return ctx->fail(GKC_ESTATE, "no result: call gkc_count first");
+    CK(cudaSetDevice(ctx->device));
+    uint64_t n = std::min(cap, ctx->n_out);
+    cudaMemcpyKind kind = mem == GKC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (n && kmers) CK(cudaMemcpyAsync(kmers, ctx->out_k.p, n * 8, kind, ctx->s));
+    if (n && counts) CK(cudaMemcpyAsync(counts, ctx->out_c.p, n * 4, kind, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    return GKC_OK;
+}
+
+int gkc_result_device(gkc_ctx *ctx, const uint64_t **kmers, const uint32_t **counts, uint64_t *n) {
+    if (!ctx) return GKC_EINVAL;
+    if (!ctx->has_result) return ctx->fail(GKC_ESTATE, "no result: call gkc_count first");
+    if (kmers) *kmers = ctx->out_k.as<uint64_t>();
+    if (counts) *counts = ctx->out_c.as<uint32_t>();
+    if (n) *n = ctx->n_out;
+    return GKC_OK;
+}
+
+int gkc_count_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads, int mem,
+                    uint32_t cmin, uint32_t cmax, uint64_t *kmers, uint32_t *counts, uint64_t cap, int out_mem,
+                    uint64_t *n_out, uint64_t *n_distinct) {
+    if (!ctx) return GKC_EINVAL;
+    RET(gkc_store_clear(ctx));
+    RET(gkc_add_reads(ctx, reads, offs, n_reads, mem));
+    uint64_t no = 0, nd = 0;
+    RET(gkc_count(ctx, cmin, cmax, &no, &nd));
+    if (n_out) *n_out = no;
+    if (n_distinct) *n_distinct = nd;
+    if (kmers || counts) {
+        if (cap < no) return ctx->fail(GKC_EINVAL, "output buffer too small (%llu < %llu)",
+                                       (unsigned long long)cap, (unsigned long long)no);
+        RET(gkc_result(ctx, kmers, counts, cap, out_mem));
+    }
+    return GKC_OK;
+}
+
+int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint32_t cmin, uint32_t cmax,
+                   uint64_t *n_out, uint64_t *n_distinct) {
+    if (!ctx || (!keys && n) || cmin > cmax) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    ctx->n_out = 0;
+    ctx->n_distinct = 0;
+    ctx->has_result = false;
+    if (ctx->opt.counter == GKC_COUNTER_HASH) {
+        const double slots = ctx->opt.table_slots > 0 ? ctx->opt.table_slots : 0.75;
+        const void *dk;
+        RET(upload(ctx, ctx->keysA, keys, n * 8, mem, &dk));
+        RET(ensure_out(ctx, n / std::max<uint32_t>(cmin, 1) + 1024));
+        CK(ctx->part_err.ensure(64));
+        CK(ctx->scal.ensure(64));
+        CK(ctx->h_scal.ensure(64));
+        for (int scale = 1;; scale *= 4) {
+            uint64_t C = next_pow2(std::max<uint64_t>(1024, (uint64_t)((double)n * slots) * scale));
+            if (C > ctx->tcap) {
+                ctx->tkeys.release();
+                ctx->tcnts.release();
+                CK(ctx->tkeys.ensure(C * 8));
+                CK(ctx->tcnts.ensure(C * 4));
+                CK(cudaMemsetAsync(ctx->tkeys.p, 0xFF, C * 8, ctx->s));
+                CK(cudaMemsetAsync(ctx->tcnts.p, 0, C * 4, ctx->s));
+                ctx->tcap = C;
+            }
+            CK(cudaMemsetAsync(ctx->part_err.p, 0, 64, ctx->s));
+            CK(cudaMemsetAsync(ctx->scal.p, 0, 64, ctx->s));
+            auto *sc = ctx->scal.as<unsigned long long>();
+            if (n) {
+                uint32_t g = (uint32_t)std::min<uint64_t>((n + H_THREADS - 1) / H_THREADS, (uint64_t)ctx->sms * 8);
+                KScope ks(ctx, GKC_K_HASH_INSERT, 8.0 * n);
+                hash_insert_keys_kernel<<<g, H_THREADS, 0, ctx->s>>>(
+                    reinterpret_cast<const uint64_t *>(dk), n, ctx->tkeys.as<unsigned long long>(),
+                    ctx->tcnts.as<uint32_t>(), C - 1, ctx->part_err.as<uint32_t>());
+                LAUNCHED();
+            }
+            HCollectParams q;
+            q.keys = ctx->tkeys.as<unsigned long long>();
+            q.cnts = ctx->tcnts.as<uint32_t>();
+            q.cap = C;
+            q.cmin = cmin;
+            q.cmax = cmax;
+            q.out_k = ctx->out_k.as<uint64_t>();
+            q.out_c = ctx->out_c.as<uint32_t>();
+            q.out_cursor = sc;
+            q.out_cap = ctx->out_cap;
+            q.distinct = sc + 1;
+            q.err = reinterpret_cast<uint32_t *>(sc + 2);
+            q.part_err = ctx->part_err.as<uint32_t>();
+            uint32_t g = (uint32_t)std::min<uint64_t>((C + H_THREADS * HC_ITEMS - 1) / (H_THREADS * HC_ITEMS),
+                                                      (uint64_t)ctx->sms * 8);
+            {
+                KScope ks(ctx, GKC_K_HASH_COLLECT, 24.0 * C);
+                hash_collect_kernel<<<g, H_THREADS, 0, ctx->s>>>(q);
+                LAUNCHED();
+            }
+            uint32_t perr = 0;
+            CK(cudaMemcpyAsync(&perr, ctx->part_err.p, 4, cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaStreamSynchronize(ctx->s));
+            if (perr & ERR_DECODE) return ctx->fail(GKC_EINVAL, "key 2^64-1 is reserved");
+            if (perr & ERR_TABLE_FULL) {
+                if (scale >= 64) return ctx->fail(GKC_EINTERNAL, "hash table retries exhausted");
+                continue;
+            }
+            auto *hs = ctx->h_scal.as<unsigned long long>();
+            ctx->n_out = hs[0];
+            ctx->n_distinct = hs[1];
+            break;
+        }
+    } else {
+        CK(ctx->keysA.ensure(n * 8 + 8));
+        CK(ctx->keysB.ensure(n * 8 + 8));
+        CK(cudaMemcpyAsync(ctx->keysA.p, keys, n * 8, mem == GKC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                           ctx->s));
+        std::vector<uint64_t> segs{n};
+        float ms = 0;
+        RET(sort_and_reduce(ctx, segs, n, 64, cmin, cmax, &ms));
+        ctx->times[3] = ms;
+    }
+    ctx->has_result = true;
+    if (n_out) *n_out = ctx->n_out;
+    if (n_distinct) *n_distinct = ctx->n_distinct;
+    return GKC_OK;
+}
+
+int gkc_set_stream(gkc_ctx *ctx, void *stream) {
+    if (!ctx) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->s));
+    ctx->s = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->own_s;
+    return GKC_OK;
+}
+
+int gkc_set_profiling(gkc_ctx *ctx, int on) {
+    if (!ctx) return GKC_EINVAL;
+    ctx->prof_flush();
+    ctx->prof = on != 0;
+    return GKC_OK;
+}
+
+int gkc_kernel_stats(gkc_ctx *ctx, double *ms, uint64_t *launches, double *bytes, int n, int reset) {
+    if (!ctx || n < 0) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    ctx->prof_flush();
+    for (int i = 0; i < n && i < GKC_K_CLASSES; i++) {
+        if (ms) ms[i] = ctx->kms[i];
+        if (launches) launches[i] = ctx->klaunch[i];
+        if (bytes) bytes[i] = ctx->kbytes[i];
+    }
+    if (reset)
+        for (int i = 0; i < GKC_K_CLASSES; i++) ctx->kms[i] = ctx->kbytes[i] = 0, ctx->klaunch[i] = 0;
+    return GKC_OK;
+}
+
+int gkc_last_timings(gkc_ctx *ctx, double *t, int n) {
+    if (!ctx || !t) return GKC_EINVAL;
+    for (int i = 0; i < n && i < 4; i++) t[i] = ctx->times[i];
+    return GKC_OK;
+}
+
+}  // extern "C"

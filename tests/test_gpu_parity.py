@@ -1,0 +1,186 @@
+"""Parity of the CUDA path (through the C ABI) with the reference's outputs:
+golden fixtures made by the reference's own CPU path, and the oracle on fresh
+seeded inputs.  Integer work: every comparison is bit-exact."""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden, partition_digest, sorted_table
+from tests_util import csr, random_reads
+
+pytestmark = pytest.mark.gpu
+U32 = 0xFFFFFFFF
+
+
+def counter(k, p, P, kind="hash", **kw):
+    from rapidgkc_b200 import KmerCounter
+    return KmerCounter(k=k, p=p, partitions=P, counter=kind, **kw)
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_golden_superkmers(case):
+    g = load_golden(case)
+    k, p, P = int(g["k"]), int(g["p"]), int(g["P"])
+    with counter(k, p, P) as c:
+        c.add_reads(g["reads"], g["offs"])
+        pb, ps, pk = c.store_stats()
+        assert np.array_equal(pb, g["part_bytes"])
+        assert np.array_equal(ps, g["part_skms"])
+        assert np.array_equal(pk, g["part_kmers"])
+        for i in range(P):
+            assert partition_digest(c.store_export(i)) == str(g["digests"][i]), f"partition {i}"
+
+
+@pytest.mark.parametrize("kind", ["hash", "sort"])
+@pytest.mark.parametrize("case", golden_cases())
+def test_golden_counts(case, kind):
+    g = load_golden(case)
+    k, p, P = int(g["k"]), int(g["p"]), int(g["P"])
+    with counter(k, p, P, kind) as c:
+        c.add_reads(g["reads"], g["offs"])
+        n, d = c.count(1, U32)
+        km, ct = sorted_table(*c.result())
+        assert d == int(g["n_distinct"]) and n == len(g["kmers"])
+        assert np.array_equal(km, g["kmers"]) and np.array_equal(ct, g["counts"])
+        # threshold [2, 5] on the same input
+        c.add_reads(g["reads"], g["offs"])
+        n, d = c.count(2, 5)
+        km, ct = sorted_table(*c.result())
+        keep = (g["counts"] >= 2) & (g["counts"] <= 5)
+        assert d == int(g["n_distinct"])
+        assert np.array_equal(km, g["kmers"][keep]) and np.array_equal(ct, g["counts"][keep])
+
+
+@pytest.mark.parametrize("k,p,P,seed", [(31, 11, 512, 1), (25, 11, 64, 2), (21, 7, 31, 3), (15, 9, 5, 4),
+                                        (32, 16, 4096, 5), (12, 3, 2, 6)])
+def test_sort_counter_order_matches_oracle(oracle, k, p, P, seed):
+    """The sort counter emits partition by partition, ascending within."""
+    reads, offs = random_reads(seed, 30_000, 1200, (k, 260), 0.01)
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P, 2, U32)
+    with counter(k, p, P, "sort") as c:
+        n, d = c.count_reads(reads, offs, 2, U32)
+        km, ct = c.result()
+    assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+
+
+@pytest.mark.parametrize("kind", ["hash", "sort"])
+def test_device_input_and_many_batches(oracle, kind):
+    import torch
+    reads, offs = random_reads(7, 50_000, 4000, (20, 400), 0.005)
+    k, p, P = 27, 10, 128
+    ko, co, do, pko = oracle.count_reads(reads, offs, k, p, P)
+    ko, co = sorted_table(ko, co)
+    # device input
+    with counter(k, p, P, kind) as c:
+        dr = torch.from_numpy(reads).cuda()
+        do_ = torch.from_numpy(offs.view(np.int64)).cuda()
+        c.add_reads(dr, do_)
+        assert np.array_equal(c.store_stats()[2], pko)
+        n, d = c.count()
+        km, ct = sorted_table(*c.result())
+        assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+    # host input split into many small batches, added in two calls
+    with counter(k, p, P, kind, batch_bases=30_000) as c:
+        h = len(offs) // 2
+        c.add_reads(reads, offs[: h + 1])
+        c.add_reads(reads[int(offs[h]):], offs[h:] - offs[h])
+        assert np.array_equal(c.store_stats()[2], pko)
+        n, d = c.count()
+        km, ct = sorted_table(*c.result())
+        assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+
+
+@pytest.mark.parametrize("kind", ["hash", "sort"])
+def test_long_and_low_complexity_reads(oracle, kind):
+    """Superkmers longer than a tile's halo (poly-A, (AT)n) and reads spanning
+    many tiles take the kernel's global-memory continuation path."""
+    r = np.random.default_rng(8)
+    rnd = lambda n: bytes(np.frombuffer(b"ACGT", np.uint8)[r.integers(0, 4, n)])
+    parts = [rnd(20_000), b"A" * 6000, rnd(100) + b"A" * 3000 + rnd(100), b"AT" * 2500,
+             rnd(31), rnd(30), b"", rnd(2047), rnd(2048), rnd(2049), b"CAG" * 1000 + rnd(3000)]
+    reads, offs = csr(parts)
+    for k, p, P in [(31, 11, 64), (25, 11, 7)]:
+        pbo, pso, pko, po, stream = oracle.skmgen(reads, offs, k, p, P)
+        ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P)
+        ko, co = sorted_table(ko, co)
+        with counter(k, p, P, kind) as c:
+            c.add_reads(reads, offs)
+            pb, ps, pk = c.store_stats()
+            assert np.array_equal(pb, pbo) and np.array_equal(ps, pso) and np.array_equal(pk, pko)
+            for i in range(P):
+                assert partition_digest(c.store_export(i)) == partition_digest(stream[int(po[i]):int(po[i + 1])])
+            n, d = c.count()
+            km, ct = sorted_table(*c.result())
+            assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+
+
+def test_reads_shorter_than_k_and_empty():
+    reads, offs = csr([b"ACGT" * 7, b"", b"A", b"ACGTACGTACGTACGTACGTACGTACGTAC"])  # all < 31
+    with counter(31, 11, 16) as c:
+        n, d = c.count_reads(reads, offs)
+        assert (n, d) == (0, 0)
+    reads, offs = csr([b"ACGTTGCAACGTTGCAACGTTGCAACGTTGC"])  # exactly k
+    with counter(31, 11, 16, "sort") as c:
+        n, d = c.count_reads(reads, offs)
+        assert (n, d) == (1, 1)
+
+
+@pytest.mark.parametrize("kind", ["hash", "sort"])
+def test_learned_order_keeps_the_multiset(oracle, kind):
+    """Any minimizer order yields the same (k-mer, count) multiset; the
+    partition contents follow the order (checked against the oracle)."""
+    k, p, P = 31, 11, 256
+    reads, offs = random_reads(9, 40_000, 3000, 150, 0.004)
+    lut = np.random.default_rng(10).permutation(4 ** p).astype(np.uint32)
+    k0, c0, d0, _ = oracle.count_reads(reads, offs, k, p, P)
+    pbo, pso, pko, _, _ = oracle.skmgen(reads, offs, k, p, P, lut)
+    with counter(k, p, P, kind) as c:
+        c.set_order(lut)
+        c.add_reads(reads, offs)
+        pb, ps, pk = c.store_stats()
+        assert np.array_equal(pb, pbo) and np.array_equal(ps, pso) and np.array_equal(pk, pko)
+        n, d = c.count()
+        km, ct = sorted_table(*c.result())
+    k0, c0 = sorted_table(k0, c0)
+    assert d == d0 and np.array_equal(km, k0) and np.array_equal(ct, c0)
+
+
+@pytest.mark.parametrize("kind", ["hash", "sort"])
+def test_hash_known_answer(kind):
+    """gpu_hash_counter.cu:693-708: 40M keys i % 1234567 + 0xffffffff."""
+    n = 40_000_000
+    keys = (np.arange(n, dtype=np.uint64) % np.uint64(1234567)) + np.uint64(0xFFFFFFFF)
+    with counter(31, 11, 1, kind) as c:
+        kept, d = c.count_keys(keys, 2, U32)
+        assert d == 1234567 and kept == 1234567
+        km, ct = sorted_table(*c.result())
+        assert np.array_equal(km, np.arange(1234567, dtype=np.uint64) + np.uint64(0xFFFFFFFF))
+        assert int(ct.sum()) == n and ct.min() == 32 and ct.max() == 33
+
+
+@pytest.mark.parametrize("kind", ["hash", "sort"])
+def test_count_keys_matches_oracle(oracle, kind):
+    r = np.random.default_rng(11)
+    keys = r.integers(0, 1 << 20, 3_000_000, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+    keys = keys[keys != np.uint64(0xFFFFFFFFFFFFFFFF)]
+    ko, co, do = oracle.count(keys, 3, 10)
+    with counter(31, 11, 1, kind) as c:
+        n, d = c.count_keys(keys, 3, 10)
+        km, ct = sorted_table(*c.result())
+    assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+
+
+def test_retries_spill_and_groups(oracle):
+    """Undersized hash tables are retried larger; a spilled store and small
+    sort groups give the same result."""
+    k, p, P = 31, 11, 64
+    reads, offs = random_reads(12, 60_000, 5000, 150, 0.01)
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P, 2, U32)
+    ko, co = sorted_table(ko, co)
+    for kw, kind in [(dict(table_slots=0.02), "hash"), (dict(spill_host=True), "hash"),
+                     (dict(spill_host=True, group_keys=50_000), "sort"), (dict(group_keys=1), "sort"),
+                     (dict(radix_bits=5), "sort")]:
+        with counter(k, p, P, kind, **kw) as c:
+            c.add_reads(reads, offs)
+            n, d = c.count(2, U32)
+            km, ct = sorted_table(*c.result())
+        assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co), kw
