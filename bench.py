@@ -155,7 +155,7 @@ def main():
     ap.add_argument("--partitions", type=int, default=512)
     ap.add_argument("--cmin", type=int, default=2)
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--cpu-fraction", type=float, default=0.01)
+    ap.add_argument("--cpu-fraction", type=float, default=0.03)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -214,6 +214,7 @@ def main():
         barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
     launches = (c.kernel_launches() - launches0) // args.steps
+    tstats = c.timings()
     kstats = c.kernel_stats(reset=True)
     c.set_profiling(False)
     if world > 1:
@@ -268,7 +269,8 @@ def main():
                        "partitions": args.partitions, "counter": args.counter, "order": "default",
                        "threshold": f">={args.cmin}", "parallelism": f"dp{world} (independent read sets)",
                        "l2": "inputs (3 GB) larger than L2; no flush", "kmers_kept": n_out,
-                       "distinct": n_dist, "gen_s": round(t_gen, 1)},
+                       "distinct": n_dist, "gen_s": round(t_gen, 1),
+                       "sub_buckets": tstats["sub_buckets"], "overflowed": tstats["overflowed_sub_buckets"]},
             "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches)}
     clk_s = clk.summary()
     if clk_s:

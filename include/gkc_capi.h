@@ -48,10 +48,12 @@ typedef struct gkc_options {
     int partitions;         /* superkmer partitions, 1..4096 (reference -skm, utilities.hpp:189)  */
     int counter;            /* GKC_COUNTER_SORT or GKC_COUNTER_HASH                               */
     int radix_bits;         /* LSD digit width of the sort counter, 4..8 (0 = 8)                  */
-    double table_slots;     /* hash slots per k-mer instance of a partition (0 = 0.75)            */
+    double table_slots;     /* hash slots per k-mer instance of a partition (0 = 0.35)            */
     uint64_t batch_bases;   /* bases per phase-1 batch for host input (0 = 1 GiB)                 */
     int spill_host;         /* keep the partition store in pinned host memory (streamed input)    */
     uint64_t group_keys;    /* max k-mer instances per sort group (0 = from free device memory)   */
+    int hash_l2_only;       /* hash counter: 0 = shared-memory sub-buckets with the L2 table for  */
+                            /* the ones that overflow; 1 = every partition through the L2 table   */
 } gkc_options;
 
 /* Fills defaults: k=31, p=11, partitions=512, hash counter. */
@@ -115,9 +117,11 @@ int gkc_count_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint6
 int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint32_t cmin, uint32_t cmax,
                    uint64_t *n_out, uint64_t *n_distinct);
 
-/* Device milliseconds of the last gkc_add_reads (phase 1) and gkc_count
- * (phase 2) calls, from CUDA events; times[0..3] = phase 1 total, phase 1
- * superkmer search, phase 2 total, phase 2 dominant kernel. */
+/* Statistics of the last gkc_add_reads (phase 1) and gkc_count (phase 2)
+ * calls (n <= 6 entries): times[0..3] = device milliseconds (CUDA events) of
+ * phase 1, its superkmer search, phase 2, and phase 2's counting kernels;
+ * times[4] = sub-buckets of the hash counter, times[5] = those that
+ * overflowed shared memory and were re-split by k-mer hash. */
 int gkc_last_timings(gkc_ctx *ctx, double *times, int n);
 
 /* Number of kernels this context launched since creation. */

@@ -47,6 +47,7 @@ class Options(C.Structure):
         ("batch_bases", C.c_uint64),
         ("spill_host", C.c_int),
         ("group_keys", C.c_uint64),
+        ("hash_l2_only", C.c_int),
     ]
 
 
@@ -120,15 +121,16 @@ class KmerCounter:
     k [-k], p [-p], partitions [-skm], counter 'hash' or 'sort'."""
 
     def __init__(self, k: int = 31, p: int = 11, partitions: int = 512, counter: str = "hash",
-                 device: int = 0, radix_bits: int = 8, table_slots: float = 0.75,
-                 batch_bases: int = 1 << 30, spill_host: bool = False, group_keys: int = 0):
+                 device: int = 0, radix_bits: int = 8, table_slots: float = 0.35,
+                 batch_bases: int = 1 << 30, spill_host: bool = False, group_keys: int = 0,
+                 hash_l2_only: bool = False):
         L = load_library()
         o = Options()
         L.gkc_default_options(C.byref(o))
         o.k, o.p, o.partitions = k, p, partitions
         o.counter = {"hash": COUNTER_HASH, "sort": COUNTER_SORT}[counter]
         o.radix_bits, o.table_slots, o.batch_bases = radix_bits, table_slots, batch_bases
-        o.spill_host, o.group_keys = int(spill_host), group_keys
+        o.spill_host, o.group_keys, o.hash_l2_only = int(spill_host), group_keys, int(hash_l2_only)
         h = C.c_void_p()
         rc = L.gkc_create(device, C.byref(o), C.byref(h))
         if rc != GKC_OK:
@@ -234,9 +236,10 @@ class KmerCounter:
         return no.value, nd.value
 
     def timings(self):
-        t = (C.c_double * 4)()
-        self._check(self._L.gkc_last_timings(self._h, t, 4))
-        return {"phase1_ms": t[0], "phase1_search_ms": t[1], "phase2_ms": t[2], "phase2_kernel_ms": t[3]}
+        t = (C.c_double * 6)()
+        self._check(self._L.gkc_last_timings(self._h, t, 6))
+        return {"phase1_ms": t[0], "phase1_search_ms": t[1], "phase2_ms": t[2], "phase2_kernel_ms": t[3],
+                "sub_buckets": int(t[4]), "overflowed_sub_buckets": int(t[5])}
 
     def kernel_launches(self) -> int:
         return int(self._L.gkc_kernel_launches(self._h))

@@ -18,7 +18,7 @@
 #include <string>
 #include <vector>
 
-#include "count_hash.cu"
+#include "count_records.cu"
 #include "count_sort.cu"
 #include "skmgen.cu"
 
@@ -68,14 +68,29 @@ struct PinBuf {
 };
 
 // One phase-1 batch worth of superkmers, partition-ordered.
+// Chunks are pooled: a cleared store keeps its buffers for the next batch,
+// so steady-state batches allocate nothing.
 struct StoreChunk {
     bool on_host = false;
-    uint8_t *bytes = nullptr;  // device or pinned host
-    uint64_t *idx = nullptr;
+    uint8_t *bytes = nullptr;  // = dbytes.p or hbytes.p
+    uint64_t *idx = nullptr;   // = didx.p or hidx.p
+    uint32_t *keys = nullptr;  // = dkeys.p or hkeys.p: minimizer key of each superkmer
     uint64_t nbytes = 0, nskm = 0;
     std::vector<uint64_t> byte_off, skm_off;  // [P+1]
     std::vector<uint64_t> kmers;              // [P]
+    DevBuf dbytes, didx, dkeys;               // device storage
+    PinBuf hbytes, hidx, hkeys;               // pinned host storage (spilled chunks)
     DevBuf d_byte_off, d_skm_off;             // device copies of the offsets
+    void release() {
+        dbytes.release();
+        didx.release();
+        dkeys.release();
+        hbytes.release();
+        hidx.release();
+        hkeys.release();
+        d_byte_off.release();
+        d_skm_off.release();
+    }
 };
 
 uint64_t next_pow2(uint64_t v) {
@@ -129,20 +144,20 @@ struct gkc_ctx {
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
     std::string err;
     uint64_t launches = 0;
-    double times[4] = {0, 0, 0, 0};
+    double times[6] = {0, 0, 0, 0, 0, 0};  // see gkc_last_timings
 
     // phase 1 buffers
     DevBuf reads[2], offs[2];
     PinBuf offs_pin[2];
     cudaEvent_t buf_free[2] = {nullptr, nullptr}, buf_ready[2] = {nullptr, nullptr};
-    DevBuf records, region_count, hist, flags, cursors, part_off;
+    DevBuf records, region_count, hist, flags, cursors, part_off, tile_read, codes;
     PinBuf h_hist, h_flags;
     DevBuf lut;
     bool has_lut = false;
     std::vector<StoreChunk *> store;
 
     // phase 2 buffers
-    DevBuf tkeys, tcnts;
+    DevBuf table;  // HSlot[tcap]
     uint64_t tcap = 0;
     DevBuf out_k, out_c;
     uint64_t out_cap = 0, n_out = 0, n_distinct = 0;
@@ -150,15 +165,37 @@ struct gkc_ctx {
     DevBuf keysA, keysB, tiles, counts, offsets, blocksums, heads_pos, heads_key, tilecnt, tileoff;
     DevBuf segoff, segcur, part_err, scal;
     DevBuf stage_bytes, stage_idx;
+    DevBuf spill_bytes, spill_idx, spill_keys;  // device staging of chunks being spilled
+    // shared-memory bucket counter
+    DevBuf bk_skms, bk_kmers, bk_off, bk_cur, bk_entries, bk_failed, bk_arena;
+    DevBuf r_work, r_count, r_off, r_cur, r_recs, r_failed;  // record sub-buckets
+    uint64_t fallback_buckets = 0;  // sub-buckets counted through the L2 table
     PinBuf h_scal;
+
+    std::vector<StoreChunk *> pool;  // cleared chunks kept for reuse
+
+    StoreChunk *take_chunk() {
+        if (pool.empty()) return new StoreChunk();
+        StoreChunk *c = pool.back();
+        pool.pop_back();
+        return c;
+    }
+    void clear_store() {
+        for (auto *c : store) pool.push_back(c);
+        store.clear();
+    }
 
     ~gkc_ctx() {
         for (auto *c : store) delete_chunk(c);
+        for (auto *c : pool) delete_chunk(c);
         store.clear();
+        pool.clear();
         DevBuf *ds[] = {&reads[0], &reads[1], &offs[0], &offs[1], &records, &region_count, &hist, &flags,
-                        &cursors, &part_off, &lut, &tkeys, &tcnts, &out_k, &out_c, &keysA, &keysB, &tiles,
+                        &cursors, &part_off, &tile_read, &codes, &lut, &table, &out_k, &out_c, &keysA, &keysB, &tiles,
                         &counts, &offsets, &blocksums, &heads_pos, &heads_key, &tilecnt, &tileoff, &segoff,
-                        &segcur, &part_err, &scal, &stage_bytes, &stage_idx};
+                        &segcur, &part_err, &scal, &stage_bytes, &stage_idx, &spill_bytes, &spill_idx, &spill_keys,
+                        &bk_skms, &bk_kmers, &bk_off, &bk_cur, &bk_entries, &bk_failed, &bk_arena,
+                        &r_work, &r_count, &r_off, &r_cur, &r_recs, &r_failed};
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal};
         for (auto *p : ps) p->release();
@@ -170,15 +207,7 @@ struct gkc_ctx {
         if (cs) cudaStreamDestroy(cs);
     }
     static void delete_chunk(StoreChunk *c) {
-        if (c->on_host) {
-            if (c->bytes) cudaFreeHost(c->bytes);
-            if (c->idx) cudaFreeHost(c->idx);
-        } else {
-            if (c->bytes) cudaFree(c->bytes);
-            if (c->idx) cudaFree(c->idx);
-        }
-        c->d_byte_off.release();
-        c->d_skm_off.release();
+        c->release();
         delete c;
     }
     int fail(int code, const char *fmt, ...) {
@@ -266,6 +295,20 @@ int scan_u32(gkc_ctx *ctx, const uint32_t *in, uint64_t n, uint64_t *out, unsign
     return GKC_OK;
 }
 
+// Hash table of at least C slots, every slot empty (the collect kernel leaves
+// the slots it reads empty, so only a new allocation is initialised).
+int ensure_table(gkc_ctx *ctx, uint64_t C) {
+    if (C <= ctx->tcap && ctx->table.p) return GKC_OK;
+    CK(cudaStreamSynchronize(ctx->s));
+    ctx->table.release();
+    CK(ctx->table.ensure(C * sizeof(HSlot)));
+    uint32_t g = (uint32_t)std::min<uint64_t>((C + 255) / 256, (uint64_t)ctx->sms * 16);
+    hash_init_kernel<<<g, 256, 0, ctx->s>>>(ctx->table.as<HSlot>(), C);
+    LAUNCHED();
+    ctx->tcap = C;
+    return GKC_OK;
+}
+
 int ensure_out(gkc_ctx *ctx, uint64_t need) {
     if (need <= ctx->out_cap && ctx->out_k.p) return GKC_OK;
     uint64_t cap = std::max<uint64_t>(need, 1024);
@@ -294,7 +337,18 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     const uint32_t P = (uint32_t)ctx->opt.partitions;
     if (total == 0 || n_reads == 0) return GKC_OK;
     const uint64_t ntiles = (total + P1_TILE - 1) / P1_TILE;
-    const uint32_t grid = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)ctx->sms * 4);
+    // the window-minimum doubling is unrolled per level count
+    const int w = ctx->opt.k - ctx->opt.p + 1;
+    int lg = 0;
+    while ((2 << lg) <= w) lg++;
+    void (*kfind)(P1Params) = lg == 0 ? find_superkmers_kernel<0> : lg == 1 ? find_superkmers_kernel<1>
+                              : lg == 2 ? find_superkmers_kernel<2> : lg == 3 ? find_superkmers_kernel<3>
+                                                                                : find_superkmers_kernel<4>;
+    size_t dyn = 3ull * P * sizeof(uint32_t);
+    CK(cudaFuncSetAttribute(kfind, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfind, P1_THREADS, dyn));
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)ctx->sms * std::max(per_sm, 1));
     const uint64_t tiles_per_cta = (ntiles + grid - 1) / grid;
     uint64_t cap = tiles_per_cta * P1_TILE / 4 + 4096;
     const uint64_t cap_max = tiles_per_cta * P1_TILE + 64;
@@ -303,10 +357,16 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     CK(ctx->flags.ensure(64));
     CK(ctx->h_hist.ensure(3ull * P * sizeof(unsigned long long)));
     CK(ctx->h_flags.ensure(64));
+    CK(ctx->tile_read.ensure(ntiles * sizeof(int64_t)));
+    CK(ctx->codes.ensure((ntiles * P1_TILE_WORDS + 4) * sizeof(uint32_t)));
+    CK(cudaMemsetAsync(ctx->codes.as<uint32_t>() + ntiles * P1_TILE_WORDS, 0, 16, ctx->s));
     auto *hist = ctx->hist.as<unsigned long long>();
     auto *hh = ctx->h_hist.as<unsigned long long>();
-    size_t dyn = 3ull * P * sizeof(uint32_t);
-    CK(cudaFuncSetAttribute(find_superkmers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    {
+        uint32_t g = (uint32_t)std::min<uint64_t>((ntiles + 255) / 256, (uint64_t)ctx->sms * 8);
+        tile_reads_kernel<<<g, 256, 0, ctx->s>>>(d_offs, (int64_t)n_reads, ntiles, ctx->tile_read.as<int64_t>());
+        LAUNCHED();
+    }
     for (int attempt = 0;; attempt++) {
         if (cap > UINT32_MAX) cap = UINT32_MAX;
         CK(ctx->records.ensure(cap * grid * sizeof(SkmRecord)));
@@ -320,20 +380,22 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
         a.k = ctx->opt.k;
         a.p = ctx->opt.p;
         a.P = P;
+        a.pmod = fastmod_m(P);
         a.lut = ctx->has_lut ? ctx->lut.as<uint32_t>() : nullptr;
         a.vec_ok = ((uintptr_t)d_reads & 15) == 0;
+        a.tile_read = ctx->tile_read.as<int64_t>();
+        a.codes = ctx->codes.as<uint32_t>();
         a.records = ctx->records.as<SkmRecord>();
         a.region_cap = (uint32_t)cap;
         a.region_count = ctx->region_count.as<uint32_t>();
         a.part_bytes = hist;
         a.part_skms = hist + P;
         a.part_kmers = hist + 2 * P;
-        a.smem_hist = 1;
         a.err = ctx->flags.as<uint32_t>();
         CK(cudaEventRecord(ctx->e0, ctx->s));
         {
             KScope ks(ctx, GKC_K_FIND_SUPERKMERS, (double)total + 8.0 * (n_reads + 1));
-            find_superkmers_kernel<<<grid, P1_THREADS, dyn, ctx->s>>>(a);
+            kfind<<<grid, P1_THREADS, dyn, ctx->s>>>(a);
             LAUNCHED();
         }
         CK(cudaEventRecord(ctx->e1, ctx->s));
@@ -355,7 +417,7 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
         break;
     }
     // ---- partition offsets, store chunk ----
-    auto *c = new StoreChunk();
+    StoreChunk *c = ctx->take_chunk();
     c->byte_off.assign(P + 1, 0);
     c->skm_off.assign(P + 1, 0);
     c->kmers.assign(P, 0);
@@ -366,34 +428,45 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     }
     c->nbytes = c->byte_off[P];
     c->nskm = c->skm_off[P];
+    c->on_host = false;
     if (ctx->prof && !ctx->pend.empty()) ctx->pend.back().bytes += 16.0 * c->nskm;  // records written
-    cudaError_t e1 = cudaMalloc((void **)&c->bytes, c->nbytes + 16);
-    cudaError_t e2 = e1 == cudaSuccess ? cudaMalloc((void **)&c->idx, std::max<uint64_t>(c->nskm, 1) * 8) : e1;
-    cudaError_t e3 = e2 == cudaSuccess ? c->d_byte_off.ensure((P + 1) * 8) : e2;
+    // a spilled chunk is scattered into shared device staging, then copied out
+    DevBuf &db = ctx->opt.spill_host ? ctx->spill_bytes : c->dbytes;
+    DevBuf &di = ctx->opt.spill_host ? ctx->spill_idx : c->didx;
+    DevBuf &dk = ctx->opt.spill_host ? ctx->spill_keys : c->dkeys;
+    cudaError_t e1 = db.ensure(c->nbytes + 32);
+    cudaError_t e2 = e1 == cudaSuccess ? di.ensure(std::max<uint64_t>(c->nskm, 1) * 8) : e1;
+    cudaError_t e2k = e2 == cudaSuccess ? dk.ensure(std::max<uint64_t>(c->nskm, 1) * 4) : e2;
+    cudaError_t e3 = e2k == cudaSuccess ? c->d_byte_off.ensure((P + 1) * 8) : e2k;
     cudaError_t e4 = e3 == cudaSuccess ? c->d_skm_off.ensure((P + 1) * 8) : e3;
     if (e4 != cudaSuccess) {
-        gkc_ctx::delete_chunk(c);
+        ctx->pool.push_back(c);
         return ctx->fail(GKC_ENOMEM, "store chunk allocation (%llu bytes): %s",
                          (unsigned long long)c->nbytes, cudaGetErrorString(e4));
     }
+    c->bytes = db.as<uint8_t>();
+    c->idx = di.as<uint64_t>();
+    c->keys = dk.as<uint32_t>();
     CK(cudaMemcpyAsync(c->d_byte_off.p, c->byte_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
     CK(cudaMemcpyAsync(c->d_skm_off.p, c->skm_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
     CK(ctx->cursors.ensure(2ull * P * sizeof(unsigned long long)));
     CK(cudaMemsetAsync(ctx->cursors.p, 0, 2ull * P * sizeof(unsigned long long), ctx->s));
     P2Params b;
-    b.reads = d_reads;
+    b.codes = ctx->codes.as<uint32_t>();
     b.records = ctx->records.as<SkmRecord>();
     b.region_cap = (uint32_t)cap;
     b.region_count = ctx->region_count.as<uint32_t>();
     b.k = ctx->opt.k;
     b.P = P;
+    b.pmod = fastmod_m(P);
     b.part_byte_off = c->d_byte_off.as<unsigned long long>();
     b.part_skm_off = c->d_skm_off.as<unsigned long long>();
     b.cur_bytes = ctx->cursors.as<unsigned long long>();
     b.cur_skms = ctx->cursors.as<unsigned long long>() + P;
     b.bytes = c->bytes;
     b.idx = c->idx;
-    size_t dyn2 = 2ull * P * sizeof(unsigned long long);
+    b.keys = c->keys;
+    size_t dyn2 = 2ull * P * (sizeof(unsigned long long) + sizeof(uint32_t));
     CK(cudaFuncSetAttribute(scatter_superkmers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn2));
     {
         KScope ks(ctx, GKC_K_SCATTER, 24.0 * c->nskm + (double)total + (double)c->nbytes);
@@ -401,126 +474,78 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
         LAUNCHED();
     }
     if (ctx->opt.spill_host) {
-        uint8_t *hb = nullptr;
-        uint64_t *hi = nullptr;
-        cudaError_t ea = cudaHostAlloc((void **)&hb, c->nbytes + 16, cudaHostAllocDefault);
-        cudaError_t eb = ea == cudaSuccess ? cudaHostAlloc((void **)&hi, std::max<uint64_t>(c->nskm, 1) * 8,
-                                                           cudaHostAllocDefault) : ea;
-        if (eb != cudaSuccess) {
-            if (hb) cudaFreeHost(hb);
-            gkc_ctx::delete_chunk(c);
-            return ctx->fail(GKC_ENOMEM, "pinned spill allocation: %s", cudaGetErrorString(eb));
+        cudaError_t ea = c->hbytes.ensure(c->nbytes + 16);
+        cudaError_t eb = ea == cudaSuccess ? c->hidx.ensure(std::max<uint64_t>(c->nskm, 1) * 8) : ea;
+        cudaError_t ec = eb == cudaSuccess ? c->hkeys.ensure(std::max<uint64_t>(c->nskm, 1) * 4) : eb;
+        if (ec != cudaSuccess) {
+            ctx->pool.push_back(c);
+            return ctx->fail(GKC_ENOMEM, "pinned spill allocation: %s", cudaGetErrorString(ec));
         }
-        CK(cudaMemcpyAsync(hb, c->bytes, c->nbytes, cudaMemcpyDeviceToHost, ctx->s));
-        CK(cudaMemcpyAsync(hi, c->idx, c->nskm * 8, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(c->hbytes.p, c->bytes, c->nbytes, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(c->hidx.p, c->idx, c->nskm * 8, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(c->hkeys.p, c->keys, c->nskm * 4, cudaMemcpyDeviceToHost, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
-        cudaFree(c->bytes);
-        cudaFree(c->idx);
-        c->bytes = hb;
-        c->idx = hi;
+        c->bytes = c->hbytes.as<uint8_t>();
+        c->idx = c->hidx.as<uint64_t>();
+        c->keys = c->hkeys.as<uint32_t>();
         c->on_host = true;
     }
     ctx->store.push_back(c);
     return GKC_OK;
 }
 
-// Device pointers of partition p of chunk c (staging spilled chunks).
-int chunk_part(gkc_ctx *ctx, StoreChunk *c, uint32_t p, const uint8_t **bytes, const uint64_t **idx,
-               uint64_t *nskm) {
-    uint64_t b0 = c->byte_off[p], b1 = c->byte_off[p + 1], s0 = c->skm_off[p], s1 = c->skm_off[p + 1];
-    *nskm = s1 - s0;
+// Device pointers of the superkmers of partitions [p0, p1) of chunk c, indexed
+// by the chunk's own partition offsets (spilled chunks are staged into `arena`
+// at *arena_used and the pointers rebased).
+int chunk_range(gkc_ctx *ctx, StoreChunk *c, uint32_t p0, uint32_t p1, DevBuf &arena, uint64_t *arena_used,
+                const uint8_t **bytes, const uint64_t **idx, const uint32_t **keys) {
     if (!c->on_host) {
-        *bytes = c->bytes + b0;
-        *idx = c->idx + s0;
+        *bytes = c->bytes;
+        *idx = c->idx;
+        *keys = c->keys;
         return GKC_OK;
     }
-    CK(cudaStreamSynchronize(ctx->s));  // staging buffers are reused
-    CK(ctx->stage_bytes.ensure(b1 - b0 + 16));
-    CK(ctx->stage_idx.ensure((s1 - s0) * 8 + 8));
-    CK(cudaMemcpyAsync(ctx->stage_bytes.p, c->bytes + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->s));
-    CK(cudaMemcpyAsync(ctx->stage_idx.p, c->idx + s0, (s1 - s0) * 8, cudaMemcpyHostToDevice, ctx->s));
-    *bytes = ctx->stage_bytes.as<uint8_t>();
-    *idx = ctx->stage_idx.as<uint64_t>();
+    const uint64_t b0 = c->byte_off[p0], b1 = c->byte_off[p1], s0 = c->skm_off[p0], s1 = c->skm_off[p1];
+    const uint64_t need = (b1 - b0 + 32 + 15) / 16 * 16 + (s1 - s0) * 8 + (s1 - s0) * 4 + 64;
+    if (*arena_used + need > arena.cap) return ctx->fail(GKC_EINTERNAL, "staging arena too small");
+    uint8_t *base = arena.as<uint8_t>() + *arena_used;
+    uint8_t *pb = base;
+    uint64_t *pi = reinterpret_cast<uint64_t *>(base + (b1 - b0 + 32 + 15) / 16 * 16);
+    uint32_t *pk = reinterpret_cast<uint32_t *>(pi + (s1 - s0));
+    CK(cudaMemcpyAsync(pb, c->bytes + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemcpyAsync(pi, c->idx + s0, (s1 - s0) * 8, cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemcpyAsync(pk, c->keys + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, ctx->s));
+    *arena_used += need;
+    // the kernels index with the chunk's absolute offsets: rebase
+    *bytes = pb - b0;
+    *idx = pi - s0;
+    *keys = pk - s0;
     return GKC_OK;
 }
 
-// ---------------------------------------------------------------------------
-// phase 2, hash counter
-int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
-    const uint32_t P = (uint32_t)ctx->opt.partitions;
-    std::vector<uint64_t> np(P, 0);
-    uint64_t N = 0;
-    for (auto *c : ctx->store)
-        for (uint32_t p = 0; p < P; p++) np[p] += c->kmers[p];
-    for (uint32_t p = 0; p < P; p++) N += np[p];
-    const double slots = ctx->opt.table_slots > 0 ? ctx->opt.table_slots : 0.75;
-    auto cap_of = [&](uint64_t n, int scale) {
-        return next_pow2(std::max<uint64_t>(1024, (uint64_t)((double)n * slots) * scale));
-    };
-    uint64_t cmax_cap = 1024;
-    for (uint32_t p = 0; p < P; p++) cmax_cap = std::max(cmax_cap, cap_of(np[p], 1));
-    if (cmax_cap > ctx->tcap) {
-        ctx->tkeys.release();
-        ctx->tcnts.release();
-        CK(ctx->tkeys.ensure(cmax_cap * 8));
-        CK(ctx->tcnts.ensure(cmax_cap * 4));
-        CK(cudaMemsetAsync(ctx->tkeys.p, 0xFF, cmax_cap * 8, ctx->s));
-        CK(cudaMemsetAsync(ctx->tcnts.p, 0, cmax_cap * 4, ctx->s));
-        ctx->tcap = cmax_cap;
-    }
-    RET(ensure_out(ctx, N / std::max<uint32_t>(cmin, 1) + 1024));
-    CK(ctx->part_err.ensure(P * 4));
-    CK(ctx->scal.ensure(64));
-    CK(ctx->h_scal.ensure(64));
-    CK(cudaMemsetAsync(ctx->part_err.p, 0, P * 4, ctx->s));
-    CK(cudaMemsetAsync(ctx->scal.p, 0, 64, ctx->s));
+// Counts the sub-buckets listed in `ids` through the L2 hash table (the
+// sub-buckets whose distinct k-mers outgrew shared memory).
+int count_buckets_l2(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const std::vector<uint64_t> &off,
+                     uint32_t cmin, uint32_t cmax) {
+    const double slots = ctx->opt.table_slots > 0 ? ctx->opt.table_slots : 0.35;
     auto *sc = ctx->scal.as<unsigned long long>();  // [0] cursor [1] distinct [2] err
-    CK(cudaMemcpyAsync(sc, &ctx->n_out, 8, cudaMemcpyHostToDevice, ctx->s));
-    CK(cudaStreamSynchronize(ctx->s));
-    float acc_insert = 0;
-    std::vector<uint32_t> todo;
-    for (uint32_t p = 0; p < P; p++) if (np[p]) todo.push_back(p);
-    std::vector<int> scale(P, 1);
-    for (int round = 0; !todo.empty(); round++) {
-        if (round > 4) return ctx->fail(GKC_EINTERNAL, "hash table retries exhausted");
-        for (uint32_t p : todo) {
-            uint64_t C = cap_of(np[p], scale[p]);
-            if (C > ctx->tcap) {  // a retried partition needs a larger table
-                CK(cudaStreamSynchronize(ctx->s));
-                ctx->tkeys.release();
-                ctx->tcnts.release();
-                CK(ctx->tkeys.ensure(C * 8));
-                CK(ctx->tcnts.ensure(C * 4));
-                CK(cudaMemsetAsync(ctx->tkeys.p, 0xFF, C * 8, ctx->s));
-                CK(cudaMemsetAsync(ctx->tcnts.p, 0, C * 4, ctx->s));
-                ctx->tcap = C;
-            }
-            CK(cudaEventRecord(ctx->e2, ctx->s));
-            for (auto *c : ctx->store) {
-                const uint8_t *pb;
-                const uint64_t *pi;
-                uint64_t ns;
-                RET(chunk_part(ctx, c, p, &pb, &pi, &ns));
-                if (!ns) continue;
-                HInsertParams h;
-                h.bytes = pb;
-                h.idx = pi;
-                h.n_skm = ns;
-                h.k = ctx->opt.k;
-                h.keys = ctx->tkeys.as<unsigned long long>();
-                h.cnts = ctx->tcnts.as<uint32_t>();
-                h.mask = C - 1;
-                h.err = ctx->part_err.as<uint32_t>() + p;
-                uint32_t g = (uint32_t)std::min<uint64_t>((ns + H_THREADS - 1) / H_THREADS, (uint64_t)ctx->sms * 8);
-                KScope ks(ctx, GKC_K_HASH_INSERT,
-                          (double)(c->byte_off[p + 1] - c->byte_off[p]) + 8.0 * ns);
-                hash_insert_kernel<<<g, H_THREADS, 0, ctx->s>>>(h);
+    for (uint32_t b : ids) {
+        const uint64_t e0 = off[b], e1 = off[b + 1];
+        for (int scale = 1;; scale *= 4) {
+            // ~12 k-mers per superkmer; an undersized table is retried larger
+            uint64_t C = next_pow2(std::max<uint64_t>(4096, (uint64_t)((double)(e1 - e0) * 12.0 * slots) * scale));
+            RET(ensure_table(ctx, C));
+            CK(cudaMemsetAsync(ctx->part_err.p, 0, 4, ctx->s));
+            {
+                uint32_t g = (uint32_t)std::min<uint64_t>((e1 - e0 + 63) / 64, (uint64_t)ctx->sms * 8);
+                KScope ks(ctx, GKC_K_HASH_INSERT, 16.0 * (e1 - e0));
+                hash_insert_entries_kernel<<<std::max(g, 1u), H_THREADS, 0, ctx->s>>>(
+                    ctx->bk_entries.as<BEntry>() + e0, e1 - e0, ctx->opt.k, ctx->table.as<HSlot>(), C - 1,
+                    ctx->part_err.as<uint32_t>());
                 LAUNCHED();
             }
-            CK(cudaEventRecord(ctx->e3, ctx->s));
             HCollectParams q;
-            q.keys = ctx->tkeys.as<unsigned long long>();
-            q.cnts = ctx->tcnts.as<uint32_t>();
+            q.tab = ctx->table.as<HSlot>();
             q.cap = C;
             q.cmin = cmin;
             q.cmax = cmax;
@@ -530,37 +555,315 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
             q.out_cap = ctx->out_cap;
             q.distinct = sc + 1;
             q.err = reinterpret_cast<uint32_t *>(sc + 2);
-            q.part_err = ctx->part_err.as<uint32_t>() + p;
-            uint32_t g = (uint32_t)std::min<uint64_t>((C + H_THREADS * HC_ITEMS - 1) / (H_THREADS * HC_ITEMS),
-                                                      (uint64_t)ctx->sms * 8);
+            q.part_err = ctx->part_err.as<uint32_t>();
             {
-                KScope ks(ctx, GKC_K_HASH_COLLECT, 24.0 * C);
+                uint32_t g = (uint32_t)std::min<uint64_t>((C + H_THREADS * HC_ITEMS - 1) / (H_THREADS * HC_ITEMS),
+                                                          (uint64_t)ctx->sms * 8);
+                KScope ks(ctx, GKC_K_HASH_COLLECT, 32.0 * C);
                 hash_collect_kernel<<<g, H_THREADS, 0, ctx->s>>>(q);
                 LAUNCHED();
             }
-            if (round == 0 && p == todo.front()) {
-                // time one partition's insert as the dominant-kernel sample
-                CK(cudaEventSynchronize(ctx->e3));
-                float ms = 0;
-                CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
-                acc_insert = ms;
+            uint32_t perr = 0;
+            CK(cudaMemcpyAsync(&perr, ctx->part_err.p, 4, cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaStreamSynchronize(ctx->s));
+            if (!(perr & ERR_TABLE_FULL)) break;
+            if (scale >= 256) return ctx->fail(GKC_EINTERNAL, "hash table retries exhausted");
+        }
+    }
+    return GKC_OK;
+}
+
+constexpr int BC_TS = 8192;  // shared-memory table slots per CTA (96 KB)
+
+// Counts the minimizer sub-buckets `ids` that overflowed shared memory: their
+// k-mers are re-split by k-mer hash into record sub-buckets of about 8k
+// instances, counted in shared memory; record sub-buckets that still
+// overflow go through the L2 table.
+int count_buckets_records(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const std::vector<uint64_t> &off,
+                          const std::vector<uint64_t> &bk_kmers, uint32_t cmin, uint32_t cmax) {
+    std::vector<RWork> work;
+    uint64_t NR = 0, inst = 0;
+    for (uint32_t b : ids) {
+        const uint64_t kb = bk_kmers[b];
+        // the sub-bucket already holds more distinct k-mers than one table:
+        // at least two record sub-buckets, about 8k instances each
+        uint32_t r_log = 1;
+        while (r_log < (uint32_t)RS_MAX_LOG && kb / (1ull << r_log) > 8192) r_log++;
+        for (uint64_t e = off[b]; e < off[b + 1]; e += RW_ENTRIES)
+            work.push_back({e, std::min<uint64_t>(e + RW_ENTRIES, off[b + 1]), (uint32_t)NR, r_log});
+        NR += 1ull << r_log;
+        inst += kb;
+    }
+    if (work.empty()) return GKC_OK;
+    CK(ctx->r_work.ensure(work.size() * sizeof(RWork)));
+    CK(ctx->r_count.ensure(NR * 4));
+    CK(ctx->r_off.ensure((NR + 1) * 8));
+    CK(ctx->r_cur.ensure(NR * 8));
+    CK(ctx->r_recs.ensure(std::max<uint64_t>(inst, 1) * sizeof(KRec)));
+    CK(ctx->r_failed.ensure((NR + 1) * 4));
+    CK(cudaMemcpyAsync(ctx->r_work.p, work.data(), work.size() * sizeof(RWork), cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemsetAsync(ctx->r_count.p, 0, NR * 4, ctx->s));
+    CK(cudaMemsetAsync(ctx->r_failed.p, 0, 4, ctx->s));
+    auto *sc = ctx->scal.as<unsigned long long>();
+    for (int pass = 0; pass < 2; pass++) {
+        if (pass == 1) {
+            RET(scan_u32(ctx, ctx->r_count.as<uint32_t>(), NR, ctx->r_off.as<uint64_t>(),
+                         ctx->r_off.as<unsigned long long>() + NR));
+            CK(cudaMemcpyAsync(ctx->r_cur.p, ctx->r_off.p, NR * 8, cudaMemcpyDeviceToDevice, ctx->s));
+        }
+        RSplitParams rp;
+        rp.entries = ctx->bk_entries.as<BEntry>();
+        rp.work = ctx->r_work.as<RWork>();
+        rp.k = ctx->opt.k;
+        rp.rcount = ctx->r_count.as<uint32_t>();
+        rp.rcursor = ctx->r_cur.as<unsigned long long>();
+        rp.recs = ctx->r_recs.as<KRec>();
+        rp.pass = pass;
+        KScope ks(ctx, GKC_K_SCAN, pass ? 16.0 * inst : 0.0);
+        rec_split_kernel<<<(unsigned)work.size(), RSP_THREADS, 0, ctx->s>>>(rp);
+        LAUNCHED();
+    }
+    RCountParams cp;
+    cp.recs = ctx->r_recs.as<KRec>();
+    cp.roff = ctx->r_off.as<uint64_t>();
+    cp.cmin = cmin;
+    cp.cmax = cmax;
+    cp.out_k = ctx->out_k.as<uint64_t>();
+    cp.out_c = ctx->out_c.as<uint32_t>();
+    cp.out_cursor = sc;
+    cp.out_cap = ctx->out_cap;
+    cp.distinct = sc + 1;
+    cp.failed = ctx->r_failed.as<uint32_t>();
+    cp.err = reinterpret_cast<uint32_t *>(sc + 2);
+    CK(cudaFuncSetAttribute(rec_count_kernel<BC_TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, BC_TS * 12));
+    {
+        KScope ks(ctx, GKC_K_HASH_COLLECT, 16.0 * inst);
+        rec_count_kernel<BC_TS><<<(unsigned)NR, BC_THREADS, BC_TS * 12, ctx->s>>>(cp);
+        LAUNCHED();
+    }
+    uint32_t nfail = 0;
+    CK(cudaMemcpyAsync(&nfail, ctx->r_failed.p, 4, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    if (!nfail) return GKC_OK;
+    std::vector<uint32_t> rids(nfail);
+    std::vector<uint64_t> roff(NR + 1);
+    CK(cudaMemcpyAsync(rids.data(), ctx->r_failed.as<uint32_t>() + 1, nfail * 4, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaMemcpyAsync(roff.data(), ctx->r_off.p, (NR + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    const double slots = ctx->opt.table_slots > 0 ? ctx->opt.table_slots : 0.35;
+    for (uint32_t r : rids) {
+        const uint64_t e0 = roff[r], e1 = roff[r + 1];
+        for (int scale = 1;; scale *= 4) {
+            uint64_t C = next_pow2(std::max<uint64_t>(4096, (uint64_t)((double)(e1 - e0) * 3.0 * slots) * scale));
+            RET(ensure_table(ctx, C));
+            CK(cudaMemsetAsync(ctx->part_err.p, 0, 4, ctx->s));
+            {
+                uint32_t g = (uint32_t)std::min<uint64_t>((e1 - e0 + H_THREADS - 1) / H_THREADS, (uint64_t)ctx->sms * 8);
+                KScope ks(ctx, GKC_K_HASH_INSERT, 16.0 * (e1 - e0));
+                hash_insert_records_kernel<<<std::max(g, 1u), H_THREADS, 0, ctx->s>>>(
+                    ctx->r_recs.as<KRec>() + e0, e1 - e0, ctx->table.as<HSlot>(), C - 1, ctx->part_err.as<uint32_t>());
+                LAUNCHED();
+            }
+            HCollectParams q;
+            q.tab = ctx->table.as<HSlot>();
+            q.cap = C;
+            q.cmin = cmin;
+            q.cmax = cmax;
+            q.out_k = ctx->out_k.as<uint64_t>();
+            q.out_c = ctx->out_c.as<uint32_t>();
+            q.out_cursor = sc;
+            q.out_cap = ctx->out_cap;
+            q.distinct = sc + 1;
+            q.err = reinterpret_cast<uint32_t *>(sc + 2);
+            q.part_err = ctx->part_err.as<uint32_t>();
+            {
+                uint32_t g = (uint32_t)std::min<uint64_t>((C + H_THREADS * HC_ITEMS - 1) / (H_THREADS * HC_ITEMS),
+                                                          (uint64_t)ctx->sms * 8);
+                KScope ks(ctx, GKC_K_HASH_COLLECT, 32.0 * C);
+                hash_collect_kernel<<<g, H_THREADS, 0, ctx->s>>>(q);
+                LAUNCHED();
+            }
+            uint32_t perr = 0;
+            CK(cudaMemcpyAsync(&perr, ctx->part_err.p, 4, cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaStreamSynchronize(ctx->s));
+            if (!(perr & ERR_TABLE_FULL)) break;
+            if (scale >= 256) return ctx->fail(GKC_EINTERNAL, "hash table retries exhausted");
+        }
+    }
+    return GKC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// phase 2, hash counter: shared-memory counting of minimizer sub-buckets, with
+// the L2 table for sub-buckets that overflow shared memory.  Device-resident
+// stores are counted in one group; a spilled store in groups of partitions
+// whose superkmers fit the device staging budget.
+
+int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    std::vector<uint64_t> np(P, 0), nbp(P, 0), nsp(P, 0);
+    bool spilled = false;
+    for (auto *c : ctx->store) {
+        spilled |= c->on_host;
+        for (uint32_t p = 0; p < P; p++) {
+            np[p] += c->kmers[p];
+            nbp[p] += c->byte_off[p + 1] - c->byte_off[p];
+            nsp[p] += c->skm_off[p + 1] - c->skm_off[p];
+        }
+    }
+    uint64_t N = 0, NS = 0;
+    for (uint32_t p = 0; p < P; p++) N += np[p], NS += nsp[p];
+    // sub-buckets per partition: about 16k k-mer instances each, so that a
+    // sub-bucket's distinct k-mers (a fraction of its instances) fit the table
+    const double mean = (double)N / P;
+    int s_log = 0;
+    while (!ctx->opt.hash_l2_only && s_log < BS_MAX_LOG && mean / (double)(1u << s_log) > 16384.0) s_log++;
+    const uint32_t S = 1u << s_log;
+    const uint64_t NB = (uint64_t)P * S;
+    ctx->times[4] = (double)NB;
+    ctx->times[5] = 0;
+    RET(ensure_out(ctx, N / std::max<uint32_t>(cmin, 1) + 1024));
+    CK(ctx->bk_skms.ensure(NB * 4));
+    CK(ctx->bk_kmers.ensure(NB * 8));
+    CK(ctx->bk_off.ensure((NB + 1) * 8));
+    CK(ctx->bk_cur.ensure(NB * 8));
+    CK(ctx->bk_failed.ensure((NB + 1) * 4));
+    CK(ctx->part_err.ensure(std::max<uint32_t>(P, 16) * 4));
+    CK(ctx->scal.ensure(64));
+    CK(ctx->h_scal.ensure(64));
+    CK(cudaMemsetAsync(ctx->scal.p, 0, 64, ctx->s));
+    auto *sc = ctx->scal.as<unsigned long long>();
+    CK(cudaMemcpyAsync(sc, &ctx->n_out, 8, cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaFuncSetAttribute(bucket_count_kernel<BC_TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            BC_TS * 12));
+    // groups of partitions
+    uint64_t budget = ~0ull;
+    if (spilled) {
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        budget = std::max<uint64_t>(1ull << 26, (uint64_t)(fr * 0.4));
+    }
+    float acc_ms = 0;
+    uint32_t p0 = 0;
+    while (p0 < P) {
+        uint32_t p1 = p0;
+        uint64_t gb = 0, gs = 0;  // staged bytes, superkmers of the group
+        while (p1 < P && (p1 == p0 || gb + nbp[p1] + 12 * nsp[p1] + 16 * nsp[p1] <= budget)) {
+            gb += nbp[p1] + 12 * nsp[p1];
+            gs += nsp[p1];
+            p1++;
+        }
+        if (!gs) {
+            p0 = p1;
+            continue;
+        }
+        uint64_t arena_used = 0;
+        if (spilled) CK(ctx->bk_arena.ensure(gb + 128 * ctx->store.size() + 64));
+        CK(ctx->bk_entries.ensure(gs * sizeof(BEntry)));
+        CK(cudaMemsetAsync(ctx->bk_skms.p, 0, NB * 4, ctx->s));
+        CK(cudaMemsetAsync(ctx->bk_kmers.p, 0, NB * 8, ctx->s));
+        std::vector<const uint8_t *> cb(ctx->store.size());
+        std::vector<const uint64_t *> ci(ctx->store.size());
+        std::vector<const uint32_t *> ck(ctx->store.size());
+        for (size_t j = 0; j < ctx->store.size(); j++)
+            RET(chunk_range(ctx, ctx->store[j], p0, p1, ctx->bk_arena, &arena_used, &cb[j], &ci[j], &ck[j]));
+        CK(cudaEventRecord(ctx->e2, ctx->s));
+        for (int pass = 0; pass < 2; pass++) {
+            if (pass == 1) {
+                RET(scan_u32(ctx, ctx->bk_skms.as<uint32_t>(), NB, ctx->bk_off.as<uint64_t>(),
+                             ctx->bk_off.as<unsigned long long>() + NB));
+                CK(cudaMemcpyAsync(ctx->bk_cur.p, ctx->bk_off.p, NB * 8, cudaMemcpyDeviceToDevice, ctx->s));
+            }
+            for (size_t j = 0; j < ctx->store.size(); j++) {
+                StoreChunk *c = ctx->store[j];
+                const uint64_t i0 = c->skm_off[p0], i1 = c->skm_off[p1];
+                if (i1 == i0) continue;
+                BSplitParams sp;
+                sp.idx = ci[j];
+                sp.keys = ck[j];
+                sp.bytes = cb[j];
+                sp.i_begin = i0;
+                sp.n_skm = i1;
+                sp.part_skm_off = c->d_skm_off.as<unsigned long long>();
+                sp.part_byte_off = c->d_byte_off.as<unsigned long long>();
+                sp.P = P;
+                sp.s_log = s_log;
+                sp.bucket_skms = ctx->bk_skms.as<uint32_t>();
+                sp.bucket_kmers = ctx->bk_kmers.as<unsigned long long>();
+                sp.bucket_cursor = ctx->bk_cur.as<unsigned long long>();
+                sp.entries = ctx->bk_entries.as<BEntry>();
+                sp.pass = pass;
+                uint32_t g = (uint32_t)((i1 - i0 + BS_PER_CTA - 1) / BS_PER_CTA);
+                KScope ks(ctx, GKC_K_SCAN, pass ? 28.0 * (i1 - i0) : 12.0 * (i1 - i0));
+                bucket_split_kernel<<<g, BS_THREADS, 0, ctx->s>>>(sp);
+                LAUNCHED();
             }
         }
-        std::vector<uint32_t> perr(P);
-        CK(cudaMemcpyAsync(perr.data(), ctx->part_err.p, P * 4, cudaMemcpyDeviceToHost, ctx->s));
-        CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemsetAsync(ctx->bk_failed.p, 0, 4, ctx->s));
+        BCountParams bp;
+        bp.entries = ctx->bk_entries.as<BEntry>();
+        bp.bucket_off = ctx->bk_off.as<uint64_t>();
+        bp.b0 = p0 * S;
+        bp.k = ctx->opt.k;
+        bp.cmin = cmin;
+        bp.cmax = cmax;
+        bp.out_k = ctx->out_k.as<uint64_t>();
+        bp.out_c = ctx->out_c.as<uint32_t>();
+        bp.out_cursor = sc;
+        bp.out_cap = ctx->out_cap;
+        bp.distinct = sc + 1;
+        bp.failed = ctx->bk_failed.as<uint32_t>();
+        bp.err = reinterpret_cast<uint32_t *>(sc + 2);
+        if (!ctx->opt.hash_l2_only) {
+            uint64_t gbytes = 0;
+            for (uint32_t p = p0; p < p1; p++) gbytes += nbp[p];
+            KScope ks(ctx, GKC_K_HASH_INSERT, (double)gbytes + 16.0 * gs);
+            bucket_count_kernel<BC_TS><<<(p1 - p0) * S, BC_THREADS, BC_TS * 12, ctx->s>>>(bp);
+            LAUNCHED();
+        }
+        CK(cudaEventRecord(ctx->e3, ctx->s));
+        uint32_t nfail = 0;
+        CK(cudaMemcpyAsync(&nfail, ctx->bk_failed.p, 4, cudaMemcpyDeviceToHost, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
-        std::vector<uint32_t> again;
-        for (uint32_t p : todo)
-            if (perr[p] & ERR_TABLE_FULL) { again.push_back(p); scale[p] *= 4; }
-        if (!again.empty()) CK(cudaMemsetAsync(ctx->part_err.p, 0, P * 4, ctx->s));
-        todo.swap(again);
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
+        acc_ms += ms;
+        std::vector<uint32_t> ids;
+        std::vector<uint64_t> off;
+        if (nfail || ctx->opt.hash_l2_only) {
+            off.resize(NB + 1);
+            CK(cudaMemcpyAsync(off.data(), ctx->bk_off.p, (NB + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
+            if (nfail) {
+                ids.resize(nfail);
+                CK(cudaMemcpyAsync(ids.data(), ctx->bk_failed.as<uint32_t>() + 1, nfail * 4,
+                                   cudaMemcpyDeviceToHost, ctx->s));
+            }
+            CK(cudaStreamSynchronize(ctx->s));
+        }
+        if (ctx->opt.hash_l2_only)  // every non-empty sub-bucket (one per partition)
+            for (uint32_t b = p0 * S; b < p1 * S; b++)
+                if (off[b + 1] > off[b]) ids.push_back(b);
+        if (!ids.empty()) {
+            if (ctx->opt.hash_l2_only) {
+                RET(count_buckets_l2(ctx, ids, off, cmin, cmax));
+            } else {
+                ctx->fallback_buckets += ids.size();
+                ctx->times[5] += (double)ids.size();
+                std::vector<uint64_t> km(NB);
+                CK(cudaMemcpyAsync(km.data(), ctx->bk_kmers.p, NB * 8, cudaMemcpyDeviceToHost, ctx->s));
+                CK(cudaStreamSynchronize(ctx->s));
+                RET(count_buckets_records(ctx, ids, off, km, cmin, cmax));
+            }
+        }
+        p0 = p1;
     }
+    CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
     auto *hs = ctx->h_scal.as<unsigned long long>();
     if ((uint32_t)hs[2] & ERR_OUTPUT_FULL) return ctx->fail(GKC_EINTERNAL, "output capacity exceeded");
     ctx->n_out = hs[0];
     ctx->n_distinct += hs[1];
-    ctx->times[3] = acc_insert;
+    ctx->times[3] = acc_ms;
     return GKC_OK;
 }
 
@@ -720,7 +1023,7 @@ int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
                 if (c->on_host) {  // stage the group's part of a spilled chunk
                     uint64_t b0 = c->byte_off[p0], b1 = c->byte_off[p1];
                     CK(cudaStreamSynchronize(ctx->s));
-                    CK(ctx->stage_bytes.ensure(b1 - b0 + 16));
+                    CK(ctx->stage_bytes.ensure(b1 - b0 + 32));
                     CK(ctx->stage_idx.ensure((i1 - i0) * 8 + 8));
                     CK(cudaMemcpyAsync(ctx->stage_bytes.p, c->bytes + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->s));
                     CK(cudaMemcpyAsync(ctx->stage_idx.p, c->idx + i0, (i1 - i0) * 8, cudaMemcpyHostToDevice, ctx->s));
@@ -782,10 +1085,11 @@ void gkc_default_options(gkc_options *o) {
     o->partitions = 512;
     o->counter = GKC_COUNTER_HASH;
     o->radix_bits = 8;
-    o->table_slots = 0.75;
+    o->table_slots = 0.35;
     o->batch_bases = 1ull << 30;
     o->spill_host = 0;
     o->group_keys = 0;
+    o->hash_l2_only = 0;
 }
 
 const char *gkc_strerror(int code) {
@@ -991,8 +1295,7 @@ int gkc_store_clear(gkc_ctx *ctx) {
     if (!ctx) return GKC_EINVAL;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->s);
-    for (auto *c : ctx->store) gkc_ctx::delete_chunk(c);
-    ctx->store.clear();
+    ctx->clear_store();  // buffers stay pooled for the next batch
     return GKC_OK;
 }
 
@@ -1069,7 +1372,7 @@ int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint
     ctx->n_distinct = 0;
     ctx->has_result = false;
     if (ctx->opt.counter == GKC_COUNTER_HASH) {
-        const double slots = ctx->opt.table_slots > 0 ? ctx->opt.table_slots : 0.75;
+        const double slots = ctx->opt.table_slots > 0 ? ctx->opt.table_slots : 0.35;
         const void *dk;
         RET(upload(ctx, ctx->keysA, keys, n * 8, mem, &dk));
         RET(ensure_out(ctx, n / std::max<uint32_t>(cmin, 1) + 1024));
@@ -1078,15 +1381,7 @@ int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint
         CK(ctx->h_scal.ensure(64));
         for (int scale = 1;; scale *= 4) {
             uint64_t C = next_pow2(std::max<uint64_t>(1024, (uint64_t)((double)n * slots) * scale));
-            if (C > ctx->tcap) {
-                ctx->tkeys.release();
-                ctx->tcnts.release();
-                CK(ctx->tkeys.ensure(C * 8));
-                CK(ctx->tcnts.ensure(C * 4));
-                CK(cudaMemsetAsync(ctx->tkeys.p, 0xFF, C * 8, ctx->s));
-                CK(cudaMemsetAsync(ctx->tcnts.p, 0, C * 4, ctx->s));
-                ctx->tcap = C;
-            }
+            RET(ensure_table(ctx, C));
             CK(cudaMemsetAsync(ctx->part_err.p, 0, 64, ctx->s));
             CK(cudaMemsetAsync(ctx->scal.p, 0, 64, ctx->s));
             auto *sc = ctx->scal.as<unsigned long long>();
@@ -1094,13 +1389,12 @@ int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint
                 uint32_t g = (uint32_t)std::min<uint64_t>((n + H_THREADS - 1) / H_THREADS, (uint64_t)ctx->sms * 8);
                 KScope ks(ctx, GKC_K_HASH_INSERT, 8.0 * n);
                 hash_insert_keys_kernel<<<g, H_THREADS, 0, ctx->s>>>(
-                    reinterpret_cast<const uint64_t *>(dk), n, ctx->tkeys.as<unsigned long long>(),
-                    ctx->tcnts.as<uint32_t>(), C - 1, ctx->part_err.as<uint32_t>());
+                    reinterpret_cast<const uint64_t *>(dk), n, ctx->table.as<HSlot>(), C - 1,
+                    ctx->part_err.as<uint32_t>());
                 LAUNCHED();
             }
             HCollectParams q;
-            q.keys = ctx->tkeys.as<unsigned long long>();
-            q.cnts = ctx->tcnts.as<uint32_t>();
+            q.tab = ctx->table.as<HSlot>();
             q.cap = C;
             q.cmin = cmin;
             q.cmax = cmax;
@@ -1179,7 +1473,7 @@ int gkc_kernel_stats(gkc_ctx *ctx, double *ms, uint64_t *launches, double *bytes
 
 int gkc_last_timings(gkc_ctx *ctx, double *t, int n) {
     if (!ctx || !t) return GKC_EINVAL;
-    for (int i = 0; i < n && i < 4; i++) t[i] = ctx->times[i];
+    for (int i = 0; i < n && i < 6; i++) t[i] = ctx->times[i];
     return GKC_OK;
 }
 

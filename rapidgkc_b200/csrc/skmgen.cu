@@ -4,16 +4,23 @@
 // GPU_ReadCompression / GPU_ExtractSKM chain (gpu_skmgen.cu:218-470) and the
 // host round trip per 2048-read batch (gpu_skmgen.cu:504-718).
 //
-// Kernel 1 (find_superkmers) walks the concatenated read bases in tiles.  A
-// CTA stages its tile's ASCII bytes in shared memory as 2-bit codes (16-byte
-// vector loads) together with a bitmap of read boundaries.  Each warp then
-// walks a strip of the tile 32 positions at a time: lane l evaluates the
-// canonical p-mer key at position c0+l; the minimum over the window of
-// w = k-p+1 p-mers is a sparse-table doubling over a 64-wide register window
-// (this chunk and the next) built from shuffles; superkmer starts and ends
-// are ballots over the chunk.  Closed superkmers are written as compact
-// records into a per-CTA region, and per-partition byte/superkmer/k-mer
-// counts accumulate in shared memory.
+// Kernel 0 (tile_reads) finds, for every tile of 2048 bases, the read that
+// holds the tile's first staged base (one binary search per tile, all tiles in
+// parallel).
+//
+// Kernel 1 (find_superkmers) walks the concatenated read bases tile by tile.
+// A CTA stages its tile's ASCII bytes in shared memory as 2-bit codes (16-byte
+// vector loads) and a bitmap of read boundaries, and writes the tile's codes
+// back to global memory packed 16 bases per word.  Each warp then walks a
+// strip of the tile 32 positions at a time: lane l evaluates the canonical
+// p-mer key at position c0+l; the minimum over the window of w = k-p+1 p-mers
+// is a sparse-table doubling over a 64-wide register window (this chunk and
+// the next) built from shuffles.  A superkmer starts at a valid k-mer that
+// begins a read or whose key differs from its predecessor's, and ends at the
+// next start or invalid position; both are ballots over the chunk, and the
+// lanes where a superkmer ends write its record (begin, k-mer count, key,
+// packing phase, trailing bases) into a per-CTA region and add it to
+// per-partition byte/superkmer/k-mer counts in shared memory.
 //
 // Kernel 2 (scatter_superkmers) reserves, per CTA and per partition, a
 // contiguous range of each partition's byte and index buffers, then writes
@@ -30,6 +37,7 @@ constexpr int P1_THREADS = P1_WARPS * 32;
 constexpr int P1_CHUNKS = 8;                          // chunks of 32 positions per warp strip
 constexpr int P1_STRIP = 32 * P1_CHUNKS;              // 256 positions
 constexpr int P1_TILE = P1_WARPS * P1_STRIP;          // 2048 positions per tile
+constexpr int P1_TILE_WORDS = P1_TILE / 16;           // packed code words per tile
 constexpr int P1_HALO = 512;                          // staged positions past the tile
 constexpr int P1_STAGE = P1_TILE + 32 + P1_HALO + 128;  // staged positions (from tile-32)
 constexpr int P1_CODE_WORDS = P1_STAGE / 16 + 2;      // 16 bases per word
@@ -42,21 +50,36 @@ struct P1Params {
     uint64_t total;            // offs[n_reads]
     int k, p;
     uint32_t P;
+    uint64_t pmod;             // fastmod multiplier of P
     const uint32_t *lut;       // 4^p ranks, or null for the default order
     int vec_ok;                // reads pointer is 16-byte aligned
+    const int64_t *tile_read;  // [ntiles] read holding the tile's first staged base
+    uint32_t *codes;           // [ntiles * P1_TILE_WORDS] packed 2-bit codes (out)
     SkmRecord *records;        // gridDim.x regions of `region_cap` records
     uint32_t region_cap;
     uint32_t *region_count;    // [gridDim.x]
     unsigned long long *part_bytes, *part_skms, *part_kmers;  // [P]
-    int smem_hist;             // per-CTA histograms in shared memory (P <= 4096)
     uint32_t *err;
 };
+
+// x % d for 32-bit x from the precomputed m = 2^64 / d + 1 (Lemire, Kaser and
+// Kurz, "Faster remainder by direct computation", 2019).
+__device__ __host__ __forceinline__ uint64_t fastmod_m(uint32_t d) { return ~0ull / d + 1; }
+__device__ __forceinline__ uint32_t fastmod(uint32_t x, uint64_t m, uint32_t d) {
+    return (uint32_t)__umul64hi(m * x, d);
+}
 
 // Packs four 2-bit codes held one per byte (byte 0 first) into 8 bits with the
 // first base in bits 7-6.
 __device__ __forceinline__ uint32_t pack4(uint32_t c) {
     uint32_t r = __byte_perm(c, 0, 0x0123);
     return (r | (r >> 6) | (r >> 12) | (r >> 18)) & 0xFFu;
+}
+
+// Reverse complement of 16 packed codes (first base in the top bits).
+__device__ __forceinline__ uint32_t rc16(uint32_t w) {
+    uint32_t r = __brev(~w);
+    return ((r >> 1) & 0x55555555u) | ((r & 0x55555555u) << 1);
 }
 
 // Index of the read containing position q (largest r with offs[r] <= q).
@@ -67,6 +90,14 @@ __device__ int64_t read_of(const uint64_t *offs, int64_t n_reads, uint64_t q) {
         if (offs[mid] <= q) lo = mid; else hi = mid;
     }
     return lo;
+}
+
+__global__ void tile_reads_kernel(const uint64_t *offs, int64_t n_reads, uint64_t ntiles, int64_t *out) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < ntiles;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        int64_t q = (int64_t)(t * P1_TILE) - 32;
+        out[t] = read_of(offs, n_reads, q < 0 ? 0 : (uint64_t)q);
+    }
 }
 
 __device__ __forceinline__ uint32_t pmer_key(uint32_t v, int p, uint32_t pmask, const uint32_t *lut) {
@@ -98,29 +129,25 @@ __device__ __forceinline__ uint32_t tail_of(uint32_t b3) {
     return (b3 & 1) ? 0u : (b3 & 2) ? 1u : (b3 & 4) ? 2u : 3u;
 }
 
+constexpr int P1_RC_BASES = 16 * P1_CODE_WORDS;
+
 struct P1Smem {
-    uint32_t codes[P1_CODE_WORDS];
+    uint32_t codes[P1_CODE_WORDS];   // staged 2-bit codes, position j at word j/16
+    uint32_t rcodes[P1_CODE_WORDS + 1];  // complement codes in reverse: position j at
+                                         // P1_RC_BASES-1-j (+1 word read past by the funnel)
     uint32_t bm[P1_BM_WORDS];
     uint32_t region_n;
     uint64_t rs0;  // start of the read containing the first staged position
 };
 
-__device__ __forceinline__ void emit_record(const P1Params &a, P1Smem &sm, uint32_t *h_bytes,
-                                            uint32_t *h_skms, uint32_t *h_kmers, uint32_t slot,
-                                            uint64_t pos, uint32_t len, uint32_t key,
-                                            uint32_t phase, uint32_t tail) {
-    uint32_t part = (~key) % a.P;
+__device__ __forceinline__ void emit_record(const P1Params &a, uint32_t *h, uint32_t slot, uint64_t pos,
+                                            uint32_t len, uint32_t key, uint32_t phase, uint32_t tail) {
+    uint32_t part = fastmod(~key, a.pmod, a.P);
     uint32_t nb = skm_nbytes(phase, len, a.k);
     if (len > IDX_MAX_LEN) atomicOr(a.err, ERR_SKM_TOO_LONG);
-    if (a.smem_hist) {
-        atomicAdd(h_bytes + part, nb);
-        atomicAdd(h_skms + part, 1u);
-        atomicAdd(h_kmers + part, len);
-    } else {
-        atomicAdd(a.part_bytes + part, (unsigned long long)nb);
-        atomicAdd(a.part_skms + part, 1ull);
-        atomicAdd(a.part_kmers + part, (unsigned long long)len);
-    }
+    atomicAdd(h + part, nb);
+    atomicAdd(h + a.P + part, 1u);
+    atomicAdd(h + 2 * a.P + part, len);
     if (slot < a.region_cap) {
         SkmRecord r;
         r.pos = rec_pack_pos(pos, phase, tail);
@@ -132,20 +159,19 @@ __device__ __forceinline__ void emit_record(const P1Params &a, P1Smem &sm, uint3
     }
 }
 
+// LOG = log2 of the largest power of two <= w (the doubling levels).
+template <int LOG>
 __global__ void __launch_bounds__(P1_THREADS)
 find_superkmers_kernel(P1Params a) {
-    extern __shared__ uint32_t dyn[];
+    extern __shared__ uint32_t hist[];  // [3P]: bytes, superkmers, k-mers per partition
     __shared__ P1Smem sm;
-    uint32_t *h_bytes = dyn, *h_skms = dyn + a.P, *h_kmers = dyn + 2 * a.P;
+    constexpr int L2 = 1 << LOG;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int k = a.k, p = a.p, w = k - p + 1;
     const uint32_t pmask = 0xFFFFFFFFu >> (32 - 2 * p);
-    int L2 = 1;
-    while (L2 * 2 <= w) L2 *= 2;  // largest power of two <= w
-    const unsigned lt_mask = (1u << lane) - 1, le_mask = lt_mask | (1u << lane);
+    const unsigned lt_mask = (1u << lane) - 1;
 
-    if (a.smem_hist)
-        for (uint32_t i = threadIdx.x; i < 3 * a.P; i += blockDim.x) dyn[i] = 0;
+    for (uint32_t i = threadIdx.x; i < 3 * a.P; i += blockDim.x) hist[i] = 0;
     if (threadIdx.x == 0) sm.region_n = 0;
 
     const uint64_t ntiles = (a.total + P1_TILE - 1) / P1_TILE;
@@ -153,7 +179,8 @@ find_superkmers_kernel(P1Params a) {
         __syncthreads();
         const int64_t t0 = (int64_t)(tile * P1_TILE);
         const int64_t sbeg = t0 - 32;  // first staged position (multiple of 16)
-        // ---- stage 2-bit codes ----
+        const int64_t r0 = a.tile_read[tile];
+        // ---- stage 2-bit codes, forward and reverse complement ----
         for (int i = threadIdx.x; i < P1_CODE_WORDS; i += blockDim.x) {
             int64_t q = sbeg + 16 * (int64_t)i;
             uint32_t word = 0;
@@ -169,60 +196,59 @@ find_superkmers_kernel(P1Params a) {
                 }
             }
             sm.codes[i] = word;
+            sm.rcodes[P1_CODE_WORDS - 1 - i] = rc16(word);
+            if (i >= 2 && i < 2 + P1_TILE_WORDS) a.codes[tile * P1_TILE_WORDS + (i - 2)] = word;
         }
         for (int i = threadIdx.x; i < P1_BM_WORDS; i += blockDim.x) sm.bm[i] = 0;
+        if (threadIdx.x == 0) sm.rs0 = a.offs[r0];
         __syncthreads();
         // ---- read-boundary bitmap: bit j <=> some offs[r] == sbeg + j ----
         {
-            __shared__ int64_t r0s;
-            if (threadIdx.x == 0) {
-                uint64_t q0 = sbeg < 0 ? 0 : (uint64_t)sbeg;
-                int64_t r0 = read_of(a.offs, a.n_reads, q0);
-                r0s = r0;
-                sm.rs0 = a.offs[r0];
-            }
-            __syncthreads();
             const int64_t send = sbeg + P1_STAGE;
-            for (int64_t r = r0s + threadIdx.x; r <= a.n_reads; r += blockDim.x) {
+            for (int64_t r = r0 + threadIdx.x; r <= a.n_reads; r += blockDim.x) {
                 int64_t o = (int64_t)a.offs[r];
                 if (o >= send) break;
                 if (o >= sbeg) atomicOr(&sm.bm[(o - sbeg) >> 5], 1u << ((o - sbeg) & 31));
             }
-            __syncthreads();
         }
+        __syncthreads();
         // ---- each warp walks its strip ----
         const int64_t strip0 = t0 + (int64_t)warp * P1_STRIP;
         if (strip0 >= (int64_t)a.total) continue;
-        const int64_t strip1 = strip0 + P1_STRIP;
+        // staged-relative limits
+        const int jstrip0 = (int)(strip0 - sbeg), jstrip1 = jstrip0 + P1_STRIP;
+        const int jmin = sbeg < 0 ? (int)(-sbeg) : 0;                     // first position >= 0
+        const int64_t jk64 = (int64_t)a.total - k - sbeg;                 // last valid k-mer start
+        const int jmaxk = jk64 > (int64_t)P1_STAGE ? P1_STAGE : (int)jk64;
+        const int64_t jt64 = (int64_t)a.total - sbeg;
+        const int jtotal = jt64 > (int64_t)P1_STAGE ? P1_STAGE : (int)jt64;
+        // last chunk start whose next chunk's p-mers and boundary bits are staged
+        const int jlimit = P1_STAGE - (128 + k);
+        const int shp = 32 - 2 * p;
 
-        auto pk_at = [&](int64_t q) -> uint32_t {  // canonical p-mer key at staged position q
-            int64_t j = q - sbeg;
-            int i = (int)(j >> 4), o = (int)(j & 15);
-            uint64_t v = ((uint64_t)sm.codes[i] << 32) | sm.codes[i + 1];
-            uint32_t f = (uint32_t)(v >> (64 - 2 * (o + p))) & pmask;
-            uint32_t r = rc32(f, p);
+        auto pk_at = [&](int j) -> uint32_t {  // canonical p-mer key at staged position j
+            int i = j >> 4, o = j & 15;
+            uint32_t f = __funnelshift_l(sm.codes[i + 1], sm.codes[i], 2 * o) >> shp;
+            int rj = P1_RC_BASES - j - p;  // reverse-complement p-mer start in rcodes
+            int ri = rj >> 4, ro = rj & 15;
+            uint32_t r = __funnelshift_l(sm.rcodes[ri + 1], sm.rcodes[ri], 2 * ro) >> shp;
             uint32_t kf = pmer_key(f, p, pmask, a.lut), kr = pmer_key(r, p, pmask, a.lut);
             return kf < kr ? kf : kr;
         };
-        auto bits_at = [&](int64_t q, int n) -> uint32_t {  // n (<=31) boundary bits from q
-            int64_t j = q - sbeg;
-            int i = (int)(j >> 5), o = (int)(j & 31);
-            uint64_t v = (uint64_t)sm.bm[i] | ((uint64_t)sm.bm[i + 1] << 32);
-            return (uint32_t)(v >> o) & ((n >= 32) ? 0xFFFFFFFFu : ((1u << n) - 1));
+        auto bits_at = [&](int j) -> uint32_t {  // 32 boundary bits from staged position j
+            return __funnelshift_r(sm.bm[j >> 5], sm.bm[(j >> 5) + 1], j & 31);
         };
+        const uint32_t vmask = (1u << (k - 1)) - 1;  // k <= 32
         // read start of the warm-up chunk's first position: the last boundary
         // bit at or before it, else the start of the read containing sbeg.
         int64_t rs;
         {
-            int64_t q0 = strip0 - 32;
-            int64_t j = q0 - sbeg;  // >= 0
-            int wi = (int)(j >> 5);
-            uint32_t own = sm.bm[wi] & (((j & 31) == 31) ? 0xFFFFFFFFu : ((2u << (j & 31)) - 1));
+            const int j = jstrip0 - 32;  // multiple of 32
             int64_t found = -1;
-            if (own) found = sbeg + ((int64_t)wi << 5) + (31 - __clz(own));
-            for (int base = wi - 1; found < 0 && base >= 0; base -= 32) {
+            for (int base = (j >> 5); found < 0 && base >= 0; base -= 32) {
                 int idx = base - lane;
                 uint32_t v = idx >= 0 ? sm.bm[idx] : 0u;
+                if (idx == (j >> 5)) v &= 1u;  // only position j itself in its own word
                 unsigned bal = __ballot_sync(FULL, v != 0);
                 if (bal) {
                     int src = __ffs(bal) - 1;  // lowest lane = highest word index
@@ -234,21 +260,20 @@ find_superkmers_kernel(P1Params a) {
         }
 
         // pipeline: A = p-mer keys of chunk c, B = of chunk c+1
-        int64_t c0 = strip0 - 32;
-        uint32_t A = pk_at(c0 + lane), B = pk_at(c0 + 32 + lane);
+        int cj = jstrip0 - 32;
+        uint32_t A = pk_at(cj + lane), B = pk_at(cj + 32 + lane);
         uint32_t carried_key = 0xFFFFFFFFu;
-        bool open = false;         // a superkmer of this warp whose end is not found yet
+        bool open = false;  // a superkmer of this warp whose end is not found yet
         int64_t o_pos = 0;
         uint32_t o_key = 0, o_phase = 0;
-        // last chunk start whose next chunk's p-mers and boundary bits are staged
-        const int64_t stage_limit = sbeg + P1_STAGE - (128 + k);
         for (;;) {
-            const bool warm = c0 < strip0;
-            const bool cont = c0 >= strip1;
+            const bool warm = cj < jstrip0;
+            const bool cont = cj >= jstrip1;
             if (cont && !open) break;
-            if (c0 > stage_limit || c0 >= (int64_t)a.total) break;
-            // ---- window minimum over w p-mers for the k-mer at c0+lane ----
+            if (cj > jlimit || cj >= jtotal) break;
+            // ---- window minimum over w p-mers for the k-mer at cj+lane ----
             uint32_t ma = A, mb = B;
+#pragma unroll
             for (int x = 1; x < L2; x <<= 1) {
                 uint32_t t = __shfl_sync(FULL, lane >= x ? ma : mb, (lane + x) & 31);
                 uint32_t tb = __shfl_down_sync(FULL, mb, x);
@@ -261,95 +286,91 @@ find_superkmers_kernel(P1Params a) {
                 uint32_t t = __shfl_sync(FULL, lane >= d ? ma : mb, (lane + d) & 31);
                 key = min(ma, t);
             }
-            const int64_t q = c0 + lane;
+            const int j = cj + lane;
             uint32_t prevkey = __shfl_up_sync(FULL, key, 1);
             if (lane == 0) prevkey = carried_key;
-            const bool valid = q >= 0 && (uint64_t)(q + k) <= a.total && bits_at(q + 1, k - 1) == 0;
-            const bool isrs = q >= 0 && bits_at(q, 1) != 0;
+            const uint32_t bits = bits_at(j);
+            const bool valid = j >= jmin && j <= jmaxk && ((bits >> 1) & vmask) == 0;
+            const bool isrs = j >= jmin && (bits & 1u);
             const bool start = valid && (isrs || key != prevkey);
             const unsigned RSB = __ballot_sync(FULL, isrs);
             const unsigned E = __ballot_sync(FULL, start || !valid);
             const unsigned S = __ballot_sync(FULL, start);
-            // read start of this lane's position
-            const unsigned rsle = RSB & le_mask;
-            const int64_t my_rs = rsle ? (c0 + 31 - __clz(rsle)) : rs;
 
             if (!warm) {
-                // close the carried superkmer at the first end/start of this chunk
-                uint32_t emit_carried = 0;
-                int64_t c_end = 0;
-                if (open && E) { emit_carried = 1; c_end = c0 + __ffs(E) - 1; }
-                // superkmers starting in this chunk (owned strip only)
-                bool my_start = start && !cont;
-                unsigned above = E & ~le_mask;
-                bool my_close = my_start && above != 0;
-                unsigned CL = __ballot_sync(FULL, my_close);
-                uint32_t n = __popc(CL) + emit_carried;
-                uint32_t base = 0;
-                if (n) {
-                    if (lane == 0) base = atomicAdd(&sm.region_n, n);
+                // a superkmer ends at each E lane whose nearest E bit below is
+                // an owned start, or (none below) at the first E lane if one
+                // is open from an earlier chunk
+                const unsigned below = E & lt_mask;
+                const int src = below ? 31 - __clz(below) : 0;
+                const uint32_t skey = __shfl_sync(FULL, key, src);
+                const bool isE = (E >> lane) & 1u;
+                const bool emit = isE && (below ? (((S >> src) & 1u) && !cont) : open);
+                const unsigned EM = __ballot_sync(FULL, emit);
+                if (EM) {
+                    uint32_t base = 0;
+                    if (lane == 0) base = atomicAdd(&sm.region_n, (uint32_t)__popc(EM));
                     base = __shfl_sync(FULL, base, 0);
+                    if (emit) {
+                        const int64_t e = sbeg + j;  // exclusive end (k-mer index)
+                        int64_t b = o_pos;
+                        uint32_t phase = o_phase, skey2 = o_key;
+                        if (below) {
+                            // read start at or before src: last boundary bit in
+                            // the chunk up to src, else the carried one
+                            const unsigned rsb = RSB & ((2u << src) - 1);
+                            const int64_t rss = rsb ? sbeg + cj + 31 - __clz(rsb) : rs;
+                            b = sbeg + cj + src;
+                            phase = (uint32_t)(b - rss) % 3u;
+                            skey2 = skey;
+                        }
+                        const uint32_t tail = tail_of(bits_at(j + k - 1) & 7u);
+                        emit_record(a, hist, base + __popc(EM & lt_mask), (uint64_t)b, (uint32_t)(e - b), skey2,
+                                    phase, tail);
+                    }
                 }
-                if (emit_carried && lane == 0) {
-                    int64_t x = c_end + k - 2;  // last base
-                    uint32_t tail = tail_of(bits_at(x + 1, 3));
-                    emit_record(a, sm, h_bytes, h_skms, h_kmers, base, (uint64_t)o_pos,
-                                (uint32_t)(c_end - o_pos), o_key, o_phase, tail);
+                // the last start with no end in this chunk stays open
+                if (E) {
+                    const int last = 31 - __clz(E);
+                    open = ((S >> last) & 1u) && !cont;
+                    if (open) {
+                        const unsigned rsb = RSB & ((2u << last) - 1);
+                        const int64_t rsl = rsb ? sbeg + cj + 31 - __clz(rsb) : rs;
+                        o_pos = sbeg + cj + last;
+                        o_key = __shfl_sync(FULL, key, last);
+                        o_phase = (uint32_t)(o_pos - rsl) % 3u;
+                    }
                 }
-                if (my_close) {
-                    int64_t e = c0 + __ffs(above) - 1;
-                    int64_t x = e + k - 2;
-                    uint32_t tail = tail_of(bits_at(x + 1, 3));
-                    uint32_t phase = (uint32_t)((q - my_rs) % 3);
-                    emit_record(a, sm, h_bytes, h_skms, h_kmers,
-                                base + emit_carried + __popc(CL & lt_mask), (uint64_t)q,
-                                (uint32_t)(e - q), key, phase, tail);
-                }
-                if (emit_carried) open = false;
-                // a start with no end in this chunk becomes the open superkmer
-                unsigned OPEN = __ballot_sync(FULL, my_start && above == 0);
-                if (OPEN) {
-                    int src = 31 - __clz(OPEN);
-                    open = true;
-                    o_pos = c0 + src;
-                    o_key = __shfl_sync(FULL, key, src);
-                    uint32_t ph = (uint32_t)((q - my_rs) % 3);
-                    o_phase = __shfl_sync(FULL, ph, src);
-                }
-                (void)S;
             }
             carried_key = __shfl_sync(FULL, key, 31);
-            if (RSB) rs = c0 + 31 - __clz(RSB);
+            if (RSB) rs = sbeg + cj + 31 - __clz(RSB);
             // advance
-            c0 += 32;
+            cj += 32;
             A = B;
-            B = (c0 + 32 + 31 - sbeg < (int64_t)P1_STAGE - 16) ? pk_at(c0 + 32 + lane) : 0xFFFFFFFFu;
+            B = (cj + 63 < P1_STAGE - 16) ? pk_at(cj + 32 + lane) : 0xFFFFFFFFu;
         }
         // superkmer running past the staged range: finish it from global memory
         if (open) {
-            uint32_t slot = 0;
             if (lane == 0) {
+                const int64_t c0 = sbeg + cj;
                 int64_t r = read_of(a.offs, a.n_reads, (uint64_t)o_pos);
                 int64_t re = (int64_t)a.offs[r + 1];
                 int64_t e = c0 > o_pos + 1 ? c0 : o_pos + 1;
                 while (e + k <= re && kmer_key_global(a, (uint64_t)e) == o_key) e++;
                 int64_t after = re - (e + k - 1);
                 uint32_t tail = after >= 3 ? 3 : (uint32_t)after;
-                slot = atomicAdd(&sm.region_n, 1u);
-                emit_record(a, sm, h_bytes, h_skms, h_kmers, slot, (uint64_t)o_pos,
-                            (uint32_t)(e - o_pos), o_key, o_phase, tail);
+                uint32_t slot = atomicAdd(&sm.region_n, 1u);
+                emit_record(a, hist, slot, (uint64_t)o_pos, (uint32_t)(e - o_pos), o_key, o_phase, tail);
             }
             __syncwarp();
         }
     }
     __syncthreads();
-    if (a.smem_hist) {
-        for (uint32_t i = threadIdx.x; i < a.P; i += blockDim.x) {
-            if (h_skms[i]) {
-                atomicAdd(a.part_bytes + i, (unsigned long long)h_bytes[i]);
-                atomicAdd(a.part_skms + i, (unsigned long long)h_skms[i]);
-                atomicAdd(a.part_kmers + i, (unsigned long long)h_kmers[i]);
-            }
+    for (uint32_t i = threadIdx.x; i < a.P; i += blockDim.x) {
+        if (hist[a.P + i]) {
+            atomicAdd(a.part_bytes + i, (unsigned long long)hist[i]);
+            atomicAdd(a.part_skms + i, (unsigned long long)hist[a.P + i]);
+            atomicAdd(a.part_kmers + i, (unsigned long long)hist[2 * a.P + i]);
         }
     }
     if (threadIdx.x == 0) a.region_count[blockIdx.x] = sm.region_n;
@@ -358,68 +379,97 @@ find_superkmers_kernel(P1Params a) {
 // ---------------------------------------------------------------------------
 // Kernel 2: scatter records into per-partition byte and index buffers.
 struct P2Params {
-    const uint8_t *reads;
+    const uint32_t *codes;     // packed 2-bit codes of the batch (16 per word)
     const SkmRecord *records;
     uint32_t region_cap;
     const uint32_t *region_count;
     int k;
     uint32_t P;
+    uint64_t pmod;
     const unsigned long long *part_byte_off;  // [P] partition start in `bytes`
     const unsigned long long *part_skm_off;   // [P] partition start in `idx`
     unsigned long long *cur_bytes, *cur_skms;  // [P] zeroed cursors
     uint8_t *bytes;
     uint64_t *idx;
+    uint32_t *keys;  // minimizer key of each superkmer, indexed like idx
 };
 
 constexpr int P2_THREADS = 512;
 
-__device__ __forceinline__ uint8_t skm_byte(const uint8_t *reads, uint64_t s, uint64_t limit, uint32_t b,
-                                            uint32_t nb, uint32_t first_h, uint32_t last_h) {
-    uint64_t q = s + 3ull * b;
-    uint32_t v = 0;
-#pragma unroll
-    for (int t = 0; t < 3; t++) {
-        uint32_t c = (q + t < limit) ? code1(reads[q + t]) : 0u;
-        v |= c << (4 - 2 * t);
-    }
-    uint32_t h = (b == nb - 1) ? last_h : (b == 0 ? first_h : 3u);
-    return (uint8_t)(v | (h << 6));
-}
-
 __global__ void __launch_bounds__(P2_THREADS)
 scatter_superkmers_kernel(P2Params a) {
-    extern __shared__ unsigned long long cur[];  // [2P]: byte and superkmer cursors
+    extern __shared__ unsigned long long sbase[];  // [2P] CTA bases in each partition
+    uint32_t *lcnt = reinterpret_cast<uint32_t *>(sbase + 2 * a.P);  // [2P] CTA-local cursors
     const uint32_t n = a.region_count[blockIdx.x] < a.region_cap ? a.region_count[blockIdx.x] : a.region_cap;
     const SkmRecord *rec = a.records + (uint64_t)blockIdx.x * a.region_cap;
-    for (uint32_t i = threadIdx.x; i < 2 * a.P; i += blockDim.x) cur[i] = 0;
+    for (uint32_t i = threadIdx.x; i < 2 * a.P; i += blockDim.x) lcnt[i] = 0;
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         SkmRecord r = rec[i];
-        uint32_t part = (~r.key) % a.P;
-        atomicAdd(&cur[part], (unsigned long long)skm_nbytes(rec_phase(r.pos), r.len, a.k));
-        atomicAdd(&cur[a.P + part], 1ull);
+        uint32_t part = fastmod(~r.key, a.pmod, a.P);
+        atomicAdd(&lcnt[part], skm_nbytes(rec_phase(r.pos), r.len, a.k));
+        atomicAdd(&lcnt[a.P + part], 1u);
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < a.P; i += blockDim.x) {
-        unsigned long long nbp = cur[i], nsp = cur[a.P + i];
-        cur[i] = nbp ? atomicAdd(a.cur_bytes + i, nbp) : 0ull;
-        cur[a.P + i] = nsp ? atomicAdd(a.cur_skms + i, nsp) : 0ull;
+        uint32_t nbp = lcnt[i], nsp = lcnt[a.P + i];
+        sbase[i] = a.part_byte_off[i] + (nbp ? atomicAdd(a.cur_bytes + i, (unsigned long long)nbp) : 0ull);
+        sbase[a.P + i] = a.part_skm_off[i] + (nsp ? atomicAdd(a.cur_skms + i, (unsigned long long)nsp) : 0ull);
+        lcnt[i] = 0;
+        lcnt[a.P + i] = 0;
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         SkmRecord r = rec[i];
-        uint32_t part = (~r.key) % a.P;
+        uint32_t part = fastmod(~r.key, a.pmod, a.P);
         uint32_t phase = rec_phase(r.pos), tail = rec_tail(r.pos);
         uint64_t g = rec_base(r.pos);
         uint32_t nb = skm_nbytes(phase, r.len, a.k);
-        unsigned long long ob = atomicAdd(&cur[part], (unsigned long long)nb);
-        unsigned long long os = atomicAdd(&cur[a.P + part], 1ull);
-        uint8_t *dst = a.bytes + a.part_byte_off[part] + ob;
-        uint64_t s = g - phase;                                 // first slot of the first byte
-        uint64_t limit = g + r.len + (uint64_t)a.k - 1 + tail;  // end of read bases used
-        uint32_t first_h = 3 - phase, last_h = (phase + r.len + (uint32_t)a.k - 1) % 3;
-        for (uint32_t b = 0; b < nb; b++) dst[b] = skm_byte(a.reads, s, limit, b, nb, first_h, last_h);
-        a.idx[a.part_skm_off[part] + os] = idx_pack(ob, r.len);
+        uint32_t ob = atomicAdd(&lcnt[part], nb);
+        uint32_t os = atomicAdd(&lcnt[a.P + part], 1u);
+        uint64_t pbase = sbase[part] - a.part_byte_off[part];  // this CTA's range in the partition
+        uint8_t *dst = a.bytes + sbase[part] + ob;
+        uint64_t pos = g - phase;                               // first slot of the first byte
+        const uint64_t limit = g + r.len + (uint64_t)a.k - 1 + tail;  // end of read bases used
+        const uint32_t first_h = 3 - phase, last_h = (phase + r.len + (uint32_t)a.k - 1) % 3;
+        // a 64-bit window of codes starting at base `pos`, refilled every ~10 bytes
+        uint64_t win = 0;
+        int avail = 0;
+        uint32_t acc = 0;
+        uint32_t b = 0;
+        while (b < nb) {
+            const uintptr_t addr = (uintptr_t)(dst + b);
+            const uint32_t lo = (uint32_t)(addr & 3);
+            const uint32_t cnt = min(4u - lo, nb - b);
+            acc = 0;
+            for (uint32_t t = 0; t < cnt; t++) {
+                if (avail < 3) {
+                    const uint64_t wi = pos >> 4;
+                    const uint32_t o = (uint32_t)(pos & 15);
+                    win = (((uint64_t)__ldg(a.codes + wi) << 32) | __ldg(a.codes + wi + 1)) << (2 * o);
+                    avail = 32 - (int)o;
+                }
+                uint32_t v = (uint32_t)(win >> 58);
+                win <<= 6;
+                avail -= 3;
+                if (pos + 3 > limit) {
+                    uint32_t keep = limit > pos ? (uint32_t)(limit - pos) : 0u;  // 0..2 bases
+                    v &= ~((1u << (6 - 2 * keep)) - 1);
+                }
+                pos += 3;
+                const uint32_t bb = b + t;
+                const uint32_t h = (bb == nb - 1) ? last_h : (bb == 0 ? first_h : 3u);
+                acc |= (v | (h << 6)) << (8 * (lo + t));
+            }
+            if (cnt == 4) {
+                *reinterpret_cast<uint32_t *>(addr) = acc;
+            } else {
+                for (uint32_t t = 0; t < cnt; t++) dst[b + t] = (uint8_t)(acc >> (8 * (lo + t)));
+            }
+            b += cnt;
+        }
+        a.idx[sbase[a.P + part] + os] = idx_pack(pbase + ob, r.len);
+        a.keys[sbase[a.P + part] + os] = r.key;
     }
 }
 

@@ -176,7 +176,8 @@ def test_retries_spill_and_groups(oracle):
     reads, offs = random_reads(12, 60_000, 5000, 150, 0.01)
     ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P, 2, U32)
     ko, co = sorted_table(ko, co)
-    for kw, kind in [(dict(table_slots=0.02), "hash"), (dict(spill_host=True), "hash"),
+    for kw, kind in [(dict(table_slots=0.02, hash_l2_only=True), "hash"), (dict(hash_l2_only=True), "hash"),
+                     (dict(spill_host=True), "hash"), (dict(spill_host=True, hash_l2_only=True), "hash"),
                      (dict(spill_host=True, group_keys=50_000), "sort"), (dict(group_keys=1), "sort"),
                      (dict(radix_bits=5), "sort")]:
         with counter(k, p, P, kind, **kw) as c:
@@ -184,3 +185,17 @@ def test_retries_spill_and_groups(oracle):
             n, d = c.count(2, U32)
             km, ct = sorted_table(*c.result())
         assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co), kw
+
+
+def test_shared_memory_overflow_falls_back(oracle):
+    """Partitions with far more distinct k-mers than a CTA's shared-memory
+    table are counted through the L2 table with the same result."""
+    k, p, P = 31, 11, 2
+    reads, offs = random_reads(13, 200_000, 3000, 150, 0.02)
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P)
+    ko, co = sorted_table(ko, co)
+    with counter(k, p, P, "hash") as c:
+        n, d = c.count_reads(reads, offs)
+        km, ct = sorted_table(*c.result())
+    assert d == do and d > 100_000
+    assert np.array_equal(km, ko) and np.array_equal(ct, co)
