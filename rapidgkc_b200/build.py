@@ -39,7 +39,7 @@ def _csrc(*names):
 
 def build_cuda(ptxas: bool = False, force: bool = False) -> str:
     out = os.path.join(PKG, "librapidgkc_b200.so")
-    srcs = _csrc("engine.cu", "skmgen.cu", "count_hash.cu", "count_sort.cu", "gkc_device.cuh")
+    srcs = [os.path.join(CSRC, n) for n in sorted(os.listdir(CSRC)) if n.endswith((".cu", ".cuh"))]
     srcs += [os.path.join(ROOT, "include", "gkc_capi.h")]
     if force or ptxas or _stale(out, srcs):
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",

@@ -6,16 +6,17 @@
 // own.  Sub-buckets are sized (S chosen from the partition sizes) so that their
 // distinct k-mers fit an open-addressing table in one CTA's shared memory:
 //   split    over all superkmers of all store chunks: a histogram of
-//            superkmers per sub-bucket (shared-memory aggregated), a scan,
-//            then a scatter of 16-byte entries {first byte address, k-mer
-//            count} into sub-bucket order;
-//   count    one CTA per sub-bucket decodes its superkmers warp-synchronously
-//            (two streams per lane, equal consecutive k-mers merged) into a
-//            shared-memory table with shared-memory atomics, then writes the
-//            k-mers whose count lies in [cmin, cmax] with one global atomic
-//            per CTA.  A sub-bucket whose distinct k-mers outgrow the table is
-//            abandoned and listed; the host counts those through the L2 hash
-//            table (count_hash.cu), so the result does not depend on skew.
+//            superkmers and k-mers per sub-bucket (shared-memory aggregated),
+//            a scan, then a scatter of 16-byte entries {first byte address,
+//            k-mer count} into sub-bucket order;
+//   count    one CTA per sub-bucket: warps decode their superkmers 32 k-mers
+//            at a time (warp_kmers below), merge equal neighbouring k-mers into
+//            runs, and add the runs to a shared-memory table with
+//            shared-memory atomics; then the k-mers whose count lies in
+//            [cmin, cmax] are written with one global atomic per CTA.  A
+//            sub-bucket whose distinct k-mers outgrow the table is abandoned
+//            and listed; the host re-splits those by k-mer hash
+//            (count_records.cu), so the result does not depend on skew.
 #include "count_hash.cu"
 
 namespace gkc {
@@ -31,6 +32,115 @@ __device__ __forceinline__ uint32_t bucket_of(uint32_t key, int s_log) {
     return s_log ? (uint32_t)(hash64(key) >> (64 - s_log)) : 0u;
 }
 
+// ---------------------------------------------------------------------------
+// Warp-cooperative superkmer decoding.
+//
+// Superkmer bytes hold three 2-bit bases in their low six bits, first base
+// highest; a superkmer's first byte holds 3 - (its header) bases of padding
+// before its first base.  The j-th k-mer of a superkmer therefore starts at
+// base slot u = pad + j, i.e. byte u/3, slot u%3, and spans at most 12 bytes.
+
+// Six-bit fields of eight bytes (byte 0 first) packed into 48 bits, byte 0's
+// bases highest.
+__device__ __forceinline__ uint64_t pack6x8(uint64_t le) {
+    uint64_t x = ((uint64_t)__byte_perm((uint32_t)le, 0, 0x0123) << 32) | __byte_perm((uint32_t)(le >> 32), 0, 0x0123);
+    x &= 0x3F3F3F3F3F3F3F3Full;
+    x = ((x >> 2) & 0x0FC00FC00FC00FC0ull) | (x & 0x003F003F003F003Full);
+    x = ((x >> 4) & 0x00FFF00000FFF000ull) | (x & 0x00000FFF00000FFFull);
+    x = ((x >> 8) & 0x0000FFFFFF000000ull) | (x & 0x0000000000FFFFFFull);
+    return x;
+}
+
+__device__ __forceinline__ uint32_t pack6x4(uint32_t le) {
+    uint32_t y = __byte_perm(le, 0, 0x0123) & 0x3F3F3F3Fu;
+    y = ((y >> 2) & 0x0FC00FC0u) | (y & 0x003F003Fu);
+    y = ((y >> 4) & 0x00FFF000u) | (y & 0x00000FFFu);
+    return y;
+}
+
+// The k-mer whose first base is slot u of the superkmer at p (k <= 32).
+// Reads the aligned 8-byte words covering bytes u/3 .. u/3+11 (store buffers
+// carry 32 bytes of padding).
+__device__ __forceinline__ uint64_t kmer_at(const uint8_t *p, uint32_t u, int k, uint64_t mask) {
+    const uint32_t bi = u / 3, s = u - 3 * bi;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p) + bi;
+    const uint64_t *w = reinterpret_cast<const uint64_t *>(a & ~(uintptr_t)7);
+    const uint32_t sh = 8 * (uint32_t)(a & 7);
+    const uint64_t w0 = w[0], w1 = w[1], w2 = w[2];
+    const uint64_t lo = sh ? (w0 >> sh) | (w1 << (64 - sh)) : w0;  // bytes 0..7
+    const uint64_t hi = sh ? (w1 >> sh) | (w2 << (64 - sh)) : w1;  // bytes 8..15
+    // 36 bases: 24 from the first eight bytes, 12 from the next four
+    const unsigned __int128 v = ((unsigned __int128)pack6x8(lo) << 24) | pack6x4((uint32_t)hi);
+    return (uint64_t)(v >> (72 - 2 * (s + (uint32_t)k))) & mask;
+}
+
+// For the entries ent[b .. b+32) of a warp (b + lane < end), calls
+// f(key, valid) on every lane once per 32 k-mers, in superkmer order:
+// lane l gets the (32*i + l)-th k-mer of the batch.  Must be called by the
+// whole warp.
+template <bool CANONICAL, class F>
+__device__ __forceinline__ void warp_kmers(const BEntry *ent, uint64_t b, uint64_t end, int k, uint64_t mask,
+                                           F &&f) {
+    const int lane = threadIdx.x & 31;
+    const bool has = b + lane < end;
+    BEntry en;
+    en.ptr = nullptr;
+    en.len = 0;
+    if (has) en = ent[b + lane];
+    const uint32_t pad = has ? 3u - (en.ptr[0] >> 6) : 0u;
+    uint32_t incl = en.len;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t y = __shfl_up_sync(FULL, incl, d);
+        if (lane >= d) incl += y;
+    }
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
+    const uint32_t excl = incl - en.len;
+    const uint64_t pv = reinterpret_cast<uint64_t>(en.ptr);
+    for (uint32_t c0 = 0; c0 < total; c0 += 32) {
+        const uint32_t g = c0 + lane;
+        const bool valid = g < total;
+        // owner: the last lane whose first k-mer index is <= g
+        int own = 0;
+#pragma unroll
+        for (int st = 16; st; st >>= 1) {
+            const int cand = own + st;
+            const uint32_t v = __shfl_sync(FULL, excl, cand & 31);
+            if (cand < 32 && v <= g) own = cand;
+        }
+        const uint32_t pos = g - __shfl_sync(FULL, excl, own);
+        const uint64_t po = __shfl_sync(FULL, pv, own);
+        const uint32_t u = __shfl_sync(FULL, pad, own) + pos;
+        uint64_t key = EMPTY_KEY;
+        if (valid) {
+            const uint64_t x = kmer_at(reinterpret_cast<const uint8_t *>(po), u, k, mask);
+            if (CANONICAL) {
+                const uint64_t r = rc64(x, k);
+                key = x < r ? x : r;
+            } else {
+                key = x;
+            }
+        }
+        f(key, valid);
+    }
+}
+
+// Runs of equal neighbouring keys among the lanes of one warp_kmers step:
+// returns true on the first lane of each run, with *run its length.  Must be
+// called by the whole warp.
+__device__ __forceinline__ bool warp_run_head(uint64_t key, bool valid, uint32_t *run) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t prev = __shfl_up_sync(FULL, key, 1);
+    const bool head = valid && (lane == 0 || key != prev);
+    const unsigned H = __ballot_sync(FULL, head), V = __ballot_sync(FULL, valid);
+    const unsigned above = H & ~((2u << lane) - 1);
+    const int next = above ? __ffs(above) - 1 : 32 - __clz(V);
+    *run = (uint32_t)(next - lane);
+    return head;
+}
+
+// ---------------------------------------------------------------------------
+// split
 constexpr int BS_THREADS = 256;
 constexpr int BS_PER_CTA = 2048;   // superkmers per split CTA
 constexpr int BS_MAX_PARTS = 4;    // partitions a split CTA aggregates in shared memory
@@ -61,16 +171,17 @@ __device__ __forceinline__ uint32_t part_of_index(const unsigned long long *off,
     return lo;
 }
 
-// Pass 0 counts superkmers per sub-bucket; pass 1 scatters entries.  A CTA
-// covers BS_PER_CTA consecutive superkmers, which span few partitions: the
-// sub-buckets of its first BS_MAX_PARTS partitions are aggregated in shared
-// memory (one global atomic per sub-bucket per CTA), any further partition
-// goes straight to global atomics.
+// Pass 0 counts superkmers and k-mers per sub-bucket; pass 1 scatters
+// entries.  A CTA covers BS_PER_CTA consecutive superkmers, which span few
+// partitions: the sub-buckets of its first BS_MAX_PARTS partitions are
+// aggregated in shared memory (one global atomic per sub-bucket per CTA), any
+// further partition goes straight to global atomics.
 __global__ void __launch_bounds__(BS_THREADS)
 bucket_split_kernel(BSplitParams a) {
     constexpr int NB = BS_MAX_PARTS << BS_MAX_LOG;
+    constexpr uint32_t BMASK = (1u << BS_MAX_LOG) - 1;
     __shared__ uint32_t cnt[NB];
-    __shared__ unsigned long long base[NB];
+    __shared__ unsigned long long base[NB];  // pass 0: k-mers; pass 1: reserved block
     __shared__ uint32_t p_first_s;
     const uint32_t S = 1u << a.s_log;  // s_log <= BS_MAX_LOG
     const uint64_t i0 = a.i_begin + blockIdx.x * (uint64_t)BS_PER_CTA;
@@ -83,8 +194,6 @@ bucket_split_kernel(BSplitParams a) {
     auto part = [&](uint64_t i) {
         return (i < a.part_skm_off[pf + 1]) ? pf : part_of_index(a.part_skm_off, a.P, i);
     };
-    // count this CTA's superkmers (and, pass 0, k-mers) per shared sub-bucket
-    // (global atomics for the rest); pass 0 sums k-mers in `base`
     for (uint64_t i = i0 + threadIdx.x; i < i1; i += BS_THREADS) {
         uint32_t p = part(i);
         uint32_t b = bucket_of(a.keys[i], a.s_log);
@@ -100,15 +209,16 @@ bucket_split_kernel(BSplitParams a) {
     if (a.pass == 0) {
         for (int t = threadIdx.x; t < NB; t += BS_THREADS)
             if (cnt[t]) {
-                atomicAdd(a.bucket_skms + (pf + (t >> BS_MAX_LOG)) * S + (t & ((1 << BS_MAX_LOG) - 1)), cnt[t]);
-                atomicAdd(a.bucket_kmers + (pf + (t >> BS_MAX_LOG)) * S + (t & ((1 << BS_MAX_LOG) - 1)), base[t]);
+                const uint64_t g = (uint64_t)(pf + (t >> BS_MAX_LOG)) * S + (t & BMASK);
+                atomicAdd(a.bucket_skms + g, cnt[t]);
+                atomicAdd(a.bucket_kmers + g, base[t]);
             }
         return;
     }
     // pass 1: reserve each shared sub-bucket's block, then write entries
     for (int t = threadIdx.x; t < NB; t += BS_THREADS) {
-        base[t] = cnt[t] ? atomicAdd(a.bucket_cursor + (pf + (t >> BS_MAX_LOG)) * S + (t & ((1 << BS_MAX_LOG) - 1)), (unsigned long long)cnt[t])
-                         : 0ull;
+        const uint64_t g = (uint64_t)(pf + (t >> BS_MAX_LOG)) * S + (t & BMASK);
+        base[t] = cnt[t] ? atomicAdd(a.bucket_cursor + g, (unsigned long long)cnt[t]) : 0ull;
         cnt[t] = 0;
     }
     __syncthreads();
@@ -131,68 +241,8 @@ bucket_split_kernel(BSplitParams a) {
     }
 }
 
-// Decoder state over one entry stream.  The first k-mer needs at most the
-// superkmer's first 12 bytes (k <= 32): they are fetched with three aligned
-// 8-byte loads issued together (store buffers carry 32 bytes of padding) and
-// assembled in registers.
-__device__ __forceinline__ void entry_begin(SkmCursor &c, const BEntry &en, int k, uint64_t mask) {
-    c.s = en.ptr;
-    c.left = en.len - 1;
-    const uintptr_t a = reinterpret_cast<uintptr_t>(en.ptr);
-    const uint64_t *w = reinterpret_cast<const uint64_t *>(a & ~(uintptr_t)7);
-    const uint32_t sh = 8 * (uint32_t)(a & 7);
-    const uint64_t w0 = w[0], w1 = w[1], w2 = w[2];
-    const uint64_t lo = sh ? (w0 >> sh) | (w1 << (64 - sh)) : w0;  // bytes 0..7
-    const uint64_t hi = sh ? (w1 >> sh) | (w2 << (64 - sh)) : w1;  // bytes 8..15
-    auto byte = [&](uint32_t i) -> uint32_t { return (uint32_t)((i < 8 ? lo >> (8 * i) : hi >> (8 * (i - 8))) & 0xFF); };
-    const uint32_t b0 = (uint32_t)(lo & 0xFF);
-    const uint32_t h = b0 >> 6;
-    uint64_t f = b0 & ((1u << (2 * h)) - 1);
-    const uint32_t need = (uint32_t)k - h;
-    const uint32_t full = need / 3, part = need % 3;
-    for (uint32_t t = 1; t <= full; t++) f = (f << 6) | (byte(t) & 63u);
-    const uint32_t nxt = byte(full + 1);
-    if (part) f = (f << (2 * part)) | ((nxt & 63u) >> (6 - 2 * part));
-    c.fwd = f & mask;
-    c.rc = rc64(c.fwd, k);
-    c.bi = full + 1;
-    c.slot = part;
-    c.cur = nxt;
-}
-
-struct EStream {
-    SkmCursor c;
-    uint64_t next, step;
-    uint64_t last;
-    uint32_t run;
-    __device__ __forceinline__ bool advance(const BEntry *ent, uint64_t end, int k, uint64_t mask, bool &flush,
-                                            uint64_t &fk, uint32_t &fc) {
-        flush = false;
-        bool have = false;
-        if (c.left) {
-            skm_step(c, k, mask);
-            have = true;
-        } else if (next < end) {
-            entry_begin(c, ent[next], k, mask);
-            next += step;
-            have = true;
-        }
-        if (have) {
-            uint64_t key = c.fwd < c.rc ? c.fwd : c.rc;
-            if (key == last) {
-                run++;
-            } else {
-                flush = run != 0;
-                fk = last;
-                fc = run;
-                last = key;
-                run = 1;
-            }
-        }
-        return have;
-    }
-};
-
+// ---------------------------------------------------------------------------
+// shared-memory counting
 constexpr int BC_THREADS = 512;
 
 struct BCountParams {
@@ -210,16 +260,16 @@ struct BCountParams {
     uint32_t *err;
 };
 
-// Shared-memory table insert.  A probe sequence longer than SM_MAX_PROBE
-// (the table is nearly full) raises *over instead of inserting; the caller
-// then abandons the table.  No shared fill counter: one would serialise
-// every new key of the CTA on a single shared-memory word.
+// Shared-memory table insert (multiplicative hash on the top bits).  A probe
+// sequence longer than SM_MAX_PROBE (the table is nearly full) raises *over
+// instead of inserting; the caller then abandons the table.
 constexpr uint32_t SM_MAX_PROBE = 128;
 
 template <int TS>
 __device__ __forceinline__ void smem_add(unsigned long long *tk, uint32_t *tc, volatile uint32_t *over,
                                          uint64_t key, uint32_t c) {
-    uint32_t h = (uint32_t)hash64(key) & (TS - 1);
+    constexpr int LOG = __builtin_ctz(TS);
+    uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (64 - LOG));
     for (uint32_t pr = 0; pr < SM_MAX_PROBE; pr++) {
         unsigned long long cur = tk[h];
         if (cur == key) {
@@ -238,10 +288,52 @@ __device__ __forceinline__ void smem_add(unsigned long long *tk, uint32_t *tc, v
     *over = 1;
 }
 
+// Writes the table's k-mers with count in [cmin, cmax] (one global atomic per
+// CTA), adds its distinct keys to *distinct.  Called by the whole CTA.
+template <int TS, int NT>
+__device__ __forceinline__ void smem_collect(const unsigned long long *tk, const uint32_t *tc, uint32_t cmin,
+                                             uint32_t cmax, uint64_t *out_k, uint32_t *out_c,
+                                             unsigned long long *out_cursor, uint64_t out_cap,
+                                             unsigned long long *distinct, uint32_t *err, uint32_t *ws,
+                                             unsigned long long *base_s) {
+    constexpr int PER = TS / NT;
+    uint32_t keep = 0, occ = 0;
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        int s = threadIdx.x * PER + t;
+        if (tk[s] != EMPTY_KEY) {
+            occ++;
+            keep += (tc[s] >= cmin && tc[s] <= cmax);
+        }
+    }
+    uint32_t tot, occ_tot;
+    uint32_t pre = block_exclusive_scan<NT>(keep, &tot, ws);
+    block_exclusive_scan<NT>(occ, &occ_tot, ws);
+    if (threadIdx.x == 0) {
+        *base_s = tot ? atomicAdd(out_cursor, (unsigned long long)tot) : 0ull;
+        if (occ_tot) atomicAdd(distinct, (unsigned long long)occ_tot);
+    }
+    __syncthreads();
+    uint64_t o = *base_s + pre;
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        int s = threadIdx.x * PER + t;
+        if (tk[s] != EMPTY_KEY && tc[s] >= cmin && tc[s] <= cmax) {
+            if (o < out_cap) {
+                out_k[o] = tk[s];
+                out_c[o] = tc[s];
+            } else {
+                atomicOr(err, ERR_OUTPUT_FULL);
+            }
+            o++;
+        }
+    }
+}
+
 template <int TS>
 __global__ void __launch_bounds__(BC_THREADS)
 bucket_count_kernel(BCountParams a) {
-    extern __shared__ unsigned long long tk[];  // [TS] keys
+    extern __shared__ unsigned long long tk[];             // [TS] keys
     uint32_t *tc = reinterpret_cast<uint32_t *>(tk + TS);  // [TS] counts
     __shared__ uint32_t ws[BC_THREADS / 32];
     __shared__ volatile uint32_t over;
@@ -255,30 +347,14 @@ bucket_count_kernel(BCountParams a) {
     }
     if (threadIdx.x == 0) over = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5;
     const uint64_t mask = kmask(a.k);
-    constexpr int NWARP = BC_THREADS / 32;
-    EStream s0, s1;
-    s0.c.left = s1.c.left = 0;
-    s0.next = e0 + (uint64_t)warp * 64 + lane;
-    s1.next = s0.next + 32;
-    s0.step = s1.step = (uint64_t)NWARP * 64;
-    s0.last = s1.last = EMPTY_KEY;
-    s0.run = s1.run = 0;
-    for (;;) {
-        bool f0, f1;
-        uint64_t k0 = 0, k1 = 0;
-        uint32_t c0 = 0, c1 = 0;
-        bool h0 = s0.advance(a.entries, e1, a.k, mask, f0, k0, c0);
-        bool h1 = s1.advance(a.entries, e1, a.k, mask, f1, k1, c1);
-        // a warp vote, so every lane of the warp leaves the loop together
-        if (!__any_sync(FULL, (h0 || h1) && over == 0)) break;
-        if (f0) smem_add<TS>(tk, tc, &over, k0, c0);
-        if (f1) smem_add<TS>(tk, tc, &over, k1, c1);
-    }
-    if (!over) {
-        if (s0.run) smem_add<TS>(tk, tc, &over, s0.last, s0.run);
-        if (s1.run) smem_add<TS>(tk, tc, &over, s1.last, s1.run);
+    for (uint64_t bb = e0 + (uint64_t)warp * 32; bb < e1; bb += BC_THREADS) {
+        if (__any_sync(FULL, over != 0)) break;  // a warp vote: the warp leaves together
+        warp_kmers<true>(a.entries, bb, e1, a.k, mask, [&](uint64_t key, bool valid) {
+            uint32_t run;
+            if (warp_run_head(key, valid, &run)) smem_add<TS>(tk, tc, &over, key, run);
+        });
     }
     __syncthreads();
     if (over) {
@@ -288,71 +364,22 @@ bucket_count_kernel(BCountParams a) {
         }
         return;
     }
-    // collect: each thread owns TS/BC_THREADS consecutive slots
-    constexpr int PER = TS / BC_THREADS;
-    uint32_t keep = 0, occ = 0;
-#pragma unroll
-    for (int t = 0; t < PER; t++) {
-        int s = threadIdx.x * PER + t;
-        if (tk[s] != EMPTY_KEY) {
-            occ++;
-            keep += (tc[s] >= a.cmin && tc[s] <= a.cmax);
-        }
-    }
-    uint32_t tot, occ_tot;
-    uint32_t pre = block_exclusive_scan<BC_THREADS>(keep, &tot, ws);
-    block_exclusive_scan<BC_THREADS>(occ, &occ_tot, ws);
-    if (threadIdx.x == 0) {
-        base_s = tot ? atomicAdd(a.out_cursor, (unsigned long long)tot) : 0ull;
-        atomicAdd(a.distinct, (unsigned long long)occ_tot);
-    }
-    __syncthreads();
-    uint64_t o = base_s + pre;
-#pragma unroll
-    for (int t = 0; t < PER; t++) {
-        int s = threadIdx.x * PER + t;
-        if (tk[s] != EMPTY_KEY && tc[s] >= a.cmin && tc[s] <= a.cmax) {
-            if (o < a.out_cap) {
-                a.out_k[o] = tk[s];
-                a.out_c[o] = tc[s];
-            } else {
-                atomicOr(a.err, ERR_OUTPUT_FULL);
-            }
-            o++;
-        }
-    }
+    smem_collect<TS, BC_THREADS>(tk, tc, a.cmin, a.cmax, a.out_k, a.out_c, a.out_cursor, a.out_cap, a.distinct,
+                                 a.err, ws, &base_s);
 }
 
-// L2-table insert of one sub-bucket's entries (the fallback of abandoned
-// sub-buckets).
+// L2-table insert of one sub-bucket's entries (hash_l2_only mode).
 __global__ void __launch_bounds__(H_THREADS)
 hash_insert_entries_kernel(const BEntry *ent, uint64_t n, int k, HSlot *tab, uint64_t tmask, uint32_t *err) {
-    const int lane = threadIdx.x & 31;
     const uint64_t nw = (uint64_t)gridDim.x * (H_THREADS / 32);
     const uint64_t gw = blockIdx.x * (uint64_t)(H_THREADS / 32) + (threadIdx.x >> 5);
     const uint64_t mask = kmask(k);
-    EStream s0, s1;
-    s0.c.left = s1.c.left = 0;
-    s0.next = gw * 64 + lane;
-    s1.next = s0.next + 32;
-    s0.step = s1.step = nw * 64;
-    s0.last = s1.last = EMPTY_KEY;
-    s0.run = s1.run = 0;
-    for (;;) {
-        bool f0, f1;
-        uint64_t k0 = 0, k1 = 0;
-        uint32_t c0 = 0, c1 = 0;
-        bool h0 = s0.advance(ent, n, k, mask, f0, k0, c0);
-        bool h1 = s1.advance(ent, n, k, mask, f1, k1, c1);
-        if (!__any_sync(FULL, h0 || h1)) break;
-        const uint64_t p0 = hash64(k0) & tmask, p1 = hash64(k1) & tmask;
-        const unsigned long long v0 = f0 ? __ldcg(&tab[p0].key) : 0ull;
-        const unsigned long long v1 = f1 ? __ldcg(&tab[p1].key) : 0ull;
-        if (f0) table_add_from(tab, tmask, k0, c0, p0, v0, err);
-        if (f1) table_add_from(tab, tmask, k1, c1, p1, v1, err);
+    for (uint64_t bb = gw * 32; bb < n; bb += nw * 32) {
+        warp_kmers<true>(ent, bb, n, k, mask, [&](uint64_t key, bool valid) {
+            uint32_t run;
+            if (warp_run_head(key, valid, &run)) table_add(tab, tmask, key, run, err);
+        });
     }
-    if (s0.run) table_add(tab, tmask, s0.last, s0.run, err);
-    if (s1.run) table_add(tab, tmask, s1.last, s1.run, err);
 }
 
 }  // namespace gkc

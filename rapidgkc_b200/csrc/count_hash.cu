@@ -48,48 +48,6 @@ __device__ __forceinline__ void table_add(HSlot *tab, uint64_t mask, uint64_t ke
     atomicOr(err, ERR_TABLE_FULL);
 }
 
-// Decoder state of one lane: the current superkmer and its rolling k-mer.
-struct SkmCursor {
-    const uint8_t *s;
-    uint32_t left;   // k-mers still to yield after the current one
-    uint32_t bi;     // byte index of the next base
-    uint32_t slot;   // slot (0..2) of the next base in byte bi
-    uint32_t cur;    // byte bi
-    uint64_t fwd, rc;
-};
-
-__device__ __forceinline__ void skm_step(SkmCursor &c, int k, uint64_t mask) {
-    uint32_t b = (c.cur >> (4 - 2 * c.slot)) & 3u;
-    c.fwd = ((c.fwd << 2) | b) & mask;
-    c.rc = (c.rc >> 2) | ((uint64_t)(3u - b) << (2 * k - 2));
-    if (++c.slot == 3) {
-        c.slot = 0;
-        c.cur = c.s[++c.bi];
-    }
-    c.left--;
-}
-
-// table_add whose first probe load (`cur` at slot h) was issued by the caller.
-__device__ __forceinline__ void table_add_from(HSlot *tab, uint64_t mask, uint64_t key, uint32_t c, uint64_t h,
-                                               unsigned long long cur, uint32_t *err) {
-    for (uint32_t pr = 0; pr < H_MAX_PROBE; pr++) {
-        if (pr) cur = __ldcg(&tab[h].key);
-        if (cur == key) {
-            atomicAdd(&tab[h].cnt, c);
-            return;
-        }
-        if (cur == EMPTY_KEY) {
-            unsigned long long old = atomicCAS(&tab[h].key, (unsigned long long)EMPTY_KEY, (unsigned long long)key);
-            if (old == EMPTY_KEY || old == key) {
-                atomicAdd(&tab[h].cnt, c);
-                return;
-            }
-        }
-        h = (h + 1) & mask;
-    }
-    atomicOr(err, ERR_TABLE_FULL);
-}
-
 // Raw 64-bit keys (no canonical step): the reference hash counter's own
 // known-answer test counts plain integers (gpu_hash_counter.cu:693-708).
 __global__ void __launch_bounds__(H_THREADS)

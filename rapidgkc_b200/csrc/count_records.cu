@@ -49,35 +49,24 @@ struct RSplitParams {
 };
 
 __device__ __forceinline__ uint32_t rec_bucket(uint64_t key, uint32_t r_log) {
-    // a different mix from the table slot hash, so records of one record
-    // sub-bucket still spread over its table
-    uint64_t z = key * 0x9E3779B97F4A7C15ull;
-    z ^= z >> 29;
-    return r_log ? (uint32_t)(z >> (64 - r_log)) : 0u;
+    // The table slot of smem_add is the top bits of key * 0x9E37..; the
+    // record sub-bucket must not depend on those bits, or the records of one
+    // record sub-bucket would share a fraction of the table.  splitmix64's
+    // top bits are independent of them.
+    return r_log ? (uint32_t)(hash64(key) >> (64 - r_log)) : 0u;
 }
 
-// Calls f(key, run) for the run-merged k-mers of entries [e0, e1), one
-// entry per thread at a time.
+// Calls f(key, run) for the run-merged k-mers of entries [e0, e1); warps take
+// 32 entries at a time.  Deterministic for a given block size, so both split
+// passes see the same records.
 template <class F>
 __device__ __forceinline__ void for_each_run(const BEntry *ent, uint64_t e0, uint64_t e1, int k, F &&f) {
     const uint64_t mask = kmask(k);
-    for (uint64_t i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
-        SkmCursor c;
-        entry_begin(c, ent[i], k, mask);
-        uint64_t last = c.fwd < c.rc ? c.fwd : c.rc;
-        uint32_t run = 1;
-        while (c.left) {
-            skm_step(c, k, mask);
-            uint64_t key = c.fwd < c.rc ? c.fwd : c.rc;
-            if (key == last) {
-                run++;
-            } else {
-                f(last, run);
-                last = key;
-                run = 1;
-            }
-        }
-        f(last, run);
+    for (uint64_t bb = e0 + (threadIdx.x & ~31u); bb < e1; bb += blockDim.x) {
+        warp_kmers<true>(ent, bb, e1, k, mask, [&](uint64_t key, bool valid) {
+            uint32_t run;
+            if (warp_run_head(key, valid, &run)) f(key, run);
+        });
     }
 }
 
@@ -168,38 +157,8 @@ rec_count_kernel(RCountParams a) {
         }
         return;
     }
-    constexpr int PER = TS / BC_THREADS;
-    uint32_t keep = 0, occ = 0;
-#pragma unroll
-    for (int t = 0; t < PER; t++) {
-        int s = threadIdx.x * PER + t;
-        if (tk[s] != EMPTY_KEY) {
-            occ++;
-            keep += (tc[s] >= a.cmin && tc[s] <= a.cmax);
-        }
-    }
-    uint32_t tot, occ_tot;
-    uint32_t pre = block_exclusive_scan<BC_THREADS>(keep, &tot, ws);
-    block_exclusive_scan<BC_THREADS>(occ, &occ_tot, ws);
-    if (threadIdx.x == 0) {
-        base_s = tot ? atomicAdd(a.out_cursor, (unsigned long long)tot) : 0ull;
-        atomicAdd(a.distinct, (unsigned long long)occ_tot);
-    }
-    __syncthreads();
-    uint64_t o = base_s + pre;
-#pragma unroll
-    for (int t = 0; t < PER; t++) {
-        int s = threadIdx.x * PER + t;
-        if (tk[s] != EMPTY_KEY && tc[s] >= a.cmin && tc[s] <= a.cmax) {
-            if (o < a.out_cap) {
-                a.out_k[o] = tk[s];
-                a.out_c[o] = tc[s];
-            } else {
-                atomicOr(a.err, ERR_OUTPUT_FULL);
-            }
-            o++;
-        }
-    }
+    smem_collect<TS, BC_THREADS>(tk, tc, a.cmin, a.cmax, a.out_k, a.out_c, a.out_cursor, a.out_cap, a.distinct,
+                                 a.err, ws, &base_s);
 }
 
 // L2-table insert of records (record sub-buckets that overflow shared memory).

@@ -34,7 +34,9 @@ struct DevBuf {
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
-        size_t want = std::max<size_t>(bytes, 256);
+        // 1/8 headroom: sizes that vary a little between calls (the overflow
+        // set of the shared-memory counter) do not reallocate every call
+        size_t want = std::max<size_t>(bytes + bytes / 8, 256);
         cudaError_t e = cudaMalloc(&p, want);
         if (e == cudaSuccess) cap = want; else p = nullptr;
         return e;
@@ -55,8 +57,9 @@ struct PinBuf {
         if (p) cudaFreeHost(p);
         p = nullptr;
         cap = 0;
-        cudaError_t e = cudaHostAlloc(&p, std::max<size_t>(bytes, 256), cudaHostAllocDefault);
-        if (e == cudaSuccess) cap = std::max<size_t>(bytes, 256); else p = nullptr;
+        const size_t want = std::max<size_t>(bytes + bytes / 8, 256);
+        cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+        if (e == cudaSuccess) cap = want; else p = nullptr;
         return e;
     }
     void release() {
