@@ -120,8 +120,9 @@ int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint
 /* Statistics of the last gkc_add_reads (phase 1) and gkc_count (phase 2)
  * calls (n <= 6 entries): times[0..3] = device milliseconds (CUDA events) of
  * phase 1, its superkmer search, phase 2, and phase 2's counting kernels;
- * times[4] = sub-buckets of the hash counter, times[5] = those that
- * overflowed shared memory and were re-split by k-mer hash. */
+ * times[4] = sub-buckets of the hash counter, times[5] = those re-split by
+ * k-mer hash (their distinct k-mers overflowed shared memory, or they held
+ * more than 65536 k-mer instances). */
 int gkc_last_timings(gkc_ctx *ctx, double *times, int n);
 
 /* Number of kernels this context launched since creation. */

@@ -1,10 +1,12 @@
 // count_bucket.cu -- phase 2, shared-memory hash counter over sub-buckets.
 //
-// Every partition of the store is split into S sub-buckets by a hash of the
-// superkmers' minimizer keys.  A canonical k-mer has one minimizer, so all its
-// occurrences land in one sub-bucket, and a sub-bucket can be counted on its
-// own.  Sub-buckets are sized (S chosen from the partition sizes) so that their
-// distinct k-mers fit an open-addressing table in one CTA's shared memory:
+// Every partition p of the store is split into 2^s_p sub-buckets by a hash of
+// the superkmers' minimizer keys.  A canonical k-mer has one minimizer, so all
+// its occurrences land in one sub-bucket, and a sub-bucket can be counted on
+// its own.  s_p is chosen from partition p's k-mer count (about 16k instances
+// per sub-bucket), so that a sub-bucket's distinct k-mers fit an
+// open-addressing table in one CTA's shared memory however skewed the
+// partitions are:
 //   split    over all superkmers of all store chunks: a histogram of
 //            superkmers and k-mers per sub-bucket (shared-memory aggregated),
 //            a scan, then a scatter of 16-byte entries {first byte address,
@@ -16,7 +18,11 @@
 //            [cmin, cmax] are written with one global atomic per CTA.  A
 //            sub-bucket whose distinct k-mers outgrow the table is abandoned
 //            and listed; the host re-splits those by k-mer hash
-//            (count_records.cu), so the result does not depend on skew.
+//            (count_records.cu), so the result does not depend on skew.  A
+//            sub-bucket of more than heavy_kmers instances (one minimizer of
+//            a low-complexity run can hold millions) is listed without being
+//            counted: one CTA would take as long as the rest of the launch,
+//            while the record split spreads it over many CTAs.
 #include "count_hash.cu"
 
 namespace gkc {
@@ -142,9 +148,11 @@ __device__ __forceinline__ bool warp_run_head(uint64_t key, bool valid, uint32_t
 // ---------------------------------------------------------------------------
 // split
 constexpr int BS_THREADS = 256;
-constexpr int BS_PER_CTA = 2048;   // superkmers per split CTA
+constexpr int BS_PER_CTA = 8192;   // superkmers per split CTA
 constexpr int BS_MAX_PARTS = 4;    // partitions a split CTA aggregates in shared memory
-constexpr int BS_MAX_LOG = 9;      // at most 512 sub-buckets per partition
+constexpr int BS_SLOTS = 4096;     // shared-memory sub-bucket counters per split CTA
+constexpr int BS_LOG_LIMIT = 14;   // at most 16384 sub-buckets per partition
+constexpr size_t BS_SMEM = (size_t)BS_SLOTS * 12;  // dynamic shared memory
 
 struct BSplitParams {
     const uint64_t *idx;                       // chunk superkmer index (partition-ordered)
@@ -154,10 +162,11 @@ struct BSplitParams {
     const unsigned long long *part_skm_off;    // [P+1]
     const unsigned long long *part_byte_off;   // [P]
     uint32_t P;
-    int s_log;                                 // S = 2^s_log sub-buckets per partition
-    uint32_t *bucket_skms;                     // [P*S] superkmers per sub-bucket (pass 0)
-    unsigned long long *bucket_kmers;          // [P*S] k-mers per sub-bucket (pass 0)
-    unsigned long long *bucket_cursor;         // [P*S] next free entry (pass 1)
+    const uint32_t *part_slog;                 // [P] s_p: partition p has 2^s_p sub-buckets
+    const uint32_t *part_bbase;                // [P] index of partition p's first sub-bucket
+    uint32_t *bucket_skms;                     // [NB] superkmers per sub-bucket (pass 0)
+    unsigned long long *bucket_kmers;          // [NB] k-mers per sub-bucket (pass 0)
+    unsigned long long *bucket_cursor;         // [NB] next free entry (pass 1)
     BEntry *entries;                           // [total superkmers] (pass 1)
     int pass;
 };
@@ -173,66 +182,84 @@ __device__ __forceinline__ uint32_t part_of_index(const unsigned long long *off,
 
 // Pass 0 counts superkmers and k-mers per sub-bucket; pass 1 scatters
 // entries.  A CTA covers BS_PER_CTA consecutive superkmers, which span few
-// partitions: the sub-buckets of its first BS_MAX_PARTS partitions are
-// aggregated in shared memory (one global atomic per sub-bucket per CTA), any
-// further partition goes straight to global atomics.
+// partitions: its first BS_MAX_PARTS partitions get consecutive ranges of
+// BS_SLOTS shared-memory counters, 2^s_p each, while they fit, so their
+// sub-buckets cost one global atomic per CTA; any other superkmer goes
+// straight to global atomics.
 __global__ void __launch_bounds__(BS_THREADS)
 bucket_split_kernel(BSplitParams a) {
-    constexpr int NB = BS_MAX_PARTS << BS_MAX_LOG;
-    constexpr uint32_t BMASK = (1u << BS_MAX_LOG) - 1;
-    __shared__ uint32_t cnt[NB];
-    __shared__ unsigned long long base[NB];  // pass 0: k-mers; pass 1: reserved block
-    __shared__ uint32_t p_first_s;
-    const uint32_t S = 1u << a.s_log;  // s_log <= BS_MAX_LOG
+    extern __shared__ unsigned long long bs_smem[];
+    unsigned long long *base = bs_smem;                                // pass 0: k-mers; pass 1: reserved block
+    uint32_t *cnt = reinterpret_cast<uint32_t *>(bs_smem + BS_SLOTS);  // superkmers
+    __shared__ uint32_t soff[BS_MAX_PARTS + 1];  // shared range of partition pf + q: [soff[q], soff[q + 1])
+    __shared__ uint32_t p_first_s, nq_s;
     const uint64_t i0 = a.i_begin + blockIdx.x * (uint64_t)BS_PER_CTA;
     if (i0 >= a.n_skm) return;
     const uint64_t i1 = min(a.n_skm, i0 + BS_PER_CTA);
-    if (threadIdx.x == 0) p_first_s = part_of_index(a.part_skm_off, a.P, i0);
-    for (int t = threadIdx.x; t < NB; t += BS_THREADS) cnt[t] = 0, base[t] = 0;
+    if (threadIdx.x == 0) {
+        const uint32_t pf = part_of_index(a.part_skm_off, a.P, i0);
+        uint32_t q = 0, o = 0;
+        soff[0] = 0;
+        while (q < BS_MAX_PARTS && pf + q < a.P && o + (1u << a.part_slog[pf + q]) <= BS_SLOTS) {
+            o += 1u << a.part_slog[pf + q];
+            soff[++q] = o;
+        }
+        p_first_s = pf;
+        nq_s = q;
+    }
+    for (int t = threadIdx.x; t < BS_SLOTS; t += BS_THREADS) cnt[t] = 0, base[t] = 0;
     __syncthreads();
-    const uint32_t pf = p_first_s;
+    const uint32_t pf = p_first_s, nq = nq_s;
     auto part = [&](uint64_t i) {
         return (i < a.part_skm_off[pf + 1]) ? pf : part_of_index(a.part_skm_off, a.P, i);
     };
+    // global sub-bucket of shared counter t (t < soff[nq])
+    auto global_of = [&](uint32_t t) {
+        uint32_t q = 0;
+        while (t >= soff[q + 1]) q++;
+        return a.part_bbase[pf + q] + (t - soff[q]);
+    };
     for (uint64_t i = i0 + threadIdx.x; i < i1; i += BS_THREADS) {
-        uint32_t p = part(i);
-        uint32_t b = bucket_of(a.keys[i], a.s_log);
-        if (p - pf < BS_MAX_PARTS) {
-            atomicAdd(&cnt[((p - pf) << BS_MAX_LOG) + b], 1u);
-            if (a.pass == 0) atomicAdd(&base[((p - pf) << BS_MAX_LOG) + b], (unsigned long long)idx_len(a.idx[i]));
+        const uint32_t p = part(i);
+        const uint32_t b = bucket_of(a.keys[i], (int)__ldg(a.part_slog + p));
+        if (p - pf < nq) {
+            const uint32_t t = soff[p - pf] + b;
+            atomicAdd(&cnt[t], 1u);
+            if (a.pass == 0) atomicAdd(&base[t], (unsigned long long)idx_len(a.idx[i]));
         } else if (a.pass == 0) {
-            atomicAdd(a.bucket_skms + p * S + b, 1u);
-            atomicAdd(a.bucket_kmers + p * S + b, (unsigned long long)idx_len(a.idx[i]));
+            const uint32_t g = __ldg(a.part_bbase + p) + b;
+            atomicAdd(a.bucket_skms + g, 1u);
+            atomicAdd(a.bucket_kmers + g, (unsigned long long)idx_len(a.idx[i]));
         }
     }
     __syncthreads();
+    const uint32_t ns = soff[nq];
     if (a.pass == 0) {
-        for (int t = threadIdx.x; t < NB; t += BS_THREADS)
+        for (uint32_t t = threadIdx.x; t < ns; t += BS_THREADS)
             if (cnt[t]) {
-                const uint64_t g = (uint64_t)(pf + (t >> BS_MAX_LOG)) * S + (t & BMASK);
+                const uint32_t g = global_of(t);
                 atomicAdd(a.bucket_skms + g, cnt[t]);
                 atomicAdd(a.bucket_kmers + g, base[t]);
             }
         return;
     }
     // pass 1: reserve each shared sub-bucket's block, then write entries
-    for (int t = threadIdx.x; t < NB; t += BS_THREADS) {
-        const uint64_t g = (uint64_t)(pf + (t >> BS_MAX_LOG)) * S + (t & BMASK);
-        base[t] = cnt[t] ? atomicAdd(a.bucket_cursor + g, (unsigned long long)cnt[t]) : 0ull;
+    for (uint32_t t = threadIdx.x; t < ns; t += BS_THREADS) {
+        if (cnt[t]) base[t] = atomicAdd(a.bucket_cursor + global_of(t), (unsigned long long)cnt[t]);
         cnt[t] = 0;
     }
     __syncthreads();
     for (uint64_t i = i0 + threadIdx.x; i < i1; i += BS_THREADS) {
-        uint32_t p = part(i);
-        uint32_t b = bucket_of(a.keys[i], a.s_log);
+        const uint32_t p = part(i);
+        const uint32_t b = bucket_of(a.keys[i], (int)__ldg(a.part_slog + p));
         uint64_t slot;
-        if (p - pf < BS_MAX_PARTS) {
-            uint32_t t = ((p - pf) << BS_MAX_LOG) + b;
+        if (p - pf < nq) {
+            const uint32_t t = soff[p - pf] + b;
             slot = base[t] + atomicAdd(&cnt[t], 1u);
         } else {
-            slot = atomicAdd(a.bucket_cursor + p * S + b, 1ull);
+            slot = atomicAdd(a.bucket_cursor + __ldg(a.part_bbase + p) + b, 1ull);
         }
-        uint64_t e = a.idx[i];
+        const uint64_t e = a.idx[i];
         BEntry en;
         en.ptr = a.bytes + a.part_byte_off[p] + idx_off(e);
         en.len = idx_len(e);
@@ -248,6 +275,8 @@ constexpr int BC_THREADS = 512;
 struct BCountParams {
     const BEntry *entries;
     const uint64_t *bucket_off;   // [nb+1] entry ranges of the sub-buckets
+    const unsigned long long *bucket_kmers;  // [nb] k-mer instances per sub-bucket
+    uint64_t heavy_kmers;         // larger sub-buckets are listed, not counted
     uint32_t b0;                  // first sub-bucket of this launch
     int k;
     uint32_t cmin, cmax;
@@ -296,11 +325,13 @@ __device__ __forceinline__ void smem_collect(const unsigned long long *tk, const
                                              unsigned long long *out_cursor, uint64_t out_cap,
                                              unsigned long long *distinct, uint32_t *err, uint32_t *ws,
                                              unsigned long long *base_s) {
+    // thread i owns slots i, i + NT, i + 2 NT, ...: conflict-free loads (the
+    // output order inside a table does not matter)
     constexpr int PER = TS / NT;
     uint32_t keep = 0, occ = 0;
 #pragma unroll
     for (int t = 0; t < PER; t++) {
-        int s = threadIdx.x * PER + t;
+        int s = t * NT + threadIdx.x;
         if (tk[s] != EMPTY_KEY) {
             occ++;
             keep += (tc[s] >= cmin && tc[s] <= cmax);
@@ -317,7 +348,7 @@ __device__ __forceinline__ void smem_collect(const unsigned long long *tk, const
     uint64_t o = *base_s + pre;
 #pragma unroll
     for (int t = 0; t < PER; t++) {
-        int s = threadIdx.x * PER + t;
+        int s = t * NT + threadIdx.x;
         if (tk[s] != EMPTY_KEY && tc[s] >= cmin && tc[s] <= cmax) {
             if (o < out_cap) {
                 out_k[o] = tk[s];
@@ -341,6 +372,13 @@ bucket_count_kernel(BCountParams a) {
     const uint32_t b = a.b0 + blockIdx.x;
     const uint64_t e0 = a.bucket_off[b], e1 = a.bucket_off[b + 1];
     if (e0 == e1) return;
+    if (a.bucket_kmers[b] > a.heavy_kmers) {
+        if (threadIdx.x == 0) {
+            uint32_t i = atomicAdd(a.failed, 1u);
+            a.failed[1 + i] = b;
+        }
+        return;
+    }
     for (int t = threadIdx.x; t < TS; t += BC_THREADS) {
         tk[t] = EMPTY_KEY;
         tc[t] = 0;

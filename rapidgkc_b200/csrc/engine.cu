@@ -170,8 +170,9 @@ struct gkc_ctx {
     DevBuf stage_bytes, stage_idx;
     DevBuf spill_bytes, spill_idx, spill_keys;  // device staging of chunks being spilled
     // shared-memory bucket counter
-    DevBuf bk_skms, bk_kmers, bk_off, bk_cur, bk_entries, bk_failed, bk_arena;
+    DevBuf bk_skms, bk_kmers, bk_off, bk_cur, bk_entries, bk_failed, bk_arena, bk_part;
     DevBuf r_work, r_count, r_off, r_cur, r_recs, r_failed;  // record sub-buckets
+    DevBuf r_stage, r_winst, r_woff, r_wrec;                  // per-work-item record segments
     uint64_t fallback_buckets = 0;  // sub-buckets counted through the L2 table
     PinBuf h_scal;
 
@@ -197,8 +198,9 @@ struct gkc_ctx {
                         &cursors, &part_off, &tile_read, &codes, &lut, &table, &out_k, &out_c, &keysA, &keysB, &tiles,
                         &counts, &offsets, &blocksums, &heads_pos, &heads_key, &tilecnt, &tileoff, &segoff,
                         &segcur, &part_err, &scal, &stage_bytes, &stage_idx, &spill_bytes, &spill_idx, &spill_keys,
-                        &bk_skms, &bk_kmers, &bk_off, &bk_cur, &bk_entries, &bk_failed, &bk_arena,
-                        &r_work, &r_count, &r_off, &r_cur, &r_recs, &r_failed};
+                        &bk_skms, &bk_kmers, &bk_off, &bk_cur, &bk_entries, &bk_failed, &bk_arena, &bk_part,
+                        &r_work, &r_count, &r_off, &r_cur, &r_recs, &r_failed, &r_stage, &r_winst,
+                        &r_woff, &r_wrec};
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal};
         for (auto *p : ps) p->release();
@@ -577,58 +579,93 @@ int count_buckets_l2(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const std::
 }
 
 constexpr int BC_TS = 8192;  // shared-memory table slots per CTA (96 KB)
+// sub-buckets of more k-mer instances go to the record split (about 4x the
+// 16k instances a sub-bucket is sized for)
+constexpr uint64_t BC_HEAVY_KMERS = 65536;
 
-// Counts the minimizer sub-buckets `ids` that overflowed shared memory: their
-// k-mers are re-split by k-mer hash into record sub-buckets of about 8k
-// instances, counted in shared memory; record sub-buckets that still
-// overflow go through the L2 table.
+// Counts the minimizer sub-buckets `ids` that overflowed shared memory or are
+// heavy: their k-mers are re-split by k-mer hash into record sub-buckets of
+// at most 4k instances, counted in shared memory; record sub-buckets that
+// still overflow go through the L2 table.
 int count_buckets_records(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const std::vector<uint64_t> &off,
                           const std::vector<uint64_t> &bk_kmers, uint32_t cmin, uint32_t cmax) {
     std::vector<RWork> work;
-    uint64_t NR = 0, inst = 0;
+    uint64_t NR = 0, inst = 0, ents = 0;
     for (uint32_t b : ids) {
         const uint64_t kb = bk_kmers[b];
-        // the sub-bucket already holds more distinct k-mers than one table:
-        // at least two record sub-buckets, about 8k instances each
+        // at least two record sub-buckets of at most 4k instances each, so a
+        // table stays at most half full even when every k-mer is distinct
         uint32_t r_log = 1;
-        while (r_log < (uint32_t)RS_MAX_LOG && kb / (1ull << r_log) > 8192) r_log++;
+        while (r_log < (uint32_t)RS_MAX_LOG && kb / (1ull << r_log) > 4096) r_log++;
         for (uint64_t e = off[b]; e < off[b + 1]; e += RW_ENTRIES)
             work.push_back({e, std::min<uint64_t>(e + RW_ENTRIES, off[b + 1]), (uint32_t)NR, r_log});
         NR += 1ull << r_log;
         inst += kb;
+        ents += off[b + 1] - off[b];
     }
     if (work.empty()) return GKC_OK;
-    CK(ctx->r_work.ensure(work.size() * sizeof(RWork)));
+    const uint32_t nw = (uint32_t)work.size();
+    CK(ctx->r_work.ensure(nw * sizeof(RWork)));
     CK(ctx->r_count.ensure(NR * 4));
     CK(ctx->r_off.ensure((NR + 1) * 8));
     CK(ctx->r_cur.ensure(NR * 8));
     CK(ctx->r_recs.ensure(std::max<uint64_t>(inst, 1) * sizeof(KRec)));
+    CK(ctx->r_stage.ensure(std::max<uint64_t>(inst, 1) * sizeof(KRec)));
+    CK(ctx->r_winst.ensure(nw * 4));
+    CK(ctx->r_woff.ensure((nw + 1) * 8));
+    CK(ctx->r_wrec.ensure(nw * 4));
     CK(ctx->r_failed.ensure((NR + 1) * 4));
-    CK(cudaMemcpyAsync(ctx->r_work.p, work.data(), work.size() * sizeof(RWork), cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemcpyAsync(ctx->r_work.p, work.data(), nw * sizeof(RWork), cudaMemcpyHostToDevice, ctx->s));
     CK(cudaMemsetAsync(ctx->r_count.p, 0, NR * 4, ctx->s));
     CK(cudaMemsetAsync(ctx->r_failed.p, 0, 4, ctx->s));
     auto *sc = ctx->scal.as<unsigned long long>();
-    for (int pass = 0; pass < 2; pass++) {
-        if (pass == 1) {
-            RET(scan_u32(ctx, ctx->r_count.as<uint32_t>(), NR, ctx->r_off.as<uint64_t>(),
-                         ctx->r_off.as<unsigned long long>() + NR));
-            CK(cudaMemcpyAsync(ctx->r_cur.p, ctx->r_off.p, NR * 8, cudaMemcpyDeviceToDevice, ctx->s));
-        }
-        RSplitParams rp;
-        rp.entries = ctx->bk_entries.as<BEntry>();
-        rp.work = ctx->r_work.as<RWork>();
-        rp.k = ctx->opt.k;
-        rp.rcount = ctx->r_count.as<uint32_t>();
-        rp.rcursor = ctx->r_cur.as<unsigned long long>();
-        rp.recs = ctx->r_recs.as<KRec>();
-        rp.pass = pass;
-        KScope ks(ctx, GKC_K_SCAN, pass ? 16.0 * inst : 0.0);
-        rec_split_kernel<<<(unsigned)work.size(), RSP_THREADS, 0, ctx->s>>>(rp);
+    {
+        KScope ks(ctx, GKC_K_SCAN, 16.0 * (double)ents + 4.0 * nw);
+        work_inst_kernel<<<(nw + 7) / 8, 256, 0, ctx->s>>>(ctx->bk_entries.as<BEntry>(), ctx->r_work.as<RWork>(),
+                                                            nw, ctx->r_winst.as<uint32_t>());
         LAUNCHED();
     }
+    RET(scan_u32(ctx, ctx->r_winst.as<uint32_t>(), nw, ctx->r_woff.as<uint64_t>(),
+                 ctx->r_woff.as<unsigned long long>() + nw));
+    {
+        RAggParams ap;
+        ap.entries = ctx->bk_entries.as<BEntry>();
+        ap.work = ctx->r_work.as<RWork>();
+        ap.woff = ctx->r_woff.as<uint64_t>();
+        ap.k = ctx->opt.k;
+        ap.stage = ctx->r_stage.as<KRec>();
+        ap.wrec = ctx->r_wrec.as<uint32_t>();
+        ap.rcount = ctx->r_count.as<uint32_t>();
+        CK(cudaFuncSetAttribute(rec_agg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RA_SMEM));
+        KScope ks(ctx, GKC_K_HASH_INSERT, 16.0 * inst);
+        rec_agg_kernel<<<nw, RSP_THREADS, RA_SMEM, ctx->s>>>(ap);
+        LAUNCHED();
+    }
+    RET(scan_u32(ctx, ctx->r_count.as<uint32_t>(), NR, ctx->r_off.as<uint64_t>(),
+                 ctx->r_off.as<unsigned long long>() + NR));
+    CK(cudaMemcpyAsync(ctx->r_cur.p, ctx->r_off.p, NR * 8, cudaMemcpyDeviceToDevice, ctx->s));
+    {
+        RScatterParams rp;
+        rp.work = ctx->r_work.as<RWork>();
+        rp.woff = ctx->r_woff.as<uint64_t>();
+        rp.wrec = ctx->r_wrec.as<uint32_t>();
+        rp.stage = ctx->r_stage.as<KRec>();
+        rp.rcursor = ctx->r_cur.as<unsigned long long>();
+        rp.recs = ctx->r_recs.as<KRec>();
+        KScope ks(ctx, GKC_K_SCAN, 32.0 * inst);
+        rec_scatter_kernel<<<nw, RSP_THREADS, 0, ctx->s>>>(rp);
+        LAUNCHED();
+    }
+    // records after pre-aggregation: one counting CTA per RC_WINDOW of them
+    uint64_t nrec = 0;
+    CK(cudaMemcpyAsync(&nrec, ctx->r_off.as<uint64_t>() + NR, 8, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    const uint64_t nwin = std::max<uint64_t>(1, (nrec + RC_WINDOW - 1) / RC_WINDOW);
+    CK(ctx->r_failed.ensure((std::max<uint64_t>(NR, nwin) + 1) * 4));
     RCountParams cp;
     cp.recs = ctx->r_recs.as<KRec>();
     cp.roff = ctx->r_off.as<uint64_t>();
+    cp.nr = NR;
     cp.cmin = cmin;
     cp.cmax = cmax;
     cp.out_k = ctx->out_k.as<uint64_t>();
@@ -640,8 +677,8 @@ int count_buckets_records(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const 
     cp.err = reinterpret_cast<uint32_t *>(sc + 2);
     CK(cudaFuncSetAttribute(rec_count_kernel<BC_TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, BC_TS * 12));
     {
-        KScope ks(ctx, GKC_K_HASH_COLLECT, 16.0 * inst);
-        rec_count_kernel<BC_TS><<<(unsigned)NR, BC_THREADS, BC_TS * 12, ctx->s>>>(cp);
+        KScope ks(ctx, GKC_K_HASH_COLLECT, 16.0 * nrec);
+        rec_count_kernel<BC_TS><<<(unsigned)nwin, BC_THREADS, BC_TS * 12, ctx->s>>>(cp);
         LAUNCHED();
     }
     uint32_t nfail = 0;
@@ -655,7 +692,12 @@ int count_buckets_records(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const 
     CK(cudaStreamSynchronize(ctx->s));
     const double slots = ctx->opt.table_slots > 0 ? ctx->opt.table_slots : 0.35;
     for (uint32_t r : rids) {
-        const uint64_t e0 = roff[r], e1 = roff[r + 1];
+        // the records of window r, as rec_count_kernel chose them
+        const uint64_t lo = std::lower_bound(roff.begin(), roff.end(), r * RC_WINDOW) - roff.begin();
+        const uint64_t hi = std::min<uint64_t>(
+            std::lower_bound(roff.begin(), roff.end(), (r + 1) * RC_WINDOW) - roff.begin(), NR);
+        if (lo >= hi) continue;
+        const uint64_t e0 = roff[lo], e1 = roff[hi];
         for (int scale = 1;; scale *= 4) {
             uint64_t C = next_pow2(std::max<uint64_t>(4096, (uint64_t)((double)(e1 - e0) * 3.0 * slots) * scale));
             RET(ensure_table(ctx, C));
@@ -716,13 +758,19 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
     }
     uint64_t N = 0, NS = 0;
     for (uint32_t p = 0; p < P; p++) N += np[p], NS += nsp[p];
-    // sub-buckets per partition: about 16k k-mer instances each, so that a
-    // sub-bucket's distinct k-mers (a fraction of its instances) fit the table
-    const double mean = (double)N / P;
-    int s_log = 0;
-    while (!ctx->opt.hash_l2_only && s_log < BS_MAX_LOG && mean / (double)(1u << s_log) > 16384.0) s_log++;
-    const uint32_t S = 1u << s_log;
-    const uint64_t NB = (uint64_t)P * S;
+    // sub-buckets of partition p: 2^s_p of about 16k k-mer instances each, so
+    // that a sub-bucket's distinct k-mers (a fraction of its instances) fit
+    // the table
+    std::vector<uint32_t> slog(2 * P);  // [0, P) s_p, [P, 2P) first sub-bucket of p
+    uint64_t NB = 0;
+    for (uint32_t p = 0; p < P; p++) {
+        uint32_t sl = 0;
+        while (!ctx->opt.hash_l2_only && sl < (uint32_t)BS_LOG_LIMIT && np[p] > (16384ull << sl)) sl++;
+        slog[p] = sl;
+        slog[P + p] = (uint32_t)NB;
+        NB += 1ull << sl;
+    }
+    auto bbase = [&](uint32_t p) -> uint64_t { return p < P ? slog[P + p] : NB; };
     ctx->times[4] = (double)NB;
     ctx->times[5] = 0;
     RET(ensure_out(ctx, N / std::max<uint32_t>(cmin, 1) + 1024));
@@ -731,6 +779,8 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
     CK(ctx->bk_off.ensure((NB + 1) * 8));
     CK(ctx->bk_cur.ensure(NB * 8));
     CK(ctx->bk_failed.ensure((NB + 1) * 4));
+    CK(ctx->bk_part.ensure(2ull * P * 4));
+    CK(cudaMemcpyAsync(ctx->bk_part.p, slog.data(), 2ull * P * 4, cudaMemcpyHostToDevice, ctx->s));
     CK(ctx->part_err.ensure(std::max<uint32_t>(P, 16) * 4));
     CK(ctx->scal.ensure(64));
     CK(ctx->h_scal.ensure(64));
@@ -739,6 +789,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
     CK(cudaMemcpyAsync(sc, &ctx->n_out, 8, cudaMemcpyHostToDevice, ctx->s));
     CK(cudaFuncSetAttribute(bucket_count_kernel<BC_TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             BC_TS * 12));
+    CK(cudaFuncSetAttribute(bucket_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BS_SMEM));
     // groups of partitions
     uint64_t budget = ~0ull;
     if (spilled) {
@@ -790,7 +841,8 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
                 sp.part_skm_off = c->d_skm_off.as<unsigned long long>();
                 sp.part_byte_off = c->d_byte_off.as<unsigned long long>();
                 sp.P = P;
-                sp.s_log = s_log;
+                sp.part_slog = ctx->bk_part.as<uint32_t>();
+                sp.part_bbase = ctx->bk_part.as<uint32_t>() + P;
                 sp.bucket_skms = ctx->bk_skms.as<uint32_t>();
                 sp.bucket_kmers = ctx->bk_kmers.as<unsigned long long>();
                 sp.bucket_cursor = ctx->bk_cur.as<unsigned long long>();
@@ -798,7 +850,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
                 sp.pass = pass;
                 uint32_t g = (uint32_t)((i1 - i0 + BS_PER_CTA - 1) / BS_PER_CTA);
                 KScope ks(ctx, GKC_K_SCAN, pass ? 28.0 * (i1 - i0) : 12.0 * (i1 - i0));
-                bucket_split_kernel<<<g, BS_THREADS, 0, ctx->s>>>(sp);
+                bucket_split_kernel<<<g, BS_THREADS, BS_SMEM, ctx->s>>>(sp);
                 LAUNCHED();
             }
         }
@@ -806,7 +858,9 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
         BCountParams bp;
         bp.entries = ctx->bk_entries.as<BEntry>();
         bp.bucket_off = ctx->bk_off.as<uint64_t>();
-        bp.b0 = p0 * S;
+        bp.bucket_kmers = ctx->bk_kmers.as<unsigned long long>();
+        bp.heavy_kmers = BC_HEAVY_KMERS;
+        bp.b0 = (uint32_t)bbase(p0);
         bp.k = ctx->opt.k;
         bp.cmin = cmin;
         bp.cmax = cmax;
@@ -821,7 +875,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
             uint64_t gbytes = 0;
             for (uint32_t p = p0; p < p1; p++) gbytes += nbp[p];
             KScope ks(ctx, GKC_K_HASH_INSERT, (double)gbytes + 16.0 * gs);
-            bucket_count_kernel<BC_TS><<<(p1 - p0) * S, BC_THREADS, BC_TS * 12, ctx->s>>>(bp);
+            bucket_count_kernel<BC_TS><<<(unsigned)(bbase(p1) - bbase(p0)), BC_THREADS, BC_TS * 12, ctx->s>>>(bp);
             LAUNCHED();
         }
         CK(cudaEventRecord(ctx->e3, ctx->s));
@@ -844,7 +898,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
             CK(cudaStreamSynchronize(ctx->s));
         }
         if (ctx->opt.hash_l2_only)  // every non-empty sub-bucket (one per partition)
-            for (uint32_t b = p0 * S; b < p1 * S; b++)
+            for (uint64_t b = bbase(p0); b < bbase(p1); b++)
                 if (off[b + 1] > off[b]) ids.push_back(b);
         if (!ids.empty()) {
             if (ctx->opt.hash_l2_only) {

@@ -199,3 +199,34 @@ def test_shared_memory_overflow_falls_back(oracle):
         km, ct = sorted_table(*c.result())
     assert d == do and d > 100_000
     assert np.array_equal(km, ko) and np.array_equal(ct, co)
+
+
+def test_heavy_and_overflowing_sub_buckets(oracle):
+    """A learned order that makes two p-mers the preferred minimizers builds
+    three kinds of sub-bucket beside ordinary ones: one with ~31k distinct
+    k-mers (overflows the shared-memory table), one with ~105k distinct k-mers
+    (above the heavy limit, so it is never counted by one CTA), and (AT)n reads
+    whose 120k k-mer instances share one or two distinct k-mers.  All take the
+    record split and give the oracle's multiset."""
+    k, p, P = 31, 11, 4
+    r = np.random.default_rng(21)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    rnd = lambda n: bytes(acgt[r.integers(0, 4, n)])
+    X, Y = b"CTTGACCGTAG", b"GATCCTAGGCA"
+    parts = [rnd(70) + X + rnd(69) for _ in range(1500)] + [rnd(60) + Y + rnd(79) for _ in range(5000)]
+    parts += [b"AT" * 75 for _ in range(1000)] + [rnd(150) for _ in range(3000)]
+    reads, offs = csr(parts)
+    code = lambda s: int("".join(str("ACGT".index(chr(ch))) for ch in s), 4)
+    lut = r.permutation(4 ** p).astype(np.uint32)
+    for v, rank in [(code(X), 0), (code(Y), 1)]:
+        j = int(np.nonzero(lut == rank)[0][0])
+        lut[j], lut[v] = lut[v], rank
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P)
+    ko, co = sorted_table(ko, co)
+    with counter(k, p, P, "hash") as c:
+        c.set_order(lut)
+        n, d = c.count_reads(reads, offs)
+        km, ct = sorted_table(*c.result())
+        t = c.timings()
+    assert t["overflowed_sub_buckets"] >= 2  # the (AT)n minimizer may share a sub-bucket
+    assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
