@@ -68,9 +68,10 @@ const char *gkc_strerror(int code);
 
 /* Minimizer order: `lut` holds 4^p ranks (uint32) indexed by the 2-bit p-mer
  * value; the canonical minimizer of a k-mer is the p-mer of least rank over
- * both strands.  NULL restores the reference's default order (value order
- * with the "rapidgkc" filter, minimizer_filter.h:20).  `mem` says where lut
- * lives. */
+ * both strands (phase 1 reads a precomputed min(rank(v), rank(rc(v))) table,
+ * one read per position).  NULL restores the reference's default order (value
+ * order with the "rapidgkc" filter, minimizer_filter.h:20).  `mem` says where
+ * lut lives. */
 int gkc_set_order(gkc_ctx *ctx, const uint32_t *lut, uint64_t n, int mem);
 
 /* Phase 1: splits a CSR batch of ASCII reads (reads[offs[i]..offs[i+1])) into
@@ -153,6 +154,51 @@ enum {
  * last reset.  Arrays of n <= GKC_K_CLASSES entries; any may be NULL. */
 int gkc_set_profiling(gkc_ctx *ctx, int on);
 int gkc_kernel_stats(gkc_ctx *ctx, double *ms, uint64_t *launches, double *bytes, int n, int reset);
+
+/* ---- learned minimizer order ------------------------------------------
+ * No counterpart in the reference: its order is fixed (value order with the
+ * "rapidgkc" filter, minimizer_filter.h:20, gpu_skmgen.cu:243-252).  A network
+ * (one-hot p-mer, 4p inputs -> 64 ReLU -> 64 ReLU -> 1, FP32) scores every
+ * p-mer; the order ranks p-mers by score, so p-mers with a high predicted
+ * load are chosen as minimizers last.  Parameters: one float vector of
+ * gkc_mlp_param_count(p) entries, W1 [4p][64] (input 4*pos + base, pos 0 = the
+ * first base), b1 [64], W2 [64][64] (row = input unit), b2 [64], w3 [64], b3.
+ * All use the context's p and device; p <= 16. */
+
+/* Number of network parameters for minimizer length p (0 if p is out of range). */
+uint64_t gkc_mlp_param_count(int p);
+
+/* k-mer instances of the store per minimizer key: loads[key & (4^p - 1)], n =
+ * 4^p.  With the default order the key is the minimizer's value (4^p - 1 also
+ * stands for k-mers without a valid p-mer); with an order table it is the
+ * minimizer's rank. */
+int gkc_minimizer_loads(gkc_ctx *ctx, uint64_t *loads, uint64_t n, int mem);
+
+/* One forward and backward pass over the n samples pmers[] (host memory):
+ * loss = norm * sum_s w_s (y_s - t_s)^2 with t_s = targets[pmers[s]] and
+ * w_s = weights[pmers[s]] (weights may be NULL: all 1); targets and weights
+ * hold 4^p floats.  grad receives d loss / d params. */
+int gkc_mlp_grad(gkc_ctx *ctx, const float *params, const uint32_t *pmers, uint64_t n, const float *targets,
+                 const float *weights, float norm, float *grad, float *loss);
+
+/* Trains params (host, in place) with Adam (lr, betas 0.9 / 0.999) on all 4^p
+ * p-mers for `epochs` passes in shuffled batches of `batch`; *loss (optional)
+ * = mean batch loss of the last pass.  Deterministic samples for a seed; the
+ * gradient sums use atomics, so results vary in the last bits. */
+int gkc_mlp_train(gkc_ctx *ctx, float *params, const float *targets, const float *weights, int epochs, int batch,
+                  float lr, uint64_t seed, float *loss);
+
+/* Scores of all 4^p p-mers (scores[v], host or device memory). */
+int gkc_mlp_scores(gkc_ctx *ctx, const float *params, float *scores, int mem);
+
+/* Makes the network's order the context's order (p <= 15).  rank(v) =
+ * (level << 2p) | mix(v), mix = a fixed bijection of 2p bits: the `heavy`
+ * p-mers of highest score (the ones predicted heavy as minimizers; 0 = 4^p / 4)
+ * get levels 1 .. 2^(32-2p)-2 by score and are chosen last; every other p-mer
+ * has level 0, so their order is pseudo-random instead of by value.  lut_out
+ * (optional, host, 4^p entries) receives the rank table (what gkc_set_order
+ * would take for the same order). */
+int gkc_mlp_order(gkc_ctx *ctx, const float *params, uint64_t heavy, uint32_t *lut_out);
 
 #ifdef __cplusplus
 }

@@ -31,6 +31,8 @@ EXPORTS = (
     "gkc_set_order", "gkc_add_reads", "gkc_store_stats", "gkc_store_export", "gkc_store_clear",
     "gkc_count", "gkc_result", "gkc_result_device", "gkc_count_reads", "gkc_count_keys",
     "gkc_last_timings", "gkc_kernel_launches", "gkc_set_stream", "gkc_set_profiling", "gkc_kernel_stats",
+    "gkc_mlp_param_count", "gkc_minimizer_loads", "gkc_mlp_grad", "gkc_mlp_train", "gkc_mlp_scores",
+    "gkc_mlp_order",
 )
 KERNEL_CLASSES = ("find_superkmers", "scatter_superkmers", "hash_insert", "hash_collect", "sort_extract",
                   "radix_hist", "radix_scatter", "scan", "rle")
@@ -94,8 +96,17 @@ def load_library(path: str = LIB_PATH):
     L.gkc_set_stream.argtypes = [vp, vp]
     L.gkc_set_profiling.argtypes = [vp, i32]
     L.gkc_kernel_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(u64), C.POINTER(C.c_double), i32, i32]
+    f32 = C.c_float
+    L.gkc_mlp_param_count.argtypes = [i32]
+    L.gkc_mlp_param_count.restype = u64
+    L.gkc_minimizer_loads.argtypes = [vp, vp, u64, i32]
+    L.gkc_mlp_grad.argtypes = [vp, vp, vp, u64, vp, vp, f32, vp, C.POINTER(f32)]
+    L.gkc_mlp_train.argtypes = [vp, vp, vp, vp, i32, i32, f32, u64, C.POINTER(f32)]
+    L.gkc_mlp_scores.argtypes = [vp, vp, vp, i32]
+    L.gkc_mlp_order.argtypes = [vp, vp, u64, vp]
     for name in EXPORTS:
-        if name not in ("gkc_default_options", "gkc_last_error", "gkc_strerror", "gkc_kernel_launches"):
+        if name not in ("gkc_default_options", "gkc_last_error", "gkc_strerror", "gkc_kernel_launches",
+                        "gkc_mlp_param_count"):
             getattr(L, name).restype = i32
     _lib = L
     return L
@@ -234,6 +245,50 @@ class KmerCounter:
         no, nd = C.c_uint64(0), C.c_uint64(0)
         self._check(self._L.gkc_count_keys(self._h, kp, len(keys), km, cmin, cmax, C.byref(no), C.byref(nd)))
         return no.value, nd.value
+
+    # -- learned minimizer order --------------------------------------------
+    def minimizer_loads(self) -> np.ndarray:
+        """k-mer instances of the store per minimizer key (4^p, uint64)."""
+        out = np.zeros(4 ** self.p, np.uint64)
+        self._check(self._L.gkc_minimizer_loads(self._h, _ptr(out)[0], len(out), MEM_HOST))
+        return out
+
+    def mlp_grad(self, params, pmers, targets, weights=None, norm: float = 1.0):
+        """(loss, gradient) of one forward/backward pass over the samples."""
+        params = np.ascontiguousarray(params, np.float32)
+        pmers = np.ascontiguousarray(pmers, np.uint32)
+        targets = np.ascontiguousarray(targets, np.float32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        grad = np.zeros_like(params)
+        loss = C.c_float(0)
+        self._check(self._L.gkc_mlp_grad(self._h, _ptr(params)[0], _ptr(pmers)[0], len(pmers), _ptr(targets)[0],
+                                         _ptr(w)[0], norm, _ptr(grad)[0], C.byref(loss)))
+        return loss.value, grad
+
+    def mlp_train(self, params, targets, weights=None, epochs: int = 4, batch: int = 4096, lr: float = 1e-3,
+                  seed: int = 0):
+        """Trains a copy of params on all 4^p p-mers; returns (params, last loss)."""
+        params = np.array(params, np.float32, copy=True)
+        targets = np.ascontiguousarray(targets, np.float32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        loss = C.c_float(0)
+        self._check(self._L.gkc_mlp_train(self._h, _ptr(params)[0], _ptr(targets)[0], _ptr(w)[0], epochs, batch,
+                                          lr, seed, C.byref(loss)))
+        return params, loss.value
+
+    def mlp_scores(self, params) -> np.ndarray:
+        params = np.ascontiguousarray(params, np.float32)
+        out = np.zeros(4 ** self.p, np.float32)
+        self._check(self._L.gkc_mlp_scores(self._h, _ptr(params)[0], _ptr(out)[0], MEM_HOST))
+        return out
+
+    def mlp_order(self, params, heavy: int = 0) -> np.ndarray:
+        """Makes the network's order the context's order (the `heavy` p-mers
+        of highest score ranked last; 0 = 4^p / 4); returns the rank table."""
+        params = np.ascontiguousarray(params, np.float32)
+        lut = np.zeros(4 ** self.p, np.uint32)
+        self._check(self._L.gkc_mlp_order(self._h, _ptr(params)[0], heavy, _ptr(lut)[0]))
+        return lut
 
     def timings(self):
         t = (C.c_double * 6)()

@@ -12,6 +12,7 @@
 #include "../../include/gkc_capi.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -20,6 +21,7 @@
 
 #include "count_records.cu"
 #include "count_sort.cu"
+#include "order_mlp.cu"
 #include "skmgen.cu"
 
 using namespace gkc;
@@ -155,8 +157,10 @@ struct gkc_ctx {
     cudaEvent_t buf_free[2] = {nullptr, nullptr}, buf_ready[2] = {nullptr, nullptr};
     DevBuf records, region_count, hist, flags, cursors, part_off, tile_read, codes;
     PinBuf h_hist, h_flags;
-    DevBuf lut;
+    DevBuf lut;             // canonical order table: min(rank(v), rank(rc(v)))
     bool has_lut = false;
+    // learned order: network training and scoring
+    DevBuf ord_loads, ord_stage, ord_list, mlp_p, mlp_m, mlp_v, mlp_g, mlp_t, mlp_w, mlp_s, mlp_scalar;
     std::vector<StoreChunk *> store;
 
     // phase 2 buffers
@@ -200,7 +204,8 @@ struct gkc_ctx {
                         &segcur, &part_err, &scal, &stage_bytes, &stage_idx, &spill_bytes, &spill_idx, &spill_keys,
                         &bk_skms, &bk_kmers, &bk_off, &bk_cur, &bk_entries, &bk_failed, &bk_arena, &bk_part,
                         &r_work, &r_count, &r_off, &r_cur, &r_recs, &r_failed, &r_stage, &r_winst,
-                        &r_woff, &r_wrec};
+                        &r_woff, &r_wrec, &ord_loads, &ord_stage, &ord_list, &mlp_p, &mlp_m, &mlp_v, &mlp_g, &mlp_t,
+                        &mlp_w, &mlp_s, &mlp_scalar};
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal};
         for (auto *p : ps) p->release();
@@ -346,9 +351,15 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     const int w = ctx->opt.k - ctx->opt.p + 1;
     int lg = 0;
     while ((2 << lg) <= w) lg++;
-    void (*kfind)(P1Params) = lg == 0 ? find_superkmers_kernel<0> : lg == 1 ? find_superkmers_kernel<1>
-                              : lg == 2 ? find_superkmers_kernel<2> : lg == 3 ? find_superkmers_kernel<3>
-                                                                                : find_superkmers_kernel<4>;
+    void (*kfind)(P1Params);
+    if (ctx->has_lut)
+        kfind = lg == 0 ? find_superkmers_kernel<0, true> : lg == 1 ? find_superkmers_kernel<1, true>
+              : lg == 2 ? find_superkmers_kernel<2, true> : lg == 3 ? find_superkmers_kernel<3, true>
+                                                                    : find_superkmers_kernel<4, true>;
+    else
+        kfind = lg == 0 ? find_superkmers_kernel<0, false> : lg == 1 ? find_superkmers_kernel<1, false>
+              : lg == 2 ? find_superkmers_kernel<2, false> : lg == 3 ? find_superkmers_kernel<3, false>
+                                                                     : find_superkmers_kernel<4, false>;
     size_t dyn = 3ull * P * sizeof(uint32_t);
     CK(cudaFuncSetAttribute(kfind, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     int per_sm = 0;
@@ -1117,6 +1128,20 @@ int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
     return GKC_OK;
 }
 
+// Makes the rank table `ranks` (device, 4^p) the context's order: phase 1
+// reads its canonical form.
+int install_order(gkc_ctx *ctx, const uint32_t *ranks) {
+    const int p = ctx->opt.p;
+    const uint32_t n = 1u << (2 * p);
+    CK(ctx->lut.ensure(n * 4ull));
+    const uint32_t g = (uint32_t)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sms * 8);
+    canonical_table_kernel<<<g, 256, 0, ctx->s>>>(ranks, n, p, ctx->lut.as<uint32_t>());
+    LAUNCHED();
+    CK(cudaStreamSynchronize(ctx->s));
+    ctx->has_lut = true;
+    return GKC_OK;
+}
+
 int upload(gkc_ctx *ctx, DevBuf &buf, const void *src, uint64_t bytes, int mem, const void **dptr) {
     if (mem == GKC_MEM_DEVICE) {
         *dptr = src;
@@ -1220,11 +1245,10 @@ int gkc_set_order(gkc_ctx *ctx, const uint32_t *lut, uint64_t n, int mem) {
     }
     uint64_t need = 1ull << (2 * ctx->opt.p);
     if (n != need) return ctx->fail(GKC_EINVAL, "order table needs 4^p = %llu entries", (unsigned long long)need);
-    CK(ctx->lut.ensure(n * 4));
-    CK(cudaMemcpyAsync(ctx->lut.p, lut, n * 4, mem == GKC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                       ctx->s));
-    CK(cudaStreamSynchronize(ctx->s));
-    ctx->has_lut = true;
+    CK(ctx->ord_stage.ensure(n * 4));
+    CK(cudaMemcpyAsync(ctx->ord_stage.p, lut, n * 4,
+                       mem == GKC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->s));
+    RET(install_order(ctx, ctx->ord_stage.as<uint32_t>()));
     return GKC_OK;
 }
 
@@ -1531,6 +1555,231 @@ int gkc_kernel_stats(gkc_ctx *ctx, double *ms, uint64_t *launches, double *bytes
 int gkc_last_timings(gkc_ctx *ctx, double *t, int n) {
     if (!ctx || !t) return GKC_EINVAL;
     for (int i = 0; i < n && i < 6; i++) t[i] = ctx->times[i];
+    return GKC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// learned minimizer order
+
+uint64_t gkc_mlp_param_count(int p) {
+    if (p < 1 || p > MLP_MAX_P) return 0;
+    return mlp_layout(p).n;
+}
+
+int gkc_minimizer_loads(gkc_ctx *ctx, uint64_t *loads, uint64_t n, int mem) {
+    if (!ctx || !loads) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    const uint64_t np = 1ull << (2 * ctx->opt.p);
+    if (n != np) return ctx->fail(GKC_EINVAL, "minimizer loads need 4^p = %llu entries", (unsigned long long)np);
+    CK(ctx->ord_loads.ensure(np * 8));
+    CK(cudaMemsetAsync(ctx->ord_loads.p, 0, np * 8, ctx->s));
+    for (StoreChunk *c : ctx->store) {
+        if (!c->nskm) continue;
+        const uint64_t *idx = c->idx;
+        const uint32_t *keys = c->keys;
+        if (c->on_host) {  // a spilled chunk: stage its index and keys
+            CK(ctx->ord_stage.ensure(c->nskm * 12));
+            CK(cudaMemcpyAsync(ctx->ord_stage.p, c->idx, c->nskm * 8, cudaMemcpyHostToDevice, ctx->s));
+            CK(cudaMemcpyAsync(ctx->ord_stage.as<uint8_t>() + c->nskm * 8, c->keys, c->nskm * 4,
+                               cudaMemcpyHostToDevice, ctx->s));
+            idx = ctx->ord_stage.as<uint64_t>();
+            keys = reinterpret_cast<const uint32_t *>(ctx->ord_stage.as<uint8_t>() + c->nskm * 8);
+        }
+        const uint32_t g = (uint32_t)std::min<uint64_t>((c->nskm + 255) / 256, (uint64_t)ctx->sms * 8);
+        minimizer_loads_kernel<<<g, 256, 0, ctx->s>>>(idx, keys, c->nskm, (uint32_t)(np - 1),
+                                                      ctx->ord_loads.as<unsigned long long>());
+        LAUNCHED();
+        if (c->on_host) CK(cudaStreamSynchronize(ctx->s));  // the staging buffer is reused
+    }
+    CK(cudaMemcpyAsync(loads, ctx->ord_loads.p, np * 8,
+                       mem == GKC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    return GKC_OK;
+}
+
+namespace {
+
+// Device copies of the network inputs; targets/weights are 4^p arrays.
+int mlp_upload(gkc_ctx *ctx, const float *params, const float *targets, const float *weights) {
+    const int p = ctx->opt.p;
+    const MlpLayout L = mlp_layout(p);
+    const uint64_t np = 1ull << (2 * p);
+    CK(ctx->mlp_p.ensure(L.n * 4));
+    CK(ctx->mlp_g.ensure(L.n * 4));
+    CK(ctx->mlp_scalar.ensure(64));
+    CK(cudaMemcpyAsync(ctx->mlp_p.p, params, L.n * 4, cudaMemcpyHostToDevice, ctx->s));
+    if (targets) {
+        CK(ctx->mlp_t.ensure(np * 4));
+        CK(cudaMemcpyAsync(ctx->mlp_t.p, targets, np * 4, cudaMemcpyHostToDevice, ctx->s));
+    }
+    if (weights) {
+        CK(ctx->mlp_w.ensure(np * 4));
+        CK(cudaMemcpyAsync(ctx->mlp_w.p, weights, np * 4, cudaMemcpyHostToDevice, ctx->s));
+    }
+    return GKC_OK;
+}
+
+int mlp_launch(gkc_ctx *ctx, const uint32_t *pmers, uint64_t s0, uint64_t n, bool weights, float norm, bool train,
+               float *scores) {
+    const int p = ctx->opt.p;
+    MlpParams a;
+    a.params = ctx->mlp_p.as<float>();
+    a.L = mlp_layout(p);
+    a.pmers = pmers;
+    a.s0 = s0;
+    a.n = n;
+    a.targets = train ? ctx->mlp_t.as<float>() : nullptr;
+    a.weights = train && weights ? ctx->mlp_w.as<float>() : nullptr;
+    a.norm = norm;
+    a.grad = train ? ctx->mlp_g.as<float>() : nullptr;
+    a.loss = train ? ctx->mlp_scalar.as<float>() : nullptr;
+    a.scores = scores;
+    const size_t sm = mlp_smem_floats(p) * 4;
+    CK(cudaFuncSetAttribute(mlp_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    mlp_tile_kernel<<<(unsigned)((n + MLP_TILE - 1) / MLP_TILE), MLP_THREADS, sm, ctx->s>>>(a);
+    LAUNCHED();
+    return GKC_OK;
+}
+
+}  // namespace
+
+int gkc_mlp_grad(gkc_ctx *ctx, const float *params, const uint32_t *pmers, uint64_t n, const float *targets,
+                 const float *weights, float norm, float *grad, float *loss) {
+    if (!ctx || !params || !pmers || !targets || !grad || n == 0) return GKC_EINVAL;
+    const int p = ctx->opt.p;
+    if (p > MLP_MAX_P) return ctx->fail(GKC_EINVAL, "the network supports p <= %d", MLP_MAX_P);
+    CK(cudaSetDevice(ctx->device));
+    const MlpLayout L = mlp_layout(p);
+    const uint64_t np = 1ull << (2 * p);
+    for (uint64_t i = 0; i < n; i++)
+        if (pmers[i] >= np) return ctx->fail(GKC_EINVAL, "sample %llu is not a %d-mer", (unsigned long long)i, p);
+    RET(mlp_upload(ctx, params, targets, weights));
+    CK(ctx->mlp_s.ensure(n * 4));
+    CK(cudaMemcpyAsync(ctx->mlp_s.p, pmers, n * 4, cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemsetAsync(ctx->mlp_g.p, 0, L.n * 4, ctx->s));
+    CK(cudaMemsetAsync(ctx->mlp_scalar.p, 0, 4, ctx->s));
+    RET(mlp_launch(ctx, ctx->mlp_s.as<uint32_t>(), 0, n, weights != nullptr, norm, true, nullptr));
+    CK(cudaMemcpyAsync(grad, ctx->mlp_g.p, L.n * 4, cudaMemcpyDeviceToHost, ctx->s));
+    if (loss) CK(cudaMemcpyAsync(loss, ctx->mlp_scalar.p, 4, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    return GKC_OK;
+}
+
+int gkc_mlp_train(gkc_ctx *ctx, float *params, const float *targets, const float *weights, int epochs, int batch,
+                  float lr, uint64_t seed, float *loss) {
+    if (!ctx || !params || !targets || epochs < 0 || batch < 1 || !(lr > 0.f)) return GKC_EINVAL;
+    const int p = ctx->opt.p;
+    if (p > MLP_MAX_P) return ctx->fail(GKC_EINVAL, "the network supports p <= %d", MLP_MAX_P);
+    CK(cudaSetDevice(ctx->device));
+    const MlpLayout L = mlp_layout(p);
+    const uint64_t np = 1ull << (2 * p);
+    RET(mlp_upload(ctx, params, targets, weights));
+    CK(ctx->mlp_m.ensure(L.n * 4));
+    CK(ctx->mlp_v.ensure(L.n * 4));
+    CK(ctx->mlp_s.ensure(np * 4));
+    CK(cudaMemsetAsync(ctx->mlp_m.p, 0, L.n * 4, ctx->s));
+    CK(cudaMemsetAsync(ctx->mlp_v.p, 0, L.n * 4, ctx->s));
+    CK(cudaMemsetAsync(ctx->mlp_g.p, 0, L.n * 4, ctx->s));
+    // batch loss = sum_s w_s e_s^2 / (batch * mean weight)
+    double wmean = 1.0;
+    if (weights) {
+        double sw = 0;
+        for (uint64_t i = 0; i < np; i++) sw += weights[i];
+        wmean = sw / (double)np;
+        if (!(wmean > 0)) return ctx->fail(GKC_EINVAL, "weights sum to zero");
+    }
+    const float norm = (float)(1.0 / ((double)batch * wmean));
+    AdamParams ap;
+    ap.params = ctx->mlp_p.as<float>();
+    ap.m = ctx->mlp_m.as<float>();
+    ap.v = ctx->mlp_v.as<float>();
+    ap.grad = ctx->mlp_g.as<float>();
+    ap.n = L.n;
+    ap.lr = lr;
+    ap.beta1 = 0.9f;
+    ap.beta2 = 0.999f;
+    ap.eps = 1e-8f;
+    uint64_t step = 0;
+    float last = 0.f;
+    for (int e = 0; e < epochs; e++) {
+        const uint32_t key = (uint32_t)(seed * 0x9E3779B97F4A7C15ull >> 32) ^ (uint32_t)(e * 0x85EBCA6Bu);
+        epoch_samples_kernel<<<(unsigned)std::min<uint64_t>((np + 255) / 256, (uint64_t)ctx->sms * 8), 256, 0,
+                               ctx->s>>>(ctx->mlp_s.as<uint32_t>(), (uint32_t)np, 2 * p, key);
+        LAUNCHED();
+        CK(cudaMemsetAsync(ctx->mlp_scalar.p, 0, 4, ctx->s));
+        for (uint64_t b0 = 0; b0 < np; b0 += (uint64_t)batch) {
+            const uint64_t nb = std::min<uint64_t>((uint64_t)batch, np - b0);
+            RET(mlp_launch(ctx, ctx->mlp_s.as<uint32_t>() + b0, 0, nb, weights != nullptr, norm, true, nullptr));
+            step++;
+            ap.c1 = (float)(1.0 / (1.0 - std::pow(0.9, (double)step)));
+            ap.c2 = (float)(1.0 / (1.0 - std::pow(0.999, (double)step)));
+            mlp_adam_kernel<<<(L.n + 255) / 256, 256, 0, ctx->s>>>(ap);
+            LAUNCHED();
+        }
+        CK(cudaMemcpyAsync(&last, ctx->mlp_scalar.p, 4, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+    }
+    // mean per-batch loss of the last epoch
+    if (loss) *loss = last / (float)((np + batch - 1) / batch);
+    CK(cudaMemcpyAsync(params, ctx->mlp_p.p, L.n * 4, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    return GKC_OK;
+}
+
+int gkc_mlp_scores(gkc_ctx *ctx, const float *params, float *scores, int mem) {
+    if (!ctx || !params || !scores) return GKC_EINVAL;
+    const int p = ctx->opt.p;
+    if (p > MLP_MAX_P) return ctx->fail(GKC_EINVAL, "the network supports p <= %d", MLP_MAX_P);
+    CK(cudaSetDevice(ctx->device));
+    const uint64_t np = 1ull << (2 * p);
+    RET(mlp_upload(ctx, params, nullptr, nullptr));
+    float *d = scores;
+    if (mem != GKC_MEM_DEVICE) {
+        CK(ctx->ord_stage.ensure(np * 4));
+        d = ctx->ord_stage.as<float>();
+    }
+    RET(mlp_launch(ctx, nullptr, 0, np, false, 0.f, false, d));
+    if (mem != GKC_MEM_DEVICE) CK(cudaMemcpyAsync(scores, d, np * 4, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    return GKC_OK;
+}
+
+int gkc_mlp_order(gkc_ctx *ctx, const float *params, uint64_t heavy, uint32_t *lut_out) {
+    if (!ctx || !params) return GKC_EINVAL;
+    const int p = ctx->opt.p;
+    if (p > ORDER_MAX_P) return ctx->fail(GKC_EINVAL, "the learned order supports p <= %d", ORDER_MAX_P);
+    CK(cudaSetDevice(ctx->device));
+    const uint32_t np = 1u << (2 * p);
+    // scores of every p-mer
+    std::vector<float> sc(np);
+    RET(gkc_mlp_scores(ctx, params, sc.data(), GKC_MEM_HOST));
+    // the `heavy` highest-scoring p-mers get levels 1 .. 2^(32-2p)-2 by score
+    const uint32_t K = (uint32_t)std::min<uint64_t>(heavy ? heavy : np / 4, np);
+    std::vector<uint32_t> ids(np);
+    for (uint32_t v = 0; v < np; v++) ids[v] = v;
+    auto higher = [&](uint32_t x, uint32_t y) { return sc[x] > sc[y] || (sc[x] == sc[y] && x < y); };
+    std::nth_element(ids.begin(), ids.begin() + K, ids.end(), higher);
+    ids.resize(K);
+    const uint32_t lmax = (1u << (32 - 2 * p)) - 2;
+    float lo = K ? sc[ids[0]] : 0.f, hi = lo;
+    for (uint32_t v : ids) lo = std::min(lo, sc[v]), hi = std::max(hi, sc[v]);
+    std::vector<uint32_t> vl(2 * (size_t)K);
+    for (uint32_t i = 0; i < K; i++) {
+        const float f = hi > lo ? (sc[ids[i]] - lo) / (hi - lo) : 0.f;
+        vl[2 * i] = ids[i];
+        vl[2 * i + 1] = 1 + std::min<uint32_t>(lmax - 1, (uint32_t)(f * (float)(lmax - 1)));
+    }
+    CK(ctx->ord_list.ensure(std::max<size_t>(vl.size(), 2) * 4));
+    CK(cudaMemcpyAsync(ctx->ord_list.p, vl.data(), vl.size() * 4, cudaMemcpyHostToDevice, ctx->s));
+    CK(ctx->ord_stage.ensure(np * 4ull));
+    uint32_t *ranks = ctx->ord_stage.as<uint32_t>();
+    const uint32_t g = (uint32_t)std::min<uint64_t>((np + 255) / 256, (uint64_t)ctx->sms * 8);
+    order_mix_kernel<<<g, 256, 0, ctx->s>>>(np, p, ranks);
+    LAUNCHED();
+    order_levels_kernel<<<(K + 255) / 256 + 1, 256, 0, ctx->s>>>(ctx->ord_list.as<uint2>(), K, p, ranks);
+    LAUNCHED();
+    if (lut_out) CK(cudaMemcpyAsync(lut_out, ranks, np * 4ull, cudaMemcpyDeviceToHost, ctx->s));
+    RET(install_order(ctx, ranks));
     return GKC_OK;
 }
 

@@ -167,4 +167,20 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T *total, T *ws) {
     return warp_prefix + x - v;
 }
 
+// ---------------------------------------------------------------------------
+// Tie-break of the learned order: a fixed bijection of `bits` bits (odd
+// multipliers are bijections modulo 2^bits, and so are xor-shifts).
+constexpr uint32_t ORDER_MIX_KEY = 0x5BD1E995u;
+
+__host__ __device__ __forceinline__ uint32_t mix_bits(uint32_t x, int bits, uint32_t key) {
+    const uint32_t mask = bits >= 32 ? 0xFFFFFFFFu : (1u << bits) - 1;
+    const int h = bits > 1 ? bits / 2 : 1;
+    x = (x ^ key) & mask;
+    x = (x * 0x9E3779B1u) & mask;
+    x ^= x >> h;
+    x = (x * 0x85EBCA77u) & mask;
+    x ^= x >> h;
+    return x;
+}
+
 }  // namespace gkc

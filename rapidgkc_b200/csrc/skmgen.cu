@@ -51,7 +51,8 @@ struct P1Params {
     int k, p;
     uint32_t P;
     uint64_t pmod;             // fastmod multiplier of P
-    const uint32_t *lut;       // 4^p ranks, or null for the default order
+    const uint32_t *lut;       // canonical order table: lut[v] = min(rank(v), rank(rc(v))),
+                               // or null for the default order
     int vec_ok;                // reads pointer is 16-byte aligned
     const int64_t *tile_read;  // [ntiles] read holding the tile's first staged base
     uint32_t *codes;           // [ntiles * P1_TILE_WORDS] packed 2-bit codes (out)
@@ -100,22 +101,29 @@ __global__ void tile_reads_kernel(const uint64_t *offs, int64_t n_reads, uint64_
     }
 }
 
-__device__ __forceinline__ uint32_t pmer_key(uint32_t v, int p, uint32_t pmask, const uint32_t *lut) {
-    if (lut) return __ldg(lut + v);
+// Default order: the p-mer's value, or the sentinel pmask when the
+// "rapidgkc" filter rejects it (minimizer_filter.h:20).
+__device__ __forceinline__ uint32_t pmer_key(uint32_t v, int p, uint32_t pmask) {
     return mm_valid(v, p) ? v : pmask;
 }
 
 // Minimizer key of k-mer q computed directly from global memory (used only
 // for superkmers that run past the staged halo).
+template <bool LUT>
 __device__ uint32_t kmer_key_global(const P1Params &a, uint64_t q) {
     const uint32_t pmask = 0xFFFFFFFFu >> (32 - 2 * a.p);
     uint32_t f = 0, best = 0xFFFFFFFFu;
     for (int j = 0; j < a.k; j++) {
         f = ((f << 2) | code1(a.reads[q + j])) & pmask;
         if (j >= a.p - 1) {
-            uint32_t r = rc32(f, a.p);
-            uint32_t kf = pmer_key(f, a.p, pmask, a.lut), kr = pmer_key(r, a.p, pmask, a.lut);
-            uint32_t m = kf < kr ? kf : kr;
+            uint32_t m;
+            if (LUT) {
+                m = __ldg(a.lut + f);
+            } else {
+                const uint32_t r = rc32(f, a.p);
+                const uint32_t kf = pmer_key(f, a.p, pmask), kr = pmer_key(r, a.p, pmask);
+                m = kf < kr ? kf : kr;
+            }
             best = m < best ? m : best;
         }
     }
@@ -159,9 +167,11 @@ __device__ __forceinline__ void emit_record(const P1Params &a, uint32_t *h, uint
     }
 }
 
-// LOG = log2 of the largest power of two <= w (the doubling levels).
-template <int LOG>
-__global__ void __launch_bounds__(P1_THREADS)
+// LOG = log2 of the largest power of two <= w (the doubling levels); LUT: the
+// key of a position is a.lut[p-mer] (an order table, already canonical), else
+// the default order over both strands.
+template <int LOG, bool LUT>
+__global__ void __launch_bounds__(P1_THREADS, 6)  // 6 CTAs (48 warps) per SM
 find_superkmers_kernel(P1Params a) {
     extern __shared__ uint32_t hist[];  // [3P]: bytes, superkmers, k-mers per partition
     __shared__ P1Smem sm;
@@ -196,7 +206,7 @@ find_superkmers_kernel(P1Params a) {
                 }
             }
             sm.codes[i] = word;
-            sm.rcodes[P1_CODE_WORDS - 1 - i] = rc16(word);
+            if (!LUT) sm.rcodes[P1_CODE_WORDS - 1 - i] = rc16(word);
             if (i >= 2 && i < 2 + P1_TILE_WORDS) a.codes[tile * P1_TILE_WORDS + (i - 2)] = word;
         }
         for (int i = threadIdx.x; i < P1_BM_WORDS; i += blockDim.x) sm.bm[i] = 0;
@@ -229,10 +239,11 @@ find_superkmers_kernel(P1Params a) {
         auto pk_at = [&](int j) -> uint32_t {  // canonical p-mer key at staged position j
             int i = j >> 4, o = j & 15;
             uint32_t f = __funnelshift_l(sm.codes[i + 1], sm.codes[i], 2 * o) >> shp;
+            if (LUT) return __ldg(a.lut + f);  // the table is canonical: one read
             int rj = P1_RC_BASES - j - p;  // reverse-complement p-mer start in rcodes
             int ri = rj >> 4, ro = rj & 15;
             uint32_t r = __funnelshift_l(sm.rcodes[ri + 1], sm.rcodes[ri], 2 * ro) >> shp;
-            uint32_t kf = pmer_key(f, p, pmask, a.lut), kr = pmer_key(r, p, pmask, a.lut);
+            uint32_t kf = pmer_key(f, p, pmask), kr = pmer_key(r, p, pmask);
             return kf < kr ? kf : kr;
         };
         auto bits_at = [&](int j) -> uint32_t {  // 32 boundary bits from staged position j
@@ -356,7 +367,7 @@ find_superkmers_kernel(P1Params a) {
                 int64_t r = read_of(a.offs, a.n_reads, (uint64_t)o_pos);
                 int64_t re = (int64_t)a.offs[r + 1];
                 int64_t e = c0 > o_pos + 1 ? c0 : o_pos + 1;
-                while (e + k <= re && kmer_key_global(a, (uint64_t)e) == o_key) e++;
+                while (e + k <= re && kmer_key_global<LUT>(a, (uint64_t)e) == o_key) e++;
                 int64_t after = re - (e + k - 1);
                 uint32_t tail = after >= 3 ? 3 : (uint32_t)after;
                 uint32_t slot = atomicAdd(&sm.region_n, 1u);
