@@ -13,7 +13,12 @@ seed (no public dataset is available).  Its 3 GB of reads exceed L2, so no L2
 flush is needed between steps.
 
 Reported (one JSON line on rank 0):
-  value      Gbp/s with the reads already in device memory (whole job, all ranks)
+  value      Gbp/s with the reads already in device memory (whole job, all ranks),
+             with the learned minimizer order (rapidgkc_b200/orders, trained on
+             skewed genomes of other seeds; --order default for the value order)
+  orders     the same timed steps with the default and the learned order:
+             Gbp/s, max/mean partition load, and whether the two (k-mer,
+             count) results are identical (order-independent checksums)
   e2e        Gbp/s through the C ABI from pinned host reads to host (k-mer,
              count) arrays, copies inside the timed region
   roofline   the dominant kernel class: algorithmic DRAM bytes per launch /
@@ -158,6 +163,8 @@ def main():
     ap.add_argument("--cpu-fraction", type=float, default=0.03)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--order", default="learned", choices=["learned", "default"],
+                    help="minimizer order of the reported value (the other is measured beside it)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -190,18 +197,37 @@ def main():
     stream = torch.cuda.Stream()
     c = KmerCounter(k=args.k, p=args.p, partitions=args.partitions, counter=args.counter, device=local)
     c.set_stream(stream)
+    learned_params = None
+    if args.order == "learned":
+        from rapidgkc_b200.order import default_order_path, load_order
+        learned_params = load_order(default_order_path(args.p))[0]
+
+    def set_order(name):
+        c.set_order(None)
+        if name == "learned":
+            c.mlp_order(learned_params)
 
     def step_device():
         return c.count_reads(d_reads, d_offs, args.cmin)
 
-    # ---- device-resident throughput ----
-    for _ in range(args.warmup):
-        n_out, n_dist = step_device()
-    torch.cuda.synchronize()
-    barrier()
-    launches0 = c.kernel_launches()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    def checksum():
+        """Order-independent digest of the (k-mer, count) result."""
+        km, ct = c.result()
+        return [int(np.bitwise_xor.reduce(km)) if len(km) else 0,
+                int(np.sum(km * ct.astype(np.uint64), dtype=np.uint64)), int(ct.sum(dtype=np.uint64))]
+
+    def timed_steps(name):
+        set_order(name)
+        c.store_clear()
+        c.add_reads(d_reads, d_offs)
+        pb, ps, pk = c.store_stats()
+        c.store_clear()
+        for _ in range(args.warmup):
+            step_device()
+        torch.cuda.synchronize()
+        barrier()
+        l0 = c.kernel_launches()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
         torch.cuda.synchronize()
         ev0.record(stream)
@@ -210,11 +236,33 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    launches = (c.kernel_launches() - launches0) // args.steps
-    tstats = c.timings()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return {"gbps": bases * world / (ms / 1e3) / 1e9, "ms_per_step": ms,
+                "maxmean_kmers": float(pk.max() / pk.mean()), "maxmean_bytes": float(pb.max() / pb.mean()),
+                "superkmers": int(ps.sum()), "store_bytes": int(pb.sum()), "kept": n_out, "distinct": n_dist,
+                "launches": (c.kernel_launches() - l0) // args.steps, "timings": c.timings(),
+                "checksum": checksum()}
+
+    # ---- device-resident throughput, default order, then the learned one ----
+    names = ["default"] + (["learned"] if learned_params is not None else [])
+    with ClockSampler(local) as clk:
+        runs = {nm: timed_steps(nm) for nm in names}
+    main_run = runs[args.order]
+    ms, launches, tstats = main_run["ms_per_step"], main_run["launches"], main_run["timings"]
+    n_out, n_dist = main_run["kept"], main_run["distinct"]
+    value = main_run["gbps"]
+    orders = {nm: {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()
+                   if k not in ("timings", "checksum", "launches")} for nm, r in runs.items()}
+    if len(runs) == 2:
+        orders["bit_exact"] = runs["default"]["checksum"] == runs["learned"]["checksum"]
+        orders["speedup"] = runs["learned"]["gbps"] / runs["default"]["gbps"]
     # per-kernel-class device times: the same steps again with every launch
-    # bracketed by events (kept out of the timed region above)
+    # bracketed by events (kept out of the timed regions above)
+    set_order(args.order)
     c.set_profiling(True)
     c.kernel_stats(reset=True)
     for _ in range(args.steps):
@@ -222,11 +270,6 @@ def main():
     torch.cuda.synchronize()
     kstats = c.kernel_stats(reset=True)
     c.set_profiling(False)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = bases * world / (ms / 1e3) / 1e9
 
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
@@ -271,13 +314,13 @@ def main():
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": args.workload, "desc": WORKLOAD_DESC.get(args.workload, ""),
                        "bases_per_rank": bases, "reads_per_rank": len(offs) - 1, "k": args.k, "p": args.p,
-                       "partitions": args.partitions, "counter": args.counter, "order": "default",
+                       "partitions": args.partitions, "counter": args.counter, "order": args.order,
                        "threshold": f">={args.cmin}", "parallelism": f"dp{world} (independent read sets)",
                        "l2": "inputs (3 GB) larger than L2; no flush", "kmers_kept": n_out,
                        "distinct": n_dist, "gen_s": round(t_gen, 1),
                        "sub_buckets": tstats["sub_buckets"], "overflowed": tstats["overflowed_sub_buckets"],
                        "phase1_ms": round(tstats["phase1_ms"], 2), "phase2_ms": round(tstats["phase2_ms"], 2)},
-            "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches)}
+            "orders": orders, "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches)}
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s
