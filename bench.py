@@ -243,7 +243,8 @@ def main():
             ms = float(t.item())
         return {"gbps": bases * world / (ms / 1e3) / 1e9, "ms_per_step": ms,
                 "maxmean_kmers": float(pk.max() / pk.mean()), "maxmean_bytes": float(pb.max() / pb.mean()),
-                "superkmers": int(ps.sum()), "store_bytes": int(pb.sum()), "kept": n_out, "distinct": n_dist,
+                "superkmers": int(ps.sum()), "store_bytes": int(pb.sum()), "kmer_instances": int(pk.sum()),
+                "kept": n_out, "distinct": n_dist,
                 "launches": (c.kernel_launches() - l0) // args.steps, "timings": c.timings(),
                 "checksum": checksum()}
 
@@ -298,6 +299,19 @@ def main():
 
     # ---- roofline of the dominant kernel class ----
     hbm, src = peaks()
+    # counting phase (phase 2) against byte models: the compulsory traffic
+    # (superkmer bytes read once + 12-byte output records) and the LSD-sort
+    # path's (superkmers + 8 B key write + 16 B per k-mer per 8-bit digit pass
+    # over 2k bits + 8 B run-length read + output)
+    N, S = main_run["kmer_instances"], main_run["store_bytes"]
+    p2 = tstats["phase2_ms"] / 1e3
+    passes = -(-2 * args.k // 8)
+    comp = S + 12 * n_out
+    sort_model = S + 8 * N + 16 * N * passes + 8 * N + 12 * n_out
+    counting = {"ms_per_step": tstats["phase2_ms"], "kmer_instances": N, "store_bytes": S,
+                "compulsory_bytes": comp, "compulsory_gbs": comp / p2 / 1e9,
+                "sort_model_bytes": sort_model, "sort_model_gbs": sort_model / p2 / 1e9,
+                "sort_model_frac": sort_model / p2 / 1e9 / hbm, "peak_gbs": hbm}
     dom = max(kstats, key=lambda k: kstats[k][0])
     kms, kl, kb = kstats[dom]
     per_launch_s = kms / 1e3 / max(kl, 1)
@@ -320,7 +334,8 @@ def main():
                        "distinct": n_dist, "gen_s": round(t_gen, 1),
                        "sub_buckets": tstats["sub_buckets"], "overflowed": tstats["overflowed_sub_buckets"],
                        "phase1_ms": round(tstats["phase1_ms"], 2), "phase2_ms": round(tstats["phase2_ms"], 2)},
-            "orders": orders, "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches)}
+            "orders": orders, "roofline": roofline, "counting_phase": counting, "e2e": e2e,
+            "gpu_launches": int(launches)}
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s

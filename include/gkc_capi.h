@@ -14,6 +14,7 @@
  *   gkc_store_stats  SKMStoreNoncon counters  skmstore.hpp:85-87
  *   gkc_store_export SKMStoreNoncon bytes     skmstore.hpp:156-187, 222-236
  *   gkc_count        kmc_counting_GPU_streams gpu_kmercounting.h:14-17, gpu_kmercounting.cu:343-548
+ *   gkc_count_partitions  the same, on the store subset one call is given
  *   gkc_result       the kmc_result vectors   gkc_main.cpp:294, gpu_kmercounting.cu:505-508
  * and add what the reference declares but never does: the count threshold
  * [min, max] (utilities.hpp:190) and an output of the counted k-mers.
@@ -100,6 +101,15 @@ int gkc_store_clear(gkc_ctx *ctx);
  * Output order: partition by partition; ascending k-mer inside a partition
  * with the sort counter, unordered with the hash counter. */
 int gkc_count(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, uint64_t *n_out, uint64_t *n_distinct);
+
+/* Phase 2 on some partitions: counts partitions parts[0..n) of the store
+ * (each at most once per store), as kmc_counting_GPU_streams counts the stores
+ * it is given (gpu_kmercounting.h:14-17, called per store subset by
+ * gkc_main.cpp:113).  The result replaces the previous one (gkc_result); the
+ * store is released once every partition has been counted.  Adding reads to
+ * a partly counted store, or counting a partition twice, is GKC_ESTATE. */
+int gkc_count_partitions(gkc_ctx *ctx, const int32_t *parts, uint64_t n, uint32_t cmin, uint32_t cmax,
+                         uint64_t *n_out, uint64_t *n_distinct);
 
 /* Copies the last gkc_count result: kmers[i] (2-bit, first base in the most
  * significant position, canonical) and counts[i], i < min(cap, n_out). */

@@ -29,7 +29,7 @@ UINT32_MAX = 0xFFFFFFFF
 EXPORTS = (
     "gkc_default_options", "gkc_create", "gkc_destroy", "gkc_last_error", "gkc_strerror",
     "gkc_set_order", "gkc_add_reads", "gkc_store_stats", "gkc_store_export", "gkc_store_clear",
-    "gkc_count", "gkc_result", "gkc_result_device", "gkc_count_reads", "gkc_count_keys",
+    "gkc_count", "gkc_count_partitions", "gkc_result", "gkc_result_device", "gkc_count_reads", "gkc_count_keys",
     "gkc_last_timings", "gkc_kernel_launches", "gkc_set_stream", "gkc_set_profiling", "gkc_kernel_stats",
     "gkc_mlp_param_count", "gkc_minimizer_loads", "gkc_mlp_grad", "gkc_mlp_train", "gkc_mlp_scores",
     "gkc_mlp_order",
@@ -85,6 +85,7 @@ def load_library(path: str = LIB_PATH):
     L.gkc_store_export.argtypes = [vp, i32, vp, u64, C.POINTER(u64)]
     L.gkc_store_clear.argtypes = [vp]
     L.gkc_count.argtypes = [vp, u32, u32, C.POINTER(u64), C.POINTER(u64)]
+    L.gkc_count_partitions.argtypes = [vp, vp, u64, u32, u32, C.POINTER(u64), C.POINTER(u64)]
     L.gkc_result.argtypes = [vp, vp, vp, u64, i32]
     L.gkc_result_device.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(u64)]
     L.gkc_count_reads.argtypes = [vp, vp, vp, u64, i32, u32, u32, vp, vp, u64, i32, C.POINTER(u64),
@@ -208,6 +209,14 @@ class KmerCounter:
         """Counts the store; returns (kept, distinct)."""
         no, nd = C.c_uint64(0), C.c_uint64(0)
         self._check(self._L.gkc_count(self._h, cmin, cmax, C.byref(no), C.byref(nd)))
+        return no.value, nd.value
+
+    def count_partitions(self, parts, cmin: int = 1, cmax: int = UINT32_MAX):
+        """Counts only partitions `parts` of the store; returns (kept, distinct)."""
+        a = np.ascontiguousarray(parts, np.int32)
+        no, nd = C.c_uint64(0), C.c_uint64(0)
+        self._check(self._L.gkc_count_partitions(self._h, _ptr(a)[0], len(a), cmin, cmax, C.byref(no),
+                                                 C.byref(nd)))
         return no.value, nd.value
 
     def result(self, n: int | None = None):

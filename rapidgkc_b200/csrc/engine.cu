@@ -169,6 +169,7 @@ struct gkc_ctx {
     DevBuf out_k, out_c;
     uint64_t out_cap = 0, n_out = 0, n_distinct = 0;
     bool has_result = false;
+    std::vector<char> counted;  // partitions already counted by gkc_count_partitions
     DevBuf keysA, keysB, tiles, counts, offsets, blocksums, heads_pos, heads_key, tilecnt, tileoff;
     DevBuf segoff, segcur, part_err, scal;
     DevBuf stage_bytes, stage_idx;
@@ -755,7 +756,8 @@ int count_buckets_records(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const 
 // stores are counted in one group; a spilled store in groups of partitions
 // whose superkmers fit the device staging budget.
 
-int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
+// want: the partitions to count (null: all)
+int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<char> *want) {
     const uint32_t P = (uint32_t)ctx->opt.partitions;
     std::vector<uint64_t> np(P, 0), nbp(P, 0), nsp(P, 0);
     bool spilled = false;
@@ -811,9 +813,14 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
     float acc_ms = 0;
     uint32_t p0 = 0;
     while (p0 < P) {
+        if (want && !(*want)[p0]) {
+            p0++;
+            continue;
+        }
         uint32_t p1 = p0;
         uint64_t gb = 0, gs = 0;  // staged bytes, superkmers of the group
-        while (p1 < P && (p1 == p0 || gb + nbp[p1] + 12 * nsp[p1] + 16 * nsp[p1] <= budget)) {
+        while (p1 < P && (!want || (*want)[p1]) &&
+               (p1 == p0 || gb + nbp[p1] + 12 * nsp[p1] + 16 * nsp[p1] <= budget)) {
             gb += nbp[p1] + 12 * nsp[p1];
             gs += nsp[p1];
             p1++;
@@ -1056,7 +1063,7 @@ int sort_and_reduce(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n,
     }
 }
 
-int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
+int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<char> *want) {
     const uint32_t P = (uint32_t)ctx->opt.partitions;
     std::vector<uint64_t> np(P, 0);
     for (auto *c : ctx->store)
@@ -1072,9 +1079,13 @@ int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax) {
     float sort_ms = 0;
     uint32_t p0 = 0;
     while (p0 < P) {
+        if (want && !(*want)[p0]) {
+            p0++;
+            continue;
+        }
         uint32_t p1 = p0;
         uint64_t n = 0;
-        while (p1 < P && (p1 == p0 || n + np[p1] <= budget)) n += np[p1++];
+        while (p1 < P && (!want || (*want)[p1]) && (p1 == p0 || n + np[p1] <= budget)) n += np[p1++];
         std::vector<uint64_t> segoff(P, 0), segs;
         uint64_t o = 0;
         for (uint32_t p = p0; p < p1; p++) { segoff[p] = o; o += np[p]; segs.push_back(np[p]); }
@@ -1255,6 +1266,8 @@ int gkc_set_order(gkc_ctx *ctx, const uint32_t *lut, uint64_t n, int mem) {
 int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads, int mem) {
     if (!ctx || (!reads && n_reads) || !offs) return GKC_EINVAL;
     CK(cudaSetDevice(ctx->device));
+    for (char c : ctx->counted)
+        if (c) return ctx->fail(GKC_ESTATE, "the store is partly counted; clear it before adding reads");
     ctx->times[0] = ctx->times[1] = 0;
     if (n_reads == 0) return GKC_OK;
     if (mem == GKC_MEM_DEVICE) {
@@ -1377,11 +1390,18 @@ int gkc_store_clear(gkc_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->s);
     ctx->clear_store();  // buffers stay pooled for the next batch
+    ctx->counted.assign(ctx->counted.size(), 0);
     return GKC_OK;
 }
 
-int gkc_count(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, uint64_t *n_out, uint64_t *n_distinct) {
-    if (!ctx || cmin > cmax) return GKC_EINVAL;
+}  // extern "C"
+
+namespace {
+
+// Counts the partitions `want` (null: all) of the store; the result replaces
+// the previous one.
+int count_store(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<char> *want, uint64_t *n_out,
+                uint64_t *n_distinct) {
     CK(cudaSetDevice(ctx->device));
     ctx->n_out = 0;
     ctx->n_distinct = 0;
@@ -1390,7 +1410,8 @@ int gkc_count(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, uint64_t *n_out, uint6
     CK(cudaEventCreate(&t0));
     CK(cudaEventCreate(&t1));
     CK(cudaEventRecord(t0, ctx->s));
-    int rc = ctx->opt.counter == GKC_COUNTER_HASH ? count_hash(ctx, cmin, cmax) : count_sort(ctx, cmin, cmax);
+    int rc = ctx->opt.counter == GKC_COUNTER_HASH ? count_hash(ctx, cmin, cmax, want)
+                                                  : count_sort(ctx, cmin, cmax, want);
     cudaEventRecord(t1, ctx->s);
     cudaEventSynchronize(t1);
     float ms = 0;
@@ -1398,11 +1419,46 @@ int gkc_count(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, uint64_t *n_out, uint6
     ctx->times[2] = ms;
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
-    gkc_store_clear(ctx);
     if (rc != GKC_OK) return rc;
     ctx->has_result = true;
     if (n_out) *n_out = ctx->n_out;
     if (n_distinct) *n_distinct = ctx->n_distinct;
+    return GKC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gkc_count(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, uint64_t *n_out, uint64_t *n_distinct) {
+    if (!ctx || cmin > cmax) return GKC_EINVAL;
+    for (char c : ctx->counted)
+        if (c) return ctx->fail(GKC_ESTATE, "partitions of this store were counted already");
+    const int rc = count_store(ctx, cmin, cmax, nullptr, n_out, n_distinct);
+    gkc_store_clear(ctx);
+    return rc;
+}
+
+int gkc_count_partitions(gkc_ctx *ctx, const int32_t *parts, uint64_t n, uint32_t cmin, uint32_t cmax,
+                         uint64_t *n_out, uint64_t *n_distinct) {
+    if (!ctx || cmin > cmax || (!parts && n)) return GKC_EINVAL;
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    if (ctx->counted.size() != P) ctx->counted.assign(P, 0);
+    std::vector<char> want(P, 0);
+    for (uint64_t i = 0; i < n; i++) {
+        if (parts[i] < 0 || (uint32_t)parts[i] >= P) return ctx->fail(GKC_EINVAL, "partition %d out of range", parts[i]);
+        if (ctx->counted[parts[i]] || want[parts[i]])
+            return ctx->fail(GKC_ESTATE, "partition %d counted twice", parts[i]);
+        want[parts[i]] = 1;
+    }
+    const int rc = count_store(ctx, cmin, cmax, &want, n_out, n_distinct);
+    if (rc != GKC_OK) return rc;
+    bool all = true;
+    for (uint32_t p = 0; p < P; p++) {
+        ctx->counted[p] |= want[p];
+        all &= ctx->counted[p] != 0;
+    }
+    if (all) gkc_store_clear(ctx);  // every partition is counted: release the store
     return GKC_OK;
 }
 

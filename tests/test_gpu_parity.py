@@ -230,3 +230,31 @@ def test_heavy_and_overflowing_sub_buckets(oracle):
         t = c.timings()
     assert t["overflowed_sub_buckets"] >= 2  # the (AT)n minimizer may share a sub-bucket
     assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+
+
+@pytest.mark.parametrize("kind", ["hash", "sort"])
+def test_count_partitions_subsets(oracle, kind):
+    """Counting a store in disjoint partition subsets (as the reference's
+    phase-2 workers do) gives each subset's k-mers; together the oracle's."""
+    k, p, P = 31, 11, 32
+    reads, offs = random_reads(51, 80_000, 6000, 150, 0.005)
+    _, _, _, po, stream = oracle.skmgen(reads, offs, k, p, P)
+    per = [oracle.count(oracle.extract(stream[int(po[q]):int(po[q + 1])], k), 1, U32) for q in range(P)]
+    subsets = [np.arange(0, P, 3), np.arange(1, P, 3), np.arange(2, P, 3)]
+    with counter(k, p, P, kind) as c:
+        c.add_reads(reads, offs)
+        tot = 0
+        for i, sub in enumerate(subsets):
+            n, d = c.count_partitions(sub)
+            km, ct = sorted_table(*c.result())
+            rk, rc = sorted_table(np.concatenate([per[q][0] for q in sub]), np.concatenate([per[q][1] for q in sub]))
+            assert d == sum(per[q][2] for q in sub)
+            assert np.array_equal(km, rk) and np.array_equal(ct, rc)
+            tot += d
+            if i == 0:
+                with pytest.raises(Exception):
+                    c.count_partitions([int(sub[0])])        # counted twice
+                with pytest.raises(Exception):
+                    c.add_reads(reads, offs)                  # store partly counted
+        assert tot == sum(x[2] for x in per)
+        assert c.store_stats()[2].sum() == 0                  # released after the last subset
