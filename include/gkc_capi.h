@@ -35,7 +35,8 @@ enum {
     GKC_ECUDA = -2,     /* CUDA runtime error */
     GKC_ENOMEM = -3,    /* device or pinned memory exhausted */
     GKC_ESTATE = -4,    /* call out of order (e.g. result before count) */
-    GKC_EINTERNAL = -5  /* retries exhausted or inconsistent internal state */
+    GKC_EINTERNAL = -5, /* retries exhausted or inconsistent internal state */
+    GKC_ELIMIT = -6     /* input or output larger than a fixed-size limit */
 };
 
 enum { GKC_COUNTER_SORT = 0, GKC_COUNTER_HASH = 1 };
@@ -209,6 +210,31 @@ int gkc_mlp_scores(gkc_ctx *ctx, const float *params, float *scores, int mem);
  * (optional, host, 4^p entries) receives the rank table (what gkc_set_order
  * would take for the same order). */
 int gkc_mlp_order(gkc_ctx *ctx, const float *params, uint64_t heavy, uint32_t *lut_out);
+
+/* ---- counting without allocation ----------------------------------------
+ * No counterpart in the reference.  gkc_count_keys_noalloc counts raw 64-bit
+ * keys like gkc_count_keys with the hash counter, but needs no context and
+ * allocates nothing: its scratch is a fixed table in the library's device
+ * memory (16 MiB, GKC_NOALLOC_SLOTS slots), which limits it to n <=
+ * GKC_NOALLOC_MAX_KEYS keys; larger n returns GKC_ELIMIT before any work.
+ * For callers that must not allocate device memory, e.g. code that already
+ * holds its own memory pool or runs where cudaMalloc / cudaFree would
+ * synchronise the device mid-pipeline.
+ *   keys         device memory, n keys, none equal to 2^64-1 (GKC_EINVAL)
+ *   out_kmers / out_counts  device memory of out_cap entries: the keys whose
+ *                count c satisfies cmin <= c <= cmax, unordered; if more than
+ *                out_cap qualify, returns GKC_ELIMIT with *n_out = the number
+ *   stream       a cudaStream_t of the current device (NULL: the default
+ *                stream); the call returns after the stream's work is done
+ * Runs on the current CUDA device.  The first call on a device looks up the
+ * scratch's address (cudaGetSymbolAddress); make that first call outside any
+ * stream capture.  All calls on one device share the one scratch table, so
+ * two calls in flight at the same time (other host threads, other streams)
+ * race and give wrong results: the caller serialises them. */
+enum { GKC_NOALLOC_SLOTS = 1 << 20, GKC_NOALLOC_MAX_KEYS = 1 << 19 };
+int gkc_count_keys_noalloc(const uint64_t *keys, uint64_t n, uint32_t cmin, uint32_t cmax, uint64_t *out_kmers,
+                           uint32_t *out_counts, uint64_t out_cap, uint64_t *n_out, uint64_t *n_distinct,
+                           void *stream);
 
 #ifdef __cplusplus
 }

@@ -20,7 +20,7 @@ import numpy as np
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "librapidgkc_b200.so")
 
-GKC_OK, GKC_EINVAL, GKC_ECUDA, GKC_ENOMEM, GKC_ESTATE, GKC_EINTERNAL = 0, -1, -2, -3, -4, -5
+GKC_OK, GKC_EINVAL, GKC_ECUDA, GKC_ENOMEM, GKC_ESTATE, GKC_EINTERNAL, GKC_ELIMIT = 0, -1, -2, -3, -4, -5, -6
 COUNTER_SORT, COUNTER_HASH = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
 UINT32_MAX = 0xFFFFFFFF
@@ -32,7 +32,7 @@ EXPORTS = (
     "gkc_count", "gkc_count_partitions", "gkc_result", "gkc_result_device", "gkc_count_reads", "gkc_count_keys",
     "gkc_last_timings", "gkc_kernel_launches", "gkc_set_stream", "gkc_set_profiling", "gkc_kernel_stats",
     "gkc_mlp_param_count", "gkc_minimizer_loads", "gkc_mlp_grad", "gkc_mlp_train", "gkc_mlp_scores",
-    "gkc_mlp_order",
+    "gkc_mlp_order", "gkc_count_keys_noalloc",
 )
 KERNEL_CLASSES = ("find_superkmers", "scatter_superkmers", "hash_insert", "hash_collect", "sort_extract",
                   "radix_hist", "radix_scatter", "scan", "rle")
@@ -105,6 +105,7 @@ def load_library(path: str = LIB_PATH):
     L.gkc_mlp_train.argtypes = [vp, vp, vp, vp, i32, i32, f32, u64, C.POINTER(f32)]
     L.gkc_mlp_scores.argtypes = [vp, vp, vp, i32]
     L.gkc_mlp_order.argtypes = [vp, vp, u64, vp]
+    L.gkc_count_keys_noalloc.argtypes = [vp, u64, u32, u32, vp, vp, u64, C.POINTER(u64), C.POINTER(u64), vp]
     for name in EXPORTS:
         if name not in ("gkc_default_options", "gkc_last_error", "gkc_strerror", "gkc_kernel_launches",
                         "gkc_mlp_param_count"):

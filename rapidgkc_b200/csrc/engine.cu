@@ -1193,6 +1193,7 @@ const char *gkc_strerror(int code) {
         case GKC_ENOMEM: return "out of memory";
         case GKC_ESTATE: return "invalid call order";
         case GKC_EINTERNAL: return "internal error";
+        case GKC_ELIMIT: return "larger than a fixed-size limit";
         default: return "unknown error";
     }
 }
@@ -1840,3 +1841,5 @@ int gkc_mlp_order(gkc_ctx *ctx, const float *params, uint64_t heavy, uint32_t *l
 }
 
 }  // extern "C"
+
+#include "count_noalloc.cu"
