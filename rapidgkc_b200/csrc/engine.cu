@@ -155,6 +155,7 @@ struct gkc_ctx {
     DevBuf reads[2], offs[2];
     PinBuf offs_pin[2];
     cudaEvent_t buf_free[2] = {nullptr, nullptr}, buf_ready[2] = {nullptr, nullptr};
+    DevBuf cta_hist, cta_base;  // phase 1: per-CTA partition counts and base offsets
     DevBuf records, region_count, hist, flags, cursors, part_off, tile_read, codes;
     PinBuf h_hist, h_flags;
     DevBuf lut;             // canonical order table: min(rank(v), rank(rc(v)))
@@ -199,7 +200,8 @@ struct gkc_ctx {
         for (auto *c : pool) delete_chunk(c);
         store.clear();
         pool.clear();
-        DevBuf *ds[] = {&reads[0], &reads[1], &offs[0], &offs[1], &records, &region_count, &hist, &flags,
+        DevBuf *ds[] = {&reads[0], &reads[1], &offs[0], &offs[1], &records, &region_count, &cta_hist, &cta_base,
+                        &hist, &flags,
                         &cursors, &part_off, &tile_read, &codes, &lut, &table, &out_k, &out_c, &keysA, &keysB, &tiles,
                         &counts, &offsets, &blocksums, &heads_pos, &heads_key, &tilecnt, &tileoff, &segoff,
                         &segcur, &part_err, &scal, &stage_bytes, &stage_idx, &spill_bytes, &spill_idx, &spill_keys,
@@ -370,6 +372,8 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     uint64_t cap = tiles_per_cta * P1_TILE / 4 + 4096;
     const uint64_t cap_max = tiles_per_cta * P1_TILE + 64;
     CK(ctx->region_count.ensure(grid * sizeof(uint32_t)));
+    CK(ctx->cta_hist.ensure(2ull * P * grid * sizeof(uint32_t)));
+    CK(ctx->cta_base.ensure(2ull * P * grid * sizeof(unsigned long long)));
     CK(ctx->hist.ensure(3ull * P * sizeof(unsigned long long)));
     CK(ctx->flags.ensure(64));
     CK(ctx->h_hist.ensure(3ull * P * sizeof(unsigned long long)));
@@ -408,10 +412,12 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
         a.part_bytes = hist;
         a.part_skms = hist + P;
         a.part_kmers = hist + 2 * P;
+        a.cta_hist = ctx->cta_hist.as<uint32_t>();
         a.err = ctx->flags.as<uint32_t>();
         CK(cudaEventRecord(ctx->e0, ctx->s));
         {
-            KScope ks(ctx, GKC_K_FIND_SUPERKMERS, (double)total + 8.0 * (n_reads + 1));
+            // reads + offsets in, 2-bit codes out (records are added below)
+            KScope ks(ctx, GKC_K_FIND_SUPERKMERS, 1.25 * (double)total + 8.0 * (n_reads + 1));
             kfind<<<grid, P1_THREADS, dyn, ctx->s>>>(a);
             LAUNCHED();
         }
@@ -466,8 +472,13 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     c->keys = dk.as<uint32_t>();
     CK(cudaMemcpyAsync(c->d_byte_off.p, c->byte_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
     CK(cudaMemcpyAsync(c->d_skm_off.p, c->skm_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
-    CK(ctx->cursors.ensure(2ull * P * sizeof(unsigned long long)));
-    CK(cudaMemsetAsync(ctx->cursors.p, 0, 2ull * P * sizeof(unsigned long long), ctx->s));
+    {
+        KScope ks(ctx, GKC_K_SCAN, 24.0 * P * grid);
+        cta_offsets_kernel<<<(P + 127) / 128, 128, 0, ctx->s>>>(
+            ctx->cta_hist.as<uint32_t>(), grid, P, c->d_byte_off.as<unsigned long long>(),
+            c->d_skm_off.as<unsigned long long>(), ctx->cta_base.as<unsigned long long>());
+        LAUNCHED();
+    }
     P2Params b;
     b.codes = ctx->codes.as<uint32_t>();
     b.records = ctx->records.as<SkmRecord>();
@@ -477,16 +488,15 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     b.P = P;
     b.pmod = fastmod_m(P);
     b.part_byte_off = c->d_byte_off.as<unsigned long long>();
-    b.part_skm_off = c->d_skm_off.as<unsigned long long>();
-    b.cur_bytes = ctx->cursors.as<unsigned long long>();
-    b.cur_skms = ctx->cursors.as<unsigned long long>() + P;
+    b.cta_base = ctx->cta_base.as<unsigned long long>();
     b.bytes = c->bytes;
     b.idx = c->idx;
     b.keys = c->keys;
     size_t dyn2 = 2ull * P * (sizeof(unsigned long long) + sizeof(uint32_t));
     CK(cudaFuncSetAttribute(scatter_superkmers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn2));
     {
-        KScope ks(ctx, GKC_K_SCATTER, 24.0 * c->nskm + (double)total + (double)c->nbytes);
+        // records (16 B) and codes in; superkmer bytes, index (8 B) and keys (4 B) out
+        KScope ks(ctx, GKC_K_SCATTER, 28.0 * c->nskm + 0.25 * (double)total + (double)c->nbytes);
         scatter_superkmers_kernel<<<grid, P2_THREADS, dyn2, ctx->s>>>(b);
         LAUNCHED();
     }

@@ -2,9 +2,9 @@
 //
 // Replaces the reference's GPU_GenMinimizer / GPU_GenSKMOffs /
 // GPU_ReadCompression / GPU_ExtractSKM chain (gpu_skmgen.cu:218-470) and the
-// host round trip per 2048-read batch (gpu_skmgen.cu:504-718).
+// host round trip per 2000-read batch (gpu_skmgen.cu:504-718).
 //
-// Kernel 0 (tile_reads) finds, for every tile of 2048 bases, the read that
+// Kernel 0 (tile_reads) finds, for every tile of 4096 bases, the read that
 // holds the tile's first staged base (one binary search per tile, all tiles in
 // parallel).
 //
@@ -20,10 +20,13 @@
 // next start or invalid position; both are ballots over the chunk, and the
 // lanes where a superkmer ends write its record (begin, k-mer count, key,
 // packing phase, trailing bases) into a per-CTA region and add it to
-// per-partition byte/superkmer/k-mer counts in shared memory.
+// per-partition byte/superkmer/k-mer counts in shared memory, which the CTA
+// also writes out (cta_hist).
 //
-// Kernel 2 (scatter_superkmers) reserves, per CTA and per partition, a
-// contiguous range of each partition's byte and index buffers, then writes
+// cta_offsets_kernel lays out, from those counts, each CTA's contiguous range
+// of every partition's byte and index buffers (CTA order: deterministic).
+//
+// Kernel 2 (scatter_superkmers) makes one pass over a CTA's records and writes
 // every superkmer in the reference's 3-bases-per-byte format
 // (cpu_funcs.cpp:200-250): a copy of the packed read whose first byte's
 // header says 3-beg%3 valid bases and whose last byte's header says
@@ -34,9 +37,9 @@ namespace gkc {
 
 constexpr int P1_WARPS = 8;
 constexpr int P1_THREADS = P1_WARPS * 32;
-constexpr int P1_CHUNKS = 8;                          // chunks of 32 positions per warp strip
-constexpr int P1_STRIP = 32 * P1_CHUNKS;              // 256 positions
-constexpr int P1_TILE = P1_WARPS * P1_STRIP;          // 2048 positions per tile
+constexpr int P1_CHUNKS = 16;                         // chunks of 32 positions per warp strip
+constexpr int P1_STRIP = 32 * P1_CHUNKS;              // 512 positions
+constexpr int P1_TILE = P1_WARPS * P1_STRIP;          // 4096 positions per tile
 constexpr int P1_TILE_WORDS = P1_TILE / 16;           // packed code words per tile
 constexpr int P1_HALO = 512;                          // staged positions past the tile
 constexpr int P1_STAGE = P1_TILE + 32 + P1_HALO + 128;  // staged positions (from tile-32)
@@ -60,6 +63,7 @@ struct P1Params {
     uint32_t region_cap;
     uint32_t *region_count;    // [gridDim.x]
     unsigned long long *part_bytes, *part_skms, *part_kmers;  // [P]
+    uint32_t *cta_hist;        // [gridDim.x][2P]: this CTA's bytes, then superkmers, per partition
     uint32_t *err;
 };
 
@@ -377,7 +381,10 @@ find_superkmers_kernel(P1Params a) {
         }
     }
     __syncthreads();
+    uint32_t *ch = a.cta_hist + (uint64_t)blockIdx.x * 2 * a.P;
     for (uint32_t i = threadIdx.x; i < a.P; i += blockDim.x) {
+        ch[i] = hist[i];
+        ch[a.P + i] = hist[a.P + i];
         if (hist[a.P + i]) {
             atomicAdd(a.part_bytes + i, (unsigned long long)hist[i]);
             atomicAdd(a.part_skms + i, (unsigned long long)hist[a.P + i]);
@@ -385,6 +392,24 @@ find_superkmers_kernel(P1Params a) {
         }
     }
     if (threadIdx.x == 0) a.region_count[blockIdx.x] = sm.region_n;
+}
+
+// Per-CTA base offsets in every partition: CTA c's range of partition p
+// starts after the bytes (superkmers) of CTAs 0..c-1 in p.  One thread per
+// partition walks the CTAs in order, so the layout is deterministic.
+__global__ void cta_offsets_kernel(const uint32_t *cta_hist, uint32_t ncta, uint32_t P,
+                                   const unsigned long long *part_byte_off, const unsigned long long *part_skm_off,
+                                   unsigned long long *cta_base) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        unsigned long long b = part_byte_off[p], s = part_skm_off[p];
+        for (uint32_t c = 0; c < ncta; c++) {
+            const uint64_t o = (uint64_t)c * 2 * P;
+            cta_base[o + p] = b;
+            cta_base[o + P + p] = s;
+            b += cta_hist[o + p];
+            s += cta_hist[o + P + p];
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -398,14 +423,15 @@ struct P2Params {
     uint32_t P;
     uint64_t pmod;
     const unsigned long long *part_byte_off;  // [P] partition start in `bytes`
-    const unsigned long long *part_skm_off;   // [P] partition start in `idx`
-    unsigned long long *cur_bytes, *cur_skms;  // [P] zeroed cursors
+    const unsigned long long *cta_base;       // [gridDim.x][2P] this CTA's first byte, superkmer per partition
     uint8_t *bytes;
     uint64_t *idx;
     uint32_t *keys;  // minimizer key of each superkmer, indexed like idx
 };
 
-constexpr int P2_THREADS = 512;
+// One thread per record at a time; 1024-thread CTAs timed faster than
+// 256 x 6 or 512 x 3 with their register caps.
+constexpr int P2_THREADS = 1024;
 
 __global__ void __launch_bounds__(P2_THREADS)
 scatter_superkmers_kernel(P2Params a) {
@@ -413,21 +439,12 @@ scatter_superkmers_kernel(P2Params a) {
     uint32_t *lcnt = reinterpret_cast<uint32_t *>(sbase + 2 * a.P);  // [2P] CTA-local cursors
     const uint32_t n = a.region_count[blockIdx.x] < a.region_cap ? a.region_count[blockIdx.x] : a.region_cap;
     const SkmRecord *rec = a.records + (uint64_t)blockIdx.x * a.region_cap;
-    for (uint32_t i = threadIdx.x; i < 2 * a.P; i += blockDim.x) lcnt[i] = 0;
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        SkmRecord r = rec[i];
-        uint32_t part = fastmod(~r.key, a.pmod, a.P);
-        atomicAdd(&lcnt[part], skm_nbytes(rec_phase(r.pos), r.len, a.k));
-        atomicAdd(&lcnt[a.P + part], 1u);
-    }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < a.P; i += blockDim.x) {
-        uint32_t nbp = lcnt[i], nsp = lcnt[a.P + i];
-        sbase[i] = a.part_byte_off[i] + (nbp ? atomicAdd(a.cur_bytes + i, (unsigned long long)nbp) : 0ull);
-        sbase[a.P + i] = a.part_skm_off[i] + (nsp ? atomicAdd(a.cur_skms + i, (unsigned long long)nsp) : 0ull);
+    // this CTA's ranges, laid out by cta_offsets_kernel from the find kernel's
+    // per-CTA counts: one pass over the records
+    const unsigned long long *cb = a.cta_base + (uint64_t)blockIdx.x * 2 * a.P;
+    for (uint32_t i = threadIdx.x; i < 2 * a.P; i += blockDim.x) {
+        sbase[i] = cb[i];
         lcnt[i] = 0;
-        lcnt[a.P + i] = 0;
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
