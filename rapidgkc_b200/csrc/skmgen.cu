@@ -447,57 +447,93 @@ scatter_superkmers_kernel(P2Params a) {
         lcnt[i] = 0;
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        SkmRecord r = rec[i];
-        uint32_t part = fastmod(~r.key, a.pmod, a.P);
-        uint32_t phase = rec_phase(r.pos), tail = rec_tail(r.pos);
-        uint64_t g = rec_base(r.pos);
-        uint32_t nb = skm_nbytes(phase, r.len, a.k);
-        uint32_t ob = atomicAdd(&lcnt[part], nb);
-        uint32_t os = atomicAdd(&lcnt[a.P + part], 1u);
-        uint64_t pbase = sbase[part] - a.part_byte_off[part];  // this CTA's range in the partition
-        uint8_t *dst = a.bytes + sbase[part] + ob;
-        uint64_t pos = g - phase;                               // first slot of the first byte
-        const uint64_t limit = g + r.len + (uint64_t)a.k - 1 + tail;  // end of read bases used
-        const uint32_t first_h = 3 - phase, last_h = (phase + r.len + (uint32_t)a.k - 1) % 3;
-        // a 64-bit window of codes starting at base `pos`, refilled every ~10 bytes
-        uint64_t win = 0;
-        int avail = 0;
-        uint32_t acc = 0;
-        uint32_t b = 0;
-        while (b < nb) {
-            const uintptr_t addr = (uintptr_t)(dst + b);
-            const uint32_t lo = (uint32_t)(addr & 3);
-            const uint32_t cnt = min(4u - lo, nb - b);
-            acc = 0;
-            for (uint32_t t = 0; t < cnt; t++) {
-                if (avail < 3) {
-                    const uint64_t wi = pos >> 4;
-                    const uint32_t o = (uint32_t)(pos & 15);
-                    win = (((uint64_t)__ldg(a.codes + wi) << 32) | __ldg(a.codes + wi + 1)) << (2 * o);
-                    avail = 32 - (int)o;
-                }
-                uint32_t v = (uint32_t)(win >> 58);
-                win <<= 6;
-                avail -= 3;
-                if (pos + 3 > limit) {
-                    uint32_t keep = limit > pos ? (uint32_t)(limit - pos) : 0u;  // 0..2 bases
-                    v &= ~((1u << (6 - 2 * keep)) - 1);
-                }
-                pos += 3;
-                const uint32_t bb = b + t;
-                const uint32_t h = (bb == nb - 1) ? last_h : (bb == 0 ? first_h : 3u);
-                acc |= (v | (h << 6)) << (8 * (lo + t));
-            }
-            if (cnt == 4) {
-                *reinterpret_cast<uint32_t *>(addr) = acc;
-            } else {
-                for (uint32_t t = 0; t < cnt; t++) dst[b + t] = (uint8_t)(acc >> (8 * (lo + t)));
-            }
-            b += cnt;
+    // Warps take 32 records at a time.  Each lane sets up its own record
+    // (destination, code slot, headers); then the warp writes the records'
+    // destination words cooperatively, one aligned 4-byte word per lane per
+    // step (no lane waits for a longer superkmer, and consecutive lanes
+    // write consecutive words).
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwarps = blockDim.x >> 5;
+    for (uint32_t base = (threadIdx.x >> 5) * 32; base < n; base += nwarps * 32) {
+        const uint32_t i = base + lane;
+        const bool has = i < n;
+        uint64_t dst = 0, pos = 0;
+        uint32_t nb = 0, rlim = 0, hdr = 0, nw = 0;
+        if (has) {
+            const SkmRecord r = rec[i];
+            const uint32_t part = fastmod(~r.key, a.pmod, a.P);
+            const uint32_t phase = rec_phase(r.pos), tail = rec_tail(r.pos);
+            nb = skm_nbytes(phase, r.len, a.k);
+            const uint32_t ob = atomicAdd(&lcnt[part], nb);
+            const uint32_t os = atomicAdd(&lcnt[a.P + part], 1u);
+            const uint64_t pbase = sbase[part] - a.part_byte_off[part];  // this CTA's range in the partition
+            dst = reinterpret_cast<uint64_t>(a.bytes + sbase[part] + ob);
+            pos = rec_base(r.pos) - phase;              // first code slot of the first byte
+            rlim = phase + r.len + (uint32_t)a.k - 1 + tail;  // read bases used, from pos
+            hdr = (3 - phase) | (((phase + r.len + (uint32_t)a.k - 1) % 3) << 2);  // first, last byte headers
+            nw = (uint32_t)((((dst + nb + 3) & ~3ull) - (dst & ~3ull)) >> 2);
+            a.idx[sbase[a.P + part] + os] = idx_pack(pbase + ob, r.len);
+            a.keys[sbase[a.P + part] + os] = r.key;
         }
-        a.idx[sbase[a.P + part] + os] = idx_pack(pbase + ob, r.len);
-        a.keys[sbase[a.P + part] + os] = r.key;
+        uint32_t incl = nw;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, incl, d);
+            if (lane >= d) incl += y;
+        }
+        const uint32_t total = __shfl_sync(FULL, incl, 31), excl = incl - nw;
+        for (uint32_t c0 = 0; c0 < total; c0 += 32) {
+            const uint32_t gi = c0 + lane;
+            int own = 0;  // the last lane whose first word index is <= gi
+#pragma unroll
+            for (int st = 16; st; st >>= 1) {
+                const int cand = own + st;
+                if (__shfl_sync(FULL, excl, cand) <= gi) own = cand;
+            }
+            const uint32_t s = gi - __shfl_sync(FULL, excl, own);
+            const uint64_t odst = __shfl_sync(FULL, dst, own), opos = __shfl_sync(FULL, pos, own);
+            const uint32_t onb = __shfl_sync(FULL, nb, own), olim = __shfl_sync(FULL, rlim, own);
+            const uint32_t ohdr = __shfl_sync(FULL, hdr, own);
+            if (gi >= total) continue;
+            const uint64_t A = (odst & ~3ull) + 4ull * s;    // this lane's destination word
+            const int b0 = (int)((int64_t)A - (int64_t)odst);  // superkmer byte at A (may be < 0)
+            auto codes_at = [&](uint64_t q) -> uint64_t {   // base q in bits 63-62, >= 17 bases
+                const uint64_t wi = q >> 4;
+                return (((uint64_t)__ldg(a.codes + wi) << 32) | __ldg(a.codes + wi + 1)) << (2 * (uint32_t)(q & 15));
+            };
+            if (b0 >= 1 && b0 + 4 < (int)onb) {
+                // interior: 12 bases -> 4 bytes of 6 code bits + header 3 (little-endian)
+                const uint32_t x = (uint32_t)(codes_at(opos + 3ull * (uint32_t)b0) >> 40);
+                *reinterpret_cast<uint32_t *>(A) = (x >> 18) | (((x >> 12) & 63u) << 8) | (((x >> 6) & 63u) << 16) |
+                                                   ((x & 63u) << 24) | 0xC0C0C0C0u;
+            } else {
+                // first or last word: byte by byte, only the superkmer's bytes
+                uint32_t word = 0, nvalid = 0;
+                for (int j = 0; j < 4; j++) {
+                    const int bb = b0 + j;
+                    if (bb < 0 || bb >= (int)onb) continue;
+                    const uint32_t q = 3u * (uint32_t)bb;  // slot of byte bb, from opos
+                    uint32_t v = (uint32_t)(codes_at(opos + q) >> 58), h = 3;
+                    if (bb == (int)onb - 1) {
+                        const uint32_t keep = olim > q ? (olim - q < 3 ? olim - q : 3u) : 0u;
+                        v &= ~((1u << (6 - 2 * keep)) - 1) & 63u;
+                        h = ohdr >> 2;
+                    } else if (bb == 0) {
+                        h = ohdr & 3;
+                    }
+                    word |= (v | (h << 6)) << (8 * j);
+                    nvalid++;
+                }
+                if (nvalid == 4) {
+                    *reinterpret_cast<uint32_t *>(A) = word;
+                } else {
+                    for (int j = 0; j < 4; j++) {
+                        const int bb = b0 + j;
+                        if (bb >= 0 && bb < (int)onb) reinterpret_cast<uint8_t *>(A)[j] = (uint8_t)(word >> (8 * j));
+                    }
+                }
+            }
+        }
     }
 }
 
