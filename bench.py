@@ -53,6 +53,12 @@ WORKLOAD_DESC = {
 }
 
 
+# DRAM bytes per read base of the main kernels, read+write, from one ncu
+# capture of a 300 Mbp case (profiles/phase1_and_counter_bacterial_small.md,
+# learned order); the roofline's `traffic` scales them to a full launch.
+TRAFFIC_PER_BASE = {"find_superkmers": 2.625, "scatter_superkmers": 7.84, "hash_insert": 2.95}
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -319,8 +325,12 @@ def main():
     classes = {k: {"ms_per_step": v[0] / args.steps, "launches_per_step": v[1] // args.steps,
                    "gbs": (v[2] / (v[0] / 1e3) / 1e9) if v[0] else 0.0}
                for k, v in kstats.items() if v[1]}
+    tpb = TRAFFIC_PER_BASE.get(dom) if args.workload == "bacterial_100m" and args.order == "learned" else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_source": src, "traffic": None,
+                "frac": achieved / hbm, "peak_source": src,
+                "traffic": tpb * bases if tpb else None,
+                "traffic_source": "ncu dram__bytes_read+write per base at 300 Mbp, scaled to the launch's bases"
+                if tpb else None,
                 "bytes_per_launch": kb / max(kl, 1), "launch_ms": per_launch_s * 1e3, "classes": classes}
 
     line = {"metric": METRIC, "value": value, "unit": "Gbp/s", "n_gpus": world, "steps": args.steps,
