@@ -83,6 +83,22 @@ int gkc_set_order(gkc_ctx *ctx, const uint32_t *lut, uint64_t n, int mem);
  * Reads shorter than k contribute nothing. */
 int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads, int mem);
 
+/* Phase 1 over caller-chosen batches of host reads: batch i holds the next
+ * batch_reads[i] reads (batches of uneven size; they add up to n_reads).
+ * Batch i+1 is copied while batch i is processed; each batch's kernels run as
+ * one CUDA graph with no host round trip (a batch whose superkmers outgrow the
+ * preallocated store chunk is redone with exact sizes).  gkc_add_reads on host
+ * input does the same with batches of opt.batch_bases bases.  No reference
+ * counterpart: the reference copies and splits 2000-read batches with a host
+ * round trip each (gpu_skmgen.cu:504-718). */
+int gkc_add_reads_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads,
+                          const uint64_t *batch_reads, uint64_t n_batches);
+
+/* Latency of each batch of the last gkc_add_reads / gkc_add_reads_batches call
+ * (milliseconds from the start of its host-to-device copy to the end of its
+ * phase 1, CUDA events): ms[i] for i < min(cap, *n); *n = batches. */
+int gkc_batch_timings(gkc_ctx *ctx, double *ms, uint64_t cap, uint64_t *n);
+
 /* Per-partition totals of the store: superkmer bytes, superkmers, k-mers
  * (SKMStoreNoncon::tot_size_bytes / skm_cnt / kmer_cnt).  Arrays of
  * opt.partitions entries; any may be NULL. */

@@ -28,7 +28,7 @@ UINT32_MAX = 0xFFFFFFFF
 # Every symbol declared in include/gkc_capi.h.
 EXPORTS = (
     "gkc_default_options", "gkc_create", "gkc_destroy", "gkc_last_error", "gkc_strerror",
-    "gkc_set_order", "gkc_add_reads", "gkc_store_stats", "gkc_store_export", "gkc_store_clear",
+    "gkc_set_order", "gkc_add_reads", "gkc_add_reads_batches", "gkc_batch_timings", "gkc_store_stats", "gkc_store_export", "gkc_store_clear",
     "gkc_count", "gkc_count_partitions", "gkc_result", "gkc_result_device", "gkc_count_reads", "gkc_count_keys",
     "gkc_last_timings", "gkc_kernel_launches", "gkc_set_stream", "gkc_set_profiling", "gkc_kernel_stats",
     "gkc_mlp_param_count", "gkc_minimizer_loads", "gkc_mlp_grad", "gkc_mlp_train", "gkc_mlp_scores",
@@ -81,6 +81,8 @@ def load_library(path: str = LIB_PATH):
     L.gkc_strerror.restype = C.c_char_p
     L.gkc_set_order.argtypes = [vp, vp, u64, i32]
     L.gkc_add_reads.argtypes = [vp, vp, vp, u64, i32]
+    L.gkc_add_reads_batches.argtypes = [vp, vp, vp, u64, vp, u64]
+    L.gkc_batch_timings.argtypes = [vp, vp, u64, C.POINTER(u64)]
     L.gkc_store_stats.argtypes = [vp, vp, vp, vp]
     L.gkc_store_export.argtypes = [vp, i32, vp, u64, C.POINTER(u64)]
     L.gkc_store_clear.argtypes = [vp]
@@ -188,6 +190,22 @@ class KmerCounter:
         if rm != om:
             raise ValueError("reads and offsets must live in the same memory")
         self._check(self._L.gkc_add_reads(self._h, rp, op, len(offs) - 1, rm))
+
+    def add_reads_batches(self, reads, offs, batch_reads):
+        """Phase 1 over host reads in caller-chosen (uneven) batches of reads."""
+        reads = np.ascontiguousarray(reads)
+        offs = np.ascontiguousarray(offs, np.uint64)
+        br = np.ascontiguousarray(batch_reads, np.uint64)
+        self._check(self._L.gkc_add_reads_batches(self._h, _ptr(reads)[0], _ptr(offs)[0], len(offs) - 1,
+                                                  _ptr(br)[0], len(br)))
+
+    def batch_timings(self) -> np.ndarray:
+        """Latency (ms) of each batch of the last add_reads call."""
+        n = C.c_uint64(0)
+        self._check(self._L.gkc_batch_timings(self._h, None, 0, C.byref(n)))
+        out = np.zeros(n.value, np.float64)
+        self._check(self._L.gkc_batch_timings(self._h, _ptr(out)[0], len(out), C.byref(n)))
+        return out
 
     def store_stats(self):
         P = self.partitions

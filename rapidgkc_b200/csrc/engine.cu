@@ -86,7 +86,16 @@ struct StoreChunk {
     DevBuf dbytes, didx, dkeys;               // device storage
     PinBuf hbytes, hidx, hkeys;               // pinned host storage (spilled chunks)
     DevBuf d_byte_off, d_skm_off;             // device copies of the offsets
+    // laid out on the device (phase1_async): k-mers per partition, error
+    // flags, and their pinned host mirror read back after the batch
+    DevBuf d_kmers, d_flags;
+    PinBuf h_meta;                            // byte_off [P+1], skm_off [P+1], kmers [P], flags
+    bool pending = false;
+    uint64_t batch = 0;                       // the batch of this chunk in the last gkc_add_reads
     void release() {
+        d_kmers.release();
+        d_flags.release();
+        h_meta.release();
         dbytes.release();
         didx.release();
         dkeys.release();
@@ -171,6 +180,8 @@ struct gkc_ctx {
     uint64_t out_cap = 0, n_out = 0, n_distinct = 0;
     bool has_result = false;
     std::vector<char> counted;  // partitions already counted by gkc_count_partitions
+    std::vector<cudaEvent_t> batch_ev;  // start / end of each batch of the last gkc_add_reads
+    std::vector<double> batch_ms;       // latency of each batch: its copy start to its phase-1 end
     DevBuf keysA, keysB, tiles, counts, offsets, blocksums, heads_pos, heads_key, tilecnt, tileoff;
     DevBuf segoff, segcur, part_err, scal;
     DevBuf stage_bytes, stage_idx;
@@ -214,6 +225,7 @@ struct gkc_ctx {
         for (auto *p : ps) p->release();
         cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_ready[0], buf_ready[1]};
         for (auto e : evs) if (e) cudaEventDestroy(e);
+        for (auto e : batch_ev) cudaEventDestroy(e);
         prof_flush();
         for (auto e : evpool) cudaEventDestroy(e);
         if (own_s) cudaStreamDestroy(own_s);
@@ -345,84 +357,147 @@ int ensure_out(gkc_ctx *ctx, uint64_t need) {
 
 // ---------------------------------------------------------------------------
 // phase 1 on a device-resident batch (offs[0] == 0)
-int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, uint64_t n_reads,
-                 uint64_t total) {
+// Launch shape of phase 1 for a batch of `total` bases.
+struct P1Plan {
+    uint64_t ntiles = 0, tiles_per_cta = 0, cap = 0, cap_max = 0;
+    uint32_t grid = 0;
+    size_t dyn = 0;
+    void (*kfind)(P1Params) = nullptr;
+};
+
+int p1_plan(gkc_ctx *ctx, uint64_t total, P1Plan *pl) {
     const uint32_t P = (uint32_t)ctx->opt.partitions;
-    if (total == 0 || n_reads == 0) return GKC_OK;
-    const uint64_t ntiles = (total + P1_TILE - 1) / P1_TILE;
+    pl->ntiles = (total + P1_TILE - 1) / P1_TILE;
     // the window-minimum doubling is unrolled per level count
     const int w = ctx->opt.k - ctx->opt.p + 1;
     int lg = 0;
     while ((2 << lg) <= w) lg++;
-    void (*kfind)(P1Params);
     if (ctx->has_lut)
-        kfind = lg == 0 ? find_superkmers_kernel<0, true> : lg == 1 ? find_superkmers_kernel<1, true>
-              : lg == 2 ? find_superkmers_kernel<2, true> : lg == 3 ? find_superkmers_kernel<3, true>
-                                                                    : find_superkmers_kernel<4, true>;
+        pl->kfind = lg == 0 ? find_superkmers_kernel<0, true> : lg == 1 ? find_superkmers_kernel<1, true>
+                  : lg == 2 ? find_superkmers_kernel<2, true> : lg == 3 ? find_superkmers_kernel<3, true>
+                                                                        : find_superkmers_kernel<4, true>;
     else
-        kfind = lg == 0 ? find_superkmers_kernel<0, false> : lg == 1 ? find_superkmers_kernel<1, false>
-              : lg == 2 ? find_superkmers_kernel<2, false> : lg == 3 ? find_superkmers_kernel<3, false>
-                                                                     : find_superkmers_kernel<4, false>;
-    size_t dyn = 3ull * P * sizeof(uint32_t);
-    CK(cudaFuncSetAttribute(kfind, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        pl->kfind = lg == 0 ? find_superkmers_kernel<0, false> : lg == 1 ? find_superkmers_kernel<1, false>
+                  : lg == 2 ? find_superkmers_kernel<2, false> : lg == 3 ? find_superkmers_kernel<3, false>
+                                                                         : find_superkmers_kernel<4, false>;
+    pl->dyn = 3ull * P * sizeof(uint32_t);
+    CK(cudaFuncSetAttribute(pl->kfind, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl->dyn));
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfind, P1_THREADS, dyn));
-    const uint32_t grid = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)ctx->sms * std::max(per_sm, 1));
-    const uint64_t tiles_per_cta = (ntiles + grid - 1) / grid;
-    uint64_t cap = tiles_per_cta * P1_TILE / 4 + 4096;
-    const uint64_t cap_max = tiles_per_cta * P1_TILE + 64;
-    CK(ctx->region_count.ensure(grid * sizeof(uint32_t)));
-    CK(ctx->cta_hist.ensure(2ull * P * grid * sizeof(uint32_t)));
-    CK(ctx->cta_base.ensure(2ull * P * grid * sizeof(unsigned long long)));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pl->kfind, P1_THREADS, pl->dyn));
+    pl->grid = (uint32_t)std::min<uint64_t>(pl->ntiles, (uint64_t)ctx->sms * std::max(per_sm, 1));
+    pl->tiles_per_cta = (pl->ntiles + pl->grid - 1) / pl->grid;
+    pl->cap = std::min<uint64_t>(pl->tiles_per_cta * P1_TILE / 4 + 4096, UINT32_MAX);  // records per CTA
+    pl->cap_max = pl->tiles_per_cta * P1_TILE + 64;
+    const size_t dyn2 = 2ull * P * (sizeof(unsigned long long) + sizeof(uint32_t));
+    CK(cudaFuncSetAttribute(scatter_superkmers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn2));
+    // per-context buffers every batch of this size needs
+    CK(ctx->region_count.ensure(pl->grid * sizeof(uint32_t)));
+    CK(ctx->cta_hist.ensure(2ull * P * pl->grid * sizeof(uint32_t)));
+    CK(ctx->cta_base.ensure(2ull * P * pl->grid * sizeof(unsigned long long)));
     CK(ctx->hist.ensure(3ull * P * sizeof(unsigned long long)));
+    CK(ctx->tile_read.ensure(pl->ntiles * sizeof(int64_t)));
+    CK(ctx->codes.ensure((pl->ntiles * P1_TILE_WORDS + 4) * sizeof(uint32_t)));
+    CK(ctx->records.ensure(pl->cap * pl->grid * sizeof(SkmRecord)));
+    return GKC_OK;
+}
+
+// tile_reads + find_superkmers of a batch (stream work only).
+int launch_find(gkc_ctx *ctx, const P1Plan &pl, const uint8_t *d_reads, const uint64_t *d_offs, uint64_t n_reads,
+                uint64_t total, uint64_t cap, uint32_t *flags) {
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    auto *hist = ctx->hist.as<unsigned long long>();
+    CK(cudaMemsetAsync(ctx->codes.as<uint32_t>() + pl.ntiles * P1_TILE_WORDS, 0, 16, ctx->s));
+    {
+        uint32_t g = (uint32_t)std::min<uint64_t>((pl.ntiles + 255) / 256, (uint64_t)ctx->sms * 8);
+        tile_reads_kernel<<<g, 256, 0, ctx->s>>>(d_offs, (int64_t)n_reads, pl.ntiles, ctx->tile_read.as<int64_t>());
+        LAUNCHED();
+    }
+    CK(cudaMemsetAsync(hist, 0, 3ull * P * sizeof(unsigned long long), ctx->s));
+    CK(cudaMemsetAsync(flags, 0, 4, ctx->s));
+    P1Params a;
+    a.reads = d_reads;
+    a.offs = d_offs;
+    a.n_reads = (int64_t)n_reads;
+    a.total = total;
+    a.k = ctx->opt.k;
+    a.p = ctx->opt.p;
+    a.P = P;
+    a.pmod = fastmod_m(P);
+    a.lut = ctx->has_lut ? ctx->lut.as<uint32_t>() : nullptr;
+    a.vec_ok = ((uintptr_t)d_reads & 15) == 0;
+    a.tile_read = ctx->tile_read.as<int64_t>();
+    a.codes = ctx->codes.as<uint32_t>();
+    a.records = ctx->records.as<SkmRecord>();
+    a.region_cap = (uint32_t)cap;
+    a.region_count = ctx->region_count.as<uint32_t>();
+    a.part_bytes = hist;
+    a.part_skms = hist + P;
+    a.part_kmers = hist + 2 * P;
+    a.cta_hist = ctx->cta_hist.as<uint32_t>();
+    a.err = flags;
+    // reads + offsets in, 2-bit codes out (records are added by the caller)
+    KScope ks(ctx, GKC_K_FIND_SUPERKMERS, 1.25 * (double)total + 8.0 * (n_reads + 1));
+    pl.kfind<<<pl.grid, P1_THREADS, pl.dyn, ctx->s>>>(a);
+    LAUNCHED();
+    return GKC_OK;
+}
+
+// cta_offsets + scatter of a batch into chunk c's device buffers (stream work only).
+int launch_scatter(gkc_ctx *ctx, const P1Plan &pl, StoreChunk *c, uint64_t total, uint64_t cap,
+                   const uint32_t *flags, double nskm_hint, double nbytes_hint) {
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    {
+        KScope ks(ctx, GKC_K_SCAN, 24.0 * P * pl.grid);
+        cta_offsets_kernel<<<(P + 127) / 128, 128, 0, ctx->s>>>(
+            ctx->cta_hist.as<uint32_t>(), pl.grid, P, c->d_byte_off.as<unsigned long long>(),
+            c->d_skm_off.as<unsigned long long>(), ctx->cta_base.as<unsigned long long>(), flags);
+        LAUNCHED();
+    }
+    P2Params b;
+    b.codes = ctx->codes.as<uint32_t>();
+    b.records = ctx->records.as<SkmRecord>();
+    b.region_cap = (uint32_t)cap;
+    b.region_count = ctx->region_count.as<uint32_t>();
+    b.k = ctx->opt.k;
+    b.P = P;
+    b.pmod = fastmod_m(P);
+    b.part_byte_off = c->d_byte_off.as<unsigned long long>();
+    b.cta_base = ctx->cta_base.as<unsigned long long>();
+    b.flags = flags;
+    b.bytes = c->bytes;
+    b.idx = c->idx;
+    b.keys = c->keys;
+    const size_t dyn2 = 2ull * P * (sizeof(unsigned long long) + sizeof(uint32_t));
+    // records (16 B) and codes in; superkmer bytes, index (8 B) and keys (4 B) out
+    KScope ks(ctx, GKC_K_SCATTER, 28.0 * nskm_hint + 0.25 * (double)total + nbytes_hint);
+    scatter_superkmers_kernel<<<pl.grid, P2_THREADS, dyn2, ctx->s>>>(b);
+    LAUNCHED();
+    return GKC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Phase 1 of one device-resident batch (offs[0] == 0), synchronously: the
+// partition totals are read back after find_superkmers and the chunk is
+// allocated to the exact size.  Used for spilled stores (the chunk is then
+// copied to pinned host memory), for profiled runs, and to redo a batch that
+// overflowed phase1_async's capacities.
+int phase1_exact(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, uint64_t n_reads,
+                 uint64_t total) {
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    if (total == 0 || n_reads == 0) return GKC_OK;
+    P1Plan pl;
+    RET(p1_plan(ctx, total, &pl));
     CK(ctx->flags.ensure(64));
     CK(ctx->h_hist.ensure(3ull * P * sizeof(unsigned long long)));
     CK(ctx->h_flags.ensure(64));
-    CK(ctx->tile_read.ensure(ntiles * sizeof(int64_t)));
-    CK(ctx->codes.ensure((ntiles * P1_TILE_WORDS + 4) * sizeof(uint32_t)));
-    CK(cudaMemsetAsync(ctx->codes.as<uint32_t>() + ntiles * P1_TILE_WORDS, 0, 16, ctx->s));
-    auto *hist = ctx->hist.as<unsigned long long>();
     auto *hh = ctx->h_hist.as<unsigned long long>();
-    {
-        uint32_t g = (uint32_t)std::min<uint64_t>((ntiles + 255) / 256, (uint64_t)ctx->sms * 8);
-        tile_reads_kernel<<<g, 256, 0, ctx->s>>>(d_offs, (int64_t)n_reads, ntiles, ctx->tile_read.as<int64_t>());
-        LAUNCHED();
-    }
+    uint64_t cap = pl.cap;
     for (int attempt = 0;; attempt++) {
-        if (cap > UINT32_MAX) cap = UINT32_MAX;
-        CK(ctx->records.ensure(cap * grid * sizeof(SkmRecord)));
-        CK(cudaMemsetAsync(hist, 0, 3ull * P * sizeof(unsigned long long), ctx->s));
-        CK(cudaMemsetAsync(ctx->flags.p, 0, 64, ctx->s));
-        P1Params a;
-        a.reads = d_reads;
-        a.offs = d_offs;
-        a.n_reads = (int64_t)n_reads;
-        a.total = total;
-        a.k = ctx->opt.k;
-        a.p = ctx->opt.p;
-        a.P = P;
-        a.pmod = fastmod_m(P);
-        a.lut = ctx->has_lut ? ctx->lut.as<uint32_t>() : nullptr;
-        a.vec_ok = ((uintptr_t)d_reads & 15) == 0;
-        a.tile_read = ctx->tile_read.as<int64_t>();
-        a.codes = ctx->codes.as<uint32_t>();
-        a.records = ctx->records.as<SkmRecord>();
-        a.region_cap = (uint32_t)cap;
-        a.region_count = ctx->region_count.as<uint32_t>();
-        a.part_bytes = hist;
-        a.part_skms = hist + P;
-        a.part_kmers = hist + 2 * P;
-        a.cta_hist = ctx->cta_hist.as<uint32_t>();
-        a.err = ctx->flags.as<uint32_t>();
+        CK(ctx->records.ensure(cap * pl.grid * sizeof(SkmRecord)));
         CK(cudaEventRecord(ctx->e0, ctx->s));
-        {
-            // reads + offsets in, 2-bit codes out (records are added below)
-            KScope ks(ctx, GKC_K_FIND_SUPERKMERS, 1.25 * (double)total + 8.0 * (n_reads + 1));
-            kfind<<<grid, P1_THREADS, dyn, ctx->s>>>(a);
-            LAUNCHED();
-        }
+        RET(launch_find(ctx, pl, d_reads, d_offs, n_reads, total, cap, ctx->flags.as<uint32_t>()));
         CK(cudaEventRecord(ctx->e1, ctx->s));
-        CK(cudaMemcpyAsync(hh, hist, 3ull * P * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(hh, ctx->hist.p, 3ull * P * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->s));
         CK(cudaMemcpyAsync(ctx->h_flags.p, ctx->flags.p, 4, cudaMemcpyDeviceToHost, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
         float ms = 0;
@@ -431,10 +506,10 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
         uint32_t f = *ctx->h_flags.as<uint32_t>();
         if (f & ERR_SKM_TOO_LONG) return ctx->fail(GKC_EINVAL, "a superkmer exceeds %u k-mers", IDX_MAX_LEN);
         if (f & ERR_RECORD_OVERFLOW) {
-            if (cap >= cap_max || attempt >= 3)
+            if (cap >= pl.cap_max || attempt >= 3)
                 return ctx->fail(GKC_EINTERNAL, "superkmer record region overflow at capacity %llu",
                                  (unsigned long long)cap);
-            cap = std::min<uint64_t>(cap * 4, cap_max);
+            cap = std::min<uint64_t>(std::min<uint64_t>(cap * 4, pl.cap_max), UINT32_MAX);
             continue;
         }
         break;
@@ -452,6 +527,7 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     c->nbytes = c->byte_off[P];
     c->nskm = c->skm_off[P];
     c->on_host = false;
+    c->pending = false;
     if (ctx->prof && !ctx->pend.empty()) ctx->pend.back().bytes += 16.0 * c->nskm;  // records written
     // a spilled chunk is scattered into shared device staging, then copied out
     DevBuf &db = ctx->opt.spill_host ? ctx->spill_bytes : c->dbytes;
@@ -472,34 +548,7 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     c->keys = dk.as<uint32_t>();
     CK(cudaMemcpyAsync(c->d_byte_off.p, c->byte_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
     CK(cudaMemcpyAsync(c->d_skm_off.p, c->skm_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
-    {
-        KScope ks(ctx, GKC_K_SCAN, 24.0 * P * grid);
-        cta_offsets_kernel<<<(P + 127) / 128, 128, 0, ctx->s>>>(
-            ctx->cta_hist.as<uint32_t>(), grid, P, c->d_byte_off.as<unsigned long long>(),
-            c->d_skm_off.as<unsigned long long>(), ctx->cta_base.as<unsigned long long>());
-        LAUNCHED();
-    }
-    P2Params b;
-    b.codes = ctx->codes.as<uint32_t>();
-    b.records = ctx->records.as<SkmRecord>();
-    b.region_cap = (uint32_t)cap;
-    b.region_count = ctx->region_count.as<uint32_t>();
-    b.k = ctx->opt.k;
-    b.P = P;
-    b.pmod = fastmod_m(P);
-    b.part_byte_off = c->d_byte_off.as<unsigned long long>();
-    b.cta_base = ctx->cta_base.as<unsigned long long>();
-    b.bytes = c->bytes;
-    b.idx = c->idx;
-    b.keys = c->keys;
-    size_t dyn2 = 2ull * P * (sizeof(unsigned long long) + sizeof(uint32_t));
-    CK(cudaFuncSetAttribute(scatter_superkmers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn2));
-    {
-        // records (16 B) and codes in; superkmer bytes, index (8 B) and keys (4 B) out
-        KScope ks(ctx, GKC_K_SCATTER, 28.0 * c->nskm + 0.25 * (double)total + (double)c->nbytes);
-        scatter_superkmers_kernel<<<grid, P2_THREADS, dyn2, ctx->s>>>(b);
-        LAUNCHED();
-    }
+    RET(launch_scatter(ctx, pl, c, total, cap, ctx->flags.as<uint32_t>(), (double)c->nskm, (double)c->nbytes));
     if (ctx->opt.spill_host) {
         cudaError_t ea = c->hbytes.ensure(c->nbytes + 16);
         cudaError_t eb = ea == cudaSuccess ? c->hidx.ensure(std::max<uint64_t>(c->nskm, 1) * 8) : ea;
@@ -519,6 +568,113 @@ int phase1_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     }
     ctx->store.push_back(c);
     return GKC_OK;
+}
+
+// Phase 1 of one device-resident batch without waiting for the device: the
+// chunk gets capacity for 2 bytes and 0.25 superkmers per base (typical data
+// needs about 1.2 and 0.09), the layout is computed on the device
+// (part_offsets_kernel), and the batch's launches are captured into one CUDA
+// graph and launched.  `rebase` != 0 first subtracts it from the batch's
+// offsets (a slice of the caller's offsets).  The chunk's layout is copied back
+// to pinned memory; phase1_finish reads it after the stream is synchronised.
+int phase1_async(gkc_ctx *ctx, const uint8_t *d_reads, uint64_t *d_offs, uint64_t n_reads, uint64_t total,
+                 uint64_t rebase, uint64_t batch) {
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    if (total == 0 || n_reads == 0) return GKC_OK;
+    P1Plan pl;
+    RET(p1_plan(ctx, total, &pl));
+    const uint64_t byte_cap = 2 * total + 65536, skm_cap = total / 4 + 4096;
+    StoreChunk *c = ctx->take_chunk();
+    cudaError_t e = c->dbytes.ensure(byte_cap + 32);
+    if (e == cudaSuccess) e = c->didx.ensure(skm_cap * 8);
+    if (e == cudaSuccess) e = c->dkeys.ensure(skm_cap * 4);
+    if (e == cudaSuccess) e = c->d_byte_off.ensure((P + 1) * 8);
+    if (e == cudaSuccess) e = c->d_skm_off.ensure((P + 1) * 8);
+    if (e == cudaSuccess) e = c->d_kmers.ensure(P * 8ull);
+    if (e == cudaSuccess) e = c->d_flags.ensure(64);
+    if (e == cudaSuccess) e = c->h_meta.ensure((3ull * P + 3) * 8);
+    if (e != cudaSuccess) {
+        ctx->pool.push_back(c);
+        return ctx->fail(GKC_ENOMEM, "store chunk allocation: %s", cudaGetErrorString(e));
+    }
+    c->bytes = c->dbytes.as<uint8_t>();
+    c->idx = c->didx.as<uint64_t>();
+    c->keys = c->dkeys.as<uint32_t>();
+    c->on_host = false;
+    c->batch = batch;
+    uint32_t *flags = c->d_flags.as<uint32_t>();
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CK(cudaStreamBeginCapture(ctx->s, cudaStreamCaptureModeThreadLocal));
+    auto work = [&]() -> int {
+        if (rebase) {
+            const uint32_t g = (uint32_t)std::min<uint64_t>((n_reads + 256) / 256, (uint64_t)ctx->sms * 8);
+            rebase_offsets_kernel<<<g, 256, 0, ctx->s>>>(d_offs, n_reads + 1, rebase);
+            LAUNCHED();
+        }
+        RET(launch_find(ctx, pl, d_reads, d_offs, n_reads, total, pl.cap, flags));
+        part_offsets_kernel<<<1, PO_THREADS, 0, ctx->s>>>(
+            ctx->hist.as<unsigned long long>(), P, byte_cap, skm_cap, c->d_byte_off.as<unsigned long long>(),
+            c->d_skm_off.as<unsigned long long>(), c->d_kmers.as<unsigned long long>(), flags);
+        LAUNCHED();
+        RET(launch_scatter(ctx, pl, c, total, pl.cap, flags, 0.09 * (double)total, 1.2 * (double)total));
+        return GKC_OK;
+    };
+    const int rc = work();
+    const cudaError_t ec = cudaStreamEndCapture(ctx->s, &graph);  // also ends a capture that failed
+    if (rc != GKC_OK || ec != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        ctx->pool.push_back(c);
+        return rc != GKC_OK ? rc : ctx->fail(GKC_ECUDA, "phase-1 graph capture: %s", cudaGetErrorString(ec));
+    }
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, ctx->s);
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        ctx->pool.push_back(c);
+        return ctx->fail(GKC_ECUDA, "phase-1 graph launch: %s", cudaGetErrorString(e));
+    }
+    auto *hm = c->h_meta.as<unsigned long long>();
+    CK(cudaMemcpyAsync(hm, c->d_byte_off.p, (P + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaMemcpyAsync(hm + P + 1, c->d_skm_off.p, (P + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaMemcpyAsync(hm + 2 * P + 2, c->d_kmers.p, P * 8ull, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaMemcpyAsync(hm + 3 * P + 2, c->d_flags.p, 4, cudaMemcpyDeviceToHost, ctx->s));
+    c->pending = true;
+    ctx->store.push_back(c);
+    return GKC_OK;
+}
+
+// After the stream is synchronised: fills the host view of every chunk
+// phase1_async wrote.  Chunks that overflowed are taken out of the store;
+// their batches are listed in `redo` (the caller runs them with phase1_exact).
+int phase1_finish(gkc_ctx *ctx, std::vector<uint64_t> *redo) {
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    std::vector<StoreChunk *> keep;
+    int rc = GKC_OK;
+    for (StoreChunk *c : ctx->store) {
+        if (!c->pending) {
+            keep.push_back(c);
+            continue;
+        }
+        c->pending = false;
+        const auto *hm = c->h_meta.as<unsigned long long>();
+        const uint32_t f = (uint32_t)hm[3 * P + 2];
+        if (f & ERR_SKM_TOO_LONG) rc = ctx->fail(GKC_EINVAL, "a superkmer exceeds %u k-mers", IDX_MAX_LEN);
+        if (f & (ERR_RECORD_OVERFLOW | ERR_CAPACITY)) {
+            redo->push_back(c->batch);
+            ctx->pool.push_back(c);
+            continue;
+        }
+        c->byte_off.assign(hm, hm + P + 1);
+        c->skm_off.assign(hm + P + 1, hm + 2 * P + 2);
+        c->kmers.assign(hm + 2 * P + 2, hm + 3 * P + 2);
+        c->nbytes = c->byte_off[P];
+        c->nskm = c->skm_off[P];
+        keep.push_back(c);
+    }
+    ctx->store.swap(keep);
+    return rc;
 }
 
 // Device pointers of the superkmers of partitions [p0, p1) of chunk c, indexed
@@ -1274,12 +1430,100 @@ int gkc_set_order(gkc_ctx *ctx, const uint32_t *lut, uint64_t n, int mem) {
     return GKC_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+struct ReadBatch {
+    uint64_t r0, r1;  // reads [r0, r1) of the caller's CSR
+};
+
+// Phase 1 over host batches: the copy of batch i+1 (copy stream, two device
+// slots) overlaps phase 1 of batch i; no batch waits for the host (phase1_async)
+// unless the store spills or kernels are profiled (phase1_exact).
+int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, const std::vector<ReadBatch> &batches) {
+    const bool exact = ctx->opt.spill_host || ctx->prof;
+    const size_t nbat = batches.size();
+    uint64_t max_b = 0, max_r = 0;
+    for (const auto &b : batches) {
+        max_b = std::max<uint64_t>(max_b, offs[b.r1] - offs[b.r0]);
+        max_r = std::max<uint64_t>(max_r, b.r1 - b.r0);
+    }
+    CK(cudaStreamSynchronize(ctx->s));  // the slots may be reallocated below
+    for (int slot = 0; slot < 2; slot++) {
+        CK(ctx->reads[slot].ensure(max_b + 64));
+        CK(ctx->offs[slot].ensure((max_r + 1) * 8));
+    }
+    while (ctx->batch_ev.size() < 2 * nbat) {
+        cudaEvent_t ev;
+        CK(cudaEventCreate(&ev));
+        ctx->batch_ev.push_back(ev);
+    }
+    auto stage = [&](size_t bi, cudaStream_t st) -> int {
+        const int slot = (int)(bi & 1);
+        const ReadBatch &b = batches[bi];
+        const uint64_t base = offs[b.r0], nb = offs[b.r1] - base, nr = b.r1 - b.r0;
+        CK(cudaStreamWaitEvent(st, ctx->buf_free[slot], 0));
+        CK(cudaEventRecord(ctx->batch_ev[2 * bi], st));  // the batch starts with its copy
+        CK(cudaMemcpyAsync(ctx->reads[slot].p, reads + base, nb, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->offs[slot].p, offs + b.r0, (nr + 1) * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaEventRecord(ctx->buf_ready[slot], st));
+        return GKC_OK;
+    };
+    auto run = [&](size_t bi, bool sync_exact) -> int {
+        const int slot = (int)(bi & 1);
+        const ReadBatch &b = batches[bi];
+        const uint64_t base = offs[b.r0], nb = offs[b.r1] - base, nr = b.r1 - b.r0;
+        CK(cudaStreamWaitEvent(ctx->s, ctx->buf_ready[slot], 0));
+        int rc;
+        if (sync_exact) {
+            const uint32_t g = (uint32_t)std::min<uint64_t>((nr + 256) / 256, (uint64_t)ctx->sms * 8);
+            rebase_offsets_kernel<<<g, 256, 0, ctx->s>>>(ctx->offs[slot].as<uint64_t>(), nr + 1, base);
+            LAUNCHED();
+            rc = phase1_exact(ctx, ctx->reads[slot].as<uint8_t>(), ctx->offs[slot].as<uint64_t>(), nr, nb);
+        } else {
+            rc = phase1_async(ctx, ctx->reads[slot].as<uint8_t>(), ctx->offs[slot].as<uint64_t>(), nr, nb, base, bi);
+        }
+        CK(cudaEventRecord(ctx->buf_free[slot], ctx->s));
+        CK(cudaEventRecord(ctx->batch_ev[2 * bi + 1], ctx->s));
+        return rc;
+    };
+    CK(cudaEventRecord(ctx->buf_free[0], ctx->s));
+    CK(cudaEventRecord(ctx->buf_free[1], ctx->s));
+    int rc = nbat ? stage(0, ctx->cs) : GKC_OK;
+    for (size_t bi = 0; rc == GKC_OK && bi < nbat; bi++) {
+        if (bi + 1 < nbat) rc = stage(bi + 1, ctx->cs);
+        if (rc == GKC_OK) rc = run(bi, exact);
+    }
+    CK(cudaStreamSynchronize(ctx->s));
+    if (rc != GKC_OK) return rc;
+    std::vector<uint64_t> redo;
+    RET(phase1_finish(ctx, &redo));
+    ctx->batch_ms.assign(nbat, 0.0);
+    for (size_t bi = 0; bi < nbat; bi++) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, ctx->batch_ev[2 * bi], ctx->batch_ev[2 * bi + 1]) == cudaSuccess)
+            ctx->batch_ms[bi] = ms;
+    }
+    for (uint64_t bi : redo) {  // capacity overflow: the batch again, with exact sizes
+        RET(stage(bi, ctx->s));
+        RET(run(bi, true));
+        CK(cudaStreamSynchronize(ctx->s));
+    }
+    return GKC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads, int mem) {
     if (!ctx || (!reads && n_reads) || !offs) return GKC_EINVAL;
     CK(cudaSetDevice(ctx->device));
     for (char c : ctx->counted)
         if (c) return ctx->fail(GKC_ESTATE, "the store is partly counted; clear it before adding reads");
     ctx->times[0] = ctx->times[1] = 0;
+    ctx->batch_ms.clear();
     if (n_reads == 0) return GKC_OK;
     if (mem == GKC_MEM_DEVICE) {
         uint64_t first = 0, total = 0;
@@ -1288,74 +1532,82 @@ int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_
         CK(cudaStreamSynchronize(ctx->s));
         if (first != 0) return ctx->fail(GKC_EINVAL, "device input needs offs[0] == 0");
         CK(cudaEventRecord(ctx->e2, ctx->s));
-        RET(phase1_batch(ctx, reinterpret_cast<const uint8_t *>(reads), offs, n_reads, total));
+        const uint8_t *dr = reinterpret_cast<const uint8_t *>(reads);
+        if (ctx->opt.spill_host || ctx->prof) {
+            RET(phase1_exact(ctx, dr, offs, n_reads, total));
+        } else {
+            // no rebase: the caller's offsets are only read
+            RET(phase1_async(ctx, dr, const_cast<uint64_t *>(offs), n_reads, total, 0, 0));
+            CK(cudaStreamSynchronize(ctx->s));
+            std::vector<uint64_t> redo;
+            RET(phase1_finish(ctx, &redo));
+            if (!redo.empty()) RET(phase1_exact(ctx, dr, offs, n_reads, total));
+        }
         CK(cudaEventRecord(ctx->e3, ctx->s));
         CK(cudaEventSynchronize(ctx->e3));
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
         ctx->times[0] = ms;
+        ctx->batch_ms.assign(1, ms);
         return GKC_OK;
     }
     if (offs[0] > offs[n_reads]) return ctx->fail(GKC_EINVAL, "offsets are not ascending");
-    // host input: batches of whole reads of about batch_bases bases, double
-    // buffered so the copy of batch i+1 overlaps phase 1 of batch i
-    struct Batch { uint64_t r0, r1; };
-    std::vector<Batch> batches;
+    // batches of whole reads of about batch_bases bases
+    std::vector<ReadBatch> batches;
     uint64_t r = 0;
     while (r < n_reads) {
-        uint64_t r1 = r + 1;
         uint64_t lim = offs[r] + ctx->opt.batch_bases;
-        // binary search the last read end within the budget
-        uint64_t lo = r + 1, hi = n_reads;
+        uint64_t lo = r + 1, hi = n_reads;  // the last read end within the budget
         while (lo < hi) {
             uint64_t mid = (lo + hi + 1) >> 1;
             if (offs[mid] <= lim) lo = mid; else hi = mid - 1;
         }
-        r1 = std::max(r1, lo);
-        batches.push_back({r, r1});
-        r = r1;
+        batches.push_back({r, std::max<uint64_t>(r + 1, lo)});
+        r = batches.back().r1;
     }
-    auto stage = [&](size_t bi) -> int {
-        int slot = (int)(bi & 1);
-        const Batch &b = batches[bi];
-        uint64_t base = offs[b.r0], nb = offs[b.r1] - base, nr = b.r1 - b.r0;
-        CK(cudaStreamWaitEvent(ctx->cs, ctx->buf_free[slot], 0));
-        CK(ctx->reads[slot].ensure(nb + 64));
-        CK(ctx->offs[slot].ensure((nr + 1) * 8));
-        CK(ctx->offs_pin[slot].ensure((nr + 1) * 8));
-        CK(cudaEventSynchronize(ctx->buf_free[slot]));  // pinned offsets buffer reuse
-        uint64_t *po = ctx->offs_pin[slot].as<uint64_t>();
-        for (uint64_t i = 0; i <= nr; i++) po[i] = offs[b.r0 + i] - base;
-        CK(cudaMemcpyAsync(ctx->reads[slot].p, reads + base, nb, cudaMemcpyHostToDevice, ctx->cs));
-        CK(cudaMemcpyAsync(ctx->offs[slot].p, po, (nr + 1) * 8, cudaMemcpyHostToDevice, ctx->cs));
-        CK(cudaEventRecord(ctx->buf_ready[slot], ctx->cs));
-        return GKC_OK;
-    };
-    cudaEvent_t t0, t1;
-    CK(cudaEventCreate(&t0));
-    CK(cudaEventCreate(&t1));
-    CK(cudaEventRecord(ctx->buf_free[0], ctx->s));
-    CK(cudaEventRecord(ctx->buf_free[1], ctx->s));
-    CK(cudaEventRecord(t0, ctx->s));
-    int rc = stage(0);
-    for (size_t bi = 0; rc == GKC_OK && bi < batches.size(); bi++) {
-        int slot = (int)(bi & 1);
-        if (bi + 1 < batches.size()) rc = stage(bi + 1);
-        if (rc != GKC_OK) break;
-        CK(cudaStreamWaitEvent(ctx->s, ctx->buf_ready[slot], 0));
-        const Batch &b = batches[bi];
-        rc = phase1_batch(ctx, ctx->reads[slot].as<uint8_t>(), ctx->offs[slot].as<uint64_t>(), b.r1 - b.r0,
-                          offs[b.r1] - offs[b.r0]);
-        CK(cudaEventRecord(ctx->buf_free[slot], ctx->s));
-    }
-    CK(cudaEventRecord(t1, ctx->s));
-    CK(cudaEventSynchronize(t1));
+    CK(cudaEventRecord(ctx->e2, ctx->s));
+    const int rc = add_host_batches(ctx, reads, offs, batches);
+    CK(cudaEventRecord(ctx->e3, ctx->s));
+    CK(cudaEventSynchronize(ctx->e3));
     float ms = 0;
-    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventElapsedTime(&ms, ctx->e2, ctx->e3);
     ctx->times[0] = ms;
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
     return rc;
+}
+
+int gkc_add_reads_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads,
+                          const uint64_t *batch_reads, uint64_t n_batches) {
+    if (!ctx || (!reads && n_reads) || !offs || (!batch_reads && n_batches)) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    for (char c : ctx->counted)
+        if (c) return ctx->fail(GKC_ESTATE, "the store is partly counted; clear it before adding reads");
+    ctx->times[0] = ctx->times[1] = 0;
+    ctx->batch_ms.clear();
+    std::vector<ReadBatch> batches;
+    uint64_t r = 0;
+    for (uint64_t i = 0; i < n_batches; i++) {
+        if (batch_reads[i] == 0) continue;
+        batches.push_back({r, r + batch_reads[i]});
+        r += batch_reads[i];
+    }
+    if (r != n_reads) return ctx->fail(GKC_EINVAL, "batch sizes add up to %llu reads, not %llu",
+                                       (unsigned long long)r, (unsigned long long)n_reads);
+    if (n_reads && offs[0] > offs[n_reads]) return ctx->fail(GKC_EINVAL, "offsets are not ascending");
+    CK(cudaEventRecord(ctx->e2, ctx->s));
+    const int rc = add_host_batches(ctx, reads, offs, batches);
+    CK(cudaEventRecord(ctx->e3, ctx->s));
+    CK(cudaEventSynchronize(ctx->e3));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->e2, ctx->e3);
+    ctx->times[0] = ms;
+    return rc;
+}
+
+int gkc_batch_timings(gkc_ctx *ctx, double *ms, uint64_t cap, uint64_t *n) {
+    if (!ctx) return GKC_EINVAL;
+    if (n) *n = ctx->batch_ms.size();
+    for (uint64_t i = 0; ms && i < cap && i < ctx->batch_ms.size(); i++) ms[i] = ctx->batch_ms[i];
+    return GKC_OK;
 }
 
 int gkc_store_stats(gkc_ctx *ctx, uint64_t *pb, uint64_t *ps, uint64_t *pk) {

@@ -102,6 +102,7 @@ enum : uint32_t {
     ERR_TABLE_FULL = 1u << 2,       // hash table probe limit (host retries larger)
     ERR_OUTPUT_FULL = 1u << 3,      // output capacity exceeded
     ERR_DECODE = 1u << 4,           // malformed superkmer stream
+    ERR_CAPACITY = 1u << 5,         // phase-1 store chunk capacity exceeded (host redoes the batch)
 };
 
 }  // namespace gkc

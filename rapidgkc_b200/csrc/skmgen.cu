@@ -399,7 +399,8 @@ find_superkmers_kernel(P1Params a) {
 // partition walks the CTAs in order, so the layout is deterministic.
 __global__ void cta_offsets_kernel(const uint32_t *cta_hist, uint32_t ncta, uint32_t P,
                                    const unsigned long long *part_byte_off, const unsigned long long *part_skm_off,
-                                   unsigned long long *cta_base) {
+                                   unsigned long long *cta_base, const uint32_t *flags) {
+    if (*flags & (ERR_RECORD_OVERFLOW | ERR_CAPACITY)) return;  // the batch is redone
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
         unsigned long long b = part_byte_off[p], s = part_skm_off[p];
         for (uint32_t c = 0; c < ncta; c++) {
@@ -409,6 +410,48 @@ __global__ void cta_offsets_kernel(const uint32_t *cta_hist, uint32_t ncta, uint
             b += cta_hist[o + p];
             s += cta_hist[o + P + p];
         }
+    }
+}
+
+// Offsets of a batch's read set relative to its first read (device copy of
+// a slice of the caller's offsets).
+__global__ void rebase_offsets_kernel(uint64_t *offs, uint64_t n, uint64_t base) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        offs[i] -= base;
+}
+
+// A batch's store chunk layout from its partition totals (hist: bytes,
+// superkmers, k-mers per partition): exclusive scans into byte_off / skm_off
+// [P+1], k-mers copied out.  Raises ERR_CAPACITY when the chunk's preallocated
+// capacity is too small (cta_offsets and scatter then write nothing and the
+// host redoes the batch).  One CTA of PO_THREADS.
+constexpr int PO_THREADS = 1024;
+
+__global__ void __launch_bounds__(PO_THREADS)
+part_offsets_kernel(const unsigned long long *hist, uint32_t P, uint64_t byte_cap, uint64_t skm_cap,
+                    unsigned long long *byte_off, unsigned long long *skm_off, unsigned long long *kmers,
+                    uint32_t *flags) {
+    __shared__ unsigned long long ws[PO_THREADS / 32];
+    const uint32_t per = (P + PO_THREADS - 1) / PO_THREADS, p0 = threadIdx.x * per;
+    unsigned long long sb = 0, ss = 0;
+    for (uint32_t p = p0; p < p0 + per && p < P; p++) {
+        sb += hist[p];
+        ss += hist[P + p];
+        kmers[p] = hist[2 * P + p];
+    }
+    unsigned long long tb, ts;
+    unsigned long long ob = block_exclusive_scan<PO_THREADS>(sb, &tb, ws);
+    unsigned long long os = block_exclusive_scan<PO_THREADS>(ss, &ts, ws);
+    for (uint32_t p = p0; p < p0 + per && p < P; p++) {
+        byte_off[p] = ob;
+        skm_off[p] = os;
+        ob += hist[p];
+        os += hist[P + p];
+    }
+    if (threadIdx.x == 0) {
+        byte_off[P] = tb;
+        skm_off[P] = ts;
+        if (tb > byte_cap || ts > skm_cap) atomicOr(flags, ERR_CAPACITY);
     }
 }
 
@@ -424,6 +467,7 @@ struct P2Params {
     uint64_t pmod;
     const unsigned long long *part_byte_off;  // [P] partition start in `bytes`
     const unsigned long long *cta_base;       // [gridDim.x][2P] this CTA's first byte, superkmer per partition
+    const uint32_t *flags;                    // the batch's error flags: nothing is written after an overflow
     uint8_t *bytes;
     uint64_t *idx;
     uint32_t *keys;  // minimizer key of each superkmer, indexed like idx
@@ -437,6 +481,7 @@ __global__ void __launch_bounds__(P2_THREADS)
 scatter_superkmers_kernel(P2Params a) {
     extern __shared__ unsigned long long sbase[];  // [2P] CTA bases in each partition
     uint32_t *lcnt = reinterpret_cast<uint32_t *>(sbase + 2 * a.P);  // [2P] CTA-local cursors
+    if (*a.flags & (ERR_RECORD_OVERFLOW | ERR_CAPACITY)) return;  // the batch is redone
     const uint32_t n = a.region_count[blockIdx.x] < a.region_cap ? a.region_count[blockIdx.x] : a.region_cap;
     const SkmRecord *rec = a.records + (uint64_t)blockIdx.x * a.region_cap;
     // this CTA's ranges, laid out by cta_offsets_kernel from the find kernel's

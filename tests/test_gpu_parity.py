@@ -258,3 +258,51 @@ def test_count_partitions_subsets(oracle, kind):
                     c.add_reads(reads, offs)                  # store partly counted
         assert tot == sum(x[2] for x in per)
         assert c.store_stats()[2].sum() == 0                  # released after the last subset
+
+
+@pytest.mark.parametrize("kind", ["hash", "sort"])
+def test_uneven_host_batches(oracle, kind):
+    """Host reads of mixed lengths in caller-chosen batches of uneven size give
+    the oracle's partitions and counts; every batch reports its latency."""
+    k, p, P = 31, 11, 64
+    r = np.random.default_rng(71)
+    short, so = random_reads(72, 200_000, 20_000, 150, 0.003)
+    long_, lo = random_reads(73, 200_000, 60, (1000, 20_000), 0.02)
+    reads, offs = csr([short[int(so[i]):int(so[i + 1])].tobytes() for i in range(len(so) - 1)] +
+                      [long_[int(lo[i]):int(lo[i + 1])].tobytes() for i in range(len(lo) - 1)])
+    perm = r.permutation(len(offs) - 1)
+    reads, offs = csr([reads[int(offs[i]):int(offs[i + 1])].tobytes() for i in perm])
+    n = len(offs) - 1
+    cuts = np.sort(r.choice(np.arange(1, n), 6, replace=False))
+    batch_reads = np.diff(np.concatenate([[0], cuts, [n]])).astype(np.uint64)
+    pbo, pso, pko, _, _ = oracle.skmgen(reads, offs, k, p, P)
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P, 2, U32)
+    ko, co = sorted_table(ko, co)
+    with counter(k, p, P, kind) as c:
+        c.add_reads_batches(reads, offs, batch_reads)
+        t = c.batch_timings()
+        assert len(t) == len(batch_reads) and (t > 0).all()
+        pb, ps, pk = c.store_stats()
+        assert np.array_equal(pb, pbo) and np.array_equal(ps, pso) and np.array_equal(pk, pko)
+        n_out, d = c.count(2, U32)
+        km, ct = sorted_table(*c.result())
+    assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+
+
+def test_capacity_overflow_is_redone(oracle):
+    """With k = p every position starts a superkmer: far more superkmers and
+    bytes per base than phase 1 preallocates, so each batch overflows and is
+    redone with exact sizes; results match the oracle."""
+    k, p, P = 11, 11, 16
+    reads, offs = random_reads(81, 30_000, 3000, 150, 0.01)
+    pbo, pso, pko, _, _ = oracle.skmgen(reads, offs, k, p, P)
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P)
+    ko, co = sorted_table(ko, co)
+    with counter(k, p, P, "hash", batch_bases=100_000) as c:
+        c.add_reads(reads, offs)
+        pb, ps, pk = c.store_stats()
+        assert pso.sum() > offs[-1] // 2  # ~one superkmer per base
+        assert np.array_equal(pb, pbo) and np.array_equal(ps, pso) and np.array_equal(pk, pko)
+        n_out, d = c.count()
+        km, ct = sorted_table(*c.result())
+    assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
