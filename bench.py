@@ -171,7 +171,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--order", default="learned", choices=["learned", "default"],
                     help="minimizer order of the reported value (the other is measured beside it)")
+    ap.add_argument("--autotune", default=None, action=argparse.BooleanOptionalAction,
+                    help="pick partitions / counter / digit width / order / host batch size on a 10%% sample "
+                         "(default: on for mixed_100m)")
+    ap.add_argument("--batch-mb", default=None,
+                    help="end to end through host batches of random size in [lo,hi] MB, e.g. 64,512 "
+                         "(default: 64,512 for mixed_100m)")
     args = ap.parse_args()
+    if args.workload == "mixed_100m":
+        args.autotune = True if args.autotune is None else args.autotune
+        args.batch_mb = "64,512" if args.batch_mb is None else args.batch_mb
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -198,10 +207,23 @@ def main():
                                       read_seed=rank)
     t_gen = time.perf_counter() - t_gen
     bases = int(offs[-1])
+    tuned = None
+    batch_bases = 1 << 30
+    radix_bits = 8
+    if args.autotune:
+        from rapidgkc_b200.autotune import autotune
+        n_s = max(1, (len(offs) - 1) // 10)
+        s_reads = np.ascontiguousarray(reads[: int(offs[n_s])])
+        s_offs = np.ascontiguousarray(offs[: n_s + 1])
+        tuned = autotune(s_reads, s_offs, k=args.k, p=args.p, cmin=args.cmin, device=local)
+        o = tuned["options"]
+        args.partitions, args.counter, args.order = o["partitions"], o["counter"], o["order"]
+        batch_bases, radix_bits = o["batch_bases"], o["radix_bits"]
     d_reads = torch.from_numpy(reads).cuda()
     d_offs = torch.from_numpy(offs.view(np.int64)).cuda()
     stream = torch.cuda.Stream()
-    c = KmerCounter(k=args.k, p=args.p, partitions=args.partitions, counter=args.counter, device=local)
+    c = KmerCounter(k=args.k, p=args.p, partitions=args.partitions, counter=args.counter, device=local,
+                    radix_bits=radix_bits, batch_bases=batch_bases)
     c.set_stream(stream)
     learned_params = None
     if args.order == "learned":
@@ -280,7 +302,58 @@ def main():
 
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
-    if not args.no_e2e:
+    batching = None
+    if not args.no_e2e and args.batch_mb:
+        # host batches of random size in [lo, hi] MB (whole reads), one pipeline
+        lo_mb, hi_mb = (float(x) for x in args.batch_mb.split(","))
+        rng = np.random.default_rng(11)
+        cuts, pos = [], 0
+        while pos < bases:
+            target = pos + int(rng.uniform(lo_mb, hi_mb) * (1 << 20))
+            r1 = int(np.searchsorted(offs, min(target, bases), side="right")) - 1
+            r1 = max(r1, (cuts[-1] if cuts else 0) + 1)
+            cuts.append(min(r1, len(offs) - 1))
+            pos = int(offs[cuts[-1]])
+        batch_reads = np.diff(np.concatenate([[0], cuts])).astype(np.uint64)
+        cap = int(n_out * 1.05) + 1024
+        hk = torch.empty(cap, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+        hc = torch.empty(cap, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+
+        def step_batched():
+            c.store_clear()
+            c.add_reads_batches(reads, offs, batch_reads)
+            lat = c.batch_timings()
+            no, _ = c.count(args.cmin)
+            c.result_into(hk, hc)
+            return no, lat
+
+        for _ in range(max(1, args.warmup // 2)):
+            step_batched()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        lats = []
+        e0.record(stream)
+        for _ in range(args.steps):
+            no, lat = step_batched()
+            lats.extend(lat.tolist())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": bases * world / (ems / 1e3) / 1e9, "unit": "Gbp/s",
+               "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)), "d2h_bytes_per_step": int(12 * no),
+               "ms_per_step": ems, "path": "gkc_add_reads_batches + gkc_count + gkc_result"}
+        sizes = np.diff(offs[np.concatenate([[0], cuts])].astype(np.int64)) / (1 << 20)
+        batching = {"batches_per_step": len(batch_reads), "batch_mb_min": float(sizes.min()),
+                    "batch_mb_max": float(sizes.max()),
+                    "latency_ms": {"p50": float(np.percentile(lats, 50)), "p95": float(np.percentile(lats, 95)),
+                                   "max": float(np.max(lats))},
+                    "note": "latency = one batch's host-to-device copy start to its phase-1 end (CUDA events)"}
+    elif not args.no_e2e:
         cap = int(n_out * 1.05) + 1024
         hk = torch.empty(cap, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
         hc = torch.empty(cap, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
@@ -340,12 +413,17 @@ def main():
                        "bases_per_rank": bases, "reads_per_rank": len(offs) - 1, "k": args.k, "p": args.p,
                        "partitions": args.partitions, "counter": args.counter, "order": args.order,
                        "threshold": f">={args.cmin}", "parallelism": f"dp{world} (independent read sets)",
-                       "l2": "inputs (3 GB) larger than L2; no flush", "kmers_kept": n_out,
+                       "l2": f"inputs ({bases / 1e9:.1f} GB) larger than L2; no flush", "kmers_kept": n_out,
                        "distinct": n_dist, "gen_s": round(t_gen, 1),
                        "sub_buckets": tstats["sub_buckets"], "overflowed": tstats["overflowed_sub_buckets"],
                        "phase1_ms": round(tstats["phase1_ms"], 2), "phase2_ms": round(tstats["phase2_ms"], 2)},
             "orders": orders, "roofline": roofline, "counting_phase": counting, "e2e": e2e,
             "gpu_launches": int(launches)}
+    if batching:
+        line["batching"] = batching
+    if tuned:
+        line["autotune"] = {"options": tuned["options"], "sample_gbps": tuned["gbps"],
+                            "trials": len(tuned["trials"]) + len(tuned["batch_trials"])}
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s

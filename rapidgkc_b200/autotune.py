@@ -1,0 +1,129 @@
+"""Autotuner for the counter's launch parameters.
+
+The reference takes its launch configuration from the command line
+(CUDAParams BpG1/TpB1/BpG2/TpB2, utilities.hpp:296-309; -skm partitions). Here
+the parameters that change throughput are measured on a sample of the
+caller's own reads, and the fastest combination is kept:
+
+  partitions    P of the store (more partitions: smaller sub-buckets and sort
+                groups; fewer: more aggregation in phase 1)
+  counter       the shared-memory hash counter or the LSD radix sort
+  radix_bits    the sort counter's digit width
+  order         the default or the learned minimizer order
+  batch_bases   host batch size of gkc_add_reads (timed end to end, from
+                pinned host reads)
+
+Every candidate counts the same sample and must give the same (k-mer, count)
+result; a candidate that does not is an error, not a slower choice.
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import os
+import time
+
+import numpy as np
+
+from .capi import KmerCounter
+
+_CACHE: dict = {}
+
+
+def _signature(offs: np.ndarray, k: int, p: int) -> str:
+    lens = np.diff(offs.astype(np.int64))
+    return json.dumps({"reads": int(len(lens)), "bases": int(offs[-1]), "mean_len": round(float(lens.mean()), 1),
+                       "max_len": int(lens.max()), "k": k, "p": p})
+
+
+def _digest(c: KmerCounter):
+    km, ct = c.result()
+    return (int(np.bitwise_xor.reduce(km)) if len(km) else 0, int(np.sum(km * ct.astype(np.uint64), dtype=np.uint64)),
+            len(km))
+
+
+def autotune(reads: np.ndarray, offs: np.ndarray, k: int = 31, p: int = 11, cmin: int = 2, device: int = 0,
+             partitions=(256, 512, 1024), counters=("hash", "sort"), radix_bits=(6, 8), orders=("default", "learned"),
+             batch_bases=(1 << 26, 1 << 28, 1 << 30), repeats: int = 2, verbose: bool = False) -> dict:
+    """Measures every combination on (reads, offs) (a host CSR sample of the
+    workload, ideally a few hundred Mbp) and returns the fastest:
+    {"options": {...}, "gbps": ..., "trials": [...]}.  Results are cached per
+    sample signature for the process."""
+    import torch
+
+    sig = _signature(offs, k, p)
+    if sig in _CACHE:
+        return _CACHE[sig]
+    from .order import default_order_path, load_order
+    learned = load_order(default_order_path(p))[0] if "learned" in orders and p == 11 else None
+    d_reads = torch.from_numpy(reads).cuda(device)
+    d_offs = torch.from_numpy(offs.view(np.int64)).cuda(device)
+    bases = int(offs[-1])
+    trials, ref = [], None
+    combos = []
+    for P, counter, order in itertools.product(partitions, counters, orders):
+        if order == "learned" and learned is None:
+            continue
+        for rb in (radix_bits if counter == "sort" else (8,)):
+            combos.append((P, counter, rb, order))
+    stream = torch.cuda.Stream(device)
+    for P, counter, rb, order in combos:
+        with KmerCounter(k=k, p=p, partitions=P, counter=counter, radix_bits=rb, device=device) as c:
+            c.set_stream(stream)
+            if order == "learned":
+                c.mlp_order(learned)
+            c.count_reads(d_reads, d_offs, cmin)  # warm-up
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(device)
+            ev0.record(stream)
+            for _ in range(repeats):
+                c.count_reads(d_reads, d_offs, cmin)
+            ev1.record(stream)
+            torch.cuda.synchronize(device)
+            ms = ev0.elapsed_time(ev1) / repeats
+            dg = _digest(c)
+        if ref is None:
+            ref = dg
+        elif dg != ref:
+            raise RuntimeError(f"autotune: results differ for P={P} counter={counter} radix_bits={rb} order={order}")
+        t = {"partitions": P, "counter": counter, "radix_bits": rb, "order": order, "gbps": bases / ms / 1e6}
+        trials.append(t)
+        if verbose:
+            print(t, flush=True)
+    best = max(trials, key=lambda t: t["gbps"])
+    # host batch size, end to end from pinned host memory, with the best device settings
+    pinned_r = torch.from_numpy(reads).pin_memory().numpy()
+    pinned_o = torch.from_numpy(offs.view(np.int64)).pin_memory().numpy().view(np.uint64)
+    bb_trials = []
+    for bb in batch_bases:
+        with KmerCounter(k=k, p=p, partitions=best["partitions"], counter=best["counter"],
+                         radix_bits=best["radix_bits"], batch_bases=bb, device=device) as c:
+            if best["order"] == "learned":
+                c.mlp_order(learned)
+            c.count_reads(pinned_r, pinned_o, cmin)
+            t0 = time.perf_counter()
+            for _ in range(repeats):
+                c.count_reads(pinned_r, pinned_o, cmin)
+            s = (time.perf_counter() - t0) / repeats
+        bb_trials.append({"batch_bases": bb, "e2e_gbps": bases / s / 1e9})
+    bbest = max(bb_trials, key=lambda t: t["e2e_gbps"])
+    out = {"options": {"partitions": best["partitions"], "counter": best["counter"],
+                       "radix_bits": best["radix_bits"], "order": best["order"],
+                       "batch_bases": bbest["batch_bases"]},
+           "gbps": best["gbps"], "e2e_gbps": bbest["e2e_gbps"], "trials": trials, "batch_trials": bb_trials,
+           "sample": json.loads(sig)}
+    _CACHE[sig] = out
+    return out
+
+
+if __name__ == "__main__":
+    import argparse
+
+    from . import synth
+
+    ap = argparse.ArgumentParser(description="autotune the counter on a sample of a synthetic workload")
+    ap.add_argument("--workload", default="mixed_100m")
+    ap.add_argument("--fraction", type=float, default=0.1)
+    args = ap.parse_args()
+    r, o = synth.make_workload(args.workload, read_fraction=args.fraction, threads=os.cpu_count() or 1)
+    print(json.dumps(autotune(r, o, verbose=True)), flush=True)

@@ -249,6 +249,14 @@ class KmerCounter:
         self._check(self._L.gkc_result(self._h, _ptr(km)[0], _ptr(ct)[0], n, MEM_HOST))
         return km[:n], ct[:n]
 
+    def result_into(self, out_kmers, out_counts) -> int:
+        """Copies the last count's result into the given arrays (host or CUDA,
+        min(len, n) entries); returns n."""
+        kp, km = _ptr(out_kmers)
+        cp, _ = _ptr(out_counts)
+        self._check(self._L.gkc_result(self._h, kp, cp, len(out_kmers), km))
+        return self.result_device()[2]
+
     def result_device(self):
         kp, cp, nn = C.c_void_p(), C.c_void_p(), C.c_uint64(0)
         self._check(self._L.gkc_result_device(self._h, C.byref(kp), C.byref(cp), C.byref(nn)))
