@@ -63,8 +63,10 @@ def build_cli(force: bool = False) -> str:
     src = os.path.join(CSRC, "gkc_main.cpp")
     lib = build_cuda()
     if os.path.exists(src) and (force or _stale(out, [src, lib])):
+        cuda = os.path.dirname(os.path.dirname(NVCC))
         _run(["g++", "-std=c++17", "-O2", "-o", out, src, "-I", os.path.join(ROOT, "include"),
-              "-L", PKG, "-lrapidgkc_b200", "-Wl,-rpath,$ORIGIN", "-pthread"])
+              "-I", os.path.join(cuda, "include"), "-L", PKG, "-lrapidgkc_b200", "-L", os.path.join(cuda, "lib64"),
+              "-lcudart", "-lz", "-Wl,-rpath,$ORIGIN", "-pthread"])
     return out
 
 

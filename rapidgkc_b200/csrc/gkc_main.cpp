@@ -1,0 +1,384 @@
+// gkc_main.cpp -- command-line k-mer counter on the B200 library.
+//
+// Takes RapidGKC's own flags (gkc_main.cpp / utilities.hpp:222-270 of the
+// reference): -k, -p, -skm, -read <files...>, and accepts its thread, launch
+// and file-store flags (the library picks launch shapes itself and keeps the
+// store in device memory).  Adds what the reference declares but never does:
+// the count threshold (utilities.hpp:190) and an output of the counted
+// k-mers.
+//
+//   gkc_main -k 31 -p 11 -skm 512 -ci 2 -o counts.bin -read reads.fq.gz [more files]
+//
+// Output (-o): binary (-of bin, default): "GKCB1\0\0\0", u32 k, u32 0, u64 n,
+// then n records of u64 k-mer (2-bit, first base in the most significant
+// position, canonical) and u32 count, little-endian, 12 bytes each; or text
+// (-of txt): "<k-mer>\t<count>\n".  Order: the library's (per partition;
+// ascending within a partition with -counter sort), or ascending k-mer with
+// -sorted.
+//
+// Input: FASTA or FASTQ, plain or gzip (zlib reads both).  A parser thread
+// fills pinned batches of about -bb MB while the main thread hands the
+// previous batch to the GPU.
+#include <cuda_runtime.h>
+#include <zlib.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <unistd.h>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "gkc_capi.h"
+
+namespace {
+
+struct Args {
+    int k = 31, p = 11, partitions = 512, device = 0;
+    uint32_t cmin = 1, cmax = 0xFFFFFFFFu;
+    std::string out, fmt = "bin", counter = "hash", order = "default";
+    bool sorted = false;
+    uint64_t batch_mb = 1024;
+    std::vector<std::string> files;
+};
+
+[[noreturn]] void usage(const char *prog, const char *why) {
+    std::fprintf(stderr,
+                 "%s\nUsage: %s -k <K> -p <P> -skm <partitions> [-ci <min count>] [-cx <max count>]\n"
+                 "       [-o <output>] [-of bin|txt] [-sorted] [-counter hash|sort]\n"
+                 "       [-order default|learned|<params.f32>] [-gpu <device>] [-bb <batch MB>] -read <files...>\n"
+                 "       (-t -tgpu -t2 -tgz -tsort -tmp -im -fb -rb -grid -block -grid2 -block2 -ns1 -ns2 -rps\n"
+                 "        -gpuonly -log -lv are accepted for compatibility and have no effect)\n",
+                 why, prog);
+    std::exit(2);
+}
+
+Args parse_args(int argc, char **argv) {
+    Args a;
+    auto need = [&](int &i) -> const char * {
+        if (i + 1 >= argc) usage(argv[0], "missing value");
+        return argv[++i];
+    };
+    for (int i = 1; i < argc; i++) {
+        const std::string f = argv[i];
+        if (f == "-k") a.k = std::atoi(need(i));
+        else if (f == "-p") a.p = std::atoi(need(i));
+        else if (f == "-skm") a.partitions = std::atoi(need(i));
+        else if (f == "-ci") a.cmin = (uint32_t)std::strtoul(need(i), nullptr, 10);
+        else if (f == "-cx") a.cmax = (uint32_t)std::strtoul(need(i), nullptr, 10);
+        else if (f == "-o") a.out = need(i);
+        else if (f == "-of") a.fmt = need(i);
+        else if (f == "-sorted") a.sorted = true;
+        else if (f == "-counter") a.counter = need(i);
+        else if (f == "-order") a.order = need(i);
+        else if (f == "-gpu") a.device = std::atoi(need(i));
+        else if (f == "-bb") a.batch_mb = std::strtoull(need(i), nullptr, 10);
+        else if (f == "-hpc") {
+            if (std::atoi(need(i)) != 0) usage(argv[0], "homopolymer compression (-hpc 1) is not supported");
+        } else if (f == "-ngpu") {
+            if (std::atoi(need(i)) > 1) usage(argv[0], "one GPU per process (-ngpu 1)");
+        } else if (f == "-cpuonly") {
+            usage(argv[0], "there is no CPU path (-cpuonly)");
+        } else if (f == "-t" || f == "-tgpu" || f == "-t2" || f == "-tgz" || f == "-tsort" || f == "-tmp" ||
+                   f == "-fb" || f == "-rb" || f == "-grid" || f == "-block" || f == "-grid2" || f == "-block2" ||
+                   f == "-ns1" || f == "-ns2" || f == "-rps" || f == "-log" || f == "-lv") {
+            need(i);
+        } else if (f == "-im" || f == "-gpuonly") {
+        } else if (f == "-read") {
+            while (i + 1 < argc && argv[i + 1][0] != '-') a.files.push_back(argv[++i]);
+        } else {
+            usage(argv[0], ("unknown argument " + f).c_str());
+        }
+    }
+    if (a.files.empty()) usage(argv[0], "no input (-read)");
+    if (a.fmt != "bin" && a.fmt != "txt") usage(argv[0], "-of must be bin or txt");
+    if (a.counter != "hash" && a.counter != "sort") usage(argv[0], "-counter must be hash or sort");
+    if (a.cmin > a.cmax) usage(argv[0], "-ci is larger than -cx");
+    return a;
+}
+
+void check(int rc, gkc_ctx *ctx, const char *what) {
+    if (rc != GKC_OK) {
+        std::fprintf(stderr, "gkc_main: %s: %s (%s)\n", what, gkc_strerror(rc), ctx ? gkc_last_error(ctx) : "");
+        std::exit(1);
+    }
+}
+
+// A batch of reads in pinned host memory (CSR).
+struct Batch {
+    char *bases = nullptr;
+    uint64_t *offs = nullptr;
+    uint64_t cap_bases = 0, cap_reads = 0, n_reads = 0;
+    void reserve(uint64_t nb, uint64_t nr) {
+        if (nb > cap_bases) {
+            if (bases) cudaFreeHost(bases);
+            cap_bases = nb + nb / 4;
+            if (cudaHostAlloc(reinterpret_cast<void **>(&bases), cap_bases, cudaHostAllocDefault) != cudaSuccess) {
+                std::fprintf(stderr, "gkc_main: pinned allocation of %llu bytes failed\n",
+                             (unsigned long long)cap_bases);
+                std::exit(1);
+            }
+        }
+        if (nr + 1 > cap_reads) {
+            if (offs) cudaFreeHost(offs);
+            cap_reads = nr + nr / 4 + 2;
+            if (cudaHostAlloc(reinterpret_cast<void **>(&offs), cap_reads * 8, cudaHostAllocDefault) != cudaSuccess) {
+                std::fprintf(stderr, "gkc_main: pinned allocation failed\n");
+                std::exit(1);
+            }
+        }
+    }
+    ~Batch() {
+        if (bases) cudaFreeHost(bases);
+        if (offs) cudaFreeHost(offs);
+    }
+};
+
+// FASTA/FASTQ records, plain or gzip, sequence lines only.
+class Reader {
+public:
+    explicit Reader(const std::string &path) : fp_(gzopen(path.c_str(), "rb")), path_(path) {
+        if (!fp_) {
+            std::fprintf(stderr, "gkc_main: cannot open %s\n", path.c_str());
+            std::exit(1);
+        }
+        gzbuffer(fp_, 1 << 20);
+    }
+    ~Reader() { gzclose(fp_); }
+    // Appends the next record's sequence to seq; false at end of input.
+    bool next(std::string &seq) {
+        seq.clear();
+        if (!line(line_)) return false;
+        while (line_.empty())
+            if (!line(line_)) return false;
+        if (line_[0] == '@') {  // FASTQ: header, sequence, '+', qualities
+            if (!line(seq)) bad();
+            std::string plus, qual;
+            if (!line(plus) || plus.empty() || plus[0] != '+' || !line(qual)) bad();
+            return true;
+        }
+        if (line_[0] == '>') {  // FASTA: header, then sequence lines up to the next '>'
+            while (peek() != '>' && peek() != EOF) {
+                if (!line(tmp_)) break;
+                seq += tmp_;
+            }
+            return true;
+        }
+        bad();
+    }
+
+private:
+    [[noreturn]] void bad() {
+        std::fprintf(stderr, "gkc_main: %s is not FASTA or FASTQ\n", path_.c_str());
+        std::exit(1);
+    }
+    int peek() {
+        const int c = gzgetc(fp_);
+        if (c != -1) gzungetc(c, fp_);
+        return c;
+    }
+    bool line(std::string &out) {
+        out.clear();
+        char buf[1 << 14];
+        while (gzgets(fp_, buf, sizeof(buf))) {
+            size_t n = std::strlen(buf);
+            const bool eol = n && buf[n - 1] == '\n';
+            if (eol) n--;
+            if (n && buf[n - 1] == '\r') n--;
+            out.append(buf, n);
+            if (eol) return true;
+        }
+        return !out.empty();
+    }
+    gzFile fp_;
+    std::string path_, line_, tmp_;
+};
+
+std::vector<float> load_params(const std::string &path, uint64_t n) {
+    std::vector<float> v(n);
+    FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f || std::fread(v.data(), 4, n, f) != n) {
+        std::fprintf(stderr, "gkc_main: cannot read %llu parameters from %s\n", (unsigned long long)n, path.c_str());
+        std::exit(1);
+    }
+    std::fclose(f);
+    return v;
+}
+
+std::string exe_dir() {
+    char buf[4096];
+    const ssize_t n = readlink("/proc/self/exe", buf, sizeof(buf) - 1);
+    if (n <= 0) return ".";
+    std::string s(buf, (size_t)n);
+    return s.substr(0, s.rfind('/'));
+}
+
+void write_output(const Args &a, const uint64_t *km, const uint32_t *ct, uint64_t n) {
+    FILE *f = std::fopen(a.out.c_str(), "wb");
+    if (!f) {
+        std::fprintf(stderr, "gkc_main: cannot write %s\n", a.out.c_str());
+        std::exit(1);
+    }
+    std::vector<char> buf;
+    buf.reserve(1 << 24);
+    auto flush = [&]() {
+        if (!buf.empty() && std::fwrite(buf.data(), 1, buf.size(), f) != buf.size()) {
+            std::fprintf(stderr, "gkc_main: write to %s failed\n", a.out.c_str());
+            std::exit(1);
+        }
+        buf.clear();
+    };
+    if (a.fmt == "bin") {
+        const char magic[8] = {'G', 'K', 'C', 'B', '1', 0, 0, 0};
+        const uint32_t hk[2] = {(uint32_t)a.k, 0};
+        buf.insert(buf.end(), magic, magic + 8);
+        buf.insert(buf.end(), reinterpret_cast<const char *>(hk), reinterpret_cast<const char *>(hk) + 8);
+        buf.insert(buf.end(), reinterpret_cast<const char *>(&n), reinterpret_cast<const char *>(&n) + 8);
+        for (uint64_t i = 0; i < n; i++) {
+            buf.insert(buf.end(), reinterpret_cast<const char *>(km + i), reinterpret_cast<const char *>(km + i) + 8);
+            buf.insert(buf.end(), reinterpret_cast<const char *>(ct + i), reinterpret_cast<const char *>(ct + i) + 4);
+            if (buf.size() > (1u << 24) - 64) flush();
+        }
+    } else {
+        char rec[64];
+        for (uint64_t i = 0; i < n; i++) {
+            for (int j = 0; j < a.k; j++) rec[j] = "ACGT"[(km[i] >> (2 * (a.k - 1 - j))) & 3];
+            const int m = std::snprintf(rec + a.k, sizeof(rec) - a.k, "\t%u\n", ct[i]);
+            buf.insert(buf.end(), rec, rec + a.k + m);
+            if (buf.size() > (1u << 24) - 64) flush();
+        }
+    }
+    flush();
+    std::fclose(f);
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    const Args a = parse_args(argc, argv);
+    const auto t_start = std::chrono::steady_clock::now();
+    auto secs = [&]() {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    };
+    gkc_options opt;
+    gkc_default_options(&opt);
+    opt.k = a.k;
+    opt.p = a.p;
+    opt.partitions = a.partitions;
+    opt.counter = a.counter == "sort" ? GKC_COUNTER_SORT : GKC_COUNTER_HASH;
+    gkc_ctx *ctx = nullptr;
+    check(gkc_create(a.device, &opt, &ctx), nullptr, "create");
+    if (a.order != "default") {
+        const std::string path = a.order == "learned" ? exe_dir() + "/orders/skewed_m" + std::to_string(a.p) + ".f32"
+                                                      : a.order;
+        const std::vector<float> params = load_params(path, gkc_mlp_param_count(a.p));
+        check(gkc_mlp_order(ctx, params.data(), 0, nullptr), ctx, "learned order");
+    }
+    // ---- phase 1: a parser thread fills one pinned batch while the GPU takes the other
+    const uint64_t batch_bases = a.batch_mb << 20;
+    Batch batches[2];
+    std::mutex mu;
+    std::condition_variable cv;
+    bool full[2] = {false, false}, eof = false;
+    uint64_t produced = 0, consumed = 0;
+    uint64_t n_reads = 0, n_bases = 0;
+    std::thread parser([&]() {  // fills slots 0, 1, 0, ... in turn
+        std::string seq;
+        size_t fi = 0;
+        Reader *rd = new Reader(a.files[0]);
+        for (int slot = 0;; slot ^= 1) {
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait(lk, [&]() { return !full[slot]; });
+            }
+            Batch &b = batches[slot];
+            uint64_t nb = 0, nr = 0;
+            bool end = false;
+            b.reserve(batch_bases + (1 << 20), 1 << 20);
+            b.offs[0] = 0;
+            while (nb < batch_bases) {
+                if (!rd->next(seq)) {
+                    delete rd;
+                    rd = nullptr;
+                    if (++fi == a.files.size()) {
+                        end = true;
+                        break;
+                    }
+                    rd = new Reader(a.files[fi]);
+                    continue;
+                }
+                b.reserve(nb + seq.size() + (1 << 20), nr + 1);
+                std::memcpy(b.bases + nb, seq.data(), seq.size());
+                nb += seq.size();
+                b.offs[++nr] = nb;
+            }
+            b.n_reads = nr;
+            std::lock_guard<std::mutex> lk(mu);
+            if (nr) {
+                full[slot] = true;
+                produced++;
+            }
+            eof = end;
+            cv.notify_all();
+            if (end) break;
+        }
+        delete rd;
+    });
+    for (int slot = 0;; slot ^= 1) {  // takes slots 0, 1, 0, ... in turn
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&]() { return full[slot] || (eof && consumed == produced); });
+            if (!full[slot]) break;
+        }
+        Batch &b = batches[slot];
+        check(gkc_add_reads(ctx, b.bases, b.offs, b.n_reads, GKC_MEM_HOST), ctx, "phase 1");
+        n_reads += b.n_reads;
+        n_bases += b.offs[b.n_reads];
+        std::lock_guard<std::mutex> lk(mu);
+        full[slot] = false;
+        consumed++;
+        cv.notify_all();
+    }
+    parser.join();
+    const double t1 = secs();
+    // ---- phase 2
+    uint64_t n_out = 0, n_distinct = 0;
+    check(gkc_count(ctx, a.cmin, a.cmax, &n_out, &n_distinct), ctx, "phase 2");
+    const double t2 = secs();
+    if (!a.out.empty()) {
+        uint64_t *km = nullptr;
+        uint32_t *ct = nullptr;
+        if (cudaHostAlloc(reinterpret_cast<void **>(&km), std::max<uint64_t>(n_out, 1) * 8, 0) != cudaSuccess ||
+            cudaHostAlloc(reinterpret_cast<void **>(&ct), std::max<uint64_t>(n_out, 1) * 4, 0) != cudaSuccess) {
+            std::fprintf(stderr, "gkc_main: pinned allocation for %llu results failed\n", (unsigned long long)n_out);
+            return 1;
+        }
+        check(gkc_result(ctx, km, ct, n_out, GKC_MEM_HOST), ctx, "result");
+        if (a.sorted) {
+            std::vector<uint64_t> ix(n_out);
+            for (uint64_t i = 0; i < n_out; i++) ix[i] = i;
+            std::sort(ix.begin(), ix.end(), [&](uint64_t x, uint64_t y) { return km[x] < km[y]; });
+            std::vector<uint64_t> k2(n_out);
+            std::vector<uint32_t> c2(n_out);
+            for (uint64_t i = 0; i < n_out; i++) k2[i] = km[ix[i]], c2[i] = ct[ix[i]];
+            write_output(a, k2.data(), c2.data(), n_out);
+        } else {
+            write_output(a, km, ct, n_out);
+        }
+        cudaFreeHost(km);
+        cudaFreeHost(ct);
+    }
+    const double t3 = secs();
+    std::fprintf(stderr,
+                 "reads %llu, bases %llu, distinct k-mers %llu, written %llu (count in [%u, %u])\n"
+                 "phase 1 %.3f s, phase 2 %.3f s, output %.3f s, total %.3f s (%.2f Gbp/s)\n",
+                 (unsigned long long)n_reads, (unsigned long long)n_bases, (unsigned long long)n_distinct,
+                 (unsigned long long)n_out, a.cmin, a.cmax, t1, t2 - t1, t3 - t2, t3, n_bases / t3 / 1e9);
+    gkc_destroy(ctx);
+    return 0;
+}

@@ -147,7 +147,10 @@ def train_order(workload: str = "skewed_200m", seeds=range(1, 9), scale: float =
 
 
 def save_order(path: str, params: np.ndarray, p: int, meta: dict) -> None:
+    """The parameters with their training metadata (.npz), and as raw
+    little-endian float32 beside it (.f32, read by gkc_main -order learned)."""
     np.savez(path, params=params.astype(np.float32), p=np.int32(p), meta=np.array(repr(meta)))
+    params.astype("<f4").tofile(os.path.splitext(path)[0] + ".f32")
 
 
 def load_order(path: str):

@@ -1,0 +1,80 @@
+"""gkc_main, the command-line counter: argument handling (CPU) and its output
+against the oracle on FASTQ / gzip FASTA input (GPU)."""
+import gzip
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, sorted_table
+from tests_util import random_reads
+
+CLI = os.path.join(ROOT, "rapidgkc_b200", "gkc_main")
+U32 = 0xFFFFFFFF
+
+
+def _run(*args, check=True):
+    p = subprocess.run([CLI, *args], capture_output=True, text=True, timeout=600)
+    if check and p.returncode != 0:
+        raise AssertionError(f"gkc_main {' '.join(args)} -> {p.returncode}\n{p.stderr}")
+    return p
+
+
+@pytest.mark.parametrize("args,msg", [([], "no input"), (["-cpuonly", "-read", "x.fq"], "no CPU path"),
+                                      (["-of", "csv", "-read", "x.fq"], "-of must be"),
+                                      (["-ngpu", "2", "-read", "x.fq"], "one GPU"),
+                                      (["-ci", "5", "-cx", "2", "-read", "x.fq"], "larger than")])
+def test_cli_rejects_bad_arguments(args, msg):
+    p = _run(*args, check=False)
+    assert p.returncode == 2 and msg in p.stderr
+
+
+def _write_inputs(tmp, reads, offs):
+    seqs = [reads[int(offs[i]):int(offs[i + 1])].tobytes() for i in range(len(offs) - 1)]
+    h = len(seqs) // 2
+    fq = os.path.join(tmp, "a.fq")
+    with open(fq, "wb") as f:
+        for i, s in enumerate(seqs[:h]):
+            f.write(b"@r%d\n%s\n+\n%s\n" % (i, s, b"I" * len(s)))
+    fa = os.path.join(tmp, "b.fa.gz")
+    with gzip.open(fa, "wb") as f:
+        for i, s in enumerate(seqs[h:]):
+            f.write(b">r%d description\n" % i)
+            for j in range(0, len(s), 60):  # multi-line FASTA, with a CRLF line
+                f.write(s[j:j + 60] + (b"\r\n" if j == 0 else b"\n"))
+    return fq, fa
+
+
+def _read_bin(path):
+    b = open(path, "rb").read()
+    assert b[:8] == b"GKCB1\0\0\0"
+    k, _, n = np.frombuffer(b[8:24], np.uint32)[0], 0, int(np.frombuffer(b[16:24], np.uint64)[0])
+    rec = np.frombuffer(b[24:], dtype=np.dtype([("k", "<u8"), ("c", "<u4")]), count=n)
+    return int(k), rec["k"].copy(), rec["c"].copy()
+
+
+@pytest.mark.gpu
+def test_cli_counts_match_oracle(oracle, tmp_path):
+    k, p, P = 25, 11, 32
+    reads, offs = random_reads(91, 30_000, 4000, (60, 400), 0.005)
+    fq, fa = _write_inputs(str(tmp_path), reads, offs)
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P, 2, U32)
+    ko, co = sorted_table(ko, co)
+    out = str(tmp_path / "counts.bin")
+    p_ = _run("-k", str(k), "-p", str(p), "-skm", str(P), "-ci", "2", "-o", out, "-sorted", "-t", "8",
+              "-read", fq, fa)
+    assert f"distinct k-mers {do}" in p_.stderr
+    kk, km, ct = _read_bin(out)
+    assert kk == k and np.all(np.diff(km.astype(np.int64)) > 0)
+    assert np.array_equal(km, ko) and np.array_equal(ct, co)
+    # text output, sort counter, learned order: the same multiset
+    out2 = str(tmp_path / "counts.txt")
+    _run("-k", str(k), "-p", str(p), "-skm", str(P), "-ci", "2", "-o", out2, "-of", "txt", "-counter", "sort",
+         "-order", "learned", "-bb", "1", "-read", fq, fa)
+    lines = open(out2).read().split()
+    code = {"A": 0, "C": 1, "G": 2, "T": 3}
+    km2 = np.array([int("".join(str(code[ch]) for ch in s), 4) for s in lines[0::2]], np.uint64)
+    ct2 = np.array(lines[1::2], np.uint32)
+    km2, ct2 = sorted_table(km2, ct2)
+    assert np.array_equal(km2, ko) and np.array_equal(ct2, co)
