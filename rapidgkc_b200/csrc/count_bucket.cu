@@ -11,9 +11,9 @@
 //            superkmers and k-mers per sub-bucket (shared-memory aggregated),
 //            a scan, then a scatter of 16-byte entries {first byte address,
 //            k-mer count} into sub-bucket order;
-//   count    one CTA per sub-bucket: warps decode their superkmers 32 k-mers
-//            at a time (warp_kmers below), merge equal neighbouring k-mers into
-//            runs, and add the runs to a shared-memory table with
+//   count    one CTA per sub-bucket: warps decode their superkmers 32 quads
+//            of consecutive k-mers at a time (warp_kmer_runs below), merge equal
+//            neighbouring k-mers into runs, and add the runs to a shared-memory table with
 //            shared-memory atomics; then the k-mers whose count lies in
 //            [cmin, cmax] are written with one global atomic per CTA.  A
 //            sub-bucket whose distinct k-mers outgrow the table is abandoned
@@ -44,7 +44,7 @@ __device__ __forceinline__ uint32_t bucket_of(uint32_t key, int s_log) {
 // Superkmer bytes hold three 2-bit bases in their low six bits, first base
 // highest; a superkmer's first byte holds 3 - (its header) bases of padding
 // before its first base.  The j-th k-mer of a superkmer therefore starts at
-// base slot u = pad + j, i.e. byte u/3, slot u%3, and spans at most 12 bytes.
+// base slot u = pad + j, i.e. byte u/3, slot u%3.
 
 // Six-bit fields of eight bytes (byte 0 first) packed into 48 bits, byte 0's
 // bases highest.
@@ -57,36 +57,20 @@ __device__ __forceinline__ uint64_t pack6x8(uint64_t le) {
     return x;
 }
 
-__device__ __forceinline__ uint32_t pack6x4(uint32_t le) {
-    uint32_t y = __byte_perm(le, 0, 0x0123) & 0x3F3F3F3Fu;
-    y = ((y >> 2) & 0x0FC00FC0u) | (y & 0x003F003Fu);
-    y = ((y >> 4) & 0x00FFF000u) | (y & 0x00000FFFu);
-    return y;
-}
+constexpr int KQ = 4;  // k-mers per lane per step (a quad)
 
-// The k-mer whose first base is slot u of the superkmer at p (k <= 32).
-// Reads the aligned 8-byte words covering bytes u/3 .. u/3+11 (store buffers
-// carry 32 bytes of padding).
-__device__ __forceinline__ uint64_t kmer_at(const uint8_t *p, uint32_t u, int k, uint64_t mask) {
-    const uint32_t bi = u / 3, s = u - 3 * bi;
-    const uintptr_t a = reinterpret_cast<uintptr_t>(p) + bi;
-    const uint64_t *w = reinterpret_cast<const uint64_t *>(a & ~(uintptr_t)7);
-    const uint32_t sh = 8 * (uint32_t)(a & 7);
-    const uint64_t w0 = w[0], w1 = w[1], w2 = w[2];
-    const uint64_t lo = sh ? (w0 >> sh) | (w1 << (64 - sh)) : w0;  // bytes 0..7
-    const uint64_t hi = sh ? (w1 >> sh) | (w2 << (64 - sh)) : w1;  // bytes 8..15
-    // 36 bases: 24 from the first eight bytes, 12 from the next four
-    const unsigned __int128 v = ((unsigned __int128)pack6x8(lo) << 24) | pack6x4((uint32_t)hi);
-    return (uint64_t)(v >> (72 - 2 * (s + (uint32_t)k))) & mask;
-}
-
-// For the entries ent[b .. b+32) of a warp (b + lane < end), calls
-// f(key, valid) on every lane once per 32 k-mers, in superkmer order:
-// lane l gets the (32*i + l)-th k-mer of the batch.  Must be called by the
-// whole warp.
-template <bool CANONICAL, class F>
-__device__ __forceinline__ void warp_kmers(const BEntry *ent, uint64_t b, uint64_t end, int k, uint64_t mask,
-                                           F &&f) {
+// Calls f(key, run) for every canonical k-mer of the entries ent[b .. b+32)
+// of a warp (entry b + lane exists when b + lane < end), equal consecutive
+// k-mers merged into runs.  Work is split into quads, up to KQ consecutive
+// k-mers of one superkmer; a warp step gives each lane one quad (a shuffle
+// prefix sum and owner search over the 32 entries).  The first k-mer of a
+// quad is decoded from a 48-base window (16 bytes from three aligned 8-byte
+// loads; store buffers carry 32 bytes of padding); the others roll in one
+// base each, forward and reverse complement.  Must be called by the whole
+// warp; f is called by single lanes and must not use warp collectives.
+template <class F>
+__device__ __forceinline__ void warp_kmer_runs(const BEntry *ent, uint64_t b, uint64_t end, int k, uint64_t mask,
+                                               F &&f) {
     const int lane = threadIdx.x & 31;
     const bool has = b + lane < end;
     BEntry en;
@@ -94,55 +78,58 @@ __device__ __forceinline__ void warp_kmers(const BEntry *ent, uint64_t b, uint64
     en.len = 0;
     if (has) en = ent[b + lane];
     const uint32_t pad = has ? 3u - (en.ptr[0] >> 6) : 0u;
-    uint32_t incl = en.len;
+    const uint32_t nq = (en.len + KQ - 1) / KQ;
+    uint32_t incl = nq;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-        uint32_t y = __shfl_up_sync(FULL, incl, d);
+        const uint32_t y = __shfl_up_sync(FULL, incl, d);
         if (lane >= d) incl += y;
     }
     const uint32_t total = __shfl_sync(FULL, incl, 31);
-    const uint32_t excl = incl - en.len;
+    const uint32_t excl = incl - nq;
     const uint64_t pv = reinterpret_cast<uint64_t>(en.ptr);
     for (uint32_t c0 = 0; c0 < total; c0 += 32) {
         const uint32_t g = c0 + lane;
-        const bool valid = g < total;
-        // owner: the last lane whose first k-mer index is <= g
-        int own = 0;
+        int own = 0;  // the last lane whose first quad index is <= g
 #pragma unroll
         for (int st = 16; st; st >>= 1) {
             const int cand = own + st;
-            const uint32_t v = __shfl_sync(FULL, excl, cand & 31);
-            if (cand < 32 && v <= g) own = cand;
+            if (__shfl_sync(FULL, excl, cand) <= g) own = cand;
         }
-        const uint32_t pos = g - __shfl_sync(FULL, excl, own);
+        const uint32_t qi = g - __shfl_sync(FULL, excl, own);
         const uint64_t po = __shfl_sync(FULL, pv, own);
-        const uint32_t u = __shfl_sync(FULL, pad, own) + pos;
-        uint64_t key = EMPTY_KEY;
-        if (valid) {
-            const uint64_t x = kmer_at(reinterpret_cast<const uint8_t *>(po), u, k, mask);
-            if (CANONICAL) {
-                const uint64_t r = rc64(x, k);
-                key = x < r ? x : r;
+        const uint32_t opad = __shfl_sync(FULL, pad, own), olen = __shfl_sync(FULL, en.len, own);
+        if (g >= total) continue;
+        const uint32_t j0 = KQ * qi;
+        const uint32_t nk = olen - j0 < (uint32_t)KQ ? olen - j0 : (uint32_t)KQ;
+        const uint32_t u = opad + j0, bi = u / 3, s = u - 3 * bi;
+        const uintptr_t addr = (uintptr_t)po + bi;
+        const uint64_t *w = reinterpret_cast<const uint64_t *>(addr & ~(uintptr_t)7);
+        const uint32_t sh = 8 * (uint32_t)(addr & 7);
+        const uint64_t w0 = w[0], w1 = w[1], w2 = w[2];
+        const uint64_t lo = sh ? (w0 >> sh) | (w1 << (64 - sh)) : w0;  // bytes 0..7
+        const uint64_t hi = sh ? (w1 >> sh) | (w2 << (64 - sh)) : w1;  // bytes 8..15
+        // 48 bases, slot 0 in bits 95-94
+        const unsigned __int128 v = ((unsigned __int128)pack6x8(lo) << 48) | pack6x8(hi);
+        uint64_t x = (uint64_t)(v >> (96 - 2 * (s + (uint32_t)k))) & mask;
+        uint64_t r = rc64(x, k);
+        uint64_t last = x < r ? x : r;
+        uint32_t run = 1;
+        for (uint32_t t = 1; t < nk; t++) {
+            const uint32_t bt = (uint32_t)(v >> (94 - 2 * (s + (uint32_t)k + t - 1))) & 3u;  // the entering base
+            x = ((x << 2) | bt) & mask;
+            r = (r >> 2) | ((uint64_t)(3u - bt) << (2 * k - 2));
+            const uint64_t key = x < r ? x : r;
+            if (key == last) {
+                run++;
             } else {
-                key = x;
+                f(last, run);
+                last = key;
+                run = 1;
             }
         }
-        f(key, valid);
+        f(last, run);
     }
-}
-
-// Runs of equal neighbouring keys among the lanes of one warp_kmers step:
-// returns true on the first lane of each run, with *run its length.  Must be
-// called by the whole warp.
-__device__ __forceinline__ bool warp_run_head(uint64_t key, bool valid, uint32_t *run) {
-    const int lane = threadIdx.x & 31;
-    const uint64_t prev = __shfl_up_sync(FULL, key, 1);
-    const bool head = valid && (lane == 0 || key != prev);
-    const unsigned H = __ballot_sync(FULL, head), V = __ballot_sync(FULL, valid);
-    const unsigned above = H & ~((2u << lane) - 1);
-    const int next = above ? __ffs(above) - 1 : 32 - __clz(V);
-    *run = (uint32_t)(next - lane);
-    return head;
 }
 
 // ---------------------------------------------------------------------------
@@ -389,10 +376,8 @@ bucket_count_kernel(BCountParams a) {
     const uint64_t mask = kmask(a.k);
     for (uint64_t bb = e0 + (uint64_t)warp * 32; bb < e1; bb += BC_THREADS) {
         if (__any_sync(FULL, over != 0)) break;  // a warp vote: the warp leaves together
-        warp_kmers<true>(a.entries, bb, e1, a.k, mask, [&](uint64_t key, bool valid) {
-            uint32_t run;
-            if (warp_run_head(key, valid, &run)) smem_add<TS>(tk, tc, &over, key, run);
-        });
+        warp_kmer_runs(a.entries, bb, e1, a.k, mask,
+                       [&](uint64_t key, uint32_t run) { smem_add<TS>(tk, tc, &over, key, run); });
     }
     __syncthreads();
     if (over) {
@@ -413,10 +398,7 @@ hash_insert_entries_kernel(const BEntry *ent, uint64_t n, int k, HSlot *tab, uin
     const uint64_t gw = blockIdx.x * (uint64_t)(H_THREADS / 32) + (threadIdx.x >> 5);
     const uint64_t mask = kmask(k);
     for (uint64_t bb = gw * 32; bb < n; bb += nw * 32) {
-        warp_kmers<true>(ent, bb, n, k, mask, [&](uint64_t key, bool valid) {
-            uint32_t run;
-            if (warp_run_head(key, valid, &run)) table_add(tab, tmask, key, run, err);
-        });
+        warp_kmer_runs(ent, bb, n, k, mask, [&](uint64_t key, uint32_t run) { table_add(tab, tmask, key, run, err); });
     }
 }
 

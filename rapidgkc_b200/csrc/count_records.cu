@@ -123,9 +123,8 @@ rec_agg_kernel(RAggParams a) {
     __syncthreads();
     const uint64_t mask = kmask(a.k);
     for (uint64_t bb = w.e0 + (threadIdx.x & ~31u); bb < w.e1; bb += RSP_THREADS) {
-        warp_kmers<true>(a.entries, bb, w.e1, a.k, mask, [&](uint64_t key, bool valid) {
-            uint32_t run;
-            if (warp_run_head(key, valid, &run) && !smem_try_add(tk, tc, key, run)) {
+        warp_kmer_runs(a.entries, bb, w.e1, a.k, mask, [&](uint64_t key, uint32_t run) {
+            if (!smem_try_add(tk, tc, key, run)) {
                 const uint32_t r = rec_bucket(key, w.r_log);
                 KRec rec;
                 rec.key = key;

@@ -334,15 +334,18 @@ int ensure_table(gkc_ctx *ctx, uint64_t C) {
     return GKC_OK;
 }
 
-int ensure_out(gkc_ctx *ctx, uint64_t need) {
+// Output capacity of at least `need` entries; a new buffer keeps the first
+// `keep` entries of the old one.
+int ensure_out(gkc_ctx *ctx, uint64_t need, uint64_t keep) {
     if (need <= ctx->out_cap && ctx->out_k.p) return GKC_OK;
     uint64_t cap = std::max<uint64_t>(need, 1024);
     DevBuf nk, nc;
     CK(nk.ensure(cap * 8));
     CK(nc.ensure(cap * 4));
-    if (ctx->n_out && ctx->out_k.p) {
-        CK(cudaMemcpyAsync(nk.p, ctx->out_k.p, ctx->n_out * 8, cudaMemcpyDeviceToDevice, ctx->s));
-        CK(cudaMemcpyAsync(nc.p, ctx->out_c.p, ctx->n_out * 4, cudaMemcpyDeviceToDevice, ctx->s));
+    keep = std::min<uint64_t>(keep, ctx->out_cap);
+    if (keep && ctx->out_k.p) {
+        CK(cudaMemcpyAsync(nk.p, ctx->out_k.p, keep * 8, cudaMemcpyDeviceToDevice, ctx->s));
+        CK(cudaMemcpyAsync(nc.p, ctx->out_c.p, keep * 4, cudaMemcpyDeviceToDevice, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
     }
     ctx->out_k.release();
@@ -689,12 +692,16 @@ int chunk_range(gkc_ctx *ctx, StoreChunk *c, uint32_t p0, uint32_t p1, DevBuf &a
         return GKC_OK;
     }
     const uint64_t b0 = c->byte_off[p0], b1 = c->byte_off[p1], s0 = c->skm_off[p0], s1 = c->skm_off[p1];
-    const uint64_t need = (b1 - b0 + 32 + 15) / 16 * 16 + (s1 - s0) * 8 + (s1 - s0) * 4 + 64;
+    // bytes (+32 B of padding), index and keys, each 16-byte aligned so the
+    // next chunk's index stays 8-byte aligned
+    auto a16 = [](uint64_t x) { return (x + 15) / 16 * 16; };
+    const uint64_t nbb = a16(b1 - b0 + 32), nib = a16((s1 - s0) * 8), nkb = a16((s1 - s0) * 4);
+    const uint64_t need = nbb + nib + nkb;
     if (*arena_used + need > arena.cap) return ctx->fail(GKC_EINTERNAL, "staging arena too small");
     uint8_t *base = arena.as<uint8_t>() + *arena_used;
     uint8_t *pb = base;
-    uint64_t *pi = reinterpret_cast<uint64_t *>(base + (b1 - b0 + 32 + 15) / 16 * 16);
-    uint32_t *pk = reinterpret_cast<uint32_t *>(pi + (s1 - s0));
+    uint64_t *pi = reinterpret_cast<uint64_t *>(base + nbb);
+    uint32_t *pk = reinterpret_cast<uint32_t *>(base + nbb + nib);
     CK(cudaMemcpyAsync(pb, c->bytes + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->s));
     CK(cudaMemcpyAsync(pi, c->idx + s0, (s1 - s0) * 8, cudaMemcpyHostToDevice, ctx->s));
     CK(cudaMemcpyAsync(pk, c->keys + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, ctx->s));
@@ -952,7 +959,15 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     auto bbase = [&](uint32_t p) -> uint64_t { return p < P ? slog[P + p] : NB; };
     ctx->times[4] = (double)NB;
     ctx->times[5] = 0;
-    RET(ensure_out(ctx, N / std::max<uint32_t>(cmin, 1) + 1024));
+    // output capacity, grown per group: the group's instances / cmin (an
+    // upper bound of its kept k-mers), at most 40% of free device memory
+    uint64_t out_budget = 0;
+    {
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        out_budget = std::max<uint64_t>(1ull << 24, (uint64_t)(fr * 0.4) / 12);
+    }
+    uint64_t out_used = ctx->n_out;  // entries written before this group
     CK(ctx->bk_skms.ensure(NB * 4));
     CK(ctx->bk_kmers.ensure(NB * 8));
     CK(ctx->bk_off.ensure((NB + 1) * 8));
@@ -995,8 +1010,13 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
             p0 = p1;
             continue;
         }
+        uint64_t gN = 0;
+        for (uint32_t p = p0; p < p1; p++) gN += np[p];
+        RET(ensure_out(ctx, out_used + std::min<uint64_t>(gN / std::max<uint32_t>(cmin, 1), out_budget) + 1024,
+                       out_used));
         uint64_t arena_used = 0;
-        if (spilled) CK(ctx->bk_arena.ensure(gb + 128 * ctx->store.size() + 64));
+        // the group's bytes and 12 B per superkmer, plus each chunk's padding (<= 32 + 3 x 15 B)
+        if (spilled) CK(ctx->bk_arena.ensure(gb + 96 * ctx->store.size() + 64));
         CK(ctx->bk_entries.ensure(gs * sizeof(BEntry)));
         CK(cudaMemsetAsync(ctx->bk_skms.p, 0, NB * 4, ctx->s));
         CK(cudaMemsetAsync(ctx->bk_kmers.p, 0, NB * 8, ctx->s));
@@ -1095,6 +1115,11 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
                 CK(cudaStreamSynchronize(ctx->s));
                 RET(count_buckets_records(ctx, ids, off, km, cmin, cmax));
             }
+        }
+        if (p1 < P) {  // entries written so far: the next group's capacity starts there
+            CK(cudaMemcpyAsync(&out_used, sc, 8, cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaStreamSynchronize(ctx->s));
+            out_used = std::min<uint64_t>(out_used, ctx->out_cap);
         }
         p0 = p1;
     }
@@ -1201,7 +1226,7 @@ int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t
         CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 8, cudaMemcpyDeviceToHost, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
         kept = ctx->h_scal.as<unsigned long long>()[0];
-        RET(ensure_out(ctx, ctx->n_out + kept));
+        RET(ensure_out(ctx, ctx->n_out + kept, ctx->n_out));
         KScope ks(ctx, GKC_K_RLE, 16.0 * d + 12.0 * kept);
         keep_write_kernel<<<(unsigned)kt, RL_THREADS, 0, ctx->s>>>(
             ctx->heads_pos.as<uint64_t>(), ctx->heads_key.as<uint64_t>(), d, n, cmin, cmax,
@@ -1775,7 +1800,7 @@ int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint
         const double slots = ctx->opt.table_slots > 0 ? ctx->opt.table_slots : 0.35;
         const void *dk;
         RET(upload(ctx, ctx->keysA, keys, n * 8, mem, &dk));
-        RET(ensure_out(ctx, n / std::max<uint32_t>(cmin, 1) + 1024));
+        RET(ensure_out(ctx, n / std::max<uint32_t>(cmin, 1) + 1024, 0));
         CK(ctx->part_err.ensure(64));
         CK(ctx->scal.ensure(64));
         CK(ctx->h_scal.ensure(64));

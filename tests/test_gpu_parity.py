@@ -178,6 +178,8 @@ def test_retries_spill_and_groups(oracle):
     ko, co = sorted_table(ko, co)
     for kw, kind in [(dict(table_slots=0.02, hash_l2_only=True), "hash"), (dict(hash_l2_only=True), "hash"),
                      (dict(spill_host=True), "hash"), (dict(spill_host=True, hash_l2_only=True), "hash"),
+                     (dict(spill_host=True, batch_bases=500_000), "hash"),  # many spilled chunks staged together
+                     (dict(spill_host=True, batch_bases=500_000), "sort"),
                      (dict(spill_host=True, group_keys=50_000), "sort"), (dict(group_keys=1), "sort"),
                      (dict(radix_bits=5), "sort")]:
         with counter(k, p, P, kind, **kw) as c:
