@@ -111,6 +111,14 @@ int gkc_store_export(gkc_ctx *ctx, int part, uint8_t *out, uint64_t cap, uint64_
 /* Drops every superkmer in the store. */
 int gkc_store_clear(gkc_ctx *ctx);
 
+/* Pins host memory for spilled chunks (opt.spill_host) until `bytes` are free
+ * in the context's host arena; *pinned (may be NULL) = bytes pinned in all.
+ * Pinning runs at a few GB/s, so a stream of known size reserves ahead.  The
+ * one call that may run on another host thread while gkc_add_reads runs.
+ * Replaces the reference's per-chunk host buffers of SKMStoreNoncon
+ * (skmstore.hpp:62-279, add_skms). */
+int gkc_reserve_host(gkc_ctx *ctx, uint64_t bytes, uint64_t *pinned);
+
 /* Phase 2: counts every partition of the store and keeps the k-mers whose
  * count c satisfies cmin <= c <= cmax.  *n_out = k-mers kept; *n_distinct =
  * distinct k-mers before the threshold (the reference's return value).  The

@@ -29,6 +29,7 @@ UINT32_MAX = 0xFFFFFFFF
 EXPORTS = (
     "gkc_default_options", "gkc_create", "gkc_destroy", "gkc_last_error", "gkc_strerror",
     "gkc_set_order", "gkc_add_reads", "gkc_add_reads_batches", "gkc_batch_timings", "gkc_store_stats", "gkc_store_export", "gkc_store_clear",
+    "gkc_reserve_host",
     "gkc_count", "gkc_count_partitions", "gkc_result", "gkc_result_device", "gkc_count_reads", "gkc_count_keys",
     "gkc_last_timings", "gkc_kernel_launches", "gkc_set_stream", "gkc_set_profiling", "gkc_kernel_stats",
     "gkc_mlp_param_count", "gkc_minimizer_loads", "gkc_mlp_grad", "gkc_mlp_train", "gkc_mlp_scores",
@@ -86,6 +87,7 @@ def load_library(path: str = LIB_PATH):
     L.gkc_store_stats.argtypes = [vp, vp, vp, vp]
     L.gkc_store_export.argtypes = [vp, i32, vp, u64, C.POINTER(u64)]
     L.gkc_store_clear.argtypes = [vp]
+    L.gkc_reserve_host.argtypes = [vp, u64, C.POINTER(u64)]
     L.gkc_count.argtypes = [vp, u32, u32, C.POINTER(u64), C.POINTER(u64)]
     L.gkc_count_partitions.argtypes = [vp, vp, u64, u32, u32, C.POINTER(u64), C.POINTER(u64)]
     L.gkc_result.argtypes = [vp, vp, vp, u64, i32]
@@ -222,6 +224,15 @@ class KmerCounter:
 
     def store_clear(self):
         self._check(self._L.gkc_store_clear(self._h))
+
+    def reserve_host(self, nbytes: int) -> int:
+        """Pins host memory for spilled chunks until `nbytes` are free; returns
+        the bytes pinned in all.  May run on another thread beside add_reads."""
+        pinned = C.c_uint64(0)
+        rc = self._L.gkc_reserve_host(self._h, int(nbytes), C.byref(pinned))
+        if rc != 0:
+            raise GkcError(rc, f"gkc_reserve_host({nbytes}): {self._L.gkc_strerror(rc).decode()}")
+        return pinned.value
 
     # -- phase 2 -------------------------------------------------------------
     def count(self, cmin: int = 1, cmax: int = UINT32_MAX):

@@ -6,17 +6,23 @@
 //   host/device CSR reads --(H2D, overlapped, batches)--> phase 1 kernels
 //   --> partition store (one chunk per batch: partition-ordered superkmer
 //   bytes + index, on the device or spilled to pinned host memory)
-//   --> phase 2 (hash: one partition at a time through an L2-resident table;
-//   sort: groups of partitions through the segmented radix sort)
+//   --> phase 2 (hash: groups of partitions split into sub-buckets counted
+//   in shared memory; sort: groups of partitions through the segmented
+//   radix sort)
 //   --> thresholded (k-mer, count) arrays on the device.
 #include "../../include/gkc_capi.h"
+
+#include <sys/mman.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "count_records.cu"
@@ -72,19 +78,117 @@ struct PinBuf {
     template <class T> T *as() const { return reinterpret_cast<T *>(p); }
 };
 
+// Pinned host memory for spilled chunks.  Pinning is slower than the
+// device-to-host copy, so it is done once: slabs of at least
+// 4 GiB are handed out front to back and rewound when the store is cleared,
+// and gkc_reserve_host can pin them ahead of time (from another thread, while
+// batches run).  Only the slab list is shared with that thread.
+struct HostArena {
+    struct Slab {
+        uint8_t *p;
+        size_t cap, used;
+    };
+    static constexpr size_t SLAB_MIN = 4ull << 30;
+    std::mutex mu;
+    std::vector<Slab> slabs;
+    size_t cur = 0;  // first slab that may have room
+
+    // A slab is anonymous memory backed by transparent huge pages, faulted in
+    // by several threads and then registered with the driver: about ten
+    // times faster than cudaHostAlloc, which zeroes and pins 4 KB pages one
+    // by one while holding the driver's lock.
+    cudaError_t add_slab(size_t bytes) {  // called without the lock held
+        const size_t cap = (std::max(bytes, SLAB_MIN) + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1);
+        void *p = mmap(nullptr, cap, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+        if (p == MAP_FAILED) return cudaErrorMemoryAllocation;
+        madvise(p, cap, MADV_HUGEPAGE);  // advisory: 4 KB pages still work
+        const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        const size_t per = (cap / nt + 4095) & ~(size_t)4095;
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; t++)
+            th.emplace_back([p, per, cap, t]() {
+                volatile uint8_t *b = (uint8_t *)p;
+                for (size_t o = t * per; o < std::min(cap, (t + 1) * per); o += 4096) b[o] = 0;
+            });
+        for (auto &x : th) x.join();
+        cudaError_t e = cudaHostRegister(p, cap, cudaHostRegisterDefault);
+        if (e != cudaSuccess) {
+            munmap(p, cap);
+            return e;
+        }
+        std::lock_guard<std::mutex> g(mu);
+        slabs.push_back({(uint8_t *)p, cap, 0});
+        return cudaSuccess;
+    }
+    size_t free_bytes() {
+        std::lock_guard<std::mutex> g(mu);
+        size_t f = 0;
+        for (size_t i = cur; i < slabs.size(); i++) f += slabs[i].cap - slabs[i].used;
+        return f;
+    }
+    size_t pinned() {
+        std::lock_guard<std::mutex> g(mu);
+        size_t f = 0;
+        for (auto &s : slabs) f += s.cap;
+        return f;
+    }
+    cudaError_t reserve(size_t bytes) {  // pins slabs until `bytes` are free
+        while (free_bytes() < bytes) {
+            const size_t need = bytes - free_bytes();
+            cudaError_t e = add_slab(std::min<size_t>(std::max<size_t>(need, SLAB_MIN), (size_t)16 << 30));
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+    // `bytes` of pinned memory, 256-byte aligned; valid until rewind()
+    cudaError_t take(size_t bytes, uint8_t **out) {
+        bytes = (bytes + 255) & ~(size_t)255;
+        for (;;) {
+            {
+                std::lock_guard<std::mutex> g(mu);
+                for (; cur < slabs.size(); cur++) {
+                    Slab &s = slabs[cur];
+                    if (s.cap - s.used >= bytes) {
+                        *out = s.p + s.used;
+                        s.used += bytes;
+                        return cudaSuccess;
+                    }
+                }
+                // slabs are filled in order: a slab that cannot take this
+                // chunk stays behind, so `cur` ends past the last slab
+            }
+            cudaError_t e = add_slab(bytes);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    void rewind() {
+        std::lock_guard<std::mutex> g(mu);
+        for (auto &s : slabs) s.used = 0;
+        cur = 0;
+    }
+    void release() {
+        std::lock_guard<std::mutex> g(mu);
+        for (auto &s : slabs) {
+            cudaHostUnregister(s.p);
+            munmap(s.p, s.cap);
+        }
+        slabs.clear();
+        cur = 0;
+    }
+};
+
 // One phase-1 batch worth of superkmers, partition-ordered.
 // Chunks are pooled: a cleared store keeps its buffers for the next batch,
 // so steady-state batches allocate nothing.
 struct StoreChunk {
     bool on_host = false;
-    uint8_t *bytes = nullptr;  // = dbytes.p or hbytes.p
-    uint64_t *idx = nullptr;   // = didx.p or hidx.p
-    uint32_t *keys = nullptr;  // = dkeys.p or hkeys.p: minimizer key of each superkmer
+    uint8_t *bytes = nullptr;  // in dbytes, or in the context's host arena
+    uint64_t *idx = nullptr;   // in didx, or in the host arena
+    uint32_t *keys = nullptr;  // in dkeys, or in the host arena: minimizer key of each superkmer
     uint64_t nbytes = 0, nskm = 0;
     std::vector<uint64_t> byte_off, skm_off;  // [P+1]
     std::vector<uint64_t> kmers;              // [P]
     DevBuf dbytes, didx, dkeys;               // device storage
-    PinBuf hbytes, hidx, hkeys;               // pinned host storage (spilled chunks)
     DevBuf d_byte_off, d_skm_off;             // device copies of the offsets
     // laid out on the device (phase1_async): k-mers per partition, error
     // flags, and their pinned host mirror read back after the batch
@@ -99,9 +203,6 @@ struct StoreChunk {
         dbytes.release();
         didx.release();
         dkeys.release();
-        hbytes.release();
-        hidx.release();
-        hkeys.release();
         d_byte_off.release();
         d_skm_off.release();
     }
@@ -194,6 +295,7 @@ struct gkc_ctx {
     PinBuf h_scal;
 
     std::vector<StoreChunk *> pool;  // cleared chunks kept for reuse
+    HostArena arena;                 // pinned host memory of spilled chunks
 
     StoreChunk *take_chunk() {
         if (pool.empty()) return new StoreChunk();
@@ -204,6 +306,7 @@ struct gkc_ctx {
     void clear_store() {
         for (auto *c : store) pool.push_back(c);
         store.clear();
+        arena.rewind();
     }
 
     ~gkc_ctx() {
@@ -223,6 +326,7 @@ struct gkc_ctx {
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal};
         for (auto *p : ps) p->release();
+        arena.release();
         cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_ready[0], buf_ready[1]};
         for (auto e : evs) if (e) cudaEventDestroy(e);
         for (auto e : batch_ev) cudaEventDestroy(e);
@@ -553,20 +657,25 @@ int phase1_exact(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     CK(cudaMemcpyAsync(c->d_skm_off.p, c->skm_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
     RET(launch_scatter(ctx, pl, c, total, cap, ctx->flags.as<uint32_t>(), (double)c->nskm, (double)c->nbytes));
     if (ctx->opt.spill_host) {
-        cudaError_t ea = c->hbytes.ensure(c->nbytes + 16);
-        cudaError_t eb = ea == cudaSuccess ? c->hidx.ensure(std::max<uint64_t>(c->nskm, 1) * 8) : ea;
-        cudaError_t ec = eb == cudaSuccess ? c->hkeys.ensure(std::max<uint64_t>(c->nskm, 1) * 4) : eb;
-        if (ec != cudaSuccess) {
+        // index and keys first (8- and 4-byte aligned), then the bytes
+        const uint64_t ni = std::max<uint64_t>(c->nskm, 1);
+        uint8_t *h = nullptr;
+        cudaError_t ea = ctx->arena.take(ni * 12 + c->nbytes + 16, &h);
+        if (ea != cudaSuccess) {
             ctx->pool.push_back(c);
-            return ctx->fail(GKC_ENOMEM, "pinned spill allocation: %s", cudaGetErrorString(ec));
+            return ctx->fail(GKC_ENOMEM, "pinned spill allocation: %s", cudaGetErrorString(ea));
         }
-        CK(cudaMemcpyAsync(c->hbytes.p, c->bytes, c->nbytes, cudaMemcpyDeviceToHost, ctx->s));
-        CK(cudaMemcpyAsync(c->hidx.p, c->idx, c->nskm * 8, cudaMemcpyDeviceToHost, ctx->s));
-        CK(cudaMemcpyAsync(c->hkeys.p, c->keys, c->nskm * 4, cudaMemcpyDeviceToHost, ctx->s));
-        CK(cudaStreamSynchronize(ctx->s));
-        c->bytes = c->hbytes.as<uint8_t>();
-        c->idx = c->hidx.as<uint64_t>();
-        c->keys = c->hkeys.as<uint32_t>();
+        uint64_t *hi = reinterpret_cast<uint64_t *>(h);
+        uint32_t *hk = reinterpret_cast<uint32_t *>(h + ni * 8);
+        uint8_t *hb = h + ni * 12;
+        // stream-ordered: later staging and exports run on the same stream,
+        // so the copies need no wait here and overlap the caller's next batch
+        CK(cudaMemcpyAsync(hb, c->bytes, c->nbytes, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(hi, c->idx, c->nskm * 8, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(hk, c->keys, c->nskm * 4, cudaMemcpyDeviceToHost, ctx->s));
+        c->bytes = hb;
+        c->idx = hi;
+        c->keys = hk;
         c->on_host = true;
     }
     ctx->store.push_back(c);
@@ -772,8 +881,8 @@ constexpr uint64_t BC_HEAVY_KMERS = 65536;
 // heavy: their k-mers are re-split by k-mer hash into record sub-buckets of
 // at most 4k instances, counted in shared memory; record sub-buckets that
 // still overflow go through the L2 table.
-int count_buckets_records(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const std::vector<uint64_t> &off,
-                          const std::vector<uint64_t> &bk_kmers, uint32_t cmin, uint32_t cmax) {
+int count_buckets_records_slice(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const std::vector<uint64_t> &off,
+                                const std::vector<uint64_t> &bk_kmers, uint32_t cmin, uint32_t cmax) {
     std::vector<RWork> work;
     uint64_t NR = 0, inst = 0, ents = 0;
     for (uint32_t b : ids) {
@@ -923,6 +1032,34 @@ int count_buckets_records(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const 
     return GKC_OK;
 }
 
+// The record path holds two 16-byte records per k-mer instance of its
+// sub-buckets (staged and sorted): heavy sub-buckets are counted in slices
+// whose records fit the free device memory.  A sub-bucket's k-mers are all in
+// that sub-bucket, so slices are independent.
+int count_buckets_records(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const std::vector<uint64_t> &off,
+                          const std::vector<uint64_t> &bk_kmers, uint32_t cmin, uint32_t cmax) {
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    const uint64_t avail = fr + ctx->r_recs.cap + ctx->r_stage.cap;  // the record buffers are reallocated
+    uint64_t cap_inst = std::max<uint64_t>(1ull << 22, (uint64_t)(avail * 0.6) / 40);
+    // GKC_RECORD_SLICE=n caps a slice at n instances, so that tests can make
+    // small inputs take several slices
+    if (const char *rs = getenv("GKC_RECORD_SLICE")) cap_inst = std::max<uint64_t>(1, strtoull(rs, nullptr, 10));
+    std::vector<uint32_t> slice;
+    uint64_t acc = 0;
+    for (uint32_t b : ids) {
+        if (!slice.empty() && acc + bk_kmers[b] > cap_inst) {
+            RET(count_buckets_records_slice(ctx, slice, off, bk_kmers, cmin, cmax));
+            slice.clear();
+            acc = 0;
+        }
+        slice.push_back(b);
+        acc += bk_kmers[b];
+    }
+    if (!slice.empty()) RET(count_buckets_records_slice(ctx, slice, off, bk_kmers, cmin, cmax));
+    return GKC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // phase 2, hash counter: shared-memory counting of minimizer sub-buckets, with
 // the L2 table for sub-buckets that overflow shared memory.  Device-resident
@@ -959,15 +1096,24 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     auto bbase = [&](uint32_t p) -> uint64_t { return p < P ? slog[P + p] : NB; };
     ctx->times[4] = (double)NB;
     ctx->times[5] = 0;
-    // output capacity, grown per group: the group's instances / cmin (an
-    // upper bound of its kept k-mers), at most 40% of free device memory
-    uint64_t out_budget = 0;
+    // output capacity, grown per group from the kept k-mers per instance of
+    // the groups before (at first the bound 1/cmin), at most 25% of free
+    // device memory; a group whose output overflows is counted again with
+    // the capacity its cursor asked for
+    size_t free0 = 0;
     {
-        size_t fr = 0, tot = 0;
-        CK(cudaMemGetInfo(&fr, &tot));
-        out_budget = std::max<uint64_t>(1ull << 24, (uint64_t)(fr * 0.4) / 12);
+        size_t tot = 0;
+        CK(cudaMemGetInfo(&free0, &tot));
     }
+    const uint64_t out_budget = std::max<uint64_t>(1ull << 24, (uint64_t)(free0 * 0.25) / 12);
+    double kept_ratio = 1.0 / std::max<uint32_t>(cmin, 1);
+    // GKC_OUT_ESTIMATE=n sets each group's first output estimate to n - 1
+    // entries, so that tests can make every group overflow and be redone
+    const char *oe = getenv("GKC_OUT_ESTIMATE");
+    const uint64_t out_est_override = oe ? strtoull(oe, nullptr, 10) : 0;
     uint64_t out_used = ctx->n_out;  // entries written before this group
+    uint64_t distinct_used = 0;      // distinct k-mers of the groups before
+    int redo = 0;                    // times the current group was counted again
     CK(ctx->bk_skms.ensure(NB * 4));
     CK(ctx->bk_kmers.ensure(NB * 8));
     CK(ctx->bk_off.ensure((NB + 1) * 8));
@@ -985,12 +1131,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
                             BC_TS * 12));
     CK(cudaFuncSetAttribute(bucket_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BS_SMEM));
     // groups of partitions
-    uint64_t budget = ~0ull;
-    if (spilled) {
-        size_t fr = 0, tot = 0;
-        CK(cudaMemGetInfo(&fr, &tot));
-        budget = std::max<uint64_t>(1ull << 26, (uint64_t)(fr * 0.4));
-    }
+    const uint64_t budget = spilled ? std::max<uint64_t>(1ull << 26, (uint64_t)(free0 * 0.3)) : ~0ull;
     float acc_ms = 0;
     uint32_t p0 = 0;
     while (p0 < P) {
@@ -1012,8 +1153,10 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         }
         uint64_t gN = 0;
         for (uint32_t p = p0; p < p1; p++) gN += np[p];
-        RET(ensure_out(ctx, out_used + std::min<uint64_t>(gN / std::max<uint32_t>(cmin, 1), out_budget) + 1024,
-                       out_used));
+        uint64_t est = std::min<uint64_t>(gN / std::max<uint32_t>(cmin, 1),
+                                          (uint64_t)((double)gN * kept_ratio * 1.25) + 65536);
+        if (out_est_override) est = out_est_override - 1;
+        RET(ensure_out(ctx, out_used + std::min<uint64_t>(est, out_budget) + 1024, out_used));
         uint64_t arena_used = 0;
         // the group's bytes and 12 B per superkmer, plus each chunk's padding (<= 32 + 3 x 15 B)
         if (spilled) CK(ctx->bk_arena.ensure(gb + 96 * ctx->store.size() + 64));
@@ -1116,11 +1259,25 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
                 RET(count_buckets_records(ctx, ids, off, km, cmin, cmax));
             }
         }
-        if (p1 < P) {  // entries written so far: the next group's capacity starts there
-            CK(cudaMemcpyAsync(&out_used, sc, 8, cudaMemcpyDeviceToHost, ctx->s));
+        // entries written so far: the next group's capacity starts there
+        unsigned long long hg[3];
+        CK(cudaMemcpyAsync(hg, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        if ((uint32_t)hg[2] & ERR_OUTPUT_FULL) {  // count the group again with room for all of it
+            if (++redo > 2) return ctx->fail(GKC_EINTERNAL, "output capacity exceeded");
+            const uint64_t need = hg[0];
+            RET(ensure_out(ctx, need + need / 16 + 1024, out_used));
+            hg[0] = out_used;
+            hg[1] = distinct_used;
+            hg[2] &= ~(unsigned long long)ERR_OUTPUT_FULL;
+            CK(cudaMemcpyAsync(sc, hg, 24, cudaMemcpyHostToDevice, ctx->s));
             CK(cudaStreamSynchronize(ctx->s));
-            out_used = std::min<uint64_t>(out_used, ctx->out_cap);
+            continue;
         }
+        if (gN) kept_ratio = std::min(1.0 / std::max<uint32_t>(cmin, 1), (double)(hg[0] - out_used) / (double)gN + 1e-3);
+        out_used = hg[0];
+        distinct_used = hg[1];
+        redo = 0;
         p0 = p1;
     }
     CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
@@ -1661,6 +1818,7 @@ int gkc_store_export(gkc_ctx *ctx, int part, uint8_t *out, uint64_t cap, uint64_
     if (!out) return GKC_OK;
     if (cap < total) return ctx->fail(GKC_EINVAL, "export buffer too small (%llu < %llu)",
                                       (unsigned long long)cap, (unsigned long long)total);
+    CK(cudaStreamSynchronize(ctx->s));  // spill copies still in flight
     uint64_t o = 0;
     for (auto *c : ctx->store) {
         uint64_t b0 = c->byte_off[part], b1 = c->byte_off[part + 1];
@@ -1671,6 +1829,15 @@ int gkc_store_export(gkc_ctx *ctx, int part, uint8_t *out, uint64_t cap, uint64_
     }
     CK(cudaStreamSynchronize(ctx->s));
     return GKC_OK;
+}
+
+int gkc_reserve_host(gkc_ctx *ctx, uint64_t bytes, uint64_t *pinned) {
+    if (!ctx) return GKC_EINVAL;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return GKC_ECUDA;
+    const cudaError_t e = ctx->arena.reserve(bytes);
+    if (pinned) *pinned = ctx->arena.pinned();
+    // not ctx->fail: the error text belongs to the thread running batches
+    return e == cudaSuccess ? GKC_OK : GKC_ENOMEM;
 }
 
 int gkc_store_clear(gkc_ctx *ctx) {

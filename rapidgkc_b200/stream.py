@@ -26,6 +26,20 @@ from . import synth
 from .capi import KmerCounter
 
 
+STORE_BYTES_PER_BASE = 2.4
+
+
+def _mem_available() -> int:
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
 def stream_count(workload: str = "human_3g", scale: float = 1.0, batch_gb: float = 1.0, order: str = "learned",
                  k: int = 31, p: int = 11, partitions: int = 512, cmin: int = 2, spill: bool = True,
                  device: int = 0, threads: int = 0) -> dict:
@@ -53,12 +67,31 @@ def stream_count(workload: str = "human_3g", scale: float = 1.0, batch_gb: float
             q.put(item)
         q.put(None)
 
+    # the spilled store takes ~2.3 bytes per base (superkmer bytes 1.2, index
+    # and keys 12 per superkmer); it must fit host memory beside two batches
+    est_store = int(STORE_BYTES_PER_BASE * n_reads * read_len) if spill else 0
+    avail = _mem_available()
+    if spill and avail and est_store > 0.8 * avail - 4 * batch_gb * 1e9:
+        raise MemoryError(f"a spilled store of ~{est_store / 1e9:.0f} GB does not fit the "
+                          f"{avail / 1e9:.0f} GB of available host memory; use a smaller scale")
     th = threading.Thread(target=producer, daemon=True)
     th.start()
     out = {"workload": workload, "scale": scale, "genome_bp": int(spec.length), "reads": n_reads,
            "batches": n_batches, "batch_gb": batch_gb, "order": order, "spill_host": spill, "partitions": partitions}
     with KmerCounter(k=k, p=p, partitions=partitions, counter="hash", spill_host=spill, device=device,
                      batch_bases=int(batch_gb * 1e9) + read_len) as c:
+        pin = {"s": 0.0, "bytes": 0, "error": None}
+        if spill:  # pin the store's host memory beside the first batches
+            def reserve():
+                t = time.perf_counter()
+                try:
+                    pin["bytes"] = c.reserve_host(est_store)
+                except Exception as e:  # the batches then pin what they need themselves
+                    pin["error"] = str(e)
+                pin["s"] = time.perf_counter() - t
+
+            pin_th = threading.Thread(target=reserve, daemon=True)
+            pin_th.start()
         if order == "learned":
             from .order import default_order_path, load_order
             c.mlp_order(load_order(default_order_path(p))[0])
@@ -77,6 +110,8 @@ def stream_count(workload: str = "human_3g", scale: float = 1.0, batch_gb: float
             bases += int(offs[-1])
             del reads, offs, item
         th.join()
+        if spill:
+            pin_th.join()
         pb, ps, pk = c.store_stats()
         t = time.perf_counter()
         kept, distinct = c.count(cmin)
@@ -87,8 +122,10 @@ def stream_count(workload: str = "human_3g", scale: float = 1.0, batch_gb: float
                 "phase1_s": t_add, "phase2_s": t_count,
                 "gbps": bases / (t_add + t_count) / 1e9,
                 "batch_latency_ms": {"p50": float(np.percentile(lat, 50)), "max": float(np.max(lat))} if lat else None,
-                "generator_s": gen_s[0], "genome_s": t_genome,
-                "note": "gbps = bases / (phase 1 calls + count), wall clock; read generation runs beside it"})
+                "generator_s": gen_s[0], "genome_s": t_genome, "host_pinned": pin["bytes"] if spill else 0,
+                "pin_s": pin["s"] if spill else 0.0, "pin_error": pin["error"] if spill else None,
+                "note": "gbps = bases / (phase 1 calls + count), wall clock; read generation and host pinning "
+                        "run beside it on other threads"})
     return out
 
 

@@ -189,6 +189,30 @@ def test_retries_spill_and_groups(oracle):
         assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co), kw
 
 
+@pytest.mark.parametrize("kind", ["hash", "sort"])
+def test_spill_arena_reserve_and_reuse(oracle, kind):
+    """Spilled chunks take pinned memory reserved ahead (from another thread)
+    and reuse it after the store is counted: the second pass pins nothing."""
+    import threading
+    k, p, P = 31, 11, 64
+    reads, offs = random_reads(14, 60_000, 5000, 150, 0.01)
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P, 2, U32)
+    ko, co = sorted_table(ko, co)
+    with counter(k, p, P, kind, spill_host=True, batch_bases=200_000) as c:
+        th = threading.Thread(target=c.reserve_host, args=(1 << 20,))
+        th.start()
+        c.add_reads(reads, offs)
+        th.join()
+        pinned = c.reserve_host(0)
+        assert pinned >= 1 << 20
+        for _ in range(2):
+            n, d = c.count(2, U32)
+            km, ct = sorted_table(*c.result())
+            assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+            c.add_reads(reads, offs)
+        assert c.reserve_host(0) == pinned
+
+
 def test_shared_memory_overflow_falls_back(oracle):
     """Partitions with far more distinct k-mers than a CTA's shared-memory
     table are counted through the L2 table with the same result."""
@@ -203,13 +227,17 @@ def test_shared_memory_overflow_falls_back(oracle):
     assert np.array_equal(km, ko) and np.array_equal(ct, co)
 
 
-def test_heavy_and_overflowing_sub_buckets(oracle):
+@pytest.mark.parametrize("record_slice", [None, "1"])
+def test_heavy_and_overflowing_sub_buckets(oracle, record_slice, monkeypatch):
     """A learned order that makes two p-mers the preferred minimizers builds
     three kinds of sub-bucket beside ordinary ones: one with ~31k distinct
     k-mers (overflows the shared-memory table), one with ~105k distinct k-mers
     (above the heavy limit, so it is never counted by one CTA), and (AT)n reads
     whose 120k k-mer instances share one or two distinct k-mers.  All take the
-    record split and give the oracle's multiset."""
+    record split and give the oracle's multiset; with record_slice each such
+    sub-bucket is counted in a record slice of its own."""
+    if record_slice:
+        monkeypatch.setenv("GKC_RECORD_SLICE", record_slice)
     k, p, P = 31, 11, 4
     r = np.random.default_rng(21)
     acgt = np.frombuffer(b"ACGT", np.uint8)
@@ -234,10 +262,15 @@ def test_heavy_and_overflowing_sub_buckets(oracle):
     assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
 
 
-@pytest.mark.parametrize("kind", ["hash", "sort"])
-def test_count_partitions_subsets(oracle, kind):
+@pytest.mark.parametrize("kind", ["hash", "sort", "hash_redo"])
+def test_count_partitions_subsets(oracle, kind, monkeypatch):
     """Counting a store in disjoint partition subsets (as the reference's
-    phase-2 workers do) gives each subset's k-mers; together the oracle's."""
+    phase-2 workers do) gives each subset's k-mers; together the oracle's.
+    hash_redo starts every group with no output room, so each group
+    overflows its output and is counted again."""
+    if kind == "hash_redo":
+        monkeypatch.setenv("GKC_OUT_ESTIMATE", "1")
+        kind = "hash"
     k, p, P = 31, 11, 32
     reads, offs = random_reads(51, 80_000, 6000, 150, 0.005)
     _, _, _, po, stream = oracle.skmgen(reads, offs, k, p, P)
