@@ -111,6 +111,25 @@ int gkc_store_export(gkc_ctx *ctx, int part, uint8_t *out, uint64_t cap, uint64_
 /* Drops every superkmer in the store. */
 int gkc_store_clear(gkc_ctx *ctx);
 
+/* Packs partitions [p0, p1) of the store into one partition-major range:
+ * each partition's superkmers from every chunk, in chunk order, into device
+ * memory `bytes` (cap_bytes), `idx` (u64) and `keys` (u32) of cap_skms
+ * entries.  counts (host, 3 x (p1 - p0)) = per partition bytes, superkmers,
+ * k-mers; with all three buffers NULL only counts are written, to size them.
+ * Index offsets stay relative to each partition's first byte, so a packed
+ * range appends to any context unchanged.  The multi-GPU exchange packs
+ * [0, P) and sends each owner its range: a step the reference does not have
+ * (its stores never leave one process, skmstore.hpp:62-279). */
+int gkc_store_pack(gkc_ctx *ctx, int p0, int p1, uint8_t *bytes, uint64_t cap_bytes, uint64_t *idx,
+                   uint32_t *keys, uint64_t cap_skms, uint64_t *counts);
+
+/* Appends a packed range of partitions [p0, p1) (gkc_store_pack's layout, in
+ * device or host memory; counts in host memory) to the store as one chunk
+ * (SKMStoreNoncon::add_skms, skmstore.hpp:189-198, for a received range).
+ * The buffers may be reused when the call returns. */
+int gkc_store_append(gkc_ctx *ctx, int p0, int p1, const uint8_t *bytes, const uint64_t *idx,
+                     const uint32_t *keys, const uint64_t *counts);
+
 /* Pins host memory for spilled chunks (opt.spill_host) until `bytes` are free
  * in the context's host arena; *pinned (may be NULL) = bytes pinned in all.
  * Pinning runs at a few GB/s, so a stream of known size reserves ahead.  The

@@ -29,7 +29,7 @@ UINT32_MAX = 0xFFFFFFFF
 EXPORTS = (
     "gkc_default_options", "gkc_create", "gkc_destroy", "gkc_last_error", "gkc_strerror",
     "gkc_set_order", "gkc_add_reads", "gkc_add_reads_batches", "gkc_batch_timings", "gkc_store_stats", "gkc_store_export", "gkc_store_clear",
-    "gkc_reserve_host",
+    "gkc_reserve_host", "gkc_store_pack", "gkc_store_append",
     "gkc_count", "gkc_count_partitions", "gkc_result", "gkc_result_device", "gkc_count_reads", "gkc_count_keys",
     "gkc_last_timings", "gkc_kernel_launches", "gkc_set_stream", "gkc_set_profiling", "gkc_kernel_stats",
     "gkc_mlp_param_count", "gkc_minimizer_loads", "gkc_mlp_grad", "gkc_mlp_train", "gkc_mlp_scores",
@@ -88,6 +88,8 @@ def load_library(path: str = LIB_PATH):
     L.gkc_store_export.argtypes = [vp, i32, vp, u64, C.POINTER(u64)]
     L.gkc_store_clear.argtypes = [vp]
     L.gkc_reserve_host.argtypes = [vp, u64, C.POINTER(u64)]
+    L.gkc_store_pack.argtypes = [vp, i32, i32, vp, u64, vp, vp, u64, vp]
+    L.gkc_store_append.argtypes = [vp, i32, i32, vp, vp, vp, vp]
     L.gkc_count.argtypes = [vp, u32, u32, C.POINTER(u64), C.POINTER(u64)]
     L.gkc_count_partitions.argtypes = [vp, vp, u64, u32, u32, C.POINTER(u64), C.POINTER(u64)]
     L.gkc_result.argtypes = [vp, vp, vp, u64, i32]
@@ -154,6 +156,7 @@ class KmerCounter:
             raise GkcError(rc, L.gkc_strerror(rc).decode())
         self._L, self._h = L, h
         self.k, self.p, self.partitions, self.counter = k, p, partitions, counter
+        self.device = device
 
     def close(self):
         if getattr(self, "_h", None):
@@ -224,6 +227,35 @@ class KmerCounter:
 
     def store_clear(self):
         self._check(self._L.gkc_store_clear(self._h))
+
+    def store_pack(self, p0: int = 0, p1: int | None = None):
+        """Packs partitions [p0, p1) into new device tensors: (bytes uint8,
+        idx int64, keys int32, counts uint64 [3, p1 - p0] of per-partition
+        bytes, superkmers, k-mers)."""
+        import torch
+
+        p1 = self.partitions if p1 is None else p1
+        n = p1 - p0
+        counts = np.zeros(3 * max(n, 1), np.uint64)
+        L, h = self._L, self._h
+        self._check(L.gkc_store_pack(h, p0, p1, None, 0, None, None, 0, _ptr(counts)[0]))
+        nb, ns = int(counts[:n].sum()), int(counts[n:2 * n].sum())
+        dev = torch.device("cuda", self.device)
+        b = torch.empty(max(nb, 1), dtype=torch.uint8, device=dev)
+        i = torch.empty(max(ns, 1), dtype=torch.int64, device=dev)
+        k = torch.empty(max(ns, 1), dtype=torch.int32, device=dev)
+        self._check(L.gkc_store_pack(h, p0, p1, _ptr(b)[0], nb, _ptr(i)[0], _ptr(k)[0], ns, _ptr(counts)[0]))
+        return b[:nb], i[:ns], k[:ns], counts[:3 * n].reshape(3, n)
+
+    def store_append(self, p0: int, p1: int, nbytes, idx, keys, counts):
+        """Appends a packed range of partitions [p0, p1) (store_pack's layout;
+        device tensors or host arrays) as one store chunk."""
+        counts = np.ascontiguousarray(np.asarray(counts, np.uint64).reshape(-1))
+        if hasattr(nbytes, "is_cuda") and nbytes.is_cuda:
+            import torch
+            torch.cuda.current_stream(nbytes.device).synchronize()  # the producer's stream, e.g. a collective's
+        self._check(self._L.gkc_store_append(self._h, p0, p1, _ptr(nbytes)[0], _ptr(idx)[0], _ptr(keys)[0],
+                                             _ptr(counts)[0]))
 
     def reserve_host(self, nbytes: int) -> int:
         """Pins host memory for spilled chunks until `nbytes` are free; returns

@@ -29,6 +29,7 @@
 #include "count_sort.cu"
 #include "order_mlp.cu"
 #include "skmgen.cu"
+#include "store_pack.cu"
 
 using namespace gkc;
 
@@ -582,6 +583,29 @@ int launch_scatter(gkc_ctx *ctx, const P1Plan &pl, StoreChunk *c, uint64_t total
     return GKC_OK;
 }
 
+// Copies a chunk from device staging (c->bytes, idx, keys) to pinned host
+// memory of the context's arena.
+int spill_chunk(gkc_ctx *ctx, StoreChunk *c) {
+    // index and keys first (8- and 4-byte aligned), then the bytes
+    const uint64_t ni = std::max<uint64_t>(c->nskm, 1);
+    uint8_t *h = nullptr;
+    cudaError_t ea = ctx->arena.take(ni * 12 + c->nbytes + 16, &h);
+    if (ea != cudaSuccess) return ctx->fail(GKC_ENOMEM, "pinned spill allocation: %s", cudaGetErrorString(ea));
+    uint64_t *hi = reinterpret_cast<uint64_t *>(h);
+    uint32_t *hk = reinterpret_cast<uint32_t *>(h + ni * 8);
+    uint8_t *hb = h + ni * 12;
+    // stream-ordered: later staging and exports run on the same stream,
+    // so the copies need no wait here and overlap the caller's next batch
+    CK(cudaMemcpyAsync(hb, c->bytes, c->nbytes, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaMemcpyAsync(hi, c->idx, c->nskm * 8, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaMemcpyAsync(hk, c->keys, c->nskm * 4, cudaMemcpyDeviceToHost, ctx->s));
+    c->bytes = hb;
+    c->idx = hi;
+    c->keys = hk;
+    c->on_host = true;
+    return GKC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Phase 1 of one device-resident batch (offs[0] == 0), synchronously: the
 // partition totals are read back after find_superkmers and the chunk is
@@ -657,26 +681,11 @@ int phase1_exact(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     CK(cudaMemcpyAsync(c->d_skm_off.p, c->skm_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
     RET(launch_scatter(ctx, pl, c, total, cap, ctx->flags.as<uint32_t>(), (double)c->nskm, (double)c->nbytes));
     if (ctx->opt.spill_host) {
-        // index and keys first (8- and 4-byte aligned), then the bytes
-        const uint64_t ni = std::max<uint64_t>(c->nskm, 1);
-        uint8_t *h = nullptr;
-        cudaError_t ea = ctx->arena.take(ni * 12 + c->nbytes + 16, &h);
-        if (ea != cudaSuccess) {
+        const int rc = spill_chunk(ctx, c);
+        if (rc != GKC_OK) {
             ctx->pool.push_back(c);
-            return ctx->fail(GKC_ENOMEM, "pinned spill allocation: %s", cudaGetErrorString(ea));
+            return rc;
         }
-        uint64_t *hi = reinterpret_cast<uint64_t *>(h);
-        uint32_t *hk = reinterpret_cast<uint32_t *>(h + ni * 8);
-        uint8_t *hb = h + ni * 12;
-        // stream-ordered: later staging and exports run on the same stream,
-        // so the copies need no wait here and overlap the caller's next batch
-        CK(cudaMemcpyAsync(hb, c->bytes, c->nbytes, cudaMemcpyDeviceToHost, ctx->s));
-        CK(cudaMemcpyAsync(hi, c->idx, c->nskm * 8, cudaMemcpyDeviceToHost, ctx->s));
-        CK(cudaMemcpyAsync(hk, c->keys, c->nskm * 4, cudaMemcpyDeviceToHost, ctx->s));
-        c->bytes = hb;
-        c->idx = hi;
-        c->keys = hk;
-        c->on_host = true;
     }
     ctx->store.push_back(c);
     return GKC_OK;
@@ -1827,6 +1836,142 @@ int gkc_store_export(gkc_ctx *ctx, int part, uint8_t *out, uint64_t cap, uint64_
                                ctx->s));
         o += b1 - b0;
     }
+    CK(cudaStreamSynchronize(ctx->s));
+    return GKC_OK;
+}
+
+int gkc_store_pack(gkc_ctx *ctx, int p0, int p1, uint8_t *bytes, uint64_t cap_bytes, uint64_t *idx, uint32_t *keys,
+                   uint64_t cap_skms, uint64_t *counts) {
+    if (!ctx || p0 < 0 || p1 < p0 || p1 > ctx->opt.partitions || !counts) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    const uint32_t n = (uint32_t)(p1 - p0);
+    for (int p = p0; p < p1; p++)
+        if (!ctx->counted.empty() && ctx->counted[p])
+            return ctx->fail(GKC_ESTATE, "partition %d was counted already", p);
+    // per-partition totals and packed offsets
+    std::vector<uint64_t> boff(n + 1, 0), soff(n + 1, 0);
+    for (uint32_t j = 0; j < n; j++) {
+        uint64_t b = 0, sk = 0, km = 0;
+        for (auto *c : ctx->store) {
+            b += c->byte_off[p0 + j + 1] - c->byte_off[p0 + j];
+            sk += c->skm_off[p0 + j + 1] - c->skm_off[p0 + j];
+            km += c->kmers[p0 + j];
+        }
+        counts[j] = b;
+        counts[n + j] = sk;
+        counts[2 * n + j] = km;
+        boff[j + 1] = boff[j] + b;
+        soff[j + 1] = soff[j] + sk;
+    }
+    if (!bytes && !idx && !keys) return GKC_OK;  // sizes only
+    if (!bytes || !idx || !keys) return ctx->fail(GKC_EINVAL, "pack needs bytes, index and keys buffers");
+    if (cap_bytes < boff[n] || cap_skms < soff[n])
+        return ctx->fail(GKC_EINVAL, "pack buffers too small (%llu < %llu bytes or %llu < %llu superkmers)",
+                         (unsigned long long)cap_bytes, (unsigned long long)boff[n], (unsigned long long)cap_skms,
+                         (unsigned long long)soff[n]);
+    std::vector<uint64_t> within(n, 0), within_s(n, 0);  // bytes / superkmers of the chunks before
+    std::vector<PackDesc> d;
+    bool spilled = false;
+    for (auto *c : ctx->store) spilled |= c->on_host;
+    if (spilled) {  // the largest chunk range staged at a time
+        uint64_t mx = 0;
+        for (auto *c : ctx->store)
+            if (c->on_host)
+                mx = std::max<uint64_t>(mx, c->byte_off[p1] - c->byte_off[p0] +
+                                                12 * (c->skm_off[p1] - c->skm_off[p0]));
+        CK(ctx->bk_arena.ensure(mx + 96 + 64));
+    }
+    // device chunks are gathered in one launch; a spilled chunk is staged and
+    // gathered on its own, since the staging buffer is reused
+    auto flush = [&]() -> int {
+        if (d.empty()) return GKC_OK;
+        CK(ctx->tiles.ensure(d.size() * sizeof(PackDesc)));
+        CK(cudaMemcpyAsync(ctx->tiles.p, d.data(), d.size() * sizeof(PackDesc), cudaMemcpyHostToDevice, ctx->s));
+        pack_gather_kernel<<<(uint32_t)d.size(), PK_THREADS, 0, ctx->s>>>(ctx->tiles.as<PackDesc>(), bytes, idx, keys);
+        LAUNCHED();
+        CK(cudaStreamSynchronize(ctx->s));  // the descriptors (pageable) and the staging are reused
+        d.clear();
+        return GKC_OK;
+    };
+    for (auto *c : ctx->store) {
+        const uint8_t *cb;
+        const uint64_t *ci;
+        const uint32_t *ck;
+        uint64_t used = 0;
+        if (c->on_host) RET(flush());
+        RET(chunk_range(ctx, c, (uint32_t)p0, (uint32_t)p1, ctx->bk_arena, &used, &cb, &ci, &ck));
+        for (uint32_t j = 0; j < n; j++) {
+            const uint32_t p = p0 + j;
+            const uint64_t nb = c->byte_off[p + 1] - c->byte_off[p], ns = c->skm_off[p + 1] - c->skm_off[p];
+            if (!nb && !ns) continue;
+            d.push_back({cb + c->byte_off[p], ci + c->skm_off[p], ck + c->skm_off[p], boff[j] + within[j],
+                         soff[j] + within_s[j], nb, ns, within[j]});
+            within[j] += nb;
+            within_s[j] += ns;
+        }
+        if (c->on_host) RET(flush());
+    }
+    RET(flush());
+    return GKC_OK;
+}
+
+int gkc_store_append(gkc_ctx *ctx, int p0, int p1, const uint8_t *bytes, const uint64_t *idx, const uint32_t *keys,
+                     const uint64_t *counts) {
+    if (!ctx || p0 < 0 || p1 < p0 || p1 > ctx->opt.partitions || !counts) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    for (char cn : ctx->counted)
+        if (cn) return ctx->fail(GKC_ESTATE, "the store is partly counted; clear it before appending");
+    const uint32_t P = (uint32_t)ctx->opt.partitions, n = (uint32_t)(p1 - p0);
+    uint64_t nb = 0, ns = 0;
+    for (uint32_t j = 0; j < n; j++) nb += counts[j], ns += counts[n + j];
+    if (!ns) return GKC_OK;
+    if (!bytes || !idx || !keys) return GKC_EINVAL;
+    StoreChunk *c = ctx->take_chunk();
+    c->byte_off.assign(P + 1, 0);
+    c->skm_off.assign(P + 1, 0);
+    c->kmers.assign(P, 0);
+    for (uint32_t p = 0; p < P; p++) {
+        const bool in = p >= (uint32_t)p0 && p < (uint32_t)p1;
+        c->byte_off[p + 1] = c->byte_off[p] + (in ? counts[p - p0] : 0);
+        c->skm_off[p + 1] = c->skm_off[p] + (in ? counts[n + p - p0] : 0);
+        c->kmers[p] = in ? counts[2 * n + p - p0] : 0;
+    }
+    c->nbytes = nb;
+    c->nskm = ns;
+    c->on_host = false;
+    c->pending = false;
+    DevBuf &db = ctx->opt.spill_host ? ctx->spill_bytes : c->dbytes;
+    DevBuf &di = ctx->opt.spill_host ? ctx->spill_idx : c->didx;
+    DevBuf &dk = ctx->opt.spill_host ? ctx->spill_keys : c->dkeys;
+    cudaError_t e = db.ensure(nb + 32);
+    if (e == cudaSuccess) e = di.ensure(ns * 8);
+    if (e == cudaSuccess) e = dk.ensure(ns * 4);
+    if (e == cudaSuccess) e = c->d_byte_off.ensure((P + 1) * 8);
+    if (e == cudaSuccess) e = c->d_skm_off.ensure((P + 1) * 8);
+    if (e != cudaSuccess) {
+        ctx->pool.push_back(c);
+        return ctx->fail(GKC_ENOMEM, "appended chunk allocation (%llu bytes): %s", (unsigned long long)nb,
+                         cudaGetErrorString(e));
+    }
+    c->bytes = db.as<uint8_t>();
+    c->idx = di.as<uint64_t>();
+    c->keys = dk.as<uint32_t>();
+    // cudaMemcpyDefault: the packed range may be in device or host memory
+    CK(cudaMemcpyAsync(c->bytes, bytes, nb, cudaMemcpyDefault, ctx->s));
+    CK(cudaMemsetAsync(c->bytes + nb, 0, 32, ctx->s));
+    CK(cudaMemcpyAsync(c->idx, idx, ns * 8, cudaMemcpyDefault, ctx->s));
+    CK(cudaMemcpyAsync(c->keys, keys, ns * 4, cudaMemcpyDefault, ctx->s));
+    CK(cudaMemcpyAsync(c->d_byte_off.p, c->byte_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemcpyAsync(c->d_skm_off.p, c->skm_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
+    if (ctx->opt.spill_host) {
+        const int rc = spill_chunk(ctx, c);
+        if (rc != GKC_OK) {
+            ctx->pool.push_back(c);
+            return rc;
+        }
+    }
+    ctx->store.push_back(c);
+    // the caller may free or reuse its buffers when this returns
     CK(cudaStreamSynchronize(ctx->s));
     return GKC_OK;
 }
