@@ -25,8 +25,12 @@ Reported (one JSON line on rank 0):
              CUDA-event launch time, against the measured HBM copy bandwidth
   cpu_baseline  the reference's own CPU path (oracle/_ref, compiled from its
              sources) on a bounded sample of the same workload, all host cores
-With --gpus N > 1 (under torchrun) each rank counts its own read set of the
-same size drawn from the same genome (weak scaling, no collective).
+With --gpus N > 1 (under torchrun) each rank holds its own read set of the
+same size drawn from the same genome (weak scaling) and every step counts the
+union exactly: phase 1 per rank, then the partition exchange (one NCCL
+all_to_all per packed array sends each partition range to its owner) and the
+count of each rank's range (rapidgkc_b200/exchange.py); --no-exchange counts
+each rank's reads on their own instead.
 """
 from __future__ import annotations
 
@@ -169,6 +173,8 @@ def main():
     ap.add_argument("--cpu-fraction", type=float, default=0.03)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-exchange", action="store_true",
+                    help="with N > 1, count each rank's reads alone (no partition exchange)")
     ap.add_argument("--order", default="learned", choices=["learned", "default"],
                     help="minimizer order of the reported value (the other is measured beside it)")
     ap.add_argument("--autotune", default=None, action=argparse.BooleanOptionalAction,
@@ -235,14 +241,38 @@ def main():
         if name == "learned":
             c.mlp_order(learned_params)
 
+    exchange = world > 1 and not args.no_exchange
+    xinfo = {}
+
+    def exchanged(r, o):
+        """Phase 1 of this rank's reads, then the partition exchange and the
+        count of this rank's range; (kept, distinct) of the whole job."""
+        from rapidgkc_b200.exchange import count_exchanged
+        c.store_clear()
+        c.add_reads(r, o)
+        res = count_exchanged(c, args.cmin)
+        xinfo.update(res)
+        return res["kept"], res["distinct"]
+
     def step_device():
+        if exchange:
+            return exchanged(d_reads, d_offs)
         return c.count_reads(d_reads, d_offs, args.cmin)
 
     def checksum():
-        """Order-independent digest of the (k-mer, count) result."""
+        """Order-independent digest of the (k-mer, count) result (of the
+        whole job: every rank holds its partitions' k-mers)."""
         km, ct = c.result()
-        return [int(np.bitwise_xor.reduce(km)) if len(km) else 0,
-                int(np.sum(km * ct.astype(np.uint64), dtype=np.uint64)), int(ct.sum(dtype=np.uint64))]
+        d = [int(np.bitwise_xor.reduce(km)) if len(km) else 0,
+             int(np.sum(km * ct.astype(np.uint64), dtype=np.uint64)), int(ct.sum(dtype=np.uint64))]
+        if world > 1:
+            t = torch.tensor([x - (1 << 64) if x >= 1 << 63 else x for x in d], dtype=torch.int64, device="cuda")
+            g = [torch.empty_like(t) for _ in range(world)]
+            dist.all_gather(g, t)
+            a = np.stack([x.cpu().numpy() for x in g]).view(np.uint64)
+            d = [int(np.bitwise_xor.reduce(a[:, 0])), int(np.sum(a[:, 1], dtype=np.uint64)),
+                 int(np.sum(a[:, 2], dtype=np.uint64))]
+        return d
 
     def timed_steps(name):
         set_order(name)
@@ -323,7 +353,11 @@ def main():
             c.store_clear()
             c.add_reads_batches(reads, offs, batch_reads)
             lat = c.batch_timings()
-            no, _ = c.count(args.cmin)
+            if exchange:
+                from rapidgkc_b200.exchange import count_exchanged
+                no = count_exchanged(c, args.cmin)["kept"]
+            else:
+                no, _ = c.count(args.cmin)
             c.result_into(hk, hc)
             return no, lat
 
@@ -345,7 +379,7 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ems = float(t.item())
         e2e = {"value": bases * world / (ems / 1e3) / 1e9, "unit": "Gbp/s",
-               "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)), "d2h_bytes_per_step": int(12 * no),
+               "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)), "d2h_bytes_per_step": int(12 * (xinfo.get("local_kept", no) if exchange else no)),
                "ms_per_step": ems, "path": "gkc_add_reads_batches + gkc_count + gkc_result"}
         sizes = np.diff(offs[np.concatenate([[0], cuts])].astype(np.int64)) / (1 << 20)
         batching = {"batches_per_step": len(batch_reads), "batch_mb_min": float(sizes.min()),
@@ -357,14 +391,21 @@ def main():
         cap = int(n_out * 1.05) + 1024
         hk = torch.empty(cap, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
         hc = torch.empty(cap, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        def step_host():
+            if exchange:
+                no, _ = exchanged(reads, offs)
+                c.result_into(hk, hc)
+                return no, None
+            return c.count_reads(reads, offs, args.cmin, out_kmers=hk, out_counts=hc)
+
         for _ in range(max(1, args.warmup // 2)):
-            c.count_reads(reads, offs, args.cmin, out_kmers=hk, out_counts=hc)
+            step_host()
         torch.cuda.synchronize()
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
-            no, _ = c.count_reads(reads, offs, args.cmin, out_kmers=hk, out_counts=hc)
+            no, _ = step_host()
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1) / args.steps
@@ -373,7 +414,7 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ems = float(t.item())
         e2e = {"value": bases * world / (ems / 1e3) / 1e9, "unit": "Gbp/s",
-               "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)), "d2h_bytes_per_step": int(12 * no),
+               "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)), "d2h_bytes_per_step": int(12 * (xinfo.get("local_kept", no) if exchange else no)),
                "ms_per_step": ems}
 
     # ---- roofline of the dominant kernel class ----
@@ -412,13 +453,19 @@ def main():
             "config": {"workload": args.workload, "desc": WORKLOAD_DESC.get(args.workload, ""),
                        "bases_per_rank": bases, "reads_per_rank": len(offs) - 1, "k": args.k, "p": args.p,
                        "partitions": args.partitions, "counter": args.counter, "order": args.order,
-                       "threshold": f">={args.cmin}", "parallelism": f"dp{world} (independent read sets)",
+                       "threshold": f">={args.cmin}",
+                       "parallelism": f"dp{world} reads + partition exchange" if exchange
+                       else f"dp{world} (independent read sets)",
                        "l2": f"inputs ({bases / 1e9:.1f} GB) larger than L2; no flush", "kmers_kept": n_out,
                        "distinct": n_dist, "gen_s": round(t_gen, 1),
                        "sub_buckets": tstats["sub_buckets"], "overflowed": tstats["overflowed_sub_buckets"],
                        "phase1_ms": round(tstats["phase1_ms"], 2), "phase2_ms": round(tstats["phase2_ms"], 2)},
             "orders": orders, "roofline": roofline, "counting_phase": counting, "e2e": e2e,
             "gpu_launches": int(launches)}
+    if exchange and xinfo:
+        line["exchange"] = {"partitions_rank0": list(xinfo["range"]), "sent_bytes_rank0": xinfo["sent_bytes"],
+                            "received_bytes_rank0": xinfo["received_bytes"],
+                            "note": "kept/distinct are of the union of all ranks' reads"}
     if batching:
         line["batching"] = batching
     if tuned:
