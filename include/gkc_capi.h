@@ -130,10 +130,12 @@ int gkc_store_pack(gkc_ctx *ctx, int p0, int p1, uint8_t *bytes, uint64_t cap_by
 int gkc_store_append(gkc_ctx *ctx, int p0, int p1, const uint8_t *bytes, const uint64_t *idx,
                      const uint32_t *keys, const uint64_t *counts);
 
-/* Pins host memory for spilled chunks (opt.spill_host) until `bytes` are free
- * in the context's host arena; *pinned (may be NULL) = bytes pinned in all.
- * Pinning runs at a few GB/s, so a stream of known size reserves ahead.  The
- * one call that may run on another host thread while gkc_add_reads runs.
+/* Pins host memory for spilled chunks (opt.spill_host) until the context's
+ * host arena holds `bytes` in all, used or free; *pinned (may be NULL) = bytes
+ * pinned.  A stream of known size reserves ahead; this is the one call that
+ * may run on another host thread while gkc_add_reads runs.  The arena never
+ * pins past the point where an eighth of physical memory (at least 8 GiB)
+ * would no longer be available: that fails with GKC_ENOMEM.
  * Replaces the reference's per-chunk host buffers of SKMStoreNoncon
  * (skmstore.hpp:62-279, add_skms). */
 int gkc_reserve_host(gkc_ctx *ctx, uint64_t bytes, uint64_t *pinned);
@@ -173,11 +175,13 @@ int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint
                    uint64_t *n_out, uint64_t *n_distinct);
 
 /* Statistics of the last gkc_add_reads (phase 1) and gkc_count (phase 2)
- * calls (n <= 6 entries): times[0..3] = device milliseconds (CUDA events) of
+ * calls (n <= 8 entries): times[0..3] = device milliseconds (CUDA events) of
  * phase 1, its superkmer search, phase 2, and phase 2's counting kernels;
  * times[4] = sub-buckets of the hash counter, times[5] = those re-split by
  * k-mer hash (their distinct k-mers overflowed shared memory, or they held
- * more than 65536 k-mer instances). */
+ * more than 65536 k-mer instances); hash counter only: times[6] = device
+ * milliseconds of staging spilled chunks back, times[7] = partition groups
+ * counted. */
 int gkc_last_timings(gkc_ctx *ctx, double *times, int n);
 
 /* Number of kernels this context launched since creation. */

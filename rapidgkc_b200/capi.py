@@ -258,8 +258,9 @@ class KmerCounter:
                                              _ptr(counts)[0]))
 
     def reserve_host(self, nbytes: int) -> int:
-        """Pins host memory for spilled chunks until `nbytes` are free; returns
-        the bytes pinned in all.  May run on another thread beside add_reads."""
+        """Pins host memory for spilled chunks until the arena holds `nbytes`
+        in all; returns the bytes pinned.  May run on another thread beside
+        add_reads."""
         pinned = C.c_uint64(0)
         rc = self._L.gkc_reserve_host(self._h, int(nbytes), C.byref(pinned))
         if rc != 0:
@@ -370,10 +371,11 @@ class KmerCounter:
         return lut
 
     def timings(self):
-        t = (C.c_double * 6)()
-        self._check(self._L.gkc_last_timings(self._h, t, 6))
+        t = (C.c_double * 8)()
+        self._check(self._L.gkc_last_timings(self._h, t, 8))
         return {"phase1_ms": t[0], "phase1_search_ms": t[1], "phase2_ms": t[2], "phase2_kernel_ms": t[3],
-                "sub_buckets": int(t[4]), "overflowed_sub_buckets": int(t[5])}
+                "sub_buckets": int(t[4]), "overflowed_sub_buckets": int(t[5]), "phase2_stage_ms": t[6],
+                "phase2_groups": int(t[7])}
 
     def kernel_launches(self) -> int:
         return int(self._L.gkc_kernel_launches(self._h))

@@ -79,11 +79,29 @@ struct PinBuf {
     template <class T> T *as() const { return reinterpret_cast<T *>(p); }
 };
 
+// /proc/meminfo fields in bytes (0 when unreadable)
+static uint64_t meminfo(const char *key) {
+    FILE *f = fopen("/proc/meminfo", "r");
+    if (!f) return 0;
+    char line[256];
+    uint64_t v = 0;
+    const size_t kl = strlen(key);
+    while (fgets(line, sizeof line, f))
+        if (!strncmp(line, key, kl) && line[kl] == ':') {
+            v = strtoull(line + kl + 1, nullptr, 10) * 1024;
+            break;
+        }
+    fclose(f);
+    return v;
+}
+static uint64_t mem_available() { return meminfo("MemAvailable"); }
+static uint64_t mem_total() { return meminfo("MemTotal"); }
+
 // Pinned host memory for spilled chunks.  Pinning is slower than the
-// device-to-host copy, so it is done once: slabs of at least
-// 4 GiB are handed out front to back and rewound when the store is cleared,
-// and gkc_reserve_host can pin them ahead of time (from another thread, while
-// batches run).  Only the slab list is shared with that thread.
+// device-to-host copy, so it is done once: regions are handed out first-fit
+// from slabs of at least 4 GiB, rewound when the store is cleared, and
+// gkc_reserve_host can pin slabs ahead of time (also from another thread
+// while batches run).  Only the slab list is shared with that thread.
 struct HostArena {
     struct Slab {
         uint8_t *p;
@@ -100,6 +118,10 @@ struct HostArena {
     // by one while holding the driver's lock.
     cudaError_t add_slab(size_t bytes) {  // called without the lock held
         const size_t cap = (std::max(bytes, SLAB_MIN) + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1);
+        // never pin the host into swapping or the out-of-memory killer: keep
+        // an eighth of physical memory (at least 8 GiB) available
+        const uint64_t avail = mem_available(), total = mem_total();
+        if (avail && cap + std::max<uint64_t>(total / 8, 8ull << 30) > avail) return cudaErrorMemoryAllocation;
         void *p = mmap(nullptr, cap, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
         if (p == MAP_FAILED) return cudaErrorMemoryAllocation;
         madvise(p, cap, MADV_HUGEPAGE);  // advisory: 4 KB pages still work
@@ -121,42 +143,39 @@ struct HostArena {
         slabs.push_back({(uint8_t *)p, cap, 0});
         return cudaSuccess;
     }
-    size_t free_bytes() {
-        std::lock_guard<std::mutex> g(mu);
-        size_t f = 0;
-        for (size_t i = cur; i < slabs.size(); i++) f += slabs[i].cap - slabs[i].used;
-        return f;
-    }
     size_t pinned() {
         std::lock_guard<std::mutex> g(mu);
         size_t f = 0;
         for (auto &s : slabs) f += s.cap;
         return f;
     }
-    cudaError_t reserve(size_t bytes) {  // pins slabs until `bytes` are free
-        while (free_bytes() < bytes) {
-            const size_t need = bytes - free_bytes();
-            cudaError_t e = add_slab(std::min<size_t>(std::max<size_t>(need, SLAB_MIN), (size_t)16 << 30));
+    // Pins slabs until the arena holds `bytes` in all, used or free (batches
+    // may be taking slabs meanwhile).  One SLAB_MIN slab at a time: the
+    // registration holds the driver's lock (about 0.1 s per slab), so
+    // batches running on another thread wait at most that long.
+    cudaError_t reserve(size_t bytes) {
+        while (pinned() < bytes) {
+            cudaError_t e = add_slab(SLAB_MIN);
             if (e != cudaSuccess) return e;
         }
         return cudaSuccess;
     }
-    // `bytes` of pinned memory, 256-byte aligned; valid until rewind()
+    // `bytes` of pinned memory, 256-byte aligned; valid until rewind().
+    // First fit over the slabs; `cur` skips slabs with no useful room left.
     cudaError_t take(size_t bytes, uint8_t **out) {
         bytes = (bytes + 255) & ~(size_t)255;
         for (;;) {
             {
                 std::lock_guard<std::mutex> g(mu);
-                for (; cur < slabs.size(); cur++) {
-                    Slab &s = slabs[cur];
+                while (cur < slabs.size() && slabs[cur].cap - slabs[cur].used < (1u << 20)) cur++;
+                for (size_t i = cur; i < slabs.size(); i++) {
+                    Slab &s = slabs[i];
                     if (s.cap - s.used >= bytes) {
                         *out = s.p + s.used;
                         s.used += bytes;
                         return cudaSuccess;
                     }
                 }
-                // slabs are filled in order: a slab that cannot take this
-                // chunk stays behind, so `cur` ends past the last slab
             }
             cudaError_t e = add_slab(bytes);
             if (e != cudaSuccess) return e;
@@ -222,6 +241,11 @@ struct gkc_ctx {
     gkc_options opt{};
     int sms = 148;
     cudaStream_t s = nullptr, cs = nullptr, own_s = nullptr;
+    // spilled chunks: two device staging slots, copied to the host arena on
+    // their own stream so the next batch's phase 1 overlaps the copy
+    cudaStream_t ss = nullptr;
+    cudaEvent_t spill_ready = nullptr, spill_done[2] = {nullptr, nullptr};
+    int spill_slot = 0;
 
     // per-kernel-class profiling (events resolved after each public call)
     struct Pending {
@@ -260,7 +284,7 @@ struct gkc_ctx {
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
     std::string err;
     uint64_t launches = 0;
-    double times[6] = {0, 0, 0, 0, 0, 0};  // see gkc_last_timings
+    double times[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // see gkc_last_timings
 
     // phase 1 buffers
     DevBuf reads[2], offs[2];
@@ -287,7 +311,7 @@ struct gkc_ctx {
     DevBuf keysA, keysB, tiles, counts, offsets, blocksums, heads_pos, heads_key, tilecnt, tileoff;
     DevBuf segoff, segcur, part_err, scal;
     DevBuf stage_bytes, stage_idx;
-    DevBuf spill_bytes, spill_idx, spill_keys;  // device staging of chunks being spilled
+    DevBuf spill_bytes[2], spill_idx[2], spill_keys[2];  // device staging of chunks being spilled
     // shared-memory bucket counter
     DevBuf bk_skms, bk_kmers, bk_off, bk_cur, bk_entries, bk_failed, bk_arena, bk_part;
     DevBuf r_work, r_count, r_off, r_cur, r_recs, r_failed;  // record sub-buckets
@@ -311,6 +335,7 @@ struct gkc_ctx {
     }
 
     ~gkc_ctx() {
+        if (ss) cudaStreamSynchronize(ss);  // spill copies into the arena
         for (auto *c : store) delete_chunk(c);
         for (auto *c : pool) delete_chunk(c);
         store.clear();
@@ -319,7 +344,8 @@ struct gkc_ctx {
                         &hist, &flags,
                         &cursors, &part_off, &tile_read, &codes, &lut, &table, &out_k, &out_c, &keysA, &keysB, &tiles,
                         &counts, &offsets, &blocksums, &heads_pos, &heads_key, &tilecnt, &tileoff, &segoff,
-                        &segcur, &part_err, &scal, &stage_bytes, &stage_idx, &spill_bytes, &spill_idx, &spill_keys,
+                        &segcur, &part_err, &scal, &stage_bytes, &stage_idx, &spill_bytes[0], &spill_idx[0], &spill_keys[0],
+                        &spill_bytes[1], &spill_idx[1], &spill_keys[1],
                         &bk_skms, &bk_kmers, &bk_off, &bk_cur, &bk_entries, &bk_failed, &bk_arena, &bk_part,
                         &r_work, &r_count, &r_off, &r_cur, &r_recs, &r_failed, &r_stage, &r_winst,
                         &r_woff, &r_wrec, &ord_loads, &ord_stage, &ord_list, &mlp_p, &mlp_m, &mlp_v, &mlp_g, &mlp_t,
@@ -328,13 +354,15 @@ struct gkc_ctx {
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal};
         for (auto *p : ps) p->release();
         arena.release();
-        cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_ready[0], buf_ready[1]};
+        cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_ready[0], buf_ready[1], spill_ready,
+                             spill_done[0], spill_done[1]};
         for (auto e : evs) if (e) cudaEventDestroy(e);
         for (auto e : batch_ev) cudaEventDestroy(e);
         prof_flush();
         for (auto e : evpool) cudaEventDestroy(e);
         if (own_s) cudaStreamDestroy(own_s);
         if (cs) cudaStreamDestroy(cs);
+        if (ss) cudaStreamDestroy(ss);
     }
     static void delete_chunk(StoreChunk *c) {
         c->release();
@@ -583,22 +611,49 @@ int launch_scatter(gkc_ctx *ctx, const P1Plan &pl, StoreChunk *c, uint64_t total
     return GKC_OK;
 }
 
-// Copies a chunk from device staging (c->bytes, idx, keys) to pinned host
-// memory of the context's arena.
+// Waits for every spill copy in flight: called before spilled chunks are
+// read, staged back, or their arena memory is rewound or freed.
+int spill_sync(gkc_ctx *ctx) {
+    if (ctx->ss) CK(cudaStreamSynchronize(ctx->ss));
+    return GKC_OK;
+}
+
+// Device staging slot for the next spilled chunk: waits until the copy that
+// last read the slot is done, then sizes it.
+int spill_slot(gkc_ctx *ctx, uint64_t nbytes, uint64_t nskm, DevBuf **db, DevBuf **di, DevBuf **dk) {
+    const int j = ctx->spill_slot;
+    CK(cudaEventSynchronize(ctx->spill_done[j]));
+    CK(ctx->spill_bytes[j].ensure(nbytes + 32));
+    CK(ctx->spill_idx[j].ensure(std::max<uint64_t>(nskm, 1) * 8));
+    CK(ctx->spill_keys[j].ensure(std::max<uint64_t>(nskm, 1) * 4));
+    *db = &ctx->spill_bytes[j];
+    *di = &ctx->spill_idx[j];
+    *dk = &ctx->spill_keys[j];
+    return GKC_OK;
+}
+
+// Copies a chunk from the current device staging slot (c->bytes, idx, keys,
+// written on ctx->s) to pinned host memory of the context's arena, on the
+// spill stream; the slot is released by spill_done when the copy ends.
 int spill_chunk(gkc_ctx *ctx, StoreChunk *c) {
-    // index and keys first (8- and 4-byte aligned), then the bytes
+    // three regions, so slabs pack tightly
     const uint64_t ni = std::max<uint64_t>(c->nskm, 1);
-    uint8_t *h = nullptr;
-    cudaError_t ea = ctx->arena.take(ni * 12 + c->nbytes + 16, &h);
+    uint8_t *hb = nullptr, *hi8 = nullptr, *hk8 = nullptr;
+    cudaError_t ea = ctx->arena.take(c->nbytes + 16, &hb);
+    if (ea == cudaSuccess) ea = ctx->arena.take(ni * 8, &hi8);
+    if (ea == cudaSuccess) ea = ctx->arena.take(ni * 4, &hk8);
     if (ea != cudaSuccess) return ctx->fail(GKC_ENOMEM, "pinned spill allocation: %s", cudaGetErrorString(ea));
-    uint64_t *hi = reinterpret_cast<uint64_t *>(h);
-    uint32_t *hk = reinterpret_cast<uint32_t *>(h + ni * 8);
-    uint8_t *hb = h + ni * 12;
-    // stream-ordered: later staging and exports run on the same stream,
-    // so the copies need no wait here and overlap the caller's next batch
-    CK(cudaMemcpyAsync(hb, c->bytes, c->nbytes, cudaMemcpyDeviceToHost, ctx->s));
-    CK(cudaMemcpyAsync(hi, c->idx, c->nskm * 8, cudaMemcpyDeviceToHost, ctx->s));
-    CK(cudaMemcpyAsync(hk, c->keys, c->nskm * 4, cudaMemcpyDeviceToHost, ctx->s));
+    uint64_t *hi = reinterpret_cast<uint64_t *>(hi8);
+    uint32_t *hk = reinterpret_cast<uint32_t *>(hk8);
+    // the copies wait for the chunk's kernels, not the other way round:
+    // readers of spilled chunks call spill_sync first
+    CK(cudaEventRecord(ctx->spill_ready, ctx->s));
+    CK(cudaStreamWaitEvent(ctx->ss, ctx->spill_ready, 0));
+    CK(cudaMemcpyAsync(hb, c->bytes, c->nbytes, cudaMemcpyDeviceToHost, ctx->ss));
+    CK(cudaMemcpyAsync(hi, c->idx, c->nskm * 8, cudaMemcpyDeviceToHost, ctx->ss));
+    CK(cudaMemcpyAsync(hk, c->keys, c->nskm * 4, cudaMemcpyDeviceToHost, ctx->ss));
+    CK(cudaEventRecord(ctx->spill_done[ctx->spill_slot], ctx->ss));
+    ctx->spill_slot ^= 1;
     c->bytes = hb;
     c->idx = hi;
     c->keys = hk;
@@ -661,12 +716,17 @@ int phase1_exact(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
     c->pending = false;
     if (ctx->prof && !ctx->pend.empty()) ctx->pend.back().bytes += 16.0 * c->nskm;  // records written
     // a spilled chunk is scattered into shared device staging, then copied out
-    DevBuf &db = ctx->opt.spill_host ? ctx->spill_bytes : c->dbytes;
-    DevBuf &di = ctx->opt.spill_host ? ctx->spill_idx : c->didx;
-    DevBuf &dk = ctx->opt.spill_host ? ctx->spill_keys : c->dkeys;
-    cudaError_t e1 = db.ensure(c->nbytes + 32);
-    cudaError_t e2 = e1 == cudaSuccess ? di.ensure(std::max<uint64_t>(c->nskm, 1) * 8) : e1;
-    cudaError_t e2k = e2 == cudaSuccess ? dk.ensure(std::max<uint64_t>(c->nskm, 1) * 4) : e2;
+    DevBuf *db = &c->dbytes, *di = &c->didx, *dk = &c->dkeys;
+    if (ctx->opt.spill_host) {
+        const int rc = spill_slot(ctx, c->nbytes, c->nskm, &db, &di, &dk);
+        if (rc != GKC_OK) {
+            ctx->pool.push_back(c);
+            return rc;
+        }
+    }
+    cudaError_t e1 = db->ensure(c->nbytes + 32);
+    cudaError_t e2 = e1 == cudaSuccess ? di->ensure(std::max<uint64_t>(c->nskm, 1) * 8) : e1;
+    cudaError_t e2k = e2 == cudaSuccess ? dk->ensure(std::max<uint64_t>(c->nskm, 1) * 4) : e2;
     cudaError_t e3 = e2k == cudaSuccess ? c->d_byte_off.ensure((P + 1) * 8) : e2k;
     cudaError_t e4 = e3 == cudaSuccess ? c->d_skm_off.ensure((P + 1) * 8) : e3;
     if (e4 != cudaSuccess) {
@@ -674,9 +734,9 @@ int phase1_exact(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, u
         return ctx->fail(GKC_ENOMEM, "store chunk allocation (%llu bytes): %s",
                          (unsigned long long)c->nbytes, cudaGetErrorString(e4));
     }
-    c->bytes = db.as<uint8_t>();
-    c->idx = di.as<uint64_t>();
-    c->keys = dk.as<uint32_t>();
+    c->bytes = db->as<uint8_t>();
+    c->idx = di->as<uint64_t>();
+    c->keys = dk->as<uint32_t>();
     CK(cudaMemcpyAsync(c->d_byte_off.p, c->byte_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
     CK(cudaMemcpyAsync(c->d_skm_off.p, c->skm_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s));
     RET(launch_scatter(ctx, pl, c, total, cap, ctx->flags.as<uint32_t>(), (double)c->nskm, (double)c->nbytes));
@@ -1105,6 +1165,8 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     auto bbase = [&](uint32_t p) -> uint64_t { return p < P ? slog[P + p] : NB; };
     ctx->times[4] = (double)NB;
     ctx->times[5] = 0;
+    float stage_ms = 0;  // host-to-device staging of spilled chunks
+    uint64_t groups = 0;
     // output capacity, grown per group from the kept k-mers per instance of
     // the groups before (at first the bound 1/cmin), at most 25% of free
     // device memory; a group whose output overflows is counted again with
@@ -1175,6 +1237,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         std::vector<const uint8_t *> cb(ctx->store.size());
         std::vector<const uint64_t *> ci(ctx->store.size());
         std::vector<const uint32_t *> ck(ctx->store.size());
+        CK(cudaEventRecord(ctx->e0, ctx->s));
         for (size_t j = 0; j < ctx->store.size(); j++)
             RET(chunk_range(ctx, ctx->store[j], p0, p1, ctx->bk_arena, &arena_used, &cb[j], &ci[j], &ck[j]));
         CK(cudaEventRecord(ctx->e2, ctx->s));
@@ -1241,6 +1304,9 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
         acc_ms += ms;
+        CK(cudaEventElapsedTime(&ms, ctx->e0, ctx->e2));
+        stage_ms += ms;
+        groups++;
         std::vector<uint32_t> ids;
         std::vector<uint64_t> off;
         if (nfail || ctx->opt.hash_l2_only) {
@@ -1296,6 +1362,8 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     ctx->n_out = hs[0];
     ctx->n_distinct += hs[1];
     ctx->times[3] = acc_ms;
+    ctx->times[6] = stage_ms;
+    ctx->times[7] = (double)groups;
     return GKC_OK;
 }
 
@@ -1582,8 +1650,12 @@ int gkc_create(int device, const gkc_options *opt, gkc_ctx **out) {
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return cleanup(GKC_ECUDA);
     ctx->sms = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&ctx->own_s, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->cs, cudaStreamNonBlocking) != cudaSuccess)
+        cudaStreamCreateWithFlags(&ctx->cs, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->ss, cudaStreamNonBlocking) != cudaSuccess)
         return cleanup(GKC_ECUDA);
+    cudaEvent_t *sevs[] = {&ctx->spill_ready, &ctx->spill_done[0], &ctx->spill_done[1]};
+    for (auto *e : sevs)
+        if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return cleanup(GKC_ECUDA);
     ctx->s = ctx->own_s;
     cudaEvent_t *evs[] = {&ctx->e0, &ctx->e1, &ctx->e2, &ctx->e3};
     for (auto *e : evs)
@@ -1821,6 +1893,7 @@ int gkc_store_stats(gkc_ctx *ctx, uint64_t *pb, uint64_t *ps, uint64_t *pk) {
 int gkc_store_export(gkc_ctx *ctx, int part, uint8_t *out, uint64_t cap, uint64_t *n) {
     if (!ctx || part < 0 || part >= ctx->opt.partitions || !n) return GKC_EINVAL;
     CK(cudaSetDevice(ctx->device));
+    RET(spill_sync(ctx));
     uint64_t total = 0;
     for (auto *c : ctx->store) total += c->byte_off[part + 1] - c->byte_off[part];
     *n = total;
@@ -1844,6 +1917,7 @@ int gkc_store_pack(gkc_ctx *ctx, int p0, int p1, uint8_t *bytes, uint64_t cap_by
                    uint64_t cap_skms, uint64_t *counts) {
     if (!ctx || p0 < 0 || p1 < p0 || p1 > ctx->opt.partitions || !counts) return GKC_EINVAL;
     CK(cudaSetDevice(ctx->device));
+    RET(spill_sync(ctx));
     const uint32_t n = (uint32_t)(p1 - p0);
     for (int p = p0; p < p1; p++)
         if (!ctx->counted.empty() && ctx->counted[p])
@@ -1940,12 +2014,17 @@ int gkc_store_append(gkc_ctx *ctx, int p0, int p1, const uint8_t *bytes, const u
     c->nskm = ns;
     c->on_host = false;
     c->pending = false;
-    DevBuf &db = ctx->opt.spill_host ? ctx->spill_bytes : c->dbytes;
-    DevBuf &di = ctx->opt.spill_host ? ctx->spill_idx : c->didx;
-    DevBuf &dk = ctx->opt.spill_host ? ctx->spill_keys : c->dkeys;
-    cudaError_t e = db.ensure(nb + 32);
-    if (e == cudaSuccess) e = di.ensure(ns * 8);
-    if (e == cudaSuccess) e = dk.ensure(ns * 4);
+    DevBuf *db = &c->dbytes, *di = &c->didx, *dk = &c->dkeys;
+    if (ctx->opt.spill_host) {
+        const int rc = spill_slot(ctx, nb, ns, &db, &di, &dk);
+        if (rc != GKC_OK) {
+            ctx->pool.push_back(c);
+            return rc;
+        }
+    }
+    cudaError_t e = db->ensure(nb + 32);
+    if (e == cudaSuccess) e = di->ensure(ns * 8);
+    if (e == cudaSuccess) e = dk->ensure(ns * 4);
     if (e == cudaSuccess) e = c->d_byte_off.ensure((P + 1) * 8);
     if (e == cudaSuccess) e = c->d_skm_off.ensure((P + 1) * 8);
     if (e != cudaSuccess) {
@@ -1953,9 +2032,9 @@ int gkc_store_append(gkc_ctx *ctx, int p0, int p1, const uint8_t *bytes, const u
         return ctx->fail(GKC_ENOMEM, "appended chunk allocation (%llu bytes): %s", (unsigned long long)nb,
                          cudaGetErrorString(e));
     }
-    c->bytes = db.as<uint8_t>();
-    c->idx = di.as<uint64_t>();
-    c->keys = dk.as<uint32_t>();
+    c->bytes = db->as<uint8_t>();
+    c->idx = di->as<uint64_t>();
+    c->keys = dk->as<uint32_t>();
     // cudaMemcpyDefault: the packed range may be in device or host memory
     CK(cudaMemcpyAsync(c->bytes, bytes, nb, cudaMemcpyDefault, ctx->s));
     CK(cudaMemsetAsync(c->bytes + nb, 0, 32, ctx->s));
@@ -1989,6 +2068,7 @@ int gkc_store_clear(gkc_ctx *ctx) {
     if (!ctx) return GKC_EINVAL;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->s);
+    spill_sync(ctx);     // the arena is rewound
     ctx->clear_store();  // buffers stay pooled for the next batch
     ctx->counted.assign(ctx->counted.size(), 0);
     return GKC_OK;
@@ -2003,6 +2083,7 @@ namespace {
 int count_store(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<char> *want, uint64_t *n_out,
                 uint64_t *n_distinct) {
     CK(cudaSetDevice(ctx->device));
+    RET(spill_sync(ctx));
     ctx->n_out = 0;
     ctx->n_distinct = 0;
     ctx->has_result = false;
@@ -2210,7 +2291,7 @@ int gkc_kernel_stats(gkc_ctx *ctx, double *ms, uint64_t *launches, double *bytes
 
 int gkc_last_timings(gkc_ctx *ctx, double *t, int n) {
     if (!ctx || !t) return GKC_EINVAL;
-    for (int i = 0; i < n && i < 6; i++) t[i] = ctx->times[i];
+    for (int i = 0; i < n && i < 8; i++) t[i] = ctx->times[i];
     return GKC_OK;
 }
 
@@ -2225,6 +2306,7 @@ uint64_t gkc_mlp_param_count(int p) {
 int gkc_minimizer_loads(gkc_ctx *ctx, uint64_t *loads, uint64_t n, int mem) {
     if (!ctx || !loads) return GKC_EINVAL;
     CK(cudaSetDevice(ctx->device));
+    RET(spill_sync(ctx));
     const uint64_t np = 1ull << (2 * ctx->opt.p);
     if (n != np) return ctx->fail(GKC_EINVAL, "minimizer loads need 4^p = %llu entries", (unsigned long long)np);
     CK(ctx->ord_loads.ensure(np * 8));

@@ -81,17 +81,16 @@ def stream_count(workload: str = "human_3g", scale: float = 1.0, batch_gb: float
     with KmerCounter(k=k, p=p, partitions=partitions, counter="hash", spill_host=spill, device=device,
                      batch_bases=int(batch_gb * 1e9) + read_len) as c:
         pin = {"s": 0.0, "bytes": 0, "error": None}
-        if spill:  # pin the store's host memory beside the first batches
-            def reserve():
-                t = time.perf_counter()
-                try:
-                    pin["bytes"] = c.reserve_host(est_store)
-                except Exception as e:  # the batches then pin what they need themselves
-                    pin["error"] = str(e)
-                pin["s"] = time.perf_counter() - t
-
-            pin_th = threading.Thread(target=reserve, daemon=True)
-            pin_th.start()
+        if spill:
+            # pin the store's host memory up front, while the producer makes
+            # the first batches: pinning beside the batches competes with
+            # them for the driver's lock and the host's cores
+            t = time.perf_counter()
+            try:
+                pin["bytes"] = c.reserve_host(est_store)
+            except Exception as e:  # the batches then pin what they need themselves
+                pin["error"] = str(e)
+            pin["s"] = time.perf_counter() - t
         if order == "learned":
             from .order import default_order_path, load_order
             c.mlp_order(load_order(default_order_path(p))[0])
@@ -110,22 +109,28 @@ def stream_count(workload: str = "human_3g", scale: float = 1.0, batch_gb: float
             bases += int(offs[-1])
             del reads, offs, item
         th.join()
-        if spill:
-            pin_th.join()
         pb, ps, pk = c.store_stats()
+        c.set_profiling(True)  # per-class kernel times of the count (CUDA events around each launch)
+        c.kernel_stats(reset=True)
         t = time.perf_counter()
         kept, distinct = c.count(cmin)
         t_count = time.perf_counter() - t
+        tm = c.timings()
+        ks = {cls: round(v[0] / 1e3, 4) for cls, v in c.kernel_stats(reset=True).items() if v[1]}
+        c.set_profiling(False)
     out.update({"bases": bases, "store_bytes": int(pb.sum()), "superkmers": int(ps.sum()),
                 "kmer_instances": int(pk.sum()), "maxmean_kmers": float(pk.max() / pk.mean()),
                 "maxmean_bytes": float(pb.max() / pb.mean()), "kept": kept, "distinct": distinct,
-                "phase1_s": t_add, "phase2_s": t_count,
+                "phase1_s": t_add, "phase2_s": t_count, "phase2_kernel_s": tm["phase2_kernel_ms"] / 1e3,
+                "phase2_stage_s": tm["phase2_stage_ms"] / 1e3, "phase2_groups": tm["phase2_groups"],
+                "phase2_kernel_classes_s": ks,
+                "gbps_incl_pinning": bases / (t_add + t_count + pin["s"]) / 1e9,
                 "gbps": bases / (t_add + t_count) / 1e9,
                 "batch_latency_ms": {"p50": float(np.percentile(lat, 50)), "max": float(np.max(lat))} if lat else None,
                 "generator_s": gen_s[0], "genome_s": t_genome, "host_pinned": pin["bytes"] if spill else 0,
                 "pin_s": pin["s"] if spill else 0.0, "pin_error": pin["error"] if spill else None,
-                "note": "gbps = bases / (phase 1 calls + count), wall clock; read generation and host pinning "
-                        "run beside it on other threads"})
+                "note": "gbps = bases / (phase 1 calls + count), wall clock; read generation runs beside it on "
+                        "another thread; host pinning (pin_s) runs before the first batch"})
     return out
 
 

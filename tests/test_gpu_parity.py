@@ -205,6 +205,7 @@ def test_spill_arena_reserve_and_reuse(oracle, kind):
         th.join()
         pinned = c.reserve_host(0)
         assert pinned >= 1 << 20
+        assert c.reserve_host(pinned // 2) == pinned   # already held: nothing more is pinned
         for _ in range(2):
             n, d = c.count(2, U32)
             km, ct = sorted_table(*c.result())
