@@ -214,7 +214,7 @@ def main():
     t_gen = time.perf_counter() - t_gen
     bases = int(offs[-1])
     tuned = None
-    batch_bases = 1 << 30
+    batch_bases = 1 << 28  # 256 MiB phase-1 batches: host copies pipeline finely, scatter slices stay in L2
     radix_bits = 8
     if args.autotune:
         from rapidgkc_b200.autotune import autotune
@@ -453,6 +453,7 @@ def main():
             "config": {"workload": args.workload, "desc": WORKLOAD_DESC.get(args.workload, ""),
                        "bases_per_rank": bases, "reads_per_rank": len(offs) - 1, "k": args.k, "p": args.p,
                        "partitions": args.partitions, "counter": args.counter, "order": args.order,
+                       "batch_bases": batch_bases,
                        "threshold": f">={args.cmin}",
                        "parallelism": f"dp{world} reads + partition exchange" if exchange
                        else f"dp{world} (independent read sets)",

@@ -51,7 +51,7 @@ typedef struct gkc_options {
     int counter;            /* GKC_COUNTER_SORT or GKC_COUNTER_HASH                               */
     int radix_bits;         /* LSD digit width of the sort counter, 4..8 (0 = 8)                  */
     double table_slots;     /* hash slots per k-mer instance of a partition (0 = 0.35)            */
-    uint64_t batch_bases;   /* bases per phase-1 batch for host input (0 = 1 GiB)                 */
+    uint64_t batch_bases;   /* bases per phase-1 batch, host and device input (0 = 1 GiB)         */
     int spill_host;         /* keep the partition store in pinned host memory (streamed input)    */
     uint64_t group_keys;    /* max k-mer instances per sort group (0 = from free device memory)   */
     int hash_l2_only;       /* hash counter: 0 = shared-memory sub-buckets with the L2 table for  */
@@ -79,7 +79,8 @@ int gkc_set_order(gkc_ctx *ctx, const uint32_t *lut, uint64_t n, int mem);
 /* Phase 1: splits a CSR batch of ASCII reads (reads[offs[i]..offs[i+1])) into
  * superkmers and appends them to the context's partition store.  Host input
  * is copied in batches of opt.batch_bases bases, overlapped with compute
- * (pinned host memory gives the overlap).  Device input requires offs[0]==0.
+ * (pinned host memory gives the overlap).  Device input requires offs[0]==0;
+ * it is processed in place, in batches of the same size. 
  * Reads shorter than k contribute nothing. */
 int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads, int mem);
 

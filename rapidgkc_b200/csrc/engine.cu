@@ -304,6 +304,11 @@ struct gkc_ctx {
     uint64_t tcap = 0;
     DevBuf out_k, out_c;
     uint64_t out_cap = 0, n_out = 0, n_distinct = 0;
+    // host arrays that the hash counter fills group by group while it counts
+    // (gkc_count_reads with host output); `streamed` entries are there
+    uint64_t *stream_k = nullptr;
+    uint32_t *stream_c = nullptr;
+    uint64_t stream_cap = 0, streamed = 0;
     bool has_result = false;
     std::vector<char> counted;  // partitions already counted by gkc_count_partitions
     std::vector<cudaEvent_t> batch_ev;  // start / end of each batch of the last gkc_add_reads
@@ -1202,7 +1207,15 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
                             BC_TS * 12));
     CK(cudaFuncSetAttribute(bucket_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BS_SMEM));
     // groups of partitions
-    const uint64_t budget = spilled ? std::max<uint64_t>(1ull << 26, (uint64_t)(free0 * 0.3)) : ~0ull;
+    uint64_t budget = spilled ? std::max<uint64_t>(1ull << 26, (uint64_t)(free0 * 0.3)) : ~0ull;
+    // streamed output: about four groups, so that each group's output is
+    // copied to the host while the next one counts
+    const bool stream_out = ctx->stream_k && ctx->stream_c;
+    if (stream_out) {
+        uint64_t tot = 0;
+        for (uint32_t p = 0; p < P; p++) tot += nbp[p] + 28 * nsp[p];
+        budget = std::min<uint64_t>(budget, std::max<uint64_t>(tot / 4 + 1, 1ull << 20));
+    }
     float acc_ms = 0;
     uint32_t p0 = 0;
     while (p0 < P) {
@@ -1227,7 +1240,9 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         uint64_t est = std::min<uint64_t>(gN / std::max<uint32_t>(cmin, 1),
                                           (uint64_t)((double)gN * kept_ratio * 1.25) + 65536);
         if (out_est_override) est = out_est_override - 1;
-        RET(ensure_out(ctx, out_used + std::min<uint64_t>(est, out_budget) + 1024, out_used));
+        const uint64_t out_need = out_used + std::min<uint64_t>(est, out_budget) + 1024;
+        if (stream_out && out_need > ctx->out_cap) CK(cudaStreamSynchronize(ctx->cs));  // copies read the old buffer
+        RET(ensure_out(ctx, out_need, out_used));
         uint64_t arena_used = 0;
         // the group's bytes and 12 B per superkmer, plus each chunk's padding (<= 32 + 3 x 15 B)
         if (spilled) CK(ctx->bk_arena.ensure(gb + 96 * ctx->store.size() + 64));
@@ -1341,6 +1356,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         if ((uint32_t)hg[2] & ERR_OUTPUT_FULL) {  // count the group again with room for all of it
             if (++redo > 2) return ctx->fail(GKC_EINTERNAL, "output capacity exceeded");
             const uint64_t need = hg[0];
+            if (stream_out) CK(cudaStreamSynchronize(ctx->cs));
             RET(ensure_out(ctx, need + need / 16 + 1024, out_used));
             hg[0] = out_used;
             hg[1] = distinct_used;
@@ -1350,6 +1366,16 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
             continue;
         }
         if (gN) kept_ratio = std::min(1.0 / std::max<uint32_t>(cmin, 1), (double)(hg[0] - out_used) / (double)gN + 1e-3);
+        // the group's output is complete (the stream was synchronised above):
+        // copy it out on the copy stream while the next group counts
+        if (stream_out && ctx->streamed == out_used && hg[0] <= ctx->stream_cap && hg[0] > out_used) {
+            const uint64_t a = out_used, n = hg[0] - out_used;
+            CK(cudaMemcpyAsync(ctx->stream_k + a, ctx->out_k.as<uint64_t>() + a, n * 8, cudaMemcpyDeviceToHost,
+                               ctx->cs));
+            CK(cudaMemcpyAsync(ctx->stream_c + a, ctx->out_c.as<uint32_t>() + a, n * 4, cudaMemcpyDeviceToHost,
+                               ctx->cs));
+            ctx->streamed = hg[0];
+        }
         out_used = hg[0];
         distinct_used = hg[1];
         redo = 0;
@@ -1364,6 +1390,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     ctx->times[3] = acc_ms;
     ctx->times[6] = stage_ms;
     ctx->times[7] = (double)groups;
+    if (stream_out) CK(cudaStreamSynchronize(ctx->cs));
     return GKC_OK;
 }
 
@@ -1776,6 +1803,71 @@ int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, cons
     return GKC_OK;
 }
 
+// Device-resident reads in batches of about batch_bases bases: each batch's
+// phase 1 reads the caller's bytes in place and a rebased copy of its
+// offsets.  Smaller batches keep the scatter's partition slices in L2 (one
+// 3 Gbp batch scatters about 40% slower than six 0.5 Gbp ones).
+int add_device_batches(gkc_ctx *ctx, const uint8_t *dr, const uint64_t *offs, uint64_t n_reads, uint64_t total) {
+    const uint64_t bb = std::max<uint64_t>(ctx->opt.batch_bases, 1);
+    const uint32_t ncut = (uint32_t)((total + bb - 1) / bb);
+    CK(ctx->tiles.ensure((ncut + 1) * 16ull));
+    uint64_t *cut_idx = ctx->tiles.as<uint64_t>(), *cut_off = cut_idx + ncut + 1;
+    batch_cuts_kernel<<<(ncut + 256) / 256, 256, 0, ctx->s>>>(offs, n_reads, bb, ncut, cut_idx, cut_off);
+    LAUNCHED();
+    std::vector<uint64_t> h(2 * (ncut + 1));
+    CK(cudaMemcpyAsync(h.data(), cut_idx, h.size() * 8, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    // batch j ends at cut j + 1; empty ones (a read longer than a batch spans
+    // several cuts) are dropped.  base / bend: offsets of the batch's bounds
+    std::vector<ReadBatch> batches;
+    std::vector<uint64_t> base, bend;
+    uint64_t max_r = 0, r0 = 0, b0 = 0;
+    for (uint32_t j = 0; j < ncut; j++) {
+        const uint64_t r1 = h[j + 1], b1 = h[ncut + 1 + j + 1];
+        if (r1 <= r0) continue;
+        batches.push_back({r0, r1});
+        base.push_back(b0);
+        bend.push_back(b1);
+        max_r = std::max<uint64_t>(max_r, r1 - r0);
+        r0 = r1;
+        b0 = b1;
+    }
+    CK(ctx->offs[0].ensure((max_r + 1) * 8));
+    uint64_t *bo = ctx->offs[0].as<uint64_t>();
+    while (ctx->batch_ev.size() < 2 * batches.size()) {
+        cudaEvent_t ev;
+        CK(cudaEventCreate(&ev));
+        ctx->batch_ev.push_back(ev);
+    }
+    // everything on ctx->s: a batch's offsets copy waits for the batch before
+    for (size_t bi = 0; bi < batches.size(); bi++) {
+        const uint64_t r0 = batches[bi].r0, nr = batches[bi].r1 - r0, nb = bend[bi] - base[bi];
+        CK(cudaEventRecord(ctx->batch_ev[2 * bi], ctx->s));
+        CK(cudaMemcpyAsync(bo, offs + r0, (nr + 1) * 8, cudaMemcpyDeviceToDevice, ctx->s));
+        RET(phase1_async(ctx, dr + base[bi], bo, nr, nb, base[bi], bi));
+        CK(cudaEventRecord(ctx->batch_ev[2 * bi + 1], ctx->s));
+    }
+    CK(cudaStreamSynchronize(ctx->s));
+    std::vector<uint64_t> redo;
+    RET(phase1_finish(ctx, &redo));
+    ctx->batch_ms.assign(batches.size(), 0.0);
+    for (size_t bi = 0; bi < batches.size(); bi++) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, ctx->batch_ev[2 * bi], ctx->batch_ev[2 * bi + 1]) == cudaSuccess)
+            ctx->batch_ms[bi] = ms;
+    }
+    for (uint64_t bi : redo) {  // capacity overflow: the batch again, with exact sizes
+        const uint64_t r0 = batches[bi].r0, nr = batches[bi].r1 - r0, nb = bend[bi] - base[bi];
+        CK(cudaMemcpyAsync(bo, offs + r0, (nr + 1) * 8, cudaMemcpyDeviceToDevice, ctx->s));
+        const uint32_t g = (uint32_t)std::min<uint64_t>((nr + 256) / 256, (uint64_t)ctx->sms * 8);
+        rebase_offsets_kernel<<<g, 256, 0, ctx->s>>>(bo, nr + 1, base[bi]);
+        LAUNCHED();
+        RET(phase1_exact(ctx, dr + base[bi], bo, nr, nb));
+        CK(cudaStreamSynchronize(ctx->s));
+    }
+    return GKC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1798,6 +1890,8 @@ int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_
         const uint8_t *dr = reinterpret_cast<const uint8_t *>(reads);
         if (ctx->opt.spill_host || ctx->prof) {
             RET(phase1_exact(ctx, dr, offs, n_reads, total));
+        } else if (total > ctx->opt.batch_bases) {
+            RET(add_device_batches(ctx, dr, offs, n_reads, total));
         } else {
             // no rebase: the caller's offsets are only read
             RET(phase1_async(ctx, dr, const_cast<uint64_t *>(offs), n_reads, total, 0, 0));
@@ -1811,7 +1905,7 @@ int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
         ctx->times[0] = ms;
-        ctx->batch_ms.assign(1, ms);
+        if (ctx->batch_ms.empty()) ctx->batch_ms.assign(1, ms);  // one batch
         return GKC_OK;
     }
     if (offs[0] > offs[n_reads]) return ctx->fail(GKC_EINVAL, "offsets are not ascending");
@@ -2171,13 +2265,25 @@ int gkc_count_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint6
     RET(gkc_store_clear(ctx));
     RET(gkc_add_reads(ctx, reads, offs, n_reads, mem));
     uint64_t no = 0, nd = 0;
-    RET(gkc_count(ctx, cmin, cmax, &no, &nd));
+    // host output with the hash counter: each group's k-mers are copied out
+    // while the next group counts
+    ctx->streamed = 0;
+    if (kmers && counts && out_mem == GKC_MEM_HOST && ctx->opt.counter == GKC_COUNTER_HASH) {
+        ctx->stream_k = kmers;
+        ctx->stream_c = counts;
+        ctx->stream_cap = cap;
+    }
+    const int rc = gkc_count(ctx, cmin, cmax, &no, &nd);
+    ctx->stream_k = nullptr;
+    ctx->stream_c = nullptr;
+    ctx->stream_cap = 0;
+    RET(rc);
     if (n_out) *n_out = no;
     if (n_distinct) *n_distinct = nd;
     if (kmers || counts) {
         if (cap < no) return ctx->fail(GKC_EINVAL, "output buffer too small (%llu < %llu)",
                                        (unsigned long long)cap, (unsigned long long)no);
-        RET(gkc_result(ctx, kmers, counts, cap, out_mem));
+        if (ctx->streamed != no) RET(gkc_result(ctx, kmers, counts, cap, out_mem));
     }
     return GKC_OK;
 }

@@ -420,6 +420,32 @@ __global__ void rebase_offsets_kernel(uint64_t *offs, uint64_t n, uint64_t base)
         offs[i] -= base;
 }
 
+// Batch cuts of device-resident reads: cut j (0 < j < ncut) is the last read
+// boundary at or below j * bb bases, found by binary search over the offsets
+// (offs[0] == 0); cut 0 is read 0 and cut ncut is n_reads.  cut_idx[j] = read
+// index, cut_off[j] = offs[that read].
+__global__ void batch_cuts_kernel(const uint64_t *__restrict__ offs, uint64_t n_reads, uint64_t bb, uint32_t ncut,
+                                  uint64_t *cut_idx, uint64_t *cut_off) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > ncut) return;
+    uint64_t r;
+    if (j == 0) {
+        r = 0;
+    } else if (j == ncut) {
+        r = n_reads;
+    } else {
+        const uint64_t target = (uint64_t)j * bb;
+        uint64_t lo = 0, hi = n_reads;  // offs[lo] <= target holds (offs[0] == 0)
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi + 1) >> 1;
+            if (offs[mid] <= target) lo = mid; else hi = mid - 1;
+        }
+        r = lo;
+    }
+    cut_idx[j] = r;
+    cut_off[j] = offs[r];
+}
+
 // A batch's store chunk layout from its partition totals (hist: bytes,
 // superkmers, k-mers per partition): exclusive scans into byte_off / skm_off
 // [P+1], k-mers copied out.  Raises ERR_CAPACITY when the chunk's preallocated

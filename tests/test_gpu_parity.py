@@ -78,6 +78,16 @@ def test_device_input_and_many_batches(oracle, kind):
         n, d = c.count()
         km, ct = sorted_table(*c.result())
         assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+    # device input in place, in many small batches (batch_cuts_kernel)
+    with counter(k, p, P, kind, batch_bases=30_000) as c:
+        dr = torch.from_numpy(reads).cuda()
+        do_ = torch.from_numpy(offs.view(np.int64)).cuda()
+        c.add_reads(dr, do_)
+        assert len(c.batch_timings()) >= int(offs[-1]) // 30_000 - 1
+        assert np.array_equal(c.store_stats()[2], pko)
+        n, d = c.count()
+        km, ct = sorted_table(*c.result())
+        assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
     # host input split into many small batches, added in two calls
     with counter(k, p, P, kind, batch_bases=30_000) as c:
         h = len(offs) // 2
@@ -111,6 +121,27 @@ def test_long_and_low_complexity_reads(oracle, kind):
             n, d = c.count()
             km, ct = sorted_table(*c.result())
             assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+
+
+@pytest.mark.parametrize("kind", ["hash", "sort"])
+def test_device_batches_with_reads_longer_than_a_batch(oracle, kind):
+    """Device input cut into batches of 1000 bases, with reads of up to 5000
+    bases (a read spans several cuts) and a 20 kb poly-A read."""
+    import torch
+    r = np.random.default_rng(17)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    parts = [bytes(acgt[r.integers(0, 4, int(n))]) for n in r.integers(20, 5000, 400)]
+    parts[100] = b"A" * 20_000
+    reads, offs = csr(parts)
+    k, p, P = 31, 11, 32
+    ko, co, do, pko = oracle.count_reads(reads, offs, k, p, P)
+    ko, co = sorted_table(ko, co)
+    with counter(k, p, P, kind, batch_bases=1000) as c:
+        c.add_reads(torch.from_numpy(reads).cuda(), torch.from_numpy(offs.view(np.int64)).cuda())
+        assert np.array_equal(c.store_stats()[2], pko)
+        n, d = c.count()
+        km, ct = sorted_table(*c.result())
+    assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
 
 
 def test_reads_shorter_than_k_and_empty():
@@ -187,6 +218,36 @@ def test_retries_spill_and_groups(oracle):
             n, d = c.count(2, U32)
             km, ct = sorted_table(*c.result())
         assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co), kw
+
+
+@pytest.mark.parametrize("pinned,redo", [(True, False), (False, False), (True, True)])
+def test_host_output_streamed_by_groups(oracle, pinned, redo, monkeypatch):
+    """count_reads into host arrays: the hash counter counts in about four
+    partition groups and copies each group's k-mers out while the next group
+    counts (forced output overflows redo every group before its copy)."""
+    import torch
+    if redo:
+        monkeypatch.setenv("GKC_OUT_ESTIMATE", "1")
+    k, p, P = 31, 11, 64
+    reads, offs = random_reads(15, 200_000, 20_000, 150, 0.01)
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P, 2, U32)
+    cap = len(ko) + 100
+    if pinned:
+        hk = torch.zeros(cap, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+        hc = torch.zeros(cap, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    else:
+        hk, hc = np.zeros(cap, np.uint64), np.zeros(cap, np.uint32)
+    with counter(k, p, P, "hash") as c:
+        for _ in range(2):
+            n, d = c.count_reads(reads, offs, 2, U32, out_kmers=hk, out_counts=hc)
+            assert c.timings()["phase2_groups"] >= 3
+            km, ct = sorted_table(hk[:n].copy(), hc[:n].copy())
+            assert d == do and n == len(ko)
+            assert np.array_equal(km, sorted_table(ko, co)[0]) and np.array_equal(ct, sorted_table(ko, co)[1])
+            rk, rc = sorted_table(*c.result())                 # the device result is the same table
+            assert np.array_equal(rk, km) and np.array_equal(rc, ct)
+        with pytest.raises(Exception):
+            c.count_reads(reads, offs, 2, U32, out_kmers=hk[:10], out_counts=hc[:10])  # too small
 
 
 @pytest.mark.parametrize("kind", ["hash", "sort"])
@@ -334,11 +395,16 @@ def test_capacity_overflow_is_redone(oracle):
     pbo, pso, pko, _, _ = oracle.skmgen(reads, offs, k, p, P)
     ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P)
     ko, co = sorted_table(ko, co)
-    with counter(k, p, P, "hash", batch_bases=100_000) as c:
-        c.add_reads(reads, offs)
-        pb, ps, pk = c.store_stats()
-        assert pso.sum() > offs[-1] // 2  # ~one superkmer per base
-        assert np.array_equal(pb, pbo) and np.array_equal(ps, pso) and np.array_equal(pk, pko)
-        n_out, d = c.count()
-        km, ct = sorted_table(*c.result())
-    assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+    import torch
+    for device_input in (False, True):  # host batches, then device batches
+        with counter(k, p, P, "hash", batch_bases=100_000) as c:
+            if device_input:
+                c.add_reads(torch.from_numpy(reads).cuda(), torch.from_numpy(offs.view(np.int64)).cuda())
+            else:
+                c.add_reads(reads, offs)
+            pb, ps, pk = c.store_stats()
+            assert pso.sum() > offs[-1] // 2  # ~one superkmer per base
+            assert np.array_equal(pb, pbo) and np.array_equal(ps, pso) and np.array_equal(pk, pko)
+            n_out, d = c.count()
+            km, ct = sorted_table(*c.result())
+        assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
