@@ -41,6 +41,7 @@ enum {
 
 enum { GKC_COUNTER_SORT = 0, GKC_COUNTER_HASH = 1 };
 enum { GKC_MEM_HOST = 0, GKC_MEM_DEVICE = 1 };
+enum { GKC_FASTQ = 0, GKC_FASTA = 1 };
 
 typedef struct gkc_ctx gkc_ctx;
 
@@ -99,6 +100,34 @@ int gkc_add_reads_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs,
  * (milliseconds from the start of its host-to-device copy to the end of its
  * phase 1, CUDA events): ms[i] for i < min(cap, *n); *n = batches. */
 int gkc_batch_timings(gkc_ctx *ctx, double *ms, uint64_t cap, uint64_t *n);
+
+/* Phase 1 from FASTQ or FASTA text (host or device memory, n bytes): the
+ * records are scanned on the GPU into reads, which gkc_add_reads then takes.
+ * Replaces the reference loader's newline search and read extraction
+ * (fileloader.hpp:201-232, 269-330).
+ *   GKC_FASTQ: 4-line records; line 4i+1 of the text is a read, counting from
+ *     *state = the line phase at the text's start (0 at a file's start; NULL
+ *     means 0).  *state is set to the phase at its end, so a file can be fed
+ *     in pieces cut after any newline, as the reference carries its phase
+ *     across buffers.
+ *   GKC_FASTA: a record is a '>' header line and the sequence lines up to the
+ *     next header, concatenated (the reference's loader takes every second
+ *     line instead, which reads multi-line FASTA wrongly).  Text that starts
+ *     with sequence lines continues a record cut from the text before; its
+ *     bases form a read of their own, so a cut record loses the k-mers that
+ *     span the cut unless the caller repeats k-1 bases.  *state is unused.
+ * '\n' and '\r' are never part of a read.  *n_reads / *n_bases (may be NULL)
+ * = reads and bases found (reads shorter than k add no k-mers). */
+int gkc_add_fastx(gkc_ctx *ctx, const char *text, uint64_t n, int mem, int format, int *state, uint64_t *n_reads,
+                  uint64_t *n_bases);
+
+/* The scan of gkc_add_fastx alone: the reads as a CSR, copied to `reads`
+ * (cap_bases bytes) and `offs` (cap_reads entries, n_reads + 1 used) in host
+ * or device memory (out_mem).  With reads and offs NULL only the sizes are
+ * returned; buffers too small give GKC_ELIMIT with the sizes set. */
+int gkc_parse_fastx(gkc_ctx *ctx, const char *text, uint64_t n, int mem, int format, int *state, char *reads,
+                    uint64_t cap_bases, uint64_t *offs, uint64_t cap_reads, int out_mem, uint64_t *n_reads,
+                    uint64_t *n_bases);
 
 /* Per-partition totals of the store: superkmer bytes, superkmers, k-mers
  * (SKMStoreNoncon::tot_size_bytes / skm_cnt / kmer_cnt).  Arrays of

@@ -23,13 +23,14 @@ LIB_PATH = os.path.join(PKG, "librapidgkc_b200.so")
 GKC_OK, GKC_EINVAL, GKC_ECUDA, GKC_ENOMEM, GKC_ESTATE, GKC_EINTERNAL, GKC_ELIMIT = 0, -1, -2, -3, -4, -5, -6
 COUNTER_SORT, COUNTER_HASH = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
+FORMATS = {"fastq": 0, "fasta": 1}
 UINT32_MAX = 0xFFFFFFFF
 
 # Every symbol declared in include/gkc_capi.h.
 EXPORTS = (
     "gkc_default_options", "gkc_create", "gkc_destroy", "gkc_last_error", "gkc_strerror",
     "gkc_set_order", "gkc_add_reads", "gkc_add_reads_batches", "gkc_batch_timings", "gkc_store_stats", "gkc_store_export", "gkc_store_clear",
-    "gkc_reserve_host", "gkc_store_pack", "gkc_store_append",
+    "gkc_reserve_host", "gkc_store_pack", "gkc_store_append", "gkc_add_fastx", "gkc_parse_fastx",
     "gkc_count", "gkc_count_partitions", "gkc_result", "gkc_result_device", "gkc_count_reads", "gkc_count_keys",
     "gkc_last_timings", "gkc_kernel_launches", "gkc_set_stream", "gkc_set_profiling", "gkc_kernel_stats",
     "gkc_mlp_param_count", "gkc_minimizer_loads", "gkc_mlp_grad", "gkc_mlp_train", "gkc_mlp_scores",
@@ -90,6 +91,9 @@ def load_library(path: str = LIB_PATH):
     L.gkc_reserve_host.argtypes = [vp, u64, C.POINTER(u64)]
     L.gkc_store_pack.argtypes = [vp, i32, i32, vp, u64, vp, vp, u64, vp]
     L.gkc_store_append.argtypes = [vp, i32, i32, vp, vp, vp, vp]
+    L.gkc_add_fastx.argtypes = [vp, vp, u64, i32, i32, C.POINTER(i32), C.POINTER(u64), C.POINTER(u64)]
+    L.gkc_parse_fastx.argtypes = [vp, vp, u64, i32, i32, C.POINTER(i32), vp, u64, vp, u64, i32, C.POINTER(u64),
+                                  C.POINTER(u64)]
     L.gkc_count.argtypes = [vp, u32, u32, C.POINTER(u64), C.POINTER(u64)]
     L.gkc_count_partitions.argtypes = [vp, vp, u64, u32, u32, C.POINTER(u64), C.POINTER(u64)]
     L.gkc_result.argtypes = [vp, vp, vp, u64, i32]
@@ -227,6 +231,35 @@ class KmerCounter:
 
     def store_clear(self):
         self._check(self._L.gkc_store_clear(self._h))
+
+    def add_fastx(self, text, fmt: str = "fastq", state: int = 0):
+        """Phase 1 from FASTQ / FASTA text (bytes, a uint8 array or a CUDA
+        tensor), scanned on the GPU.  Returns (reads, bases, state): state is
+        the FASTQ line phase at the text's end, to pass with the next piece."""
+        if isinstance(text, (bytes, bytearray)):
+            text = np.frombuffer(bytes(text), np.uint8)
+        tp, tm = _ptr(text)
+        st, nr, nb = C.c_int32(state), C.c_uint64(0), C.c_uint64(0)
+        n = text.numel() if hasattr(text, "numel") else len(text)
+        self._check(self._L.gkc_add_fastx(self._h, tp, n, tm, FORMATS[fmt], C.byref(st), C.byref(nr), C.byref(nb)))
+        return nr.value, nb.value, st.value
+
+    def parse_fastx(self, text, fmt: str = "fastq", state: int = 0):
+        """The GPU scan alone: (reads uint8, offs uint64, state) on the host."""
+        if isinstance(text, (bytes, bytearray)):
+            text = np.frombuffer(bytes(text), np.uint8)
+        tp, tm = _ptr(text)
+        n = text.numel() if hasattr(text, "numel") else len(text)
+        st, nr, nb = C.c_int32(state), C.c_uint64(0), C.c_uint64(0)
+        self._check(self._L.gkc_parse_fastx(self._h, tp, n, tm, FORMATS[fmt], C.byref(st), None, 0, None, 0,
+                                            MEM_HOST, C.byref(nr), C.byref(nb)))
+        reads = np.zeros(max(nb.value, 1), np.uint8)
+        offs = np.zeros(nr.value + 1, np.uint64)
+        st = C.c_int32(state)
+        self._check(self._L.gkc_parse_fastx(self._h, tp, n, tm, FORMATS[fmt], C.byref(st), _ptr(reads)[0],
+                                            len(reads), _ptr(offs)[0], len(offs), MEM_HOST, C.byref(nr),
+                                            C.byref(nb)))
+        return reads[: nb.value], offs, st.value
 
     def store_pack(self, p0: int = 0, p1: int | None = None):
         """Packs partitions [p0, p1) into new device tensors: (bytes uint8,

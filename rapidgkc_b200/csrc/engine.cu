@@ -30,6 +30,7 @@
 #include "order_mlp.cu"
 #include "skmgen.cu"
 #include "store_pack.cu"
+#include "fastx.cu"
 
 using namespace gkc;
 
@@ -297,6 +298,8 @@ struct gkc_ctx {
     bool has_lut = false;
     // learned order: network training and scoring
     DevBuf ord_loads, ord_stage, ord_list, mlp_p, mlp_m, mlp_v, mlp_g, mlp_t, mlp_w, mlp_s, mlp_scalar;
+    // FASTQ / FASTA scanning: staged text, tile transforms and carries, the CSR
+    DevBuf fx_text, fx_tiles, fx_state, fx_kept, fx_reads, fx_res, fx_out, fx_offs;
     std::vector<StoreChunk *> store;
 
     // phase 2 buffers
@@ -354,7 +357,8 @@ struct gkc_ctx {
                         &bk_skms, &bk_kmers, &bk_off, &bk_cur, &bk_entries, &bk_failed, &bk_arena, &bk_part,
                         &r_work, &r_count, &r_off, &r_cur, &r_recs, &r_failed, &r_stage, &r_winst,
                         &r_woff, &r_wrec, &ord_loads, &ord_stage, &ord_list, &mlp_p, &mlp_m, &mlp_v, &mlp_g, &mlp_t,
-                        &mlp_w, &mlp_s, &mlp_scalar};
+                        &mlp_w, &mlp_s, &mlp_scalar, &fx_text, &fx_tiles, &fx_state, &fx_kept,
+                        &fx_reads, &fx_res, &fx_out, &fx_offs};
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal};
         for (auto *p : ps) p->release();
@@ -1803,6 +1807,72 @@ int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, cons
     return GKC_OK;
 }
 
+// FASTQ (format 0) or FASTA (1) text -> the CSR in ctx->fx_out / fx_offs.
+// state_in: FASTQ line phase at the text's start (0 at a file's start).
+int parse_fastx(gkc_ctx *ctx, const char *text, uint64_t n, int mem, int format, int state_in, uint64_t *n_reads,
+                uint64_t *n_bases, int *state_out) {
+    if ((format != GKC_FASTQ && format != GKC_FASTA) || state_in < 0 || state_in > 3 || (!text && n))
+        return ctx->fail(GKC_EINVAL, "fastx: format must be GKC_FASTQ or GKC_FASTA and the state 0..3");
+    const bool fasta = format == GKC_FASTA;
+    *n_reads = *n_bases = 0;
+    *state_out = fasta ? 0 : state_in;
+    if (n == 0) return GKC_OK;
+    // staged into an aligned buffer: the tile kernels read 16-byte words
+    CK(ctx->fx_text.ensure(n + 64));
+    CK(cudaMemcpyAsync(ctx->fx_text.p, text, n, mem == GKC_MEM_DEVICE ? cudaMemcpyDeviceToDevice
+                                                                      : cudaMemcpyHostToDevice, ctx->s));
+    const uint64_t ntiles = (n + FX_TILE - 1) / FX_TILE;
+    CK(ctx->fx_tiles.ensure(ntiles * sizeof(FxT)));
+    CK(ctx->fx_state.ensure(ntiles));
+    CK(ctx->fx_kept.ensure(ntiles * 8));
+    CK(ctx->fx_reads.ensure(ntiles * 8));
+    CK(ctx->fx_res.ensure(64));
+    CK(ctx->h_scal.ensure(64));
+    // a read already open at the text's start: FASTQ phase 1, or FASTA text
+    // that starts with sequence lines (a record continued from the text before)
+    uint8_t first = 0;
+    CK(cudaMemcpyAsync(&first, ctx->fx_text.p, 1, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    const int virtual_read = fasta ? (first != '>') : (state_in == 1);
+    FxParams a;
+    a.text = ctx->fx_text.as<uint8_t>();
+    a.n = n;
+    a.tiles = ctx->fx_tiles.as<FxT>();
+    a.ntiles = ntiles;
+    a.tile_state = ctx->fx_state.as<uint8_t>();
+    a.tile_kept = ctx->fx_kept.as<uint64_t>();
+    a.tile_reads = ctx->fx_reads.as<uint64_t>();
+    a.result = ctx->fx_res.as<uint64_t>();
+    a.state_in = state_in;
+    a.out = nullptr;
+    a.offs = nullptr;
+    if (fasta) fastx_tile_kernel<true><<<(uint32_t)ntiles, FX_THREADS, 0, ctx->s>>>(a);
+    else fastx_tile_kernel<false><<<(uint32_t)ntiles, FX_THREADS, 0, ctx->s>>>(a);
+    LAUNCHED();
+    fastx_carry_kernel<<<1, FX_CARRY_THREADS, 0, ctx->s>>>(a, virtual_read);
+    LAUNCHED();
+    uint64_t *hr = ctx->h_scal.as<uint64_t>();
+    CK(cudaMemcpyAsync(hr, ctx->fx_res.p, 24, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    const uint64_t kept = hr[0], reads = hr[1];
+    const int st = (int)hr[2];
+    CK(ctx->fx_out.ensure(kept + 64));
+    CK(ctx->fx_offs.ensure((reads + 1) * 8));
+    a.out = ctx->fx_out.as<uint8_t>();
+    a.offs = ctx->fx_offs.as<uint64_t>();
+    if (virtual_read) CK(cudaMemsetAsync(a.offs, 0, 8, ctx->s));
+    if (fasta) fastx_write_kernel<true><<<(uint32_t)ntiles, FX_THREADS, 0, ctx->s>>>(a);
+    else fastx_write_kernel<false><<<(uint32_t)ntiles, FX_THREADS, 0, ctx->s>>>(a);
+    LAUNCHED();
+    hr[3] = kept;
+    CK(cudaMemcpyAsync(a.offs + reads, hr + 3, 8, cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    *n_reads = reads;
+    *n_bases = kept;
+    *state_out = fasta ? 0 : st;
+    return GKC_OK;
+}
+
 // Device-resident reads in batches of about batch_bases bases: each batch's
 // phase 1 reads the caller's bytes in place and a rebased copy of its
 // offsets.  Smaller batches keep the scatter's partition slices in L2 (one
@@ -1965,6 +2035,41 @@ int gkc_batch_timings(gkc_ctx *ctx, double *ms, uint64_t cap, uint64_t *n) {
     if (n) *n = ctx->batch_ms.size();
     for (uint64_t i = 0; ms && i < cap && i < ctx->batch_ms.size(); i++) ms[i] = ctx->batch_ms[i];
     return GKC_OK;
+}
+
+int gkc_parse_fastx(gkc_ctx *ctx, const char *text, uint64_t n, int mem, int format, int *state, char *reads,
+                    uint64_t cap_bases, uint64_t *offs, uint64_t cap_reads, int out_mem, uint64_t *n_reads,
+                    uint64_t *n_bases) {
+    if (!ctx || !n_reads || !n_bases) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    int st = 0;
+    RET(parse_fastx(ctx, text, n, mem, format, state ? *state : 0, n_reads, n_bases, &st));
+    if (state) *state = st;
+    if (!reads && !offs) return GKC_OK;  // sizes only
+    if (!reads || !offs || cap_bases < *n_bases || cap_reads < *n_reads + 1) return GKC_ELIMIT;
+    const cudaMemcpyKind kind = out_mem == GKC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (*n_bases) CK(cudaMemcpyAsync(reads, ctx->fx_out.p, *n_bases, kind, ctx->s));
+    if (*n_reads) CK(cudaMemcpyAsync(offs, ctx->fx_offs.p, (*n_reads + 1) * 8, kind, ctx->s));
+    else if (out_mem == GKC_MEM_DEVICE) CK(cudaMemsetAsync(offs, 0, 8, ctx->s));
+    else offs[0] = 0;
+    CK(cudaStreamSynchronize(ctx->s));
+    return GKC_OK;
+}
+
+int gkc_add_fastx(gkc_ctx *ctx, const char *text, uint64_t n, int mem, int format, int *state, uint64_t *n_reads,
+                  uint64_t *n_bases) {
+    if (!ctx) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    for (char c : ctx->counted)
+        if (c) return ctx->fail(GKC_ESTATE, "the store is partly counted; clear it before adding reads");
+    uint64_t nr = 0, nb = 0;
+    int st = 0;
+    RET(parse_fastx(ctx, text, n, mem, format, state ? *state : 0, &nr, &nb, &st));
+    if (state) *state = st;
+    if (n_reads) *n_reads = nr;
+    if (n_bases) *n_bases = nb;
+    if (!nr) return GKC_OK;
+    return gkc_add_reads(ctx, ctx->fx_out.as<char>(), ctx->fx_offs.as<uint64_t>(), nr, GKC_MEM_DEVICE);
 }
 
 int gkc_store_stats(gkc_ctx *ctx, uint64_t *pb, uint64_t *ps, uint64_t *pk) {

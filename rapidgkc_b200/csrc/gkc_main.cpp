@@ -16,9 +16,10 @@
 // ascending within a partition with -counter sort), or ascending k-mer with
 // -sorted.
 //
-// Input: FASTA or FASTQ, plain or gzip (zlib reads both).  A parser thread
-// fills pinned batches of about -bb MB while the main thread hands the
-// previous batch to the GPU.
+// Input: FASTA or FASTQ, plain or gzip (zlib reads both).  A reader thread
+// fills pinned blocks of about -bb MB of decompressed text while the main
+// thread hands the previous block to the GPU, which scans its records
+// (gkc_add_fastx) and splits the reads into superkmers.
 #include <cuda_runtime.h>
 #include <zlib.h>
 
@@ -109,94 +110,145 @@ void check(int rc, gkc_ctx *ctx, const char *what) {
     }
 }
 
-// A batch of reads in pinned host memory (CSR).
-struct Batch {
-    char *bases = nullptr;
-    uint64_t *offs = nullptr;
-    uint64_t cap_bases = 0, cap_reads = 0, n_reads = 0;
-    void reserve(uint64_t nb, uint64_t nr) {
-        if (nb > cap_bases) {
-            if (bases) cudaFreeHost(bases);
-            cap_bases = nb + nb / 4;
-            if (cudaHostAlloc(reinterpret_cast<void **>(&bases), cap_bases, cudaHostAllocDefault) != cudaSuccess) {
-                std::fprintf(stderr, "gkc_main: pinned allocation of %llu bytes failed\n",
-                             (unsigned long long)cap_bases);
-                std::exit(1);
-            }
+// A block of FASTA / FASTQ text in pinned host memory, cut where the GPU
+// scanner can pick up again (TextReader::next).
+struct TextBlock {
+    char *p = nullptr;
+    uint64_t cap = 0, n = 0;
+    int fmt = GKC_FASTQ;
+    bool file_start = false;  // the first block of a file: the FASTQ phase restarts
+    uint64_t repeated = 0;    // bases repeated from the block before (FASTA, see below)
+    void reserve(uint64_t want) {
+        if (want <= cap) return;
+        char *q = nullptr;
+        const uint64_t c = want + want / 4;
+        if (cudaHostAlloc(reinterpret_cast<void **>(&q), c, cudaHostAllocDefault) != cudaSuccess) {
+            std::fprintf(stderr, "gkc_main: pinned allocation of %llu bytes failed\n", (unsigned long long)c);
+            std::exit(1);
         }
-        if (nr + 1 > cap_reads) {
-            if (offs) cudaFreeHost(offs);
-            cap_reads = nr + nr / 4 + 2;
-            if (cudaHostAlloc(reinterpret_cast<void **>(&offs), cap_reads * 8, cudaHostAllocDefault) != cudaSuccess) {
-                std::fprintf(stderr, "gkc_main: pinned allocation failed\n");
-                std::exit(1);
-            }
-        }
+        if (n) std::memcpy(q, p, n);
+        if (p) cudaFreeHost(p);
+        p = q;
+        cap = c;
     }
-    ~Batch() {
-        if (bases) cudaFreeHost(bases);
-        if (offs) cudaFreeHost(offs);
+    ~TextBlock() {
+        if (p) cudaFreeHost(p);
     }
 };
 
-// FASTA/FASTQ records, plain or gzip, sequence lines only.
-class Reader {
+// Decompressed text of one file (plain or gzip) in blocks of about `block`
+// bytes.  FASTQ blocks end after a newline: the GPU scanner carries the line
+// phase across them, as the reference loader does (fileloader.hpp:201-232).
+// FASTA blocks end before a '>' header line, so records stay whole; a record
+// longer than a block is cut after a newline, and its last k - 1 bases are
+// repeated at the start of the next block, so every k-mer across the cut is
+// counted once.
+class TextReader {
 public:
-    explicit Reader(const std::string &path) : fp_(gzopen(path.c_str(), "rb")), path_(path) {
+    TextReader(const std::string &path, uint64_t block, int k)
+        : fp_(gzopen(path.c_str(), "rb")), path_(path), block_(block), k_(k) {
         if (!fp_) {
             std::fprintf(stderr, "gkc_main: cannot open %s\n", path.c_str());
             std::exit(1);
         }
-        gzbuffer(fp_, 1 << 20);
+        gzbuffer(fp_, 1 << 22);
     }
-    ~Reader() { gzclose(fp_); }
-    // Appends the next record's sequence to seq; false at end of input.
-    bool next(std::string &seq) {
-        seq.clear();
-        if (!line(line_)) return false;
-        while (line_.empty())
-            if (!line(line_)) return false;
-        if (line_[0] == '@') {  // FASTQ: header, sequence, '+', qualities
-            if (!line(seq)) bad();
-            std::string plus, qual;
-            if (!line(plus) || plus.empty() || plus[0] != '+' || !line(qual)) bad();
-            return true;
-        }
-        if (line_[0] == '>') {  // FASTA: header, then sequence lines up to the next '>'
-            while (peek() != '>' && peek() != EOF) {
-                if (!line(tmp_)) break;
-                seq += tmp_;
+    ~TextReader() { gzclose(fp_); }
+    // The next block; false at the end of the file.
+    bool next(TextBlock &b) {
+        b.n = 0;
+        b.repeated = repeat_;
+        b.file_start = first_;
+        b.reserve(std::max<uint64_t>(block_, carry_.size()) + 64);
+        std::memcpy(b.p, carry_.data(), carry_.size());
+        b.n = carry_.size();
+        carry_.clear();
+        repeat_ = 0;
+        for (;;) {  // fill the block; grow it while it holds no place to cut
+            while (!eof_ && b.n < b.cap - 64) {
+                const uint64_t want = std::min<uint64_t>(b.cap - 64 - b.n, 1u << 30);
+                const int got = gzread(fp_, b.p + b.n, (unsigned)want);
+                if (got < 0) {
+                    std::fprintf(stderr, "gkc_main: read error in %s\n", path_.c_str());
+                    std::exit(1);
+                }
+                if (got == 0) eof_ = true;
+                b.n += (uint64_t)got;
+                if (b.n >= block_) break;
             }
-            return true;
+            if (first_) detect(b);
+            first_ = false;
+            if (eof_ || cut(b)) break;
+            b.reserve(b.cap * 2);
         }
-        bad();
+        b.fmt = fmt_;
+        return b.n > 0;
     }
 
 private:
-    [[noreturn]] void bad() {
-        std::fprintf(stderr, "gkc_main: %s is not FASTA or FASTQ\n", path_.c_str());
-        std::exit(1);
-    }
-    int peek() {
-        const int c = gzgetc(fp_);
-        if (c != -1) gzungetc(c, fp_);
-        return c;
-    }
-    bool line(std::string &out) {
-        out.clear();
-        char buf[1 << 14];
-        while (gzgets(fp_, buf, sizeof(buf))) {
-            size_t n = std::strlen(buf);
-            const bool eol = n && buf[n - 1] == '\n';
-            if (eol) n--;
-            if (n && buf[n - 1] == '\r') n--;
-            out.append(buf, n);
-            if (eol) return true;
+    void detect(const TextBlock &b) {
+        uint64_t i = 0;
+        while (i < b.n && (b.p[i] == '\n' || b.p[i] == '\r' || b.p[i] == ' ')) i++;
+        if (i == b.n) return;  // empty: either format gives no reads
+        if (b.p[i] == '@') fmt_ = GKC_FASTQ;
+        else if (b.p[i] == '>') fmt_ = GKC_FASTA;
+        else {
+            std::fprintf(stderr, "gkc_main: %s is not FASTA or FASTQ\n", path_.c_str());
+            std::exit(1);
         }
-        return !out.empty();
+    }
+    // Cuts the block at a place the scanner can resume from and keeps the
+    // rest for the next block; false if there is none yet.
+    bool cut(TextBlock &b) {
+        uint64_t c = b.n;
+        if (fmt_ == GKC_FASTA) {  // before the last header line
+            for (uint64_t i = b.n; i-- > 1;)
+                if (b.p[i] == '>' && b.p[i - 1] == '\n') {
+                    c = i;
+                    break;
+                }
+            if (c < b.n) {
+                carry_.assign(b.p + c, b.n - c);
+                b.n = c;
+                return true;
+            }
+        }
+        uint64_t nl = b.n;  // after the last newline
+        for (uint64_t i = b.n; i-- > 0;)
+            if (b.p[i] == '\n') {
+                nl = i + 1;
+                break;
+            }
+        if (nl == b.n && (b.n == 0 || b.p[b.n - 1] != '\n')) return false;
+        carry_.assign(b.p + nl, b.n - nl);
+        b.n = nl;
+        if (fmt_ == GKC_FASTA) {  // inside a record: repeat its last k - 1 bases
+            // the block holds no header line but perhaps one at its start
+            uint64_t s0 = 0;
+            if (b.p[0] == '>') {
+                s0 = nl;
+                for (uint64_t i = 0; i < nl; i++)
+                    if (b.p[i] == '\n') {
+                        s0 = i + 1;
+                        break;
+                    }
+            }
+            std::string tail;
+            for (uint64_t i = nl; i-- > s0 && (int)tail.size() < k_ - 1;)
+                if (b.p[i] != '\n' && b.p[i] != '\r') tail.push_back(b.p[i]);
+            std::reverse(tail.begin(), tail.end());
+            repeat_ = tail.size();
+            carry_.insert(0, tail + "\n");
+        }
+        return true;
     }
     gzFile fp_;
-    std::string path_, line_, tmp_;
+    std::string path_, carry_;
+    uint64_t block_;
+    int k_;
+    int fmt_ = GKC_FASTQ;
+    bool first_ = true, eof_ = false;
+    uint64_t repeat_ = 0;
 };
 
 std::vector<float> load_params(const std::string &path, uint64_t n) {
@@ -279,66 +331,53 @@ int main(int argc, char **argv) {
         const std::vector<float> params = load_params(path, gkc_mlp_param_count(a.p));
         check(gkc_mlp_order(ctx, params.data(), 0, nullptr), ctx, "learned order");
     }
-    // ---- phase 1: a parser thread fills one pinned batch while the GPU takes the other
-    const uint64_t batch_bases = a.batch_mb << 20;
-    Batch batches[2];
+    // ---- phase 1: a reader thread fills one pinned text block while the GPU
+    // scans and splits the other
+    const uint64_t block = a.batch_mb << 20;
+    TextBlock blocks[2];
     std::mutex mu;
     std::condition_variable cv;
     bool full[2] = {false, false}, eof = false;
     uint64_t produced = 0, consumed = 0;
     uint64_t n_reads = 0, n_bases = 0;
     std::thread parser([&]() {  // fills slots 0, 1, 0, ... in turn
-        std::string seq;
         size_t fi = 0;
-        Reader *rd = new Reader(a.files[0]);
-        for (int slot = 0;; slot ^= 1) {
+        TextReader *rd = new TextReader(a.files[0], block, a.k);
+        for (int slot = 0;;) {
             {
                 std::unique_lock<std::mutex> lk(mu);
                 cv.wait(lk, [&]() { return !full[slot]; });
             }
-            Batch &b = batches[slot];
-            uint64_t nb = 0, nr = 0;
-            bool end = false;
-            b.reserve(batch_bases + (1 << 20), 1 << 20);
-            b.offs[0] = 0;
-            while (nb < batch_bases) {
-                if (!rd->next(seq)) {
-                    delete rd;
-                    rd = nullptr;
-                    if (++fi == a.files.size()) {
-                        end = true;
-                        break;
-                    }
-                    rd = new Reader(a.files[fi]);
-                    continue;
-                }
-                b.reserve(nb + seq.size() + (1 << 20), nr + 1);
-                std::memcpy(b.bases + nb, seq.data(), seq.size());
-                nb += seq.size();
-                b.offs[++nr] = nb;
+            if (!rd->next(blocks[slot])) {
+                delete rd;
+                rd = nullptr;
+                if (++fi == a.files.size()) break;
+                rd = new TextReader(a.files[fi], block, a.k);
+                continue;
             }
-            b.n_reads = nr;
             std::lock_guard<std::mutex> lk(mu);
-            if (nr) {
-                full[slot] = true;
-                produced++;
-            }
-            eof = end;
+            full[slot] = true;
+            produced++;
             cv.notify_all();
-            if (end) break;
+            slot ^= 1;
         }
-        delete rd;
+        std::lock_guard<std::mutex> lk(mu);
+        eof = true;
+        cv.notify_all();
     });
+    int state = 0;  // FASTQ line phase, carried from block to block
     for (int slot = 0;; slot ^= 1) {  // takes slots 0, 1, 0, ... in turn
         {
             std::unique_lock<std::mutex> lk(mu);
             cv.wait(lk, [&]() { return full[slot] || (eof && consumed == produced); });
             if (!full[slot]) break;
         }
-        Batch &b = batches[slot];
-        check(gkc_add_reads(ctx, b.bases, b.offs, b.n_reads, GKC_MEM_HOST), ctx, "phase 1");
-        n_reads += b.n_reads;
-        n_bases += b.offs[b.n_reads];
+        TextBlock &b = blocks[slot];
+        if (b.file_start) state = 0;
+        uint64_t nr = 0, nb = 0;
+        check(gkc_add_fastx(ctx, b.p, b.n, GKC_MEM_HOST, b.fmt, &state, &nr, &nb), ctx, "phase 1");
+        n_reads += nr;
+        n_bases += nb - b.repeated;
         std::lock_guard<std::mutex> lk(mu);
         full[slot] = false;
         consumed++;

@@ -78,3 +78,30 @@ def test_cli_counts_match_oracle(oracle, tmp_path):
     ct2 = np.array(lines[1::2], np.uint32)
     km2, ct2 = sorted_table(km2, ct2)
     assert np.array_equal(km2, ko) and np.array_equal(ct2, co)
+
+
+@pytest.mark.gpu
+def test_cli_fasta_records_longer_than_a_block(oracle, tmp_path):
+    """-bb 1 reads 1 MB blocks: a 2.5 Mbp FASTA record (wrapped at 80) is cut
+    inside twice, and the k-1 bases repeated across each cut keep its k-mers
+    exact; short records around it stay whole."""
+    r = np.random.default_rng(5)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    big = bytes(acgt[r.integers(0, 4, 2_500_000)])
+    small = [bytes(acgt[r.integers(0, 4, int(n))]) for n in r.integers(40, 400, 50)]
+    seqs = small[:25] + [big] + small[25:]
+    path = str(tmp_path / "g.fa")
+    with open(path, "wb") as f:
+        for i, s in enumerate(seqs):
+            f.write(b">s%d\n" % i + b"\n".join(s[j:j + 80] for j in range(0, len(s), 80)) + b"\n")
+    reads = np.frombuffer(b"".join(seqs), np.uint8).copy()
+    offs = np.zeros(len(seqs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(s) for s in seqs])
+    k, p, P = 31, 11, 64
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P, 1, U32)
+    ko, co = sorted_table(ko, co)
+    out = str(tmp_path / "c.bin")
+    p_ = _run("-k", str(k), "-p", str(p), "-skm", str(P), "-ci", "1", "-o", out, "-sorted", "-bb", "1", "-read", path)
+    assert f"distinct k-mers {do}" in p_.stderr and f"bases {len(reads)}," in p_.stderr
+    _, km, ct = _read_bin(out)
+    assert np.array_equal(km, ko) and np.array_equal(ct, co)
