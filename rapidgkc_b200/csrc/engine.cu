@@ -326,6 +326,7 @@ struct gkc_ctx {
     DevBuf r_stage, r_winst, r_woff, r_wrec;                  // per-work-item record segments
     uint64_t fallback_buckets = 0;  // sub-buckets counted through the L2 table
     PinBuf h_scal;
+    PinBuf h_off, h_km, h_ids, h_work;  // pinned staging of the record path's host round trips
 
     std::vector<StoreChunk *> pool;  // cleared chunks kept for reuse
     HostArena arena;                 // pinned host memory of spilled chunks
@@ -360,7 +361,7 @@ struct gkc_ctx {
                         &mlp_w, &mlp_s, &mlp_scalar, &fx_text, &fx_tiles, &fx_state, &fx_kept,
                         &fx_reads, &fx_res, &fx_out, &fx_offs};
         for (auto *d : ds) d->release();
-        PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal};
+        PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work};
         for (auto *p : ps) p->release();
         arena.release();
         cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_ready[0], buf_ready[1], spill_ready,
@@ -987,7 +988,10 @@ int count_buckets_records_slice(gkc_ctx *ctx, const std::vector<uint32_t> &ids, 
     CK(ctx->r_woff.ensure((nw + 1) * 8));
     CK(ctx->r_wrec.ensure(nw * 4));
     CK(ctx->r_failed.ensure((NR + 1) * 4));
-    CK(cudaMemcpyAsync(ctx->r_work.p, work.data(), nw * sizeof(RWork), cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));  // the pinned work list of an earlier slice may still be in flight
+    CK(ctx->h_work.ensure(nw * sizeof(RWork)));
+    std::memcpy(ctx->h_work.p, work.data(), nw * sizeof(RWork));
+    CK(cudaMemcpyAsync(ctx->r_work.p, ctx->h_work.p, nw * sizeof(RWork), cudaMemcpyHostToDevice, ctx->s));
     CK(cudaMemsetAsync(ctx->r_count.p, 0, NR * 4, ctx->s));
     CK(cudaMemsetAsync(ctx->r_failed.p, 0, 4, ctx->s));
     auto *sc = ctx->scal.as<unsigned long long>();
@@ -1057,11 +1061,13 @@ int count_buckets_records_slice(gkc_ctx *ctx, const std::vector<uint32_t> &ids, 
     CK(cudaMemcpyAsync(&nfail, ctx->r_failed.p, 4, cudaMemcpyDeviceToHost, ctx->s));
     CK(cudaStreamSynchronize(ctx->s));
     if (!nfail) return GKC_OK;
-    std::vector<uint32_t> rids(nfail);
-    std::vector<uint64_t> roff(NR + 1);
-    CK(cudaMemcpyAsync(rids.data(), ctx->r_failed.as<uint32_t>() + 1, nfail * 4, cudaMemcpyDeviceToHost, ctx->s));
-    CK(cudaMemcpyAsync(roff.data(), ctx->r_off.p, (NR + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
+    CK(ctx->h_ids.ensure(nfail * 4ull));
+    CK(ctx->h_off.ensure((NR + 1) * 8));
+    CK(cudaMemcpyAsync(ctx->h_ids.p, ctx->r_failed.as<uint32_t>() + 1, nfail * 4, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaMemcpyAsync(ctx->h_off.p, ctx->r_off.p, (NR + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
     CK(cudaStreamSynchronize(ctx->s));
+    const std::vector<uint32_t> rids(ctx->h_ids.as<uint32_t>(), ctx->h_ids.as<uint32_t>() + nfail);
+    const std::vector<uint64_t> roff(ctx->h_off.as<uint64_t>(), ctx->h_off.as<uint64_t>() + NR + 1);
     const double slots = ctx->opt.table_slots > 0 ? ctx->opt.table_slots : 0.35;
     for (uint32_t r : rids) {
         // the records of window r, as rec_count_kernel chose them
@@ -1329,14 +1335,18 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         std::vector<uint32_t> ids;
         std::vector<uint64_t> off;
         if (nfail || ctx->opt.hash_l2_only) {
-            off.resize(NB + 1);
-            CK(cudaMemcpyAsync(off.data(), ctx->bk_off.p, (NB + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
+            // through pinned buffers: pageable copies stage through the driver
+            // and stall with the host's load
+            CK(ctx->h_off.ensure((NB + 1) * 8));
+            CK(cudaMemcpyAsync(ctx->h_off.p, ctx->bk_off.p, (NB + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
             if (nfail) {
-                ids.resize(nfail);
-                CK(cudaMemcpyAsync(ids.data(), ctx->bk_failed.as<uint32_t>() + 1, nfail * 4,
+                CK(ctx->h_ids.ensure(nfail * 4));
+                CK(cudaMemcpyAsync(ctx->h_ids.p, ctx->bk_failed.as<uint32_t>() + 1, nfail * 4,
                                    cudaMemcpyDeviceToHost, ctx->s));
             }
             CK(cudaStreamSynchronize(ctx->s));
+            off.assign(ctx->h_off.as<uint64_t>(), ctx->h_off.as<uint64_t>() + NB + 1);
+            if (nfail) ids.assign(ctx->h_ids.as<uint32_t>(), ctx->h_ids.as<uint32_t>() + nfail);
         }
         if (ctx->opt.hash_l2_only)  // every non-empty sub-bucket (one per partition)
             for (uint64_t b = bbase(p0); b < bbase(p1); b++)
@@ -1347,9 +1357,10 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
             } else {
                 ctx->fallback_buckets += ids.size();
                 ctx->times[5] += (double)ids.size();
-                std::vector<uint64_t> km(NB);
-                CK(cudaMemcpyAsync(km.data(), ctx->bk_kmers.p, NB * 8, cudaMemcpyDeviceToHost, ctx->s));
+                CK(ctx->h_km.ensure(NB * 8));
+                CK(cudaMemcpyAsync(ctx->h_km.p, ctx->bk_kmers.p, NB * 8, cudaMemcpyDeviceToHost, ctx->s));
                 CK(cudaStreamSynchronize(ctx->s));
+                std::vector<uint64_t> km(ctx->h_km.as<uint64_t>(), ctx->h_km.as<uint64_t>() + NB);
                 RET(count_buckets_records(ctx, ids, off, km, cmin, cmax));
             }
         }
