@@ -141,13 +141,20 @@ constexpr int BS_SLOTS = 4096;     // shared-memory sub-bucket counters per spli
 constexpr int BS_LOG_LIMIT = 14;   // at most 16384 sub-buckets per partition
 constexpr size_t BS_SMEM = (size_t)BS_SLOTS * 12;  // dynamic shared memory
 
-struct BSplitParams {
+// One store chunk's part of a split launch.
+struct BSChunk {
     const uint64_t *idx;                       // chunk superkmer index (partition-ordered)
     const uint32_t *keys;                      // chunk superkmer minimizer keys
     const uint8_t *bytes;                      // chunk bytes
     uint64_t i_begin, n_skm;                   // superkmer index range [i_begin, n_skm)
     const unsigned long long *part_skm_off;    // [P+1]
     const unsigned long long *part_byte_off;   // [P]
+    uint32_t cta0;                             // the chunk's first CTA in the launch
+};
+
+struct BSplitParams {
+    const BSChunk *chunks;                     // ascending cta0; one launch covers them all
+    uint32_t nchunks;
     uint32_t P;
     const uint32_t *part_slog;                 // [P] s_p: partition p has 2^s_p sub-buckets
     const uint32_t *part_bbase;                // [P] index of partition p's first sub-bucket
@@ -168,7 +175,9 @@ __device__ __forceinline__ uint32_t part_of_index(const unsigned long long *off,
 }
 
 // Pass 0 counts superkmers and k-mers per sub-bucket; pass 1 scatters
-// entries.  A CTA covers BS_PER_CTA consecutive superkmers, which span few
+// entries.  One launch covers every chunk of a group (chunk of a CTA: the last
+// with cta0 <= blockIdx.x).  A CTA covers BS_PER_CTA consecutive superkmers of
+// its chunk, which span few
 // partitions: its first BS_MAX_PARTS partitions get consecutive ranges of
 // BS_SLOTS shared-memory counters, 2^s_p each, while they fit, so their
 // sub-buckets cost one global atomic per CTA; any other superkmer goes
@@ -180,11 +189,17 @@ bucket_split_kernel(BSplitParams a) {
     uint32_t *cnt = reinterpret_cast<uint32_t *>(bs_smem + BS_SLOTS);  // superkmers
     __shared__ uint32_t soff[BS_MAX_PARTS + 1];  // shared range of partition pf + q: [soff[q], soff[q + 1])
     __shared__ uint32_t p_first_s, nq_s;
-    const uint64_t i0 = a.i_begin + blockIdx.x * (uint64_t)BS_PER_CTA;
-    if (i0 >= a.n_skm) return;
-    const uint64_t i1 = min(a.n_skm, i0 + BS_PER_CTA);
+    uint32_t lo = 0, hi = a.nchunks;  // chunks[lo].cta0 <= blockIdx.x < chunks[hi].cta0
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a.chunks[mid].cta0 <= blockIdx.x) lo = mid; else hi = mid;
+    }
+    const BSChunk ch = a.chunks[lo];
+    const uint64_t i0 = ch.i_begin + (blockIdx.x - ch.cta0) * (uint64_t)BS_PER_CTA;
+    if (i0 >= ch.n_skm) return;
+    const uint64_t i1 = min(ch.n_skm, i0 + BS_PER_CTA);
     if (threadIdx.x == 0) {
-        const uint32_t pf = part_of_index(a.part_skm_off, a.P, i0);
+        const uint32_t pf = part_of_index(ch.part_skm_off, a.P, i0);
         uint32_t q = 0, o = 0;
         soff[0] = 0;
         while (q < BS_MAX_PARTS && pf + q < a.P && o + (1u << a.part_slog[pf + q]) <= BS_SLOTS) {
@@ -198,7 +213,7 @@ bucket_split_kernel(BSplitParams a) {
     __syncthreads();
     const uint32_t pf = p_first_s, nq = nq_s;
     auto part = [&](uint64_t i) {
-        return (i < a.part_skm_off[pf + 1]) ? pf : part_of_index(a.part_skm_off, a.P, i);
+        return (i < ch.part_skm_off[pf + 1]) ? pf : part_of_index(ch.part_skm_off, a.P, i);
     };
     // global sub-bucket of shared counter t (t < soff[nq])
     auto global_of = [&](uint32_t t) {
@@ -208,15 +223,15 @@ bucket_split_kernel(BSplitParams a) {
     };
     for (uint64_t i = i0 + threadIdx.x; i < i1; i += BS_THREADS) {
         const uint32_t p = part(i);
-        const uint32_t b = bucket_of(a.keys[i], (int)__ldg(a.part_slog + p));
+        const uint32_t b = bucket_of(ch.keys[i], (int)__ldg(a.part_slog + p));
         if (p - pf < nq) {
             const uint32_t t = soff[p - pf] + b;
             atomicAdd(&cnt[t], 1u);
-            if (a.pass == 0) atomicAdd(&base[t], (unsigned long long)idx_len(a.idx[i]));
+            if (a.pass == 0) atomicAdd(&base[t], (unsigned long long)idx_len(ch.idx[i]));
         } else if (a.pass == 0) {
             const uint32_t g = __ldg(a.part_bbase + p) + b;
             atomicAdd(a.bucket_skms + g, 1u);
-            atomicAdd(a.bucket_kmers + g, (unsigned long long)idx_len(a.idx[i]));
+            atomicAdd(a.bucket_kmers + g, (unsigned long long)idx_len(ch.idx[i]));
         }
     }
     __syncthreads();
@@ -238,7 +253,7 @@ bucket_split_kernel(BSplitParams a) {
     __syncthreads();
     for (uint64_t i = i0 + threadIdx.x; i < i1; i += BS_THREADS) {
         const uint32_t p = part(i);
-        const uint32_t b = bucket_of(a.keys[i], (int)__ldg(a.part_slog + p));
+        const uint32_t b = bucket_of(ch.keys[i], (int)__ldg(a.part_slog + p));
         uint64_t slot;
         if (p - pf < nq) {
             const uint32_t t = soff[p - pf] + b;
@@ -246,9 +261,9 @@ bucket_split_kernel(BSplitParams a) {
         } else {
             slot = atomicAdd(a.bucket_cursor + __ldg(a.part_bbase + p) + b, 1ull);
         }
-        const uint64_t e = a.idx[i];
+        const uint64_t e = ch.idx[i];
         BEntry en;
-        en.ptr = a.bytes + a.part_byte_off[p] + idx_off(e);
+        en.ptr = ch.bytes + ch.part_byte_off[p] + idx_off(e);
         en.len = idx_len(e);
         en.pad = 0;
         a.entries[slot] = en;

@@ -321,12 +321,13 @@ struct gkc_ctx {
     DevBuf stage_bytes, stage_idx;
     DevBuf spill_bytes[2], spill_idx[2], spill_keys[2];  // device staging of chunks being spilled
     // shared-memory bucket counter
-    DevBuf bk_skms, bk_kmers, bk_off, bk_cur, bk_entries, bk_failed, bk_arena, bk_part;
+    DevBuf bk_skms, bk_kmers, bk_off, bk_cur, bk_entries, bk_failed, bk_arena, bk_part, bk_desc;
     DevBuf r_work, r_count, r_off, r_cur, r_recs, r_failed;  // record sub-buckets
     DevBuf r_stage, r_winst, r_woff, r_wrec;                  // per-work-item record segments
     uint64_t fallback_buckets = 0;  // sub-buckets counted through the L2 table
     PinBuf h_scal;
     PinBuf h_off, h_km, h_ids, h_work;  // pinned staging of the record path's host round trips
+    PinBuf h_desc;                      // split descriptors of a group
 
     std::vector<StoreChunk *> pool;  // cleared chunks kept for reuse
     HostArena arena;                 // pinned host memory of spilled chunks
@@ -355,13 +356,14 @@ struct gkc_ctx {
                         &counts, &offsets, &blocksums, &heads_pos, &heads_key, &tilecnt, &tileoff, &segoff,
                         &segcur, &part_err, &scal, &stage_bytes, &stage_idx, &spill_bytes[0], &spill_idx[0], &spill_keys[0],
                         &spill_bytes[1], &spill_idx[1], &spill_keys[1],
-                        &bk_skms, &bk_kmers, &bk_off, &bk_cur, &bk_entries, &bk_failed, &bk_arena, &bk_part,
+                        &bk_skms, &bk_kmers, &bk_off, &bk_cur, &bk_entries, &bk_failed, &bk_arena, &bk_part, &bk_desc,
                         &r_work, &r_count, &r_off, &r_cur, &r_recs, &r_failed, &r_stage, &r_winst,
                         &r_woff, &r_wrec, &ord_loads, &ord_stage, &ord_list, &mlp_p, &mlp_m, &mlp_v, &mlp_g, &mlp_t,
                         &mlp_w, &mlp_s, &mlp_scalar, &fx_text, &fx_tiles, &fx_state, &fx_kept,
                         &fx_reads, &fx_res, &fx_out, &fx_offs};
         for (auto *d : ds) d->release();
-        PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work};
+        PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work,
+                        &h_desc};
         for (auto *p : ps) p->release();
         arena.release();
         cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_ready[0], buf_ready[1], spill_ready,
@@ -594,7 +596,7 @@ int launch_scatter(gkc_ctx *ctx, const P1Plan &pl, StoreChunk *c, uint64_t total
     const uint32_t P = (uint32_t)ctx->opt.partitions;
     {
         KScope ks(ctx, GKC_K_SCAN, 24.0 * P * pl.grid);
-        cta_offsets_kernel<<<(P + 127) / 128, 128, 0, ctx->s>>>(
+        cta_offsets_kernel<<<P, CO_THREADS, 0, ctx->s>>>(
             ctx->cta_hist.as<uint32_t>(), pl.grid, P, c->d_byte_off.as<unsigned long long>(),
             c->d_skm_off.as<unsigned long long>(), ctx->cta_base.as<unsigned long long>(), flags);
         LAUNCHED();
@@ -1266,37 +1268,45 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         for (size_t j = 0; j < ctx->store.size(); j++)
             RET(chunk_range(ctx, ctx->store[j], p0, p1, ctx->bk_arena, &arena_used, &cb[j], &ci[j], &ck[j]));
         CK(cudaEventRecord(ctx->e2, ctx->s));
+        // the split of every chunk's part of the group, one launch per pass
+        std::vector<BSChunk> bsc;
+        uint32_t ncta = 0;
+        for (size_t j = 0; j < ctx->store.size(); j++) {
+            StoreChunk *c = ctx->store[j];
+            const uint64_t i0 = c->skm_off[p0], i1 = c->skm_off[p1];
+            if (i1 == i0) continue;
+            bsc.push_back({ci[j], ck[j], cb[j], i0, i1, c->d_skm_off.as<unsigned long long>(),
+                           c->d_byte_off.as<unsigned long long>(), ncta});
+            ncta += (uint32_t)((i1 - i0 + BS_PER_CTA - 1) / BS_PER_CTA);
+        }
+        if (!bsc.empty()) {
+            CK(ctx->h_desc.ensure(bsc.size() * sizeof(BSChunk)));
+            CK(ctx->bk_desc.ensure(bsc.size() * sizeof(BSChunk)));
+            std::memcpy(ctx->h_desc.p, bsc.data(), bsc.size() * sizeof(BSChunk));
+            CK(cudaMemcpyAsync(ctx->bk_desc.p, ctx->h_desc.p, bsc.size() * sizeof(BSChunk), cudaMemcpyHostToDevice,
+                               ctx->s));
+        }
         for (int pass = 0; pass < 2; pass++) {
             if (pass == 1) {
                 RET(scan_u32(ctx, ctx->bk_skms.as<uint32_t>(), NB, ctx->bk_off.as<uint64_t>(),
                              ctx->bk_off.as<unsigned long long>() + NB));
                 CK(cudaMemcpyAsync(ctx->bk_cur.p, ctx->bk_off.p, NB * 8, cudaMemcpyDeviceToDevice, ctx->s));
             }
-            for (size_t j = 0; j < ctx->store.size(); j++) {
-                StoreChunk *c = ctx->store[j];
-                const uint64_t i0 = c->skm_off[p0], i1 = c->skm_off[p1];
-                if (i1 == i0) continue;
-                BSplitParams sp;
-                sp.idx = ci[j];
-                sp.keys = ck[j];
-                sp.bytes = cb[j];
-                sp.i_begin = i0;
-                sp.n_skm = i1;
-                sp.part_skm_off = c->d_skm_off.as<unsigned long long>();
-                sp.part_byte_off = c->d_byte_off.as<unsigned long long>();
-                sp.P = P;
-                sp.part_slog = ctx->bk_part.as<uint32_t>();
-                sp.part_bbase = ctx->bk_part.as<uint32_t>() + P;
-                sp.bucket_skms = ctx->bk_skms.as<uint32_t>();
-                sp.bucket_kmers = ctx->bk_kmers.as<unsigned long long>();
-                sp.bucket_cursor = ctx->bk_cur.as<unsigned long long>();
-                sp.entries = ctx->bk_entries.as<BEntry>();
-                sp.pass = pass;
-                uint32_t g = (uint32_t)((i1 - i0 + BS_PER_CTA - 1) / BS_PER_CTA);
-                KScope ks(ctx, GKC_K_SCAN, pass ? 28.0 * (i1 - i0) : 12.0 * (i1 - i0));
-                bucket_split_kernel<<<g, BS_THREADS, BS_SMEM, ctx->s>>>(sp);
-                LAUNCHED();
-            }
+            if (!ncta) continue;
+            BSplitParams sp;
+            sp.chunks = ctx->bk_desc.as<BSChunk>();
+            sp.nchunks = (uint32_t)bsc.size();
+            sp.P = P;
+            sp.part_slog = ctx->bk_part.as<uint32_t>();
+            sp.part_bbase = ctx->bk_part.as<uint32_t>() + P;
+            sp.bucket_skms = ctx->bk_skms.as<uint32_t>();
+            sp.bucket_kmers = ctx->bk_kmers.as<unsigned long long>();
+            sp.bucket_cursor = ctx->bk_cur.as<unsigned long long>();
+            sp.entries = ctx->bk_entries.as<BEntry>();
+            sp.pass = pass;
+            KScope ks(ctx, GKC_K_SCAN, pass ? 28.0 * gs : 12.0 * gs);
+            bucket_split_kernel<<<ncta, BS_THREADS, BS_SMEM, ctx->s>>>(sp);
+            LAUNCHED();
         }
         CK(cudaMemsetAsync(ctx->bk_failed.p, 0, 4, ctx->s));
         BCountParams bp;

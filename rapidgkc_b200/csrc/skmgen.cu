@@ -395,21 +395,33 @@ find_superkmers_kernel(P1Params a) {
 }
 
 // Per-CTA base offsets in every partition: CTA c's range of partition p
-// starts after the bytes (superkmers) of CTAs 0..c-1 in p.  One thread per
-// partition walks the CTAs in order, so the layout is deterministic.
-__global__ void cta_offsets_kernel(const uint32_t *cta_hist, uint32_t ncta, uint32_t P,
-                                   const unsigned long long *part_byte_off, const unsigned long long *part_skm_off,
-                                   unsigned long long *cta_base, const uint32_t *flags) {
-    if (*flags & (ERR_RECORD_OVERFLOW | ERR_CAPACITY)) return;  // the batch is redone
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
-        unsigned long long b = part_byte_off[p], s = part_skm_off[p];
-        for (uint32_t c = 0; c < ncta; c++) {
-            const uint64_t o = (uint64_t)c * 2 * P;
-            cta_base[o + p] = b;
-            cta_base[o + P + p] = s;
-            b += cta_hist[o + p];
-            s += cta_hist[o + P + p];
-        }
+// starts after the bytes (superkmers) of CTAs 0..c-1 in p.  One CTA per
+// partition: each thread sums a contiguous run of CTAs, a block scan orders
+// the runs, and the thread writes its run's bases (CTA order: deterministic).
+constexpr int CO_THREADS = 256;
+__global__ void __launch_bounds__(CO_THREADS) cta_offsets_kernel(const uint32_t *cta_hist, uint32_t ncta, uint32_t P,
+                                                                  const unsigned long long *part_byte_off,
+                                                                  const unsigned long long *part_skm_off,
+                                                                  unsigned long long *cta_base, const uint32_t *flags) {
+    __shared__ unsigned long long ws[CO_THREADS / 32];
+    if (*flags & (ERR_RECORD_OVERFLOW | ERR_CAPACITY)) return;  // the batch is redone (uniform over the grid)
+    const uint32_t p = blockIdx.x;
+    const uint32_t per = (ncta + CO_THREADS - 1) / CO_THREADS;
+    const uint32_t c0 = threadIdx.x * per, c1 = c0 + per < ncta ? c0 + per : ncta;
+    unsigned long long b = 0, s = 0, tb, ts;
+    for (uint32_t c = c0; c < c1; c++) {
+        const uint64_t o = (uint64_t)c * 2 * P;
+        b += cta_hist[o + p];
+        s += cta_hist[o + P + p];
+    }
+    b = part_byte_off[p] + block_exclusive_scan<CO_THREADS>(b, &tb, ws);
+    s = part_skm_off[p] + block_exclusive_scan<CO_THREADS>(s, &ts, ws);
+    for (uint32_t c = c0; c < c1; c++) {
+        const uint64_t o = (uint64_t)c * 2 * P;
+        cta_base[o + p] = b;
+        cta_base[o + P + p] = s;
+        b += cta_hist[o + p];
+        s += cta_hist[o + P + p];
     }
 }
 
