@@ -59,8 +59,9 @@ WORKLOAD_DESC = {
 
 # DRAM bytes per read base of the main kernels, read+write, from one ncu
 # capture of a 300 Mbp case (profiles/phase1_and_counter_bacterial_small.md,
-# learned order); the roofline's `traffic` scales them to a full launch.
-TRAFFIC_PER_BASE = {"find_superkmers": 2.625, "scatter_superkmers": 7.84, "hash_insert": 2.95}
+# learned order, 256 MiB batches); the roofline's `traffic` scales them to the
+# bases of one launch.
+TRAFFIC_PER_BASE = {"find_superkmers": 2.62, "scatter_superkmers": 7.87}  # one launch per batch each
 
 
 def peaks():
@@ -442,9 +443,9 @@ def main():
     tpb = TRAFFIC_PER_BASE.get(dom) if args.workload == "bacterial_100m" and args.order == "learned" else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": src,
-                "traffic": tpb * bases if tpb else None,
-                "traffic_source": "ncu dram__bytes_read+write per base at 300 Mbp, scaled to the launch's bases"
-                if tpb else None,
+                "traffic": tpb * bases / max(1, kl // args.steps) if tpb else None,
+                "traffic_source": "ncu dram__bytes_read+write per base (a 268 Mbp batch of a 300 Mbp case), "
+                                  "scaled to the launch's bases" if tpb else None,
                 "bytes_per_launch": kb / max(kl, 1), "launch_ms": per_launch_s * 1e3, "classes": classes}
 
     line = {"metric": METRIC, "value": value, "unit": "Gbp/s", "n_gpus": world, "steps": args.steps,

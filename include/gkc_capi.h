@@ -239,7 +239,9 @@ enum {
  * launching stream; gkc_kernel_stats then returns, per class, the summed
  * device milliseconds, the number of launches and the algorithmic DRAM bytes
  * (compulsory reads + writes of the class's inputs and outputs) since the
- * last reset.  Arrays of n <= GKC_K_CLASSES entries; any may be NULL. */
+ * last reset.  Phase 1 keeps its batches; each batch's kernels are launched
+ * directly instead of as one CUDA graph, since timing events do not time
+ * inside a graph.  Arrays of n <= GKC_K_CLASSES entries; any may be NULL. */
 int gkc_set_profiling(gkc_ctx *ctx, int on);
 int gkc_kernel_stats(gkc_ctx *ctx, double *ms, uint64_t *launches, double *bytes, int n, int reset);
 

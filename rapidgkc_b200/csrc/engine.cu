@@ -217,6 +217,8 @@ struct StoreChunk {
     PinBuf h_meta;                            // byte_off [P+1], skm_off [P+1], kmers [P], flags
     bool pending = false;
     uint64_t batch = 0;                       // the batch of this chunk in the last gkc_add_reads
+    uint64_t bases = 0;                       // read bases of the batch
+    int64_t pend_find = -1, pend_scatter = -1;  // profiled launches whose bytes wait for the layout
     void release() {
         d_kmers.release();
         d_flags.release();
@@ -677,8 +679,8 @@ int spill_chunk(gkc_ctx *ctx, StoreChunk *c) {
 // Phase 1 of one device-resident batch (offs[0] == 0), synchronously: the
 // partition totals are read back after find_superkmers and the chunk is
 // allocated to the exact size.  Used for spilled stores (the chunk is then
-// copied to pinned host memory), for profiled runs, and to redo a batch that
-// overflowed phase1_async's capacities.
+// copied to pinned host memory) and to redo a batch that overflowed
+// phase1_async's capacities.
 int phase1_exact(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, uint64_t n_reads,
                  uint64_t total) {
     const uint32_t P = (uint32_t)ctx->opt.partitions;
@@ -798,7 +800,8 @@ int phase1_async(gkc_ctx *ctx, const uint8_t *d_reads, uint64_t *d_offs, uint64_
     uint32_t *flags = c->d_flags.as<uint32_t>();
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    CK(cudaStreamBeginCapture(ctx->s, cudaStreamCaptureModeThreadLocal));
+    c->bases = total;
+    c->pend_find = c->pend_scatter = -1;
     auto work = [&]() -> int {
         if (rebase) {
             const uint32_t g = (uint32_t)std::min<uint64_t>((n_reads + 256) / 256, (uint64_t)ctx->sms * 8);
@@ -806,27 +809,40 @@ int phase1_async(gkc_ctx *ctx, const uint8_t *d_reads, uint64_t *d_offs, uint64_
             LAUNCHED();
         }
         RET(launch_find(ctx, pl, d_reads, d_offs, n_reads, total, pl.cap, flags));
+        if (ctx->prof) c->pend_find = (int64_t)ctx->pend.size() - 1;
         part_offsets_kernel<<<1, PO_THREADS, 0, ctx->s>>>(
             ctx->hist.as<unsigned long long>(), P, byte_cap, skm_cap, c->d_byte_off.as<unsigned long long>(),
             c->d_skm_off.as<unsigned long long>(), c->d_kmers.as<unsigned long long>(), flags);
         LAUNCHED();
         RET(launch_scatter(ctx, pl, c, total, pl.cap, flags, 0.09 * (double)total, 1.2 * (double)total));
+        if (ctx->prof) c->pend_scatter = (int64_t)ctx->pend.size() - 1;
         return GKC_OK;
     };
-    const int rc = work();
-    const cudaError_t ec = cudaStreamEndCapture(ctx->s, &graph);  // also ends a capture that failed
-    if (rc != GKC_OK || ec != cudaSuccess) {
-        if (graph) cudaGraphDestroy(graph);
-        ctx->pool.push_back(c);
-        return rc != GKC_OK ? rc : ctx->fail(GKC_ECUDA, "phase-1 graph capture: %s", cudaGetErrorString(ec));
-    }
-    e = cudaGraphInstantiate(&exec, graph, 0);
-    if (e == cudaSuccess) e = cudaGraphLaunch(exec, ctx->s);
-    if (exec) cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-        ctx->pool.push_back(c);
-        return ctx->fail(GKC_ECUDA, "phase-1 graph launch: %s", cudaGetErrorString(e));
+    if (ctx->prof) {
+        // profiling brackets each launch with timing events, which do not time
+        // inside a graph: the same launches go straight to the stream
+        const int rc = work();
+        if (rc != GKC_OK) {
+            ctx->pool.push_back(c);
+            return rc;
+        }
+    } else {
+        CK(cudaStreamBeginCapture(ctx->s, cudaStreamCaptureModeThreadLocal));
+        const int rc = work();
+        const cudaError_t ec = cudaStreamEndCapture(ctx->s, &graph);  // also ends a capture that failed
+        if (rc != GKC_OK || ec != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            ctx->pool.push_back(c);
+            return rc != GKC_OK ? rc : ctx->fail(GKC_ECUDA, "phase-1 graph capture: %s", cudaGetErrorString(ec));
+        }
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(exec, ctx->s);
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            ctx->pool.push_back(c);
+            return ctx->fail(GKC_ECUDA, "phase-1 graph launch: %s", cudaGetErrorString(e));
+        }
     }
     auto *hm = c->h_meta.as<unsigned long long>();
     CK(cudaMemcpyAsync(hm, c->d_byte_off.p, (P + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
@@ -864,6 +880,13 @@ int phase1_finish(gkc_ctx *ctx, std::vector<uint64_t> *redo) {
         c->kmers.assign(hm + 2 * P + 2, hm + 3 * P + 2);
         c->nbytes = c->byte_off[P];
         c->nskm = c->skm_off[P];
+        // profiled launches: the byte models' superkmer terms, now known
+        // (records written by find; records, index, keys and bytes by scatter)
+        if (c->pend_find >= 0 && (size_t)c->pend_find < ctx->pend.size())
+            ctx->pend[c->pend_find].bytes += 16.0 * (double)c->nskm;
+        if (c->pend_scatter >= 0 && (size_t)c->pend_scatter < ctx->pend.size())
+            ctx->pend[c->pend_scatter].bytes = 28.0 * (double)c->nskm + 0.25 * (double)c->bases + (double)c->nbytes;
+        c->pend_find = c->pend_scatter = -1;
         keep.push_back(c);
     }
     ctx->store.swap(keep);
@@ -1755,9 +1778,9 @@ struct ReadBatch {
 
 // Phase 1 over host batches: the copy of batch i+1 (copy stream, two device
 // slots) overlaps phase 1 of batch i; no batch waits for the host (phase1_async)
-// unless the store spills or kernels are profiled (phase1_exact).
+// unless the store spills (phase1_exact).
 int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, const std::vector<ReadBatch> &batches) {
-    const bool exact = ctx->opt.spill_host || ctx->prof;
+    const bool exact = ctx->opt.spill_host;
     const size_t nbat = batches.size();
     uint64_t max_b = 0, max_r = 0;
     for (const auto &b : batches) {
@@ -1979,7 +2002,7 @@ int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_
         if (first != 0) return ctx->fail(GKC_EINVAL, "device input needs offs[0] == 0");
         CK(cudaEventRecord(ctx->e2, ctx->s));
         const uint8_t *dr = reinterpret_cast<const uint8_t *>(reads);
-        if (ctx->opt.spill_host || ctx->prof) {
+        if (ctx->opt.spill_host) {
             RET(phase1_exact(ctx, dr, offs, n_reads, total));
         } else if (total > ctx->opt.batch_bases) {
             RET(add_device_batches(ctx, dr, offs, n_reads, total));
