@@ -160,6 +160,19 @@ int gkc_store_pack(gkc_ctx *ctx, int p0, int p1, uint8_t *bytes, uint64_t cap_by
 int gkc_store_append(gkc_ctx *ctx, int p0, int p1, const uint8_t *bytes, const uint64_t *idx,
                      const uint32_t *keys, const uint64_t *counts);
 
+/* Appends superkmers given as the reference's .skm bytes (skmstore.hpp:
+ * 129-141: a partition's superkmers in skm_3x format, concatenated; the bytes
+ * gkc_store_export gives): partition p's bytes are bytes[part_off[p] ..
+ * part_off[p+1]) (part_off: P+1 entries in host memory; bytes in host or
+ * device memory, mem).  The superkmer bounds are found on the GPU, and each
+ * superkmer's minimizer is recomputed under the context's order from its
+ * first k-mer.  GKC_EINVAL, and nothing appended, if a partition ends inside a
+ * superkmer, a superkmer holds fewer than k bases, or a minimizer maps to
+ * another partition than the one its bytes came in (bytes written with
+ * another order, p or partition count).  Lets this counter count a store the
+ * reference wrote (its phase 1, .skm files), and the reference count ours. */
+int gkc_add_skm(gkc_ctx *ctx, const uint8_t *bytes, const uint64_t *part_off, int mem);
+
 /* Pins host memory for spilled chunks (opt.spill_host) until the context's
  * host arena holds `bytes` in all, used or free; *pinned (may be NULL) = bytes
  * pinned.  A stream of known size reserves ahead; this is the one call that

@@ -30,7 +30,7 @@ UINT32_MAX = 0xFFFFFFFF
 EXPORTS = (
     "gkc_default_options", "gkc_create", "gkc_destroy", "gkc_last_error", "gkc_strerror",
     "gkc_set_order", "gkc_add_reads", "gkc_add_reads_batches", "gkc_batch_timings", "gkc_store_stats", "gkc_store_export", "gkc_store_clear",
-    "gkc_reserve_host", "gkc_store_pack", "gkc_store_append", "gkc_add_fastx", "gkc_parse_fastx",
+    "gkc_reserve_host", "gkc_store_pack", "gkc_store_append", "gkc_add_fastx", "gkc_parse_fastx", "gkc_add_skm",
     "gkc_count", "gkc_count_partitions", "gkc_result", "gkc_result_device", "gkc_count_reads", "gkc_count_keys",
     "gkc_last_timings", "gkc_kernel_launches", "gkc_set_stream", "gkc_set_profiling", "gkc_kernel_stats",
     "gkc_mlp_param_count", "gkc_minimizer_loads", "gkc_mlp_grad", "gkc_mlp_train", "gkc_mlp_scores",
@@ -91,6 +91,7 @@ def load_library(path: str = LIB_PATH):
     L.gkc_reserve_host.argtypes = [vp, u64, C.POINTER(u64)]
     L.gkc_store_pack.argtypes = [vp, i32, i32, vp, u64, vp, vp, u64, vp]
     L.gkc_store_append.argtypes = [vp, i32, i32, vp, vp, vp, vp]
+    L.gkc_add_skm.argtypes = [vp, vp, vp, i32]
     L.gkc_add_fastx.argtypes = [vp, vp, u64, i32, i32, C.POINTER(i32), C.POINTER(u64), C.POINTER(u64)]
     L.gkc_parse_fastx.argtypes = [vp, vp, u64, i32, i32, C.POINTER(i32), vp, u64, vp, u64, i32, C.POINTER(u64),
                                   C.POINTER(u64)]
@@ -231,6 +232,17 @@ class KmerCounter:
 
     def store_clear(self):
         self._check(self._L.gkc_store_clear(self._h))
+
+    def add_skm(self, data, part_off):
+        """Appends superkmers in the reference's .skm byte format: partition p
+        is data[part_off[p]:part_off[p+1]] (uint8 array or CUDA tensor)."""
+        po = np.ascontiguousarray(np.asarray(part_off, np.uint64))
+        if len(po) != self.partitions + 1:
+            raise ValueError(f"part_off needs {self.partitions + 1} entries")
+        if isinstance(data, (bytes, bytearray)):
+            data = np.frombuffer(bytes(data), np.uint8)
+        dp, dm = _ptr(data)
+        self._check(self._L.gkc_add_skm(self._h, dp, _ptr(po)[0], dm))
 
     def add_fastx(self, text, fmt: str = "fastq", state: int = 0):
         """Phase 1 from FASTQ / FASTA text (bytes, a uint8 array or a CUDA

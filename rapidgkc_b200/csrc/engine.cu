@@ -31,6 +31,7 @@
 #include "skmgen.cu"
 #include "store_pack.cu"
 #include "fastx.cu"
+#include "skm_load.cu"
 
 using namespace gkc;
 
@@ -302,6 +303,8 @@ struct gkc_ctx {
     DevBuf ord_loads, ord_stage, ord_list, mlp_p, mlp_m, mlp_v, mlp_g, mlp_t, mlp_w, mlp_s, mlp_scalar;
     // FASTQ / FASTA scanning: staged text, tile transforms and carries, the CSR
     DevBuf fx_text, fx_tiles, fx_state, fx_kept, fx_reads, fx_res, fx_out, fx_offs;
+    // .skm loading: tile transforms and carries, superkmer starts, k-mer counts
+    DevBuf sk_tiles, sk_state, sk_tstarts, sk_res, sk_starts, sk_k32;
     std::vector<StoreChunk *> store;
 
     // phase 2 buffers
@@ -362,7 +365,8 @@ struct gkc_ctx {
                         &r_work, &r_count, &r_off, &r_cur, &r_recs, &r_failed, &r_stage, &r_winst,
                         &r_woff, &r_wrec, &ord_loads, &ord_stage, &ord_list, &mlp_p, &mlp_m, &mlp_v, &mlp_g, &mlp_t,
                         &mlp_w, &mlp_s, &mlp_scalar, &fx_text, &fx_tiles, &fx_state, &fx_kept,
-                        &fx_reads, &fx_res, &fx_out, &fx_offs};
+                        &fx_reads, &fx_res, &fx_out, &fx_offs, &sk_tiles, &sk_state, &sk_tstarts, &sk_res,
+                        &sk_starts, &sk_k32};
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work,
                         &h_desc};
@@ -2097,6 +2101,125 @@ int gkc_parse_fastx(gkc_ctx *ctx, const char *text, uint64_t n, int mem, int for
     else if (out_mem == GKC_MEM_DEVICE) CK(cudaMemsetAsync(offs, 0, 8, ctx->s));
     else offs[0] = 0;
     CK(cudaStreamSynchronize(ctx->s));
+    return GKC_OK;
+}
+
+int gkc_add_skm(gkc_ctx *ctx, const uint8_t *bytes, const uint64_t *part_off, int mem) {
+    if (!ctx || !part_off) return GKC_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    for (char cn : ctx->counted)
+        if (cn) return ctx->fail(GKC_ESTATE, "the store is partly counted; clear it before appending");
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    if (part_off[0] != 0) return ctx->fail(GKC_EINVAL, "part_off[0] must be 0");
+    for (uint32_t p = 0; p < P; p++)
+        if (part_off[p + 1] < part_off[p]) return ctx->fail(GKC_EINVAL, "part_off is not ascending");
+    const uint64_t n = part_off[P];
+    if (n == 0) return GKC_OK;
+    if (!bytes) return GKC_EINVAL;
+    StoreChunk *c = ctx->take_chunk();
+    auto fail = [&](int rc) {
+        ctx->pool.push_back(c);
+        return rc;
+    };
+    cudaError_t e = c->dbytes.ensure(n + 32);
+    if (e == cudaSuccess) e = c->d_byte_off.ensure((P + 1) * 8);
+    if (e == cudaSuccess) e = c->d_skm_off.ensure((P + 1) * 8);
+    if (e == cudaSuccess) e = c->d_kmers.ensure(P * 8ull);
+    if (e == cudaSuccess) e = c->h_meta.ensure((3ull * P + 3) * 8);
+    if (e != cudaSuccess) return fail(ctx->fail(GKC_ENOMEM, "skm chunk allocation: %s", cudaGetErrorString(e)));
+    c->byte_off.assign(part_off, part_off + P + 1);
+    uint8_t *db = c->dbytes.as<uint8_t>();
+    if (cudaMemcpyAsync(db, bytes, n, mem == GKC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                        ctx->s) != cudaSuccess ||
+        cudaMemsetAsync(db + n, 0, 32, ctx->s) != cudaSuccess ||
+        cudaMemcpyAsync(c->d_byte_off.p, c->byte_off.data(), (P + 1) * 8, cudaMemcpyHostToDevice, ctx->s) !=
+            cudaSuccess)
+        return fail(ctx->fail(GKC_ECUDA, "skm staging copy failed"));
+    // superkmer bounds
+    const uint64_t ntiles = (n + gkc::SL_TILE - 1) / gkc::SL_TILE;
+    if (ctx->sk_tiles.ensure(ntiles * sizeof(gkc::SlT)) != cudaSuccess || ctx->sk_state.ensure(ntiles) != cudaSuccess ||
+        ctx->sk_tstarts.ensure(ntiles * 8) != cudaSuccess || ctx->sk_res.ensure(64) != cudaSuccess ||
+        ctx->h_scal.ensure(64) != cudaSuccess)
+        return fail(ctx->fail(GKC_ENOMEM, "skm scan buffers"));
+    gkc::SlParams a;
+    a.bytes = db;
+    a.n = n;
+    a.part_off = c->d_byte_off.as<unsigned long long>();
+    a.P = P;
+    a.tiles = ctx->sk_tiles.as<gkc::SlT>();
+    a.ntiles = ntiles;
+    a.tile_state = ctx->sk_state.as<uint8_t>();
+    a.tile_starts = ctx->sk_tstarts.as<uint64_t>();
+    a.result = ctx->sk_res.as<uint64_t>();
+    a.err = reinterpret_cast<uint32_t *>(ctx->sk_res.as<uint64_t>() + 1);
+    a.starts = nullptr;
+    CK(cudaMemsetAsync(ctx->sk_res.p, 0, 64, ctx->s));
+    gkc::skm_tile_kernel<<<(uint32_t)ntiles, gkc::SL_THREADS, 0, ctx->s>>>(a);
+    LAUNCHED();
+    gkc::skm_carry_kernel<<<1, gkc::SL_CARRY_THREADS, 0, ctx->s>>>(a);
+    LAUNCHED();
+    uint64_t *hr = ctx->h_scal.as<uint64_t>();
+    CK(cudaMemcpyAsync(hr, ctx->sk_res.p, 16, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    const uint64_t nskm = hr[0];
+    if (ctx->sk_starts.ensure(std::max<uint64_t>(nskm, 1) * 8) != cudaSuccess ||
+        ctx->sk_k32.ensure(std::max<uint64_t>(nskm, 1) * 4) != cudaSuccess ||
+        c->didx.ensure(std::max<uint64_t>(nskm, 1) * 8) != cudaSuccess ||
+        c->dkeys.ensure(std::max<uint64_t>(nskm, 1) * 4) != cudaSuccess)
+        return fail(ctx->fail(GKC_ENOMEM, "skm index allocation (%llu superkmers)", (unsigned long long)nskm));
+    a.starts = ctx->sk_starts.as<uint64_t>();
+    gkc::skm_starts_kernel<<<(uint32_t)ntiles, gkc::SL_THREADS, 0, ctx->s>>>(a);
+    LAUNCHED();
+    gkc::SiParams x;
+    x.bytes = db;
+    x.n = n;
+    x.part_off = a.part_off;
+    x.P = P;
+    x.pmod = gkc::fastmod_m(P);
+    x.k = ctx->opt.k;
+    x.p = ctx->opt.p;
+    x.lut = ctx->has_lut ? ctx->lut.as<uint32_t>() : nullptr;
+    x.starts = a.starts;
+    x.nskm = nskm;
+    x.idx = c->didx.as<uint64_t>();
+    x.keys = c->dkeys.as<uint32_t>();
+    x.part_kmers32 = ctx->sk_k32.as<uint32_t>();
+    x.err = a.err;
+    const uint32_t g = (uint32_t)std::min<uint64_t>((nskm + 255) / 256, (uint64_t)ctx->sms * 8);
+    if (nskm) {
+        if (x.lut) gkc::skm_index_kernel<true><<<g, 256, 0, ctx->s>>>(x);
+        else gkc::skm_index_kernel<false><<<g, 256, 0, ctx->s>>>(x);
+        LAUNCHED();
+    }
+    gkc::skm_part_totals_kernel<<<P, 256, 0, ctx->s>>>(a.part_off, P, a.starts, nskm, x.part_kmers32,
+                                                        c->d_skm_off.as<unsigned long long>(),
+                                                        c->d_kmers.as<unsigned long long>());
+    LAUNCHED();
+    auto *hm = c->h_meta.as<unsigned long long>();
+    CK(cudaMemcpyAsync(hm, c->d_skm_off.p, (P + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaMemcpyAsync(hm + P + 1, c->d_kmers.p, P * 8ull, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaMemcpyAsync(hr, ctx->sk_res.p, 16, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    const uint32_t err = (uint32_t)hr[1];
+    if (err & gkc::SKM_ERR_TRUNCATED) return fail(ctx->fail(GKC_EINVAL, "skm bytes: a partition ends inside a superkmer"));
+    if (err & gkc::SKM_ERR_SHORT) return fail(ctx->fail(GKC_EINVAL, "skm bytes: a superkmer holds fewer than k bases"));
+    if (err & gkc::SKM_ERR_PARTITION)
+        return fail(ctx->fail(GKC_EINVAL, "skm bytes: superkmers whose minimizer maps to another partition "
+                                          "(written with another minimizer order, partition count or p)"));
+    c->skm_off.assign(hm, hm + P + 1);
+    c->kmers.assign(hm + P + 1, hm + 2 * P + 1);
+    c->nbytes = n;
+    c->nskm = nskm;
+    c->bytes = db;
+    c->idx = c->didx.as<uint64_t>();
+    c->keys = c->dkeys.as<uint32_t>();
+    c->on_host = false;
+    c->pending = false;
+    if (ctx->opt.spill_host) {
+        const int rc = spill_chunk(ctx, c);
+        if (rc != GKC_OK) return fail(rc);
+    }
+    ctx->store.push_back(c);
     return GKC_OK;
 }
 
