@@ -57,6 +57,8 @@ typedef struct gkc_options {
     uint64_t group_keys;    /* max k-mer instances per sort group (0 = from free device memory)   */
     int hash_l2_only;       /* hash counter: 0 = shared-memory sub-buckets with the L2 table for  */
                             /* the ones that overflow; 1 = every partition through the L2 table   */
+    int hpc;                /* 1: homopolymer compression of every read before phase 1: a run of  */
+                            /* equal bytes counts as one base (reference -hpc, gpu_skmgen.cu:145) */
 } gkc_options;
 
 /* Fills defaults: k=31, p=11, partitions=512, hash counter. */

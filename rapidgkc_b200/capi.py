@@ -52,6 +52,7 @@ class Options(C.Structure):
         ("spill_host", C.c_int),
         ("group_keys", C.c_uint64),
         ("hash_l2_only", C.c_int),
+        ("hpc", C.c_int),
     ]
 
 
@@ -147,7 +148,7 @@ class KmerCounter:
     def __init__(self, k: int = 31, p: int = 11, partitions: int = 512, counter: str = "hash",
                  device: int = 0, radix_bits: int = 8, table_slots: float = 0.35,
                  batch_bases: int = 1 << 30, spill_host: bool = False, group_keys: int = 0,
-                 hash_l2_only: bool = False):
+                 hash_l2_only: bool = False, hpc: bool = False):
         L = load_library()
         o = Options()
         L.gkc_default_options(C.byref(o))
@@ -155,6 +156,7 @@ class KmerCounter:
         o.counter = {"hash": COUNTER_HASH, "sort": COUNTER_SORT}[counter]
         o.radix_bits, o.table_slots, o.batch_bases = radix_bits, table_slots, batch_bases
         o.spill_host, o.group_keys, o.hash_l2_only = int(spill_host), group_keys, int(hash_l2_only)
+        o.hpc = int(hpc)
         h = C.c_void_p()
         rc = L.gkc_create(device, C.byref(o), C.byref(h))
         if rc != GKC_OK:

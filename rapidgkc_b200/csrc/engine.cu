@@ -32,6 +32,7 @@
 #include "store_pack.cu"
 #include "fastx.cu"
 #include "skm_load.cu"
+#include "hpc.cu"
 
 using namespace gkc;
 
@@ -305,6 +306,7 @@ struct gkc_ctx {
     DevBuf fx_text, fx_tiles, fx_state, fx_kept, fx_reads, fx_res, fx_out, fx_offs;
     // .skm loading: tile transforms and carries, superkmer starts, k-mer counts
     DevBuf sk_tiles, sk_state, sk_tstarts, sk_res, sk_starts, sk_k32;
+    DevBuf hpc_tiles, hpc_tbase, hpc_reads, hpc_offs;  // homopolymer-compressed batch
     std::vector<StoreChunk *> store;
 
     // phase 2 buffers
@@ -366,7 +368,7 @@ struct gkc_ctx {
                         &r_woff, &r_wrec, &ord_loads, &ord_stage, &ord_list, &mlp_p, &mlp_m, &mlp_v, &mlp_g, &mlp_t,
                         &mlp_w, &mlp_s, &mlp_scalar, &fx_text, &fx_tiles, &fx_state, &fx_kept,
                         &fx_reads, &fx_res, &fx_out, &fx_offs, &sk_tiles, &sk_state, &sk_tstarts, &sk_res,
-                        &sk_starts, &sk_k32};
+                        &sk_starts, &sk_k32, &hpc_tiles, &hpc_tbase, &hpc_reads, &hpc_offs};
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work,
                         &h_desc};
@@ -1687,6 +1689,7 @@ void gkc_default_options(gkc_options *o) {
     o->spill_host = 0;
     o->group_keys = 0;
     o->hash_l2_only = 0;
+    o->hpc = 0;
 }
 
 const char *gkc_strerror(int code) {
@@ -1780,6 +1783,45 @@ struct ReadBatch {
     uint64_t r0, r1;  // reads [r0, r1) of the caller's CSR
 };
 
+// Homopolymer compression of a device batch (read r at offs[r] - base) into
+// ctx->hpc_reads / hpc_offs (offsets from 0); *kept = the compressed bases.
+int hpc_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, uint64_t n_reads, uint64_t base,
+              uint64_t total, uint64_t *kept) {
+    const uint64_t ntiles = std::max<uint64_t>((total + gkc::HPC_TILE - 1) / gkc::HPC_TILE, 1);
+    CK(ctx->hpc_tiles.ensure(ntiles * 4));
+    CK(ctx->hpc_tbase.ensure((ntiles + 1) * 8));
+    CK(ctx->hpc_reads.ensure(total + 64));
+    CK(ctx->hpc_offs.ensure((n_reads + 1) * 8));
+    gkc::HpcParams a;
+    a.reads = d_reads;
+    a.offs = d_offs;
+    a.n_reads = n_reads;
+    a.base = base;
+    a.n = total;
+    a.tile_kept = ctx->hpc_tiles.as<uint32_t>();
+    a.tile_base = ctx->hpc_tbase.as<uint64_t>();
+    a.out = ctx->hpc_reads.as<uint8_t>();
+    a.out_offs = ctx->hpc_offs.as<uint64_t>();
+    unsigned long long *dtot = ctx->hpc_tbase.as<unsigned long long>() + ntiles;
+    if (total) {
+        gkc::hpc_count_kernel<<<(uint32_t)ntiles, gkc::HPC_THREADS, 0, ctx->s>>>(a);
+        LAUNCHED();
+        RET(scan_u32(ctx, a.tile_kept, ntiles, ctx->hpc_tbase.as<uint64_t>(), dtot));
+        gkc::hpc_write_kernel<<<(uint32_t)ntiles, gkc::HPC_THREADS, 0, ctx->s>>>(a);
+        LAUNCHED();
+    } else {
+        CK(cudaMemsetAsync(dtot, 0, 8, ctx->s));
+    }
+    const uint32_t g = (uint32_t)std::min<uint64_t>((n_reads + 256) / 256, (uint64_t)ctx->sms * 8);
+    gkc::hpc_tail_offsets_kernel<<<g, 256, 0, ctx->s>>>(d_offs, n_reads, base, total, dtot, a.out_offs);
+    LAUNCHED();
+    CK(ctx->h_scal.ensure(64));
+    CK(cudaMemcpyAsync(ctx->h_scal.p, dtot, 8, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    *kept = *ctx->h_scal.as<uint64_t>();
+    return GKC_OK;
+}
+
 // Phase 1 over host batches: the copy of batch i+1 (copy stream, two device
 // slots) overlaps phase 1 of batch i; no batch waits for the host (phase1_async)
 // unless the store spills (phase1_exact).
@@ -1818,7 +1860,13 @@ int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, cons
         const uint64_t base = offs[b.r0], nb = offs[b.r1] - base, nr = b.r1 - b.r0;
         CK(cudaStreamWaitEvent(ctx->s, ctx->buf_ready[slot], 0));
         int rc;
-        if (sync_exact) {
+        if (ctx->opt.hpc) {  // phase 1 reads the compressed copy, offsets from 0
+            uint64_t kept = 0;
+            RET(hpc_batch(ctx, ctx->reads[slot].as<uint8_t>(), ctx->offs[slot].as<uint64_t>(), nr, base, nb, &kept));
+            const uint8_t *hr = ctx->hpc_reads.as<uint8_t>();
+            uint64_t *ho = ctx->hpc_offs.as<uint64_t>();
+            rc = sync_exact ? phase1_exact(ctx, hr, ho, nr, kept) : phase1_async(ctx, hr, ho, nr, kept, 0, bi);
+        } else if (sync_exact) {
             const uint32_t g = (uint32_t)std::min<uint64_t>((nr + 256) / 256, (uint64_t)ctx->sms * 8);
             rebase_offsets_kernel<<<g, 256, 0, ctx->s>>>(ctx->offs[slot].as<uint64_t>(), nr + 1, base);
             LAUNCHED();
@@ -2006,6 +2054,11 @@ int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_
         if (first != 0) return ctx->fail(GKC_EINVAL, "device input needs offs[0] == 0");
         CK(cudaEventRecord(ctx->e2, ctx->s));
         const uint8_t *dr = reinterpret_cast<const uint8_t *>(reads);
+        if (ctx->opt.hpc) {  // phase 1 reads the compressed copy
+            RET(hpc_batch(ctx, dr, offs, n_reads, 0, total, &total));
+            dr = ctx->hpc_reads.as<uint8_t>();
+            offs = ctx->hpc_offs.as<uint64_t>();
+        }
         if (ctx->opt.spill_host) {
             RET(phase1_exact(ctx, dr, offs, n_reads, total));
         } else if (total > ctx->opt.batch_bases) {

@@ -43,7 +43,7 @@ struct Args {
     int k = 31, p = 11, partitions = 512, device = 0;
     uint32_t cmin = 1, cmax = 0xFFFFFFFFu;
     std::string out, fmt = "bin", counter = "hash", order = "default";
-    bool sorted = false;
+    bool sorted = false, hpc = false;
     uint64_t batch_mb = 1024;
     std::vector<std::string> files;
 };
@@ -52,7 +52,8 @@ struct Args {
     std::fprintf(stderr,
                  "%s\nUsage: %s -k <K> -p <P> -skm <partitions> [-ci <min count>] [-cx <max count>]\n"
                  "       [-o <output>] [-of bin|txt] [-sorted] [-counter hash|sort]\n"
-                 "       [-order default|learned|<params.f32>] [-gpu <device>] [-bb <batch MB>] -read <files...>\n"
+                 "       [-order default|learned|<params.f32>] [-gpu <device>] [-bb <batch MB>] [-hpc 0|1]\n"
+                 "       -read <files...>\n"
                  "       (-t -tgpu -t2 -tgz -tsort -tmp -im -fb -rb -grid -block -grid2 -block2 -ns1 -ns2 -rps\n"
                  "        -gpuonly -log -lv are accepted for compatibility and have no effect)\n",
                  why, prog);
@@ -79,9 +80,8 @@ Args parse_args(int argc, char **argv) {
         else if (f == "-order") a.order = need(i);
         else if (f == "-gpu") a.device = std::atoi(need(i));
         else if (f == "-bb") a.batch_mb = std::strtoull(need(i), nullptr, 10);
-        else if (f == "-hpc") {
-            if (std::atoi(need(i)) != 0) usage(argv[0], "homopolymer compression (-hpc 1) is not supported");
-        } else if (f == "-ngpu") {
+        else if (f == "-hpc") a.hpc = std::atoi(need(i)) != 0;
+        else if (f == "-ngpu") {
             if (std::atoi(need(i)) > 1) usage(argv[0], "one GPU per process (-ngpu 1)");
         } else if (f == "-cpuonly") {
             usage(argv[0], "there is no CPU path (-cpuonly)");
@@ -323,6 +323,7 @@ int main(int argc, char **argv) {
     opt.p = a.p;
     opt.partitions = a.partitions;
     opt.counter = a.counter == "sort" ? GKC_COUNTER_SORT : GKC_COUNTER_HASH;
+    opt.hpc = a.hpc ? 1 : 0;
     gkc_ctx *ctx = nullptr;
     check(gkc_create(a.device, &opt, &ctx), nullptr, "create");
     if (a.order != "default") {
