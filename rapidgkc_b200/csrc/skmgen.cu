@@ -37,9 +37,12 @@ namespace gkc {
 
 constexpr int P1_WARPS = 8;
 constexpr int P1_THREADS = P1_WARPS * 32;
-constexpr int P1_CHUNKS = 16;                         // chunks of 32 positions per warp strip
-constexpr int P1_STRIP = 32 * P1_CHUNKS;              // 512 positions
-constexpr int P1_TILE = P1_WARPS * P1_STRIP;          // 4096 positions per tile
+// chunks of 32 positions per warp strip: a strip pays a warm-up chunk and,
+// usually, one chunk past its end for the superkmer still open there, so
+// longer strips waste less (32 chunks: phase 1 5% faster than 16)
+constexpr int P1_CHUNKS = 32;
+constexpr int P1_STRIP = 32 * P1_CHUNKS;              // 1024 positions
+constexpr int P1_TILE = P1_WARPS * P1_STRIP;          // 8192 positions per tile
 constexpr int P1_TILE_WORDS = P1_TILE / 16;           // packed code words per tile
 constexpr int P1_HALO = 512;                          // staged positions past the tile
 constexpr int P1_STAGE = P1_TILE + 32 + P1_HALO + 128;  // staged positions (from tile-32)
