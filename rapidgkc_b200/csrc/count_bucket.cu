@@ -134,7 +134,7 @@ __device__ __forceinline__ void warp_kmer_runs(const BEntry *ent, uint64_t b, ui
 
 // ---------------------------------------------------------------------------
 // split
-constexpr int BS_THREADS = 256;
+constexpr int BS_THREADS = 512;
 constexpr int BS_PER_CTA = 8192;   // superkmers per split CTA
 constexpr int BS_MAX_PARTS = 4;    // partitions a split CTA aggregates in shared memory
 constexpr int BS_SLOTS = 4096;     // shared-memory sub-bucket counters per split CTA
