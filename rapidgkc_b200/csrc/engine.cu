@@ -329,6 +329,7 @@ struct gkc_ctx {
     DevBuf spill_bytes[2], spill_idx[2], spill_keys[2];  // device staging of chunks being spilled
     // shared-memory bucket counter
     DevBuf bk_skms, bk_kmers, bk_off, bk_cur, bk_entries, bk_failed, bk_arena, bk_part, bk_desc;
+    DevBuf bk_arena2;  // second staging arena: a spilled store's next group is staged beside the current one
     DevBuf r_work, r_count, r_off, r_cur, r_recs, r_failed;  // record sub-buckets
     DevBuf r_stage, r_winst, r_woff, r_wrec;                  // per-work-item record segments
     uint64_t fallback_buckets = 0;  // sub-buckets counted through the L2 table
@@ -364,6 +365,7 @@ struct gkc_ctx {
                         &segcur, &part_err, &scal, &stage_bytes, &stage_idx, &spill_bytes[0], &spill_idx[0], &spill_keys[0],
                         &spill_bytes[1], &spill_idx[1], &spill_keys[1],
                         &bk_skms, &bk_kmers, &bk_off, &bk_cur, &bk_entries, &bk_failed, &bk_arena, &bk_part, &bk_desc,
+                        &bk_arena2,
                         &r_work, &r_count, &r_off, &r_cur, &r_recs, &r_failed, &r_stage, &r_winst,
                         &r_woff, &r_wrec, &ord_loads, &ord_stage, &ord_list, &mlp_p, &mlp_m, &mlp_v, &mlp_g, &mlp_t,
                         &mlp_w, &mlp_s, &mlp_scalar, &fx_text, &fx_tiles, &fx_state, &fx_kept,
@@ -903,7 +905,8 @@ int phase1_finish(gkc_ctx *ctx, std::vector<uint64_t> *redo) {
 // by the chunk's own partition offsets (spilled chunks are staged into `arena`
 // at *arena_used and the pointers rebased).
 int chunk_range(gkc_ctx *ctx, StoreChunk *c, uint32_t p0, uint32_t p1, DevBuf &arena, uint64_t *arena_used,
-                const uint8_t **bytes, const uint64_t **idx, const uint32_t **keys) {
+                const uint8_t **bytes, const uint64_t **idx, const uint32_t **keys, cudaStream_t st = nullptr) {
+    if (!st) st = ctx->s;
     if (!c->on_host) {
         *bytes = c->bytes;
         *idx = c->idx;
@@ -921,9 +924,9 @@ int chunk_range(gkc_ctx *ctx, StoreChunk *c, uint32_t p0, uint32_t p1, DevBuf &a
     uint8_t *pb = base;
     uint64_t *pi = reinterpret_cast<uint64_t *>(base + nbb);
     uint32_t *pk = reinterpret_cast<uint32_t *>(base + nbb + nib);
-    CK(cudaMemcpyAsync(pb, c->bytes + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->s));
-    CK(cudaMemcpyAsync(pi, c->idx + s0, (s1 - s0) * 8, cudaMemcpyHostToDevice, ctx->s));
-    CK(cudaMemcpyAsync(pk, c->keys + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemcpyAsync(pb, c->bytes + b0, b1 - b0, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(pi, c->idx + s0, (s1 - s0) * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(pk, c->keys + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, st));
     *arena_used += need;
     // the kernels index with the chunk's absolute offsets: rebase
     *bytes = pb - b0;
@@ -1248,7 +1251,8 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
                             BC_TS * 12));
     CK(cudaFuncSetAttribute(bucket_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BS_SMEM));
     // groups of partitions
-    uint64_t budget = spilled ? std::max<uint64_t>(1ull << 26, (uint64_t)(free0 * 0.3)) : ~0ull;
+    // a spilled store holds two staging arenas (this group's and the next's)
+    uint64_t budget = spilled ? std::max<uint64_t>(1ull << 26, (uint64_t)(free0 * 0.1)) : ~0ull;
     // streamed output: about four groups, so that each group's output is
     // copied to the host while the next one counts
     const bool stream_out = ctx->stream_k && ctx->stream_c;
@@ -1258,24 +1262,78 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         budget = std::min<uint64_t>(budget, std::max<uint64_t>(tot / 4 + 1, 1ull << 20));
     }
     float acc_ms = 0;
-    uint32_t p0 = 0;
-    while (p0 < P) {
-        if (want && !(*want)[p0]) {
-            p0++;
+    // the groups of partitions, formed up front
+    struct Grp {
+        uint32_t p0, p1;
+        uint64_t gb, gs;  // staged bytes, superkmers
+    };
+    std::vector<Grp> grps;
+    for (uint32_t q0 = 0; q0 < P;) {
+        if (want && !(*want)[q0]) {
+            q0++;
             continue;
         }
-        uint32_t p1 = p0;
-        uint64_t gb = 0, gs = 0;  // staged bytes, superkmers of the group
-        while (p1 < P && (!want || (*want)[p1]) &&
-               (p1 == p0 || gb + nbp[p1] + 12 * nsp[p1] + 16 * nsp[p1] <= budget)) {
-            gb += nbp[p1] + 12 * nsp[p1];
-            gs += nsp[p1];
-            p1++;
+        uint32_t q1 = q0;
+        uint64_t gb = 0, gs = 0;
+        while (q1 < P && (!want || (*want)[q1]) &&
+               (q1 == q0 || gb + nbp[q1] + 12 * nsp[q1] + 16 * nsp[q1] <= budget)) {
+            gb += nbp[q1] + 12 * nsp[q1];
+            gs += nsp[q1];
+            q1++;
         }
-        if (!gs) {
-            p0 = p1;
-            continue;
+        if (gs) grps.push_back({q0, q1, gb, gs});
+        q0 = q1;
+    }
+    // Spilled store: group g's chunk ranges are staged into arena g % 2 on the
+    // copy stream, and group g + 1's are staged while group g counts.  The
+    // counting waits for its staging; the staging into an arena waits for the
+    // end of the group that used it before.
+    const size_t nst = ctx->store.size();
+    DevBuf *arena[2] = {&ctx->bk_arena, &ctx->bk_arena2};
+    std::vector<const uint8_t *> cbs[2];
+    std::vector<const uint64_t *> cis[2];
+    std::vector<const uint32_t *> cks[2];
+    cudaEvent_t staged[2] = {nullptr, nullptr}, freed[2] = {nullptr, nullptr}, st0[2] = {nullptr, nullptr};
+    long staged_g[2] = {-1, -1};
+    struct EvBack {  // the events go back to the pool on every exit
+        gkc_ctx *c;
+        cudaEvent_t *e[3];
+        ~EvBack() {
+            for (auto *a : e)
+                for (int i = 0; i < 2; i++)
+                    if (a[i]) c->evpool.push_back(a[i]);
         }
+    } evback{ctx, {staged, freed, st0}};
+    if (spilled) {
+        uint64_t mx = 0;
+        for (const auto &g : grps) mx = std::max<uint64_t>(mx, g.gb);
+        for (int i = 0; i < 2; i++) {
+            // each chunk's range adds at most 32 + 3 x 15 bytes of padding
+            CK(arena[i]->ensure(mx + 96 * nst + 64));
+            cbs[i].resize(nst);
+            cis[i].resize(nst);
+            cks[i].resize(nst);
+            staged[i] = ctx->take_event();
+            freed[i] = ctx->take_event();
+            st0[i] = ctx->take_event();
+            CK(cudaEventRecord(freed[i], ctx->s));
+        }
+    }
+    auto stage = [&](size_t gi) -> int {
+        const int sl = (int)(gi & 1);
+        uint64_t used = 0;
+        CK(cudaStreamWaitEvent(ctx->cs, freed[sl], 0));
+        CK(cudaEventRecord(st0[sl], ctx->cs));
+        for (size_t j = 0; j < nst; j++)
+            RET(chunk_range(ctx, ctx->store[j], grps[gi].p0, grps[gi].p1, *arena[sl], &used, &cbs[sl][j],
+                            &cis[sl][j], &cks[sl][j], ctx->cs));
+        CK(cudaEventRecord(staged[sl], ctx->cs));
+        staged_g[sl] = (long)gi;
+        return GKC_OK;
+    };
+    for (size_t gi = 0; gi < grps.size();) {
+        const uint32_t p0 = grps[gi].p0, p1 = grps[gi].p1;
+        const uint64_t gs = grps[gi].gs;
         uint64_t gN = 0;
         for (uint32_t p = p0; p < p1; p++) gN += np[p];
         uint64_t est = std::min<uint64_t>(gN / std::max<uint32_t>(cmin, 1),
@@ -1284,18 +1342,25 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         const uint64_t out_need = out_used + std::min<uint64_t>(est, out_budget) + 1024;
         if (stream_out && out_need > ctx->out_cap) CK(cudaStreamSynchronize(ctx->cs));  // copies read the old buffer
         RET(ensure_out(ctx, out_need, out_used));
-        uint64_t arena_used = 0;
-        // the group's bytes and 12 B per superkmer, plus each chunk's padding (<= 32 + 3 x 15 B)
-        if (spilled) CK(ctx->bk_arena.ensure(gb + 96 * ctx->store.size() + 64));
         CK(ctx->bk_entries.ensure(gs * sizeof(BEntry)));
         CK(cudaMemsetAsync(ctx->bk_skms.p, 0, NB * 4, ctx->s));
         CK(cudaMemsetAsync(ctx->bk_kmers.p, 0, NB * 8, ctx->s));
-        std::vector<const uint8_t *> cb(ctx->store.size());
-        std::vector<const uint64_t *> ci(ctx->store.size());
-        std::vector<const uint32_t *> ck(ctx->store.size());
-        CK(cudaEventRecord(ctx->e0, ctx->s));
-        for (size_t j = 0; j < ctx->store.size(); j++)
-            RET(chunk_range(ctx, ctx->store[j], p0, p1, ctx->bk_arena, &arena_used, &cb[j], &ci[j], &ck[j]));
+        std::vector<const uint8_t *> cb(nst);
+        std::vector<const uint64_t *> ci(nst);
+        std::vector<const uint32_t *> ck(nst);
+        if (spilled) {
+            const int sl = (int)(gi & 1);
+            if (staged_g[sl] != (long)gi) RET(stage(gi));
+            if (gi + 1 < grps.size() && staged_g[(gi + 1) & 1] != (long)(gi + 1)) RET(stage(gi + 1));
+            CK(cudaStreamWaitEvent(ctx->s, staged[sl], 0));
+            cb = cbs[sl];
+            ci = cis[sl];
+            ck = cks[sl];
+        } else {  // device chunks: their own pointers, no copies
+            uint64_t unused = 0;
+            for (size_t j = 0; j < nst; j++)
+                RET(chunk_range(ctx, ctx->store[j], p0, p1, ctx->bk_arena, &unused, &cb[j], &ci[j], &ck[j]));
+        }
         CK(cudaEventRecord(ctx->e2, ctx->s));
         // the split of every chunk's part of the group, one launch per pass
         std::vector<BSChunk> bsc;
@@ -1368,8 +1433,6 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
         acc_ms += ms;
-        CK(cudaEventElapsedTime(&ms, ctx->e0, ctx->e2));
-        stage_ms += ms;
         groups++;
         std::vector<uint32_t> ids;
         std::vector<uint64_t> off;
@@ -1433,7 +1496,13 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         out_used = hg[0];
         distinct_used = hg[1];
         redo = 0;
-        p0 = p1;
+        if (spilled) {  // the arena is free once this group's work (waited for above) is done
+            const int sl = (int)(gi & 1);
+            float sms = 0;
+            if (cudaEventElapsedTime(&sms, st0[sl], staged[sl]) == cudaSuccess) stage_ms += sms;
+            CK(cudaEventRecord(freed[sl], ctx->s));
+        }
+        gi++;
     }
     CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
     CK(cudaStreamSynchronize(ctx->s));

@@ -324,21 +324,26 @@ def test_heavy_and_overflowing_sub_buckets(oracle, record_slice, monkeypatch):
     assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
 
 
-@pytest.mark.parametrize("kind", ["hash", "sort", "hash_redo"])
+@pytest.mark.parametrize("kind", ["hash", "sort", "hash_redo", "hash_spill", "hash_spill_redo"])
 def test_count_partitions_subsets(oracle, kind, monkeypatch):
     """Counting a store in disjoint partition subsets (as the reference's
     phase-2 workers do) gives each subset's k-mers; together the oracle's.
-    hash_redo starts every group with no output room, so each group
-    overflows its output and is counted again."""
-    if kind == "hash_redo":
+    Every third partition makes every partition a group of its own.
+    *_redo starts every group with no output room, so each group overflows
+    its output and is counted again; *_spill stages each group from pinned
+    host memory while the group before counts."""
+    kw = {}
+    if kind.endswith("_redo"):
         monkeypatch.setenv("GKC_OUT_ESTIMATE", "1")
-        kind = "hash"
+    if "spill" in kind:
+        kw = dict(spill_host=True, batch_bases=150_000)
+    kind = kind.split("_")[0]
     k, p, P = 31, 11, 32
     reads, offs = random_reads(51, 80_000, 6000, 150, 0.005)
     _, _, _, po, stream = oracle.skmgen(reads, offs, k, p, P)
     per = [oracle.count(oracle.extract(stream[int(po[q]):int(po[q + 1])], k), 1, U32) for q in range(P)]
     subsets = [np.arange(0, P, 3), np.arange(1, P, 3), np.arange(2, P, 3)]
-    with counter(k, p, P, kind) as c:
+    with counter(k, p, P, kind, **kw) as c:
         c.add_reads(reads, offs)
         tot = 0
         for i, sub in enumerate(subsets):
