@@ -336,6 +336,8 @@ struct gkc_ctx {
     PinBuf h_scal;
     PinBuf h_off, h_km, h_ids, h_work;  // pinned staging of the record path's host round trips
     PinBuf h_desc;                      // split descriptors of a group
+    PinBuf h_cur;                       // output cursor, distinct count and error flags of a group
+    uint64_t free_hint = 0;             // free device memory at the start of the count
 
     std::vector<StoreChunk *> pool;  // cleared chunks kept for reuse
     HostArena arena;                 // pinned host memory of spilled chunks
@@ -373,7 +375,7 @@ struct gkc_ctx {
                         &sk_starts, &sk_k32, &hpc_tiles, &hpc_tbase, &hpc_reads, &hpc_offs};
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work,
-                        &h_desc};
+                        &h_desc, &h_cur};
         for (auto *p : ps) p->release();
         arena.release();
         cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_ready[0], buf_ready[1], spill_ready,
@@ -1022,7 +1024,8 @@ int count_buckets_records_slice(gkc_ctx *ctx, const std::vector<uint32_t> &ids, 
     CK(ctx->r_woff.ensure((nw + 1) * 8));
     CK(ctx->r_wrec.ensure(nw * 4));
     CK(ctx->r_failed.ensure((NR + 1) * 4));
-    CK(cudaStreamSynchronize(ctx->s));  // the pinned work list of an earlier slice may still be in flight
+    // (a slice ends with a wait on the stream, so the pinned work list of the
+    // slice before has been copied)
     CK(ctx->h_work.ensure(nw * sizeof(RWork)));
     std::memcpy(ctx->h_work.p, work.data(), nw * sizeof(RWork));
     CK(cudaMemcpyAsync(ctx->r_work.p, ctx->h_work.p, nw * sizeof(RWork), cudaMemcpyHostToDevice, ctx->s));
@@ -1156,10 +1159,15 @@ int count_buckets_records_slice(gkc_ctx *ctx, const std::vector<uint32_t> &ids, 
 // that sub-bucket, so slices are independent.
 int count_buckets_records(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const std::vector<uint64_t> &off,
                           const std::vector<uint64_t> &bk_kmers, uint32_t cmin, uint32_t cmax) {
-    size_t fr = 0, tot = 0;
-    CK(cudaMemGetInfo(&fr, &tot));
-    const uint64_t avail = fr + ctx->r_recs.cap + ctx->r_stage.cap;  // the record buffers are reallocated
-    uint64_t cap_inst = std::max<uint64_t>(1ull << 22, (uint64_t)(avail * 0.6) / 40);
+    uint64_t inst = 0;
+    for (uint32_t b : ids) inst += bk_kmers[b];
+    uint64_t cap_inst = ~0ull;
+    if ((double)inst * 40 > 0.3 * (double)ctx->free_hint) {  // large: size the slices from the memory free now
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        const uint64_t avail = fr + ctx->r_recs.cap + ctx->r_stage.cap;  // the record buffers are reallocated
+        cap_inst = std::max<uint64_t>(1ull << 22, (uint64_t)(avail * 0.6) / 40);
+    }
     // GKC_RECORD_SLICE=n caps a slice at n instances, so that tests can make
     // small inputs take several slices
     if (const char *rs = getenv("GKC_RECORD_SLICE")) cap_inst = std::max<uint64_t>(1, strtoull(rs, nullptr, 10));
@@ -1225,6 +1233,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         size_t tot = 0;
         CK(cudaMemGetInfo(&free0, &tot));
     }
+    ctx->free_hint = free0;
     const uint64_t out_budget = std::max<uint64_t>(1ull << 24, (uint64_t)(free0 * 0.25) / 12);
     double kept_ratio = 1.0 / std::max<uint32_t>(cmin, 1);
     // GKC_OUT_ESTIMATE=n sets each group's first output estimate to n - 1
@@ -1427,9 +1436,20 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
             LAUNCHED();
         }
         CK(cudaEventRecord(ctx->e3, ctx->s));
-        uint32_t nfail = 0;
-        CK(cudaMemcpyAsync(&nfail, ctx->bk_failed.p, 4, cudaMemcpyDeviceToHost, ctx->s));
+        // one host round trip: the failed sub-buckets, the sub-bucket offsets and
+        // k-mer counts the record path needs for them, and the output cursor
+        // (pinned buffers: pageable copies stage through the driver and stall
+        // with the host's load; every wait is a chance to catch such a stall)
+        CK(ctx->h_ids.ensure((NB + 1) * 4));
+        CK(ctx->h_off.ensure((NB + 1) * 8));
+        CK(ctx->h_km.ensure(NB * 8));
+        CK(ctx->h_cur.ensure(32));
+        CK(cudaMemcpyAsync(ctx->h_ids.p, ctx->bk_failed.p, (NB + 1) * 4, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(ctx->h_off.p, ctx->bk_off.p, (NB + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(ctx->h_km.p, ctx->bk_kmers.p, NB * 8, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(ctx->h_cur.p, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
+        const uint32_t nfail = std::min<uint32_t>(ctx->h_ids.as<uint32_t>()[0], (uint32_t)NB);
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
         acc_ms += ms;
@@ -1437,18 +1457,8 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         std::vector<uint32_t> ids;
         std::vector<uint64_t> off;
         if (nfail || ctx->opt.hash_l2_only) {
-            // through pinned buffers: pageable copies stage through the driver
-            // and stall with the host's load
-            CK(ctx->h_off.ensure((NB + 1) * 8));
-            CK(cudaMemcpyAsync(ctx->h_off.p, ctx->bk_off.p, (NB + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
-            if (nfail) {
-                CK(ctx->h_ids.ensure(nfail * 4));
-                CK(cudaMemcpyAsync(ctx->h_ids.p, ctx->bk_failed.as<uint32_t>() + 1, nfail * 4,
-                                   cudaMemcpyDeviceToHost, ctx->s));
-            }
-            CK(cudaStreamSynchronize(ctx->s));
             off.assign(ctx->h_off.as<uint64_t>(), ctx->h_off.as<uint64_t>() + NB + 1);
-            if (nfail) ids.assign(ctx->h_ids.as<uint32_t>(), ctx->h_ids.as<uint32_t>() + nfail);
+            if (nfail) ids.assign(ctx->h_ids.as<uint32_t>() + 1, ctx->h_ids.as<uint32_t>() + 1 + nfail);
         }
         if (ctx->opt.hash_l2_only)  // every non-empty sub-bucket (one per partition)
             for (uint64_t b = bbase(p0); b < bbase(p1); b++)
@@ -1459,17 +1469,20 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
             } else {
                 ctx->fallback_buckets += ids.size();
                 ctx->times[5] += (double)ids.size();
-                CK(ctx->h_km.ensure(NB * 8));
-                CK(cudaMemcpyAsync(ctx->h_km.p, ctx->bk_kmers.p, NB * 8, cudaMemcpyDeviceToHost, ctx->s));
-                CK(cudaStreamSynchronize(ctx->s));
                 std::vector<uint64_t> km(ctx->h_km.as<uint64_t>(), ctx->h_km.as<uint64_t>() + NB);
                 RET(count_buckets_records(ctx, ids, off, km, cmin, cmax));
             }
         }
-        // entries written so far: the next group's capacity starts there
+        // entries written so far: the next group's capacity starts there (read
+        // again only if the record path or the L2 table wrote more)
         unsigned long long hg[3];
-        CK(cudaMemcpyAsync(hg, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
-        CK(cudaStreamSynchronize(ctx->s));
+        if (ids.empty()) {
+            std::memcpy(hg, ctx->h_cur.p, 24);
+        } else {
+            CK(cudaMemcpyAsync(ctx->h_cur.p, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaStreamSynchronize(ctx->s));
+            std::memcpy(hg, ctx->h_cur.p, 24);
+        }
         if ((uint32_t)hg[2] & ERR_OUTPUT_FULL) {  // count the group again with room for all of it
             if (++redo > 2) return ctx->fail(GKC_EINTERNAL, "output capacity exceeded");
             const uint64_t need = hg[0];
