@@ -61,7 +61,7 @@ WORKLOAD_DESC = {
 # capture of a 300 Mbp case (profiles/phase1_and_counter_bacterial_small.md,
 # learned order, 256 MiB batches); the roofline's `traffic` scales them to the
 # bases of one launch.
-TRAFFIC_PER_BASE = {"find_superkmers": 2.62, "scatter_superkmers": 7.87}  # one launch per batch each
+TRAFFIC_PER_BASE = {"find_superkmers": 2.61, "scatter_superkmers": 7.85}  # one launch per batch each
 
 
 def peaks():
