@@ -46,7 +46,10 @@ enum { GKC_FASTQ = 0, GKC_FASTA = 1 };
 typedef struct gkc_ctx gkc_ctx;
 
 typedef struct gkc_options {
-    int k;                  /* k-mer length, p <= k <= 32 (reference -k, utilities.hpp:187)      */
+    int k;                  /* k-mer length, p <= k <= 64 (reference -k, utilities.hpp:187); k   */
+                            /* > 32 is the reference's 128-bit LONGERKMER build (types.h:34-35,  */
+                            /* utilities.hpp:280-281): k-mers take two words and are counted by  */
+                            /* the sort counter whatever `counter` says                          */
     int p;                  /* minimizer length, 3 <= p <= 16 (reference -p, utilities.hpp:188)   */
     int partitions;         /* superkmer partitions, 1..4096 (reference -skm, utilities.hpp:189)  */
     int counter;            /* GKC_COUNTER_SORT or GKC_COUNTER_HASH                               */
@@ -203,19 +206,25 @@ int gkc_count_partitions(gkc_ctx *ctx, const int32_t *parts, uint64_t n, uint32_
                          uint64_t *n_out, uint64_t *n_distinct);
 
 /* Copies the last gkc_count result: kmers[i] (2-bit, first base in the most
- * significant position, canonical) and counts[i], i < min(cap, n_out). */
+ * significant position, canonical) and counts[i], i < min(cap, n_out).  For
+ * k > 32 a k-mer takes two words, kmers[2i] (low) and kmers[2i+1] (high):
+ * the memory layout of an unsigned __int128 on a little-endian host, the
+ * reference's T_kmer under LONGERKMER (types.h:34-35); cap counts k-mers. */
 int gkc_result(gkc_ctx *ctx, uint64_t *kmers, uint32_t *counts, uint64_t cap, int mem);
 
-/* Device pointers to the last result (valid until the next call). */
+/* Device pointers to the last result (valid until the next call; two words
+ * per k-mer for k > 32, as gkc_result). */
 int gkc_result_device(gkc_ctx *ctx, const uint64_t **kmers, const uint32_t **counts, uint64_t *n);
 
-/* One call: gkc_store_clear + gkc_add_reads + gkc_count + gkc_result. */
+/* One call: gkc_store_clear + gkc_add_reads + gkc_count + gkc_result (cap in
+ * k-mers: 2 * cap words for k > 32). */
 int gkc_count_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads, int mem,
                     uint32_t cmin, uint32_t cmax, uint64_t *kmers, uint32_t *counts, uint64_t cap,
                     int out_mem, uint64_t *n_out, uint64_t *n_distinct);
 
 /* Counts raw 64-bit keys (no superkmers, no canonical step) with the
- * configured counter; results as gkc_count.  keys must not be 2^64-1. */
+ * configured counter; results as gkc_count, one word per key whatever the
+ * context's k.  keys must not be 2^64-1. */
 int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint32_t cmin, uint32_t cmax,
                    uint64_t *n_out, uint64_t *n_distinct);
 

@@ -263,3 +263,78 @@ int64_t orc_count(uint64_t *keys, int64_t n, uint32_t cmin, uint32_t cmax,
     if (n_distinct) *n_distinct = d;
     return w;
 }
+
+/* ------------------------------------------------------------------------
+ * k-mers longer than 32 bases (the reference's LONGERKMER build, k <= 64,
+ * T_kmer = unsigned __int128, types.h:34-35; utilities.hpp:280-281).  Keys
+ * are passed as two u64 words per k-mer, low word first: the memory layout of
+ * an unsigned __int128 on a little-endian host. */
+typedef unsigned __int128 orc_u128;
+
+static orc_u128 orc_revcomp128(orc_u128 x, int k) {
+    orc_u128 r = 0; int i;
+    x = ~x;
+    for (i = 0; i < k; i++) { r = (r << 2) | (x & 3u); x >>= 2; }
+    return r;
+}
+
+static void orc_put128(uint64_t *out, int64_t n, orc_u128 x, int k) {
+    orc_u128 rc = orc_revcomp128(x, k), m = x < rc ? x : rc;
+    out[2 * n] = (uint64_t)m;
+    out[2 * n + 1] = (uint64_t)(m >> 64);
+}
+
+/* orc_extract for k <= 64 (cpu_funcs.cpp:437-515 with a 128-bit T_kmer). */
+int64_t orc_extract_wide(const uint8_t *bytes, uint64_t nbytes, int k, uint64_t *kmers2) {
+    orc_u128 mask = k >= 64 ? ~(orc_u128)0 : (((orc_u128)1 << (2 * k)) - 1);
+    uint64_t i = 0;
+    int64_t n = 0;
+    while (i < nbytes) {
+        int h = bytes[i] >> 6, have = 0, t;
+        orc_u128 x = 0;
+        for (t = 3 - h; t < 3; t++) { x = ((x << 2) | ((bytes[i] >> (4 - 2 * t)) & 3u)) & mask; have++; }
+        if (have >= k) { if (kmers2) orc_put128(kmers2, n, x, k); n++; }
+        i++;
+        for (;;) {
+            if (i >= nbytes) return -1;
+            int c = bytes[i] >> 6;
+            for (t = 0; t < c; t++) {
+                x = ((x << 2) | ((bytes[i] >> (4 - 2 * t)) & 3u)) & mask;
+                if (++have >= k) { if (kmers2) orc_put128(kmers2, n, x, k); n++; }
+            }
+            i++;
+            if (c != 3) break;
+        }
+    }
+    return n;
+}
+
+static int orc_cmp128(const void *a, const void *b) {
+    const uint64_t *x = (const uint64_t *)a, *y = (const uint64_t *)b;
+    if (x[1] != y[1]) return x[1] < y[1] ? -1 : 1;
+    if (x[0] != y[0]) return x[0] < y[0] ? -1 : 1;
+    return 0;
+}
+
+/* orc_count for k <= 64: sorts the (low, high) pairs ascending as 128-bit
+ * values, run-length encodes and applies [cmin, cmax]. */
+int64_t orc_count_wide(uint64_t *keys2, int64_t n, uint32_t cmin, uint32_t cmax,
+                       uint64_t *out_k2, uint32_t *out_c, int64_t *n_distinct) {
+    int64_t i = 0, w = 0, d = 0;
+    if (n > 1) qsort(keys2, (size_t)n, 16, orc_cmp128);
+    while (i < n) {
+        int64_t j = i + 1;
+        while (j < n && keys2[2 * j] == keys2[2 * i] && keys2[2 * j + 1] == keys2[2 * i + 1]) j++;
+        uint64_t run = (uint64_t)(j - i);
+        uint32_t c = run > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)run;
+        if (c >= cmin && c <= cmax) {
+            if (out_k2) { out_k2[2 * w] = keys2[2 * i]; out_k2[2 * w + 1] = keys2[2 * i + 1]; }
+            if (out_c) out_c[w] = c;
+            w++;
+        }
+        d++;
+        i = j;
+    }
+    if (n_distinct) *n_distinct = d;
+    return w;
+}

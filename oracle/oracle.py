@@ -9,7 +9,12 @@ Two oracles are exposed:
 * ``Oracle`` -- the C restatement in oracle/gkc_oracle.c of the reference
   algorithm (each C function cites the reference file:line it follows);
 * ``RefOracle`` -- the reference's own CPU path (cpu_funcs.cpp compiled from
-  the reference tree by oracle/Makefile into oracle/_ref/libgkc_ref.so).
+  the reference tree by oracle/Makefile into oracle/_ref/libgkc_ref.so, and
+  with -DLONGERKMER into oracle/_ref/libgkc_ref_long.so for k > 32).
+
+For k <= 32 k-mers are u64 arrays; for 32 < k <= 64 they are (n, 2) u64
+arrays of (low word, high word), the layout of the reference's 128-bit
+T_kmer (types.h:34-35), ordered as 128-bit values.
 """
 from __future__ import annotations
 
@@ -56,6 +61,11 @@ class Oracle:
         L.orc_revcomp.restype = C.c_uint64
         L.orc_sort_u64.argtypes = [_u64p, C.c_int64]
         L.orc_sort_u64.restype = None
+        L.orc_extract_wide.argtypes = [_u8p, C.c_uint64, C.c_int, C.c_void_p]
+        L.orc_extract_wide.restype = C.c_int64
+        L.orc_count_wide.argtypes = [_u64p, C.c_int64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
+                                     C.POINTER(C.c_int64)]
+        L.orc_count_wide.restype = C.c_int64
 
     # -- phase 1 ---------------------------------------------------------
     def kmer_keys(self, read: bytes, k: int, p: int, lut=None) -> np.ndarray:
@@ -91,21 +101,26 @@ class Oracle:
     # -- phase 2 ---------------------------------------------------------
     def extract(self, stream: np.ndarray, k: int) -> np.ndarray:
         stream = np.ascontiguousarray(stream, np.uint8)
-        n = self.lib.orc_extract(stream, len(stream), k, None)
+        fn = self.lib.orc_extract_wide if k > 32 else self.lib.orc_extract
+        n = fn(stream, len(stream), k, None)
         if n < 0:
             raise ValueError("malformed superkmer stream")
-        out = np.zeros(n, np.uint64)
-        self.lib.orc_extract(stream, len(stream), k, out.ctypes.data_as(C.c_void_p))
+        out = np.zeros((n, 2) if k > 32 else n, np.uint64)
+        fn(stream, len(stream), k, out.ctypes.data_as(C.c_void_p))
         return out
 
     def count(self, keys: np.ndarray, cmin: int = 1, cmax: int = 0xFFFFFFFF):
-        """Sort + RLE + threshold.  Returns (kmers, counts, n_distinct)."""
+        """Sort + RLE + threshold.  Returns (kmers, counts, n_distinct); keys
+        of shape (n, 2) are 128-bit (low, high) pairs."""
         keys = np.array(keys, np.uint64, copy=True)
-        ok = np.zeros(len(keys), np.uint64)
-        oc = np.zeros(len(keys), np.uint32)
+        wide = keys.ndim == 2
+        n = len(keys)
+        ok = np.zeros(keys.shape, np.uint64)
+        oc = np.zeros(n, np.uint32)
         d = C.c_int64(0)
-        w = self.lib.orc_count(keys, len(keys), cmin, cmax, ok.ctypes.data_as(C.c_void_p),
-                               oc.ctypes.data_as(C.c_void_p), C.byref(d))
+        fn = self.lib.orc_count_wide if wide else self.lib.orc_count
+        w = fn(keys.reshape(-1) if wide else keys, n, cmin, cmax, ok.ctypes.data_as(C.c_void_p),
+               oc.ctypes.data_as(C.c_void_p), C.byref(d))
         return ok[:w].copy(), oc[:w].copy(), int(d.value)
 
     def count_reads(self, reads, offs, k, p, P, cmin=1, cmax=0xFFFFFFFF, lut=None):
@@ -124,13 +139,18 @@ class Oracle:
 
 
 class RefOracle:
-    """The reference's own CPU path (oracle/_ref/libgkc_ref.so)."""
+    """The reference's own CPU path (oracle/_ref/libgkc_ref.so; with
+    ``wide=True`` its 128-bit LONGERKMER build, oracle/_ref/libgkc_ref_long.so,
+    for k <= 64)."""
 
-    def __init__(self, path: str | None = None):
-        path = path or os.path.join(HERE, "_ref", "libgkc_ref.so")
+    def __init__(self, path: str | None = None, wide: bool = False):
+        path = path or os.path.join(HERE, "_ref", "libgkc_ref_long.so" if wide else "libgkc_ref.so")
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
         L = self.lib = C.CDLL(path)
+        L.ref_kmer_bits.argtypes = []
+        L.ref_kmer_bits.restype = C.c_int
+        self.wide = L.ref_kmer_bits() == 128
         L.ref_gen_skm_offs.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, _i32p, _u32p]
         L.ref_gen_skm_offs.restype = C.c_int
         L.ref_phase1.argtypes = [_u8p, _u64p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -171,7 +191,9 @@ class RefOracle:
 
     def count_bytes(self, stream, n_kmers, k, cmin=1, cmax=0xFFFFFFFF):
         stream = np.ascontiguousarray(stream, np.uint8)
-        ok = np.zeros(max(1, n_kmers), np.uint64)
+        if (k > 32) != self.wide:
+            raise ValueError(f"k={k} needs the {'128' if k > 32 else '64'}-bit reference build")
+        ok = np.zeros((max(1, n_kmers), 2) if self.wide else max(1, n_kmers), np.uint64)
         oc = np.zeros(max(1, n_kmers), np.uint32)
         d = C.c_int64(0)
         w = self.lib.ref_count_bytes(stream if len(stream) else np.zeros(1, np.uint8), len(stream),

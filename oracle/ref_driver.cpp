@@ -12,6 +12,11 @@
 //   _h_process_bytes  cpu_funcs.cpp:437-515  (superkmer bytes -> canonical k-mers)
 //   sort_kmers        cpu_funcs.cpp:365-392  (in-tree MSD radix + std::sort)
 //   KmerCountingCPU   cpu_funcs.cpp:586-651  (phase 2 of one partition)
+//
+// oracle/Makefile builds it twice: libgkc_ref.so with the reference's default
+// 64-bit T_kmer (k <= 32) and libgkc_ref_long.so with -DLONGERKMER, the
+// reference's own 128-bit build for k <= 64 (types.h:34-35, CMakeLists.txt
+// target l_<name>).
 #include "cpu_funcs.h"
 #include "utilities.hpp"
 
@@ -119,7 +124,8 @@ int64_t ref_part_bytes(void *h, int part, uint8_t *out) {
 
 // Counts a partition's superkmer bytes with the reference's own extraction
 // and sort, then run-length encodes and applies [cmin, cmax].  Keys are
-// written in ascending order.  Returns the number written.
+// written in ascending order, two u64 words each (low first) in the
+// LONGERKMER build.  Returns the number written.
 int64_t ref_count_bytes(const uint8_t *bytes, uint64_t nbytes, uint64_t n_kmers, int k,
                         uint32_t cmin, uint32_t cmax, uint64_t *out_k, uint32_t *out_c,
                         int64_t *n_distinct) {
@@ -139,7 +145,15 @@ int64_t ref_count_bytes(const uint8_t *bytes, uint64_t nbytes, uint64_t n_kmers,
         size_t run = j - i;
         uint32_t c = run > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)run;
         if (c >= cmin && c <= cmax) {
+#ifdef LONGERKMER
+            // two words per k-mer, low word first
+            if (out_k) {
+                out_k[2 * w] = (uint64_t)kmers[i];
+                out_k[2 * w + 1] = (uint64_t)(kmers[i] >> 64);
+            }
+#else
             if (out_k) out_k[w] = kmers[i];
+#endif
             if (out_c) out_c[w] = c;
             w++;
         }
@@ -149,6 +163,9 @@ int64_t ref_count_bytes(const uint8_t *bytes, uint64_t nbytes, uint64_t n_kmers,
     *n_distinct = d;
     return w;
 }
+
+// Bits of the reference's T_kmer in this build (64, or 128 under LONGERKMER).
+int ref_kmer_bits() { return (int)(8 * sizeof(T_kmer)); }
 
 void ref_free(void *h) {
     auto *res = (Phase1Result *)h;

@@ -143,7 +143,11 @@ def _ptr(a):
 
 class KmerCounter:
     """A counting context on one CUDA device (reference CLI names in brackets):
-    k [-k], p [-p], partitions [-skm], counter 'hash' or 'sort'."""
+    k [-k], p [-p], partitions [-skm], counter 'hash' or 'sort'.
+
+    k <= 32 gives uint64 k-mers.  32 < k <= 64 (the reference's 128-bit
+    LONGERKMER build) counts with the sort counter and gives k-mers as (n, 2)
+    uint64 arrays of (low word, high word), ordered as 128-bit values."""
 
     def __init__(self, k: int = 31, p: int = 11, partitions: int = 512, counter: str = "hash",
                  device: int = 0, radix_bits: int = 8, table_slots: float = 0.35,
@@ -164,6 +168,7 @@ class KmerCounter:
         self._L, self._h = L, h
         self.k, self.p, self.partitions, self.counter = k, p, partitions, counter
         self.device = device
+        self._kw = 1  # u64 words per k-mer of the last result
 
     def close(self):
         if getattr(self, "_h", None):
@@ -319,6 +324,7 @@ class KmerCounter:
         """Counts the store; returns (kept, distinct)."""
         no, nd = C.c_uint64(0), C.c_uint64(0)
         self._check(self._L.gkc_count(self._h, cmin, cmax, C.byref(no), C.byref(nd)))
+        self._kw = 2 if self.k > 32 else 1
         return no.value, nd.value
 
     def count_partitions(self, parts, cmin: int = 1, cmax: int = UINT32_MAX):
@@ -327,15 +333,17 @@ class KmerCounter:
         no, nd = C.c_uint64(0), C.c_uint64(0)
         self._check(self._L.gkc_count_partitions(self._h, _ptr(a)[0], len(a), cmin, cmax, C.byref(no),
                                                  C.byref(nd)))
+        self._kw = 2 if self.k > 32 else 1
         return no.value, nd.value
 
     def result(self, n: int | None = None):
-        """The last count's (kmers uint64, counts uint32) as host arrays."""
+        """The last count's (kmers uint64, counts uint32) as host arrays
+        (kmers of shape (n, 2) for k > 32)."""
         if n is None:
             kp, cp, nn = C.c_void_p(), C.c_void_p(), C.c_uint64(0)
             self._check(self._L.gkc_result_device(self._h, C.byref(kp), C.byref(cp), C.byref(nn)))
             n = nn.value
-        km = np.zeros(max(1, n), np.uint64)
+        km = np.zeros((max(1, n), 2) if self._kw == 2 else max(1, n), np.uint64)
         ct = np.zeros(max(1, n), np.uint32)
         self._check(self._L.gkc_result(self._h, _ptr(km)[0], _ptr(ct)[0], n, MEM_HOST))
         return km[:n], ct[:n]
@@ -364,6 +372,7 @@ class KmerCounter:
         no, nd = C.c_uint64(0), C.c_uint64(0)
         self._check(self._L.gkc_count_reads(self._h, rp, op, len(offs) - 1, rm, cmin, cmax, kp, cp, cap,
                                             km, C.byref(no), C.byref(nd)))
+        self._kw = 2 if self.k > 32 else 1
         return no.value, nd.value
 
     def count_keys(self, keys, cmin: int = 1, cmax: int = UINT32_MAX):
@@ -371,6 +380,7 @@ class KmerCounter:
         kp, km = _ptr(keys)
         no, nd = C.c_uint64(0), C.c_uint64(0)
         self._check(self._L.gkc_count_keys(self._h, kp, len(keys), km, cmin, cmax, C.byref(no), C.byref(nd)))
+        self._kw = 1
         return no.value, nd.value
 
     # -- learned minimizer order --------------------------------------------

@@ -14,6 +14,8 @@
 //            (counts saturate at 2^32-1, types.h:101-102) -> threshold
 //            [cmin, cmax] (utilities.hpp:190) -> compaction that keeps the
 //            ascending order inside every partition.
+// Keys are u64 for k <= 32 and u128 for k <= 64 (the reference's LONGERKMER
+// build, types.h:34-35): every kernel is a template over the key type.
 #include "gkc_device.cuh"
 
 namespace gkc {
@@ -29,15 +31,17 @@ struct SExtractParams {
     uint32_t P;
     int k;
     int canonical;
-    uint64_t *keys;                      // key buffer
+    void *keys;                          // key buffer (u64, or u128 for k > 32)
     const unsigned long long *seg_off;   // [P] partition segment starts in keys
     unsigned long long *seg_cursor;      // [P] keys written per partition
 };
 
 constexpr int SX_THREADS = 256;
 
+template <class KT>
 __global__ void __launch_bounds__(SX_THREADS)
 sort_extract_kernel(SExtractParams a) {
+    KT *keys = static_cast<KT *>(a.keys);
     const int lane = threadIdx.x & 31;
     for (uint64_t base = a.i_begin + blockIdx.x * (uint64_t)SX_THREADS; base < a.n_skm;
          base += (uint64_t)gridDim.x * SX_THREADS) {
@@ -79,10 +83,12 @@ sort_extract_kernel(SExtractParams a) {
         if (has) {
             const uint8_t *pb = a.bytes + a.part_byte_off[part];
             uint64_t o = dst;
-            if (a.canonical)
-                for_each_kmer<true>(pb, e, a.k, [&](uint64_t key) { a.keys[o++] = key; });
+            if constexpr (sizeof(KT) == 16)
+                for_each_kmer_wide(pb, e, a.k, [&](u128 key) { keys[o++] = key; });
+            else if (a.canonical)
+                for_each_kmer<true>(pb, e, a.k, [&](uint64_t key) { keys[o++] = key; });
             else
-                for_each_kmer<false>(pb, e, a.k, [&](uint64_t key) { a.keys[o++] = key; });
+                for_each_kmer<false>(pb, e, a.k, [&](uint64_t key) { keys[o++] = key; });
         }
     }
 }
@@ -165,9 +171,9 @@ constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_ITEMS = 16;
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // 4096 keys
 
-template <int RB>
+template <int RB, class KT>
 __global__ void __launch_bounds__(RS_THREADS)
-radix_hist_kernel(const uint64_t *keys, const TileDesc *tiles, int shift, uint32_t *counts) {
+radix_hist_kernel(const KT *keys, const TileDesc *tiles, int shift, uint32_t *counts) {
     constexpr int NB = 1 << RB;
     __shared__ uint32_t hist[NB];
     const TileDesc td = tiles[blockIdx.x];
@@ -177,17 +183,16 @@ radix_hist_kernel(const uint64_t *keys, const TileDesc *tiles, int shift, uint32
 #pragma unroll 4
     for (int i = 0; i < RS_ITEMS; i++) {
         uint32_t j = (uint32_t)i * RS_THREADS + threadIdx.x;
-        if (j < td.n) atomicAdd(&hist[(keys[td.start + j] >> shift) & dmask], 1u);
+        if (j < td.n) atomicAdd(&hist[(uint32_t)((keys[td.start + j] >> shift) & dmask)], 1u);
     }
     __syncthreads();
     for (int d = threadIdx.x; d < NB; d += RS_THREADS)
         counts[td.cnt_base + (uint64_t)d * td.nt + td.t] = hist[d];
 }
 
-template <int RB>
+template <int RB, class KT>
 __global__ void __launch_bounds__(RS_THREADS)
-radix_scatter_kernel(const uint64_t *in, uint64_t *out, const TileDesc *tiles, int shift,
-                     const uint64_t *offsets) {
+radix_scatter_kernel(const KT *in, KT *out, const TileDesc *tiles, int shift, const uint64_t *offsets) {
     constexpr int NB = 1 << RB;
     __shared__ uint32_t wcnt[RS_WARPS][NB];
     const TileDesc td = tiles[blockIdx.x];
@@ -196,14 +201,14 @@ radix_scatter_kernel(const uint64_t *in, uint64_t *out, const TileDesc *tiles, i
     for (int d = threadIdx.x; d < RS_WARPS * NB; d += RS_THREADS) (&wcnt[0][0])[d] = 0;
     __syncthreads();
     const uint64_t dmask = NB - 1;
-    uint64_t key[RS_ITEMS];
+    KT key[RS_ITEMS];
     uint32_t rank[RS_ITEMS];
     // warp-striped: warp w owns keys [w*32*ITEMS, (w+1)*32*ITEMS) of the tile
 #pragma unroll
     for (int i = 0; i < RS_ITEMS; i++) {
         uint32_t j = (uint32_t)warp * 32 * RS_ITEMS + (uint32_t)i * 32 + lane;
         bool valid = j < td.n;
-        key[i] = valid ? in[td.start + j] : 0ull;
+        key[i] = valid ? in[td.start + j] : KT(0);
         unsigned act = __ballot_sync(FULL, valid);
         rank[i] = 0;
         if (valid) {
@@ -247,8 +252,9 @@ constexpr int RL_TILE = RL_THREADS * RL_ITEMS;
 
 // Heads per tile: i == 0 or key[i] != key[i-1].  Equal keys never straddle
 // two partitions (a canonical k-mer has one minimizer, so one partition).
+template <class KT>
 __global__ void __launch_bounds__(RL_THREADS)
-rle_count_kernel(const uint64_t *keys, uint64_t n, uint32_t *tile_cnt) {
+rle_count_kernel(const KT *keys, uint64_t n, uint32_t *tile_cnt) {
     __shared__ uint32_t ws[RL_THREADS / 32];
     uint64_t t0 = blockIdx.x * (uint64_t)RL_TILE + (uint64_t)threadIdx.x * RL_ITEMS;
     uint32_t c = 0;
@@ -261,9 +267,9 @@ rle_count_kernel(const uint64_t *keys, uint64_t n, uint32_t *tile_cnt) {
     if (threadIdx.x == 0) tile_cnt[blockIdx.x] = tot;
 }
 
+template <class KT>
 __global__ void __launch_bounds__(RL_THREADS)
-rle_write_kernel(const uint64_t *keys, uint64_t n, const uint64_t *tile_off, uint64_t *head_pos,
-                 uint64_t *head_key) {
+rle_write_kernel(const KT *keys, uint64_t n, const uint64_t *tile_off, uint64_t *head_pos, KT *head_key) {
     __shared__ uint32_t ws[RL_THREADS / 32];
     uint64_t t0 = blockIdx.x * (uint64_t)RL_TILE + (uint64_t)threadIdx.x * RL_ITEMS;
     uint32_t c = 0;
@@ -306,10 +312,10 @@ keep_count_kernel(const uint64_t *head_pos, uint64_t d, uint64_t n, uint32_t cmi
     if (threadIdx.x == 0) tile_cnt[blockIdx.x] = tot;
 }
 
+template <class KT>
 __global__ void __launch_bounds__(RL_THREADS)
-keep_write_kernel(const uint64_t *head_pos, const uint64_t *head_key, uint64_t d, uint64_t n,
-                  uint32_t cmin, uint32_t cmax, const uint64_t *tile_off, uint64_t *out_k,
-                  uint32_t *out_c) {
+keep_write_kernel(const uint64_t *head_pos, const KT *head_key, uint64_t d, uint64_t n, uint32_t cmin,
+                  uint32_t cmax, const uint64_t *tile_off, KT *out_k, uint32_t *out_c) {
     __shared__ uint32_t ws[RL_THREADS / 32];
     uint64_t t0 = blockIdx.x * (uint64_t)RL_TILE + (uint64_t)threadIdx.x * RL_ITEMS;
     uint32_t c = 0;

@@ -314,6 +314,7 @@ struct gkc_ctx {
     uint64_t tcap = 0;
     DevBuf out_k, out_c;
     uint64_t out_cap = 0, n_out = 0, n_distinct = 0;
+    int res_kw = 1;  // u64 words per k-mer of the result: 2 for k > 32 (u128, low word first)
     // host arrays that the hash counter fills group by group while it counts
     // (gkc_count_reads with host output); `streamed` entries are there
     uint64_t *stream_k = nullptr;
@@ -495,13 +496,14 @@ int ensure_table(gkc_ctx *ctx, uint64_t C) {
 // `keep` entries of the old one.
 int ensure_out(gkc_ctx *ctx, uint64_t need, uint64_t keep) {
     if (need <= ctx->out_cap && ctx->out_k.p) return GKC_OK;
+    const uint64_t kb = ctx->opt.k > 32 ? 16 : 8;  // key bytes per entry
     uint64_t cap = std::max<uint64_t>(need, 1024);
     DevBuf nk, nc;
-    CK(nk.ensure(cap * 8));
+    CK(nk.ensure(cap * kb));
     CK(nc.ensure(cap * 4));
     keep = std::min<uint64_t>(keep, ctx->out_cap);
     if (keep && ctx->out_k.p) {
-        CK(cudaMemcpyAsync(nk.p, ctx->out_k.p, keep * 8, cudaMemcpyDeviceToDevice, ctx->s));
+        CK(cudaMemcpyAsync(nk.p, ctx->out_k.p, keep * kb, cudaMemcpyDeviceToDevice, ctx->s));
         CK(cudaMemcpyAsync(nc.p, ctx->out_c.p, keep * 4, cudaMemcpyDeviceToDevice, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
     }
@@ -532,14 +534,17 @@ int p1_plan(gkc_ctx *ctx, uint64_t total, P1Plan *pl) {
     const int w = ctx->opt.k - ctx->opt.p + 1;
     int lg = 0;
     while ((2 << lg) <= w) lg++;
-    if (ctx->has_lut)
-        pl->kfind = lg == 0 ? find_superkmers_kernel<0, true> : lg == 1 ? find_superkmers_kernel<1, true>
-                  : lg == 2 ? find_superkmers_kernel<2, true> : lg == 3 ? find_superkmers_kernel<3, true>
-                                                                        : find_superkmers_kernel<4, true>;
+    if (ctx->opt.k > 32)  // w >= 33 - 16 + 1 = 18: four or five levels
+        pl->kfind = ctx->has_lut ? (lg >= 5 ? find_superkmers_kernel<5, true, true> : find_superkmers_kernel<4, true, true>)
+                                 : (lg >= 5 ? find_superkmers_kernel<5, false, true> : find_superkmers_kernel<4, false, true>);
+    else if (ctx->has_lut)
+        pl->kfind = lg == 0 ? find_superkmers_kernel<0, true, false> : lg == 1 ? find_superkmers_kernel<1, true, false>
+                  : lg == 2 ? find_superkmers_kernel<2, true, false> : lg == 3 ? find_superkmers_kernel<3, true, false>
+                                                                               : find_superkmers_kernel<4, true, false>;
     else
-        pl->kfind = lg == 0 ? find_superkmers_kernel<0, false> : lg == 1 ? find_superkmers_kernel<1, false>
-                  : lg == 2 ? find_superkmers_kernel<2, false> : lg == 3 ? find_superkmers_kernel<3, false>
-                                                                         : find_superkmers_kernel<4, false>;
+        pl->kfind = lg == 0 ? find_superkmers_kernel<0, false, false> : lg == 1 ? find_superkmers_kernel<1, false, false>
+                  : lg == 2 ? find_superkmers_kernel<2, false, false> : lg == 3 ? find_superkmers_kernel<3, false, false>
+                                                                                : find_superkmers_kernel<4, false, false>;
     pl->dyn = 3ull * P * sizeof(uint32_t);
     CK(cudaFuncSetAttribute(pl->kfind, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl->dyn));
     int per_sm = 0;
@@ -1531,11 +1536,13 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
 }
 
 // ---------------------------------------------------------------------------
-// phase 2, sort counter: sorts `n` keys already in keysA split into segments
-// segs (sizes), then RLE + threshold, appending to the output.
-template <int RB>
+// phase 2, sort counter: sorts `n` keys (KT: u64, or u128 for k > 32) already
+// in keysA split into segments segs (sizes), then RLE + threshold, appending
+// to the output.
+template <int RB, class KT>
 int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, int nbits, uint32_t cmin,
                        uint32_t cmax, float *sort_ms) {
+    constexpr double KB = sizeof(KT);
     // tiles
     std::vector<TileDesc> td;
     uint64_t start = 0, cnt_base = 0;
@@ -1563,19 +1570,19 @@ int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t
         CK(cudaMemcpyAsync(ctx->tiles.p, td.data(), ntiles * sizeof(TileDesc), cudaMemcpyHostToDevice, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));  // td is host memory about to go out of scope
     }
-    uint64_t *src = ctx->keysA.as<uint64_t>(), *dst = ctx->keysB.as<uint64_t>();
+    KT *src = ctx->keysA.as<KT>(), *dst = ctx->keysB.as<KT>();
     CK(cudaEventRecord(ctx->e2, ctx->s));
     for (int shift = 0; shift < nbits && ntiles; shift += RB) {
         {
-            KScope ks(ctx, GKC_K_RADIX_HIST, 8.0 * n + 4.0 * ncounts);
-            radix_hist_kernel<RB><<<(unsigned)ntiles, RS_THREADS, 0, ctx->s>>>(src, ctx->tiles.as<TileDesc>(), shift,
-                                                                                 ctx->counts.as<uint32_t>());
+            KScope ks(ctx, GKC_K_RADIX_HIST, KB * n + 4.0 * ncounts);
+            radix_hist_kernel<RB, KT><<<(unsigned)ntiles, RS_THREADS, 0, ctx->s>>>(
+                src, ctx->tiles.as<TileDesc>(), shift, ctx->counts.as<uint32_t>());
             LAUNCHED();
         }
         RET(scan_u32(ctx, ctx->counts.as<uint32_t>(), ncounts, ctx->offsets.as<uint64_t>(), nullptr));
         {
-            KScope ks(ctx, GKC_K_RADIX_SCATTER, 16.0 * n + 8.0 * ncounts);
-            radix_scatter_kernel<RB><<<(unsigned)ntiles, RS_THREADS, 0, ctx->s>>>(
+            KScope ks(ctx, GKC_K_RADIX_SCATTER, 2 * KB * n + 8.0 * ncounts);
+            radix_scatter_kernel<RB, KT><<<(unsigned)ntiles, RS_THREADS, 0, ctx->s>>>(
                 src, dst, ctx->tiles.as<TileDesc>(), shift, ctx->offsets.as<uint64_t>());
             LAUNCHED();
         }
@@ -1592,8 +1599,8 @@ int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t
     uint64_t d = 0;
     if (rt) {
         {
-            KScope ks(ctx, GKC_K_RLE, 8.0 * n);
-            rle_count_kernel<<<(unsigned)rt, RL_THREADS, 0, ctx->s>>>(src, n, ctx->tilecnt.as<uint32_t>());
+            KScope ks(ctx, GKC_K_RLE, KB * n);
+            rle_count_kernel<KT><<<(unsigned)rt, RL_THREADS, 0, ctx->s>>>(src, n, ctx->tilecnt.as<uint32_t>());
             LAUNCHED();
         }
         RET(scan_u32(ctx, ctx->tilecnt.as<uint32_t>(), rt, ctx->tileoff.as<uint64_t>(), sc));
@@ -1601,11 +1608,11 @@ int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t
         CK(cudaStreamSynchronize(ctx->s));
         d = ctx->h_scal.as<unsigned long long>()[0];
         CK(ctx->heads_pos.ensure(std::max<uint64_t>(d, 1) * 8));
-        CK(ctx->heads_key.ensure(std::max<uint64_t>(d, 1) * 8));
-        KScope ks(ctx, GKC_K_RLE, 8.0 * n + 16.0 * d);
-        rle_write_kernel<<<(unsigned)rt, RL_THREADS, 0, ctx->s>>>(src, n, ctx->tileoff.as<uint64_t>(),
-                                                                   ctx->heads_pos.as<uint64_t>(),
-                                                                   ctx->heads_key.as<uint64_t>());
+        CK(ctx->heads_key.ensure(std::max<uint64_t>(d, 1) * sizeof(KT)));
+        KScope ks(ctx, GKC_K_RLE, KB * n + (8 + KB) * d);
+        rle_write_kernel<KT><<<(unsigned)rt, RL_THREADS, 0, ctx->s>>>(src, n, ctx->tileoff.as<uint64_t>(),
+                                                                       ctx->heads_pos.as<uint64_t>(),
+                                                                       ctx->heads_key.as<KT>());
         LAUNCHED();
     }
     uint64_t kept = 0;
@@ -1624,11 +1631,10 @@ int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t
         CK(cudaStreamSynchronize(ctx->s));
         kept = ctx->h_scal.as<unsigned long long>()[0];
         RET(ensure_out(ctx, ctx->n_out + kept, ctx->n_out));
-        KScope ks(ctx, GKC_K_RLE, 16.0 * d + 12.0 * kept);
-        keep_write_kernel<<<(unsigned)kt, RL_THREADS, 0, ctx->s>>>(
-            ctx->heads_pos.as<uint64_t>(), ctx->heads_key.as<uint64_t>(), d, n, cmin, cmax,
-            ctx->tileoff.as<uint64_t>(), ctx->out_k.as<uint64_t>() + ctx->n_out,
-            ctx->out_c.as<uint32_t>() + ctx->n_out);
+        KScope ks(ctx, GKC_K_RLE, (8 + KB) * d + (4 + KB) * kept);
+        keep_write_kernel<KT><<<(unsigned)kt, RL_THREADS, 0, ctx->s>>>(
+            ctx->heads_pos.as<uint64_t>(), ctx->heads_key.as<KT>(), d, n, cmin, cmax,
+            ctx->tileoff.as<uint64_t>(), ctx->out_k.as<KT>() + ctx->n_out, ctx->out_c.as<uint32_t>() + ctx->n_out);
         LAUNCHED();
     }
     float ms = 0;
@@ -1640,17 +1646,22 @@ int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t
     return GKC_OK;
 }
 
+template <class KT = uint64_t>
 int sort_and_reduce(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, int nbits, uint32_t cmin,
                     uint32_t cmax, float *sort_ms) {
     switch (ctx->opt.radix_bits) {
-        case 4: return sort_and_reduce_rb<4>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
-        case 5: return sort_and_reduce_rb<5>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
-        case 6: return sort_and_reduce_rb<6>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
-        case 7: return sort_and_reduce_rb<7>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
-        default: return sort_and_reduce_rb<8>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        case 4: return sort_and_reduce_rb<4, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        case 5: return sort_and_reduce_rb<5, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        case 6: return sort_and_reduce_rb<6, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        case 7: return sort_and_reduce_rb<7, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        default: return sort_and_reduce_rb<8, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
     }
 }
 
+// Sort counter over the store's partitions (all, or those in `want`), in
+// groups of partitions whose keys fit the memory budget.  KT = u128 counts
+// k-mers of 33 to 64 bases.
+template <class KT>
 int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<char> *want) {
     const uint32_t P = (uint32_t)ctx->opt.partitions;
     std::vector<uint64_t> np(P, 0);
@@ -1660,7 +1671,7 @@ int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     if (!budget) {
         size_t fr = 0, tot = 0;
         CK(cudaMemGetInfo(&fr, &tot));
-        budget = std::max<uint64_t>(1ull << 20, (uint64_t)(fr * 0.5) / 40);
+        budget = std::max<uint64_t>(1ull << 20, (uint64_t)(fr * 0.5) / (5 * sizeof(KT)));
     }
     CK(ctx->segoff.ensure(P * 8));
     CK(ctx->segcur.ensure(P * 8));
@@ -1678,8 +1689,8 @@ int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         uint64_t o = 0;
         for (uint32_t p = p0; p < p1; p++) { segoff[p] = o; o += np[p]; segs.push_back(np[p]); }
         if (n) {
-            CK(ctx->keysA.ensure(n * 8));
-            CK(ctx->keysB.ensure(n * 8));
+            CK(ctx->keysA.ensure(n * sizeof(KT)));
+            CK(ctx->keysB.ensure(n * sizeof(KT)));
             CK(cudaMemcpyAsync(ctx->segoff.p, segoff.data(), P * 8, cudaMemcpyHostToDevice, ctx->s));
             CK(cudaMemsetAsync(ctx->segcur.p, 0, P * 8, ctx->s));
             for (auto *c : ctx->store) {
@@ -1707,7 +1718,7 @@ int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
                 x.P = P;
                 x.k = ctx->opt.k;
                 x.canonical = 1;
-                x.keys = ctx->keysA.as<uint64_t>();
+                x.keys = ctx->keysA.p;
                 x.seg_off = ctx->segoff.as<unsigned long long>();
                 x.seg_cursor = ctx->segcur.as<unsigned long long>();
                 x.i_begin = i0;
@@ -1715,11 +1726,11 @@ int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
                 uint64_t kx = 0;
                 for (uint32_t p = p0; p < p1; p++) kx += c->kmers[p];
                 KScope ks(ctx, GKC_K_SORT_EXTRACT,
-                          (double)(c->byte_off[p1] - c->byte_off[p0]) + 8.0 * (i1 - i0) + 8.0 * kx);
-                sort_extract_kernel<<<g, SX_THREADS, 0, ctx->s>>>(x);
+                          (double)(c->byte_off[p1] - c->byte_off[p0]) + 8.0 * (i1 - i0) + (double)sizeof(KT) * kx);
+                sort_extract_kernel<KT><<<g, SX_THREADS, 0, ctx->s>>>(x);
                 LAUNCHED();
             }
-            RET(sort_and_reduce(ctx, segs, n, 2 * ctx->opt.k, cmin, cmax, &sort_ms));
+            RET(sort_and_reduce<KT>(ctx, segs, n, 2 * ctx->opt.k, cmin, cmax, &sort_ms));
         }
         p0 = p1;
     }
@@ -1797,7 +1808,7 @@ int gkc_create(int device, const gkc_options *opt, gkc_ctx **out) {
     gkc_options o;
     gkc_default_options(&o);
     if (opt) o = *opt;
-    if (o.p < 3 || o.p > 16 || o.k < o.p || o.k > 32 || o.partitions < 1 || o.partitions > 4096 ||
+    if (o.p < 3 || o.p > 16 || o.k < o.p || o.k > 64 || o.partitions < 1 || o.partitions > 4096 ||
         (o.counter != GKC_COUNTER_SORT && o.counter != GKC_COUNTER_HASH) || o.radix_bits < 0 || o.radix_bits > 8 ||
         (o.radix_bits != 0 && o.radix_bits < 4))
         return GKC_EINVAL;
@@ -2592,8 +2603,11 @@ int count_store(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<ch
     CK(cudaEventCreate(&t0));
     CK(cudaEventCreate(&t1));
     CK(cudaEventRecord(t0, ctx->s));
-    int rc = ctx->opt.counter == GKC_COUNTER_HASH ? count_hash(ctx, cmin, cmax, want)
-                                                  : count_sort(ctx, cmin, cmax, want);
+    // k > 32: u128 keys, sort counter only
+    ctx->res_kw = ctx->opt.k > 32 ? 2 : 1;
+    int rc = ctx->opt.k > 32                         ? count_sort<u128>(ctx, cmin, cmax, want)
+             : ctx->opt.counter == GKC_COUNTER_HASH ? count_hash(ctx, cmin, cmax, want)
+                                                    : count_sort<uint64_t>(ctx, cmin, cmax, want);
     cudaEventRecord(t1, ctx->s);
     cudaEventSynchronize(t1);
     float ms = 0;
@@ -2650,7 +2664,7 @@ int gkc_result(gkc_ctx *ctx, uint64_t *kmers, uint32_t *counts, uint64_t cap, in
     CK(cudaSetDevice(ctx->device));
     uint64_t n = std::min(cap, ctx->n_out);
     cudaMemcpyKind kind = mem == GKC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-    if (n && kmers) CK(cudaMemcpyAsync(kmers, ctx->out_k.p, n * 8, kind, ctx->s));
+    if (n && kmers) CK(cudaMemcpyAsync(kmers, ctx->out_k.p, n * 8 * ctx->res_kw, kind, ctx->s));
     if (n && counts) CK(cudaMemcpyAsync(counts, ctx->out_c.p, n * 4, kind, ctx->s));
     CK(cudaStreamSynchronize(ctx->s));
     return GKC_OK;
@@ -2675,7 +2689,7 @@ int gkc_count_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint6
     // host output with the hash counter: each group's k-mers are copied out
     // while the next group counts
     ctx->streamed = 0;
-    if (kmers && counts && out_mem == GKC_MEM_HOST && ctx->opt.counter == GKC_COUNTER_HASH) {
+    if (kmers && counts && out_mem == GKC_MEM_HOST && ctx->opt.counter == GKC_COUNTER_HASH && ctx->opt.k <= 32) {
         ctx->stream_k = kmers;
         ctx->stream_c = counts;
         ctx->stream_cap = cap;
@@ -2702,6 +2716,7 @@ int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint
     ctx->n_out = 0;
     ctx->n_distinct = 0;
     ctx->has_result = false;
+    ctx->res_kw = 1;  // the keys are u64 whatever the context's k
     if (ctx->opt.counter == GKC_COUNTER_HASH) {
         const double slots = ctx->opt.table_slots > 0 ? ctx->opt.table_slots : 0.35;
         const void *dk;

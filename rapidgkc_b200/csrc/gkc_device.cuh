@@ -138,6 +138,31 @@ __device__ __forceinline__ void for_each_kmer(const uint8_t *bytes, uint64_t e, 
     }
 }
 
+// k-mers of 33 to 64 bases: the reference's LONGERKMER build keeps them in an
+// unsigned __int128 (types.h:34-35); stored as two u64 words, low word first.
+using u128 = unsigned __int128;
+
+// for_each_kmer<true> for k <= 64: calls f(canonical u128 k-mer).
+template <class F>
+__device__ __forceinline__ void for_each_kmer_wide(const uint8_t *bytes, uint64_t e, int k, F &&f) {
+    const uint8_t *s = bytes + idx_off(e);
+    const uint32_t L = idx_len(e);
+    const u128 mask = k >= 64 ? ~(u128)0 : (((u128)1 << (2 * k)) - 1);
+    const int sh = 2 * k - 2;
+    uint32_t cur = s[0];
+    uint32_t slot = 3 - (cur >> 6);
+    uint32_t bi = 0;
+    u128 fwd = 0, rc = 0;
+    const uint32_t nbases = (uint32_t)k + L - 1;
+    for (uint32_t j = 0; j < nbases; j++) {
+        const uint32_t c = (cur >> (4 - 2 * slot)) & 3u;
+        fwd = ((fwd << 2) | c) & mask;
+        rc = (rc >> 2) | ((u128)(3u - c) << sh);
+        if (j + 1 >= (uint32_t)k) f(fwd < rc ? fwd : rc);
+        if (++slot == 3) { slot = 0; cur = s[++bi]; }
+    }
+}
+
 // Exclusive scan of one value per thread over a block of NT threads.
 // Returns the prefix; *total receives the block total.  `ws` holds NT/32
 // words of shared memory.  Must be called by every thread of the block.

@@ -11,7 +11,8 @@
 //
 // Output (-o): binary (-of bin, default): "GKCB1\0\0\0", u32 k, u32 0, u64 n,
 // then n records of u64 k-mer (2-bit, first base in the most significant
-// position, canonical) and u32 count, little-endian, 12 bytes each; or text
+// position, canonical) and u32 count, little-endian, 12 bytes each (for
+// k > 32: the k-mer's low then high u64, 20 bytes each); or text
 // (-of txt): "<k-mer>\t<count>\n".  Order: the library's (per partition;
 // ascending within a partition with -counter sort), or ascending k-mer with
 // -sorted.
@@ -270,7 +271,8 @@ std::string exe_dir() {
     return s.substr(0, s.rfind('/'));
 }
 
-void write_output(const Args &a, const uint64_t *km, const uint32_t *ct, uint64_t n) {
+// km holds kw u64 words per k-mer (kw = 2 for k > 32: low word first).
+void write_output(const Args &a, const uint64_t *km, int kw, const uint32_t *ct, uint64_t n) {
     FILE *f = std::fopen(a.out.c_str(), "wb");
     if (!f) {
         std::fprintf(stderr, "gkc_main: cannot write %s\n", a.out.c_str());
@@ -292,14 +294,16 @@ void write_output(const Args &a, const uint64_t *km, const uint32_t *ct, uint64_
         buf.insert(buf.end(), reinterpret_cast<const char *>(hk), reinterpret_cast<const char *>(hk) + 8);
         buf.insert(buf.end(), reinterpret_cast<const char *>(&n), reinterpret_cast<const char *>(&n) + 8);
         for (uint64_t i = 0; i < n; i++) {
-            buf.insert(buf.end(), reinterpret_cast<const char *>(km + i), reinterpret_cast<const char *>(km + i) + 8);
+            buf.insert(buf.end(), reinterpret_cast<const char *>(km + kw * i),
+                       reinterpret_cast<const char *>(km + kw * (i + 1)));
             buf.insert(buf.end(), reinterpret_cast<const char *>(ct + i), reinterpret_cast<const char *>(ct + i) + 4);
             if (buf.size() > (1u << 24) - 64) flush();
         }
     } else {
-        char rec[64];
+        char rec[96];
         for (uint64_t i = 0; i < n; i++) {
-            for (int j = 0; j < a.k; j++) rec[j] = "ACGT"[(km[i] >> (2 * (a.k - 1 - j))) & 3];
+            const unsigned __int128 x = kw == 2 ? ((unsigned __int128)km[2 * i + 1] << 64) | km[2 * i] : km[i];
+            for (int j = 0; j < a.k; j++) rec[j] = "ACGT"[(int)(x >> (2 * (a.k - 1 - j))) & 3];
             const int m = std::snprintf(rec + a.k, sizeof(rec) - a.k, "\t%u\n", ct[i]);
             buf.insert(buf.end(), rec, rec + a.k + m);
             if (buf.size() > (1u << 24) - 64) flush();
@@ -391,9 +395,10 @@ int main(int argc, char **argv) {
     check(gkc_count(ctx, a.cmin, a.cmax, &n_out, &n_distinct), ctx, "phase 2");
     const double t2 = secs();
     if (!a.out.empty()) {
+        const int kw = a.k > 32 ? 2 : 1;  // u64 words per k-mer
         uint64_t *km = nullptr;
         uint32_t *ct = nullptr;
-        if (cudaHostAlloc(reinterpret_cast<void **>(&km), std::max<uint64_t>(n_out, 1) * 8, 0) != cudaSuccess ||
+        if (cudaHostAlloc(reinterpret_cast<void **>(&km), std::max<uint64_t>(n_out, 1) * 8 * kw, 0) != cudaSuccess ||
             cudaHostAlloc(reinterpret_cast<void **>(&ct), std::max<uint64_t>(n_out, 1) * 4, 0) != cudaSuccess) {
             std::fprintf(stderr, "gkc_main: pinned allocation for %llu results failed\n", (unsigned long long)n_out);
             return 1;
@@ -402,13 +407,19 @@ int main(int argc, char **argv) {
         if (a.sorted) {
             std::vector<uint64_t> ix(n_out);
             for (uint64_t i = 0; i < n_out; i++) ix[i] = i;
-            std::sort(ix.begin(), ix.end(), [&](uint64_t x, uint64_t y) { return km[x] < km[y]; });
-            std::vector<uint64_t> k2(n_out);
+            auto key = [&](uint64_t i) {
+                return kw == 2 ? ((unsigned __int128)km[2 * i + 1] << 64) | km[2 * i] : (unsigned __int128)km[i];
+            };
+            std::sort(ix.begin(), ix.end(), [&](uint64_t x, uint64_t y) { return key(x) < key(y); });
+            std::vector<uint64_t> k2(n_out * kw);
             std::vector<uint32_t> c2(n_out);
-            for (uint64_t i = 0; i < n_out; i++) k2[i] = km[ix[i]], c2[i] = ct[ix[i]];
-            write_output(a, k2.data(), c2.data(), n_out);
+            for (uint64_t i = 0; i < n_out; i++) {
+                for (int w = 0; w < kw; w++) k2[kw * i + w] = km[kw * ix[i] + w];
+                c2[i] = ct[ix[i]];
+            }
+            write_output(a, k2.data(), kw, c2.data(), n_out);
         } else {
-            write_output(a, km, ct, n_out);
+            write_output(a, km, kw, ct, n_out);
         }
         cudaFreeHost(km);
         cudaFreeHost(ct);

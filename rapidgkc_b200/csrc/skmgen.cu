@@ -176,13 +176,19 @@ __device__ __forceinline__ void emit_record(const P1Params &a, uint32_t *h, uint
 
 // LOG = log2 of the largest power of two <= w (the doubling levels); LUT: the
 // key of a position is a.lut[p-mer] (an order table, already canonical), else
-// the default order over both strands.
-template <int LOG, bool LUT>
+// the default order over both strands.  KW: k > 32 (the reference's 128-bit
+// LONGERKMER build, k <= 64): a k-mer's read-boundary test spans 64 bits, and
+// LOG = 5 takes windows of 32 < w <= 62 p-mers over three chunks in
+// registers: the 32-wide minimum of this chunk and of the next, combined at
+// offset w - 32.
+template <int LOG, bool LUT, bool KW>
 __global__ void __launch_bounds__(P1_THREADS, 6)  // 6 CTAs (48 warps) per SM
 find_superkmers_kernel(P1Params a) {
     extern __shared__ uint32_t hist[];  // [3P]: bytes, superkmers, k-mers per partition
     __shared__ P1Smem sm;
-    constexpr int L2 = 1 << LOG;
+    static_assert(LOG < 5 || KW, "windows of more than 31 p-mers need k > 32");
+    constexpr bool W3 = LOG == 5;  // three-chunk window
+    constexpr int L2 = 1 << (W3 ? 4 : LOG);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int k = a.k, p = a.p, w = k - p + 1;
     const uint32_t pmask = 0xFFFFFFFFu >> (32 - 2 * p);
@@ -256,7 +262,19 @@ find_superkmers_kernel(P1Params a) {
         auto bits_at = [&](int j) -> uint32_t {  // 32 boundary bits from staged position j
             return __funnelshift_r(sm.bm[j >> 5], sm.bm[(j >> 5) + 1], j & 31);
         };
-        const uint32_t vmask = (1u << (k - 1)) - 1;  // k <= 32
+        const uint32_t vmask = (1u << ((k - 1) & 31)) - 1;  // k <= 32
+        const uint64_t vmask64 = (1ull << ((k - 1) & 63)) - 1;  // KW: k <= 64
+        // minimum over [lane, lane + 32) of the 64 keys of two chunks (W3)
+        auto win32 = [&](uint32_t ma, uint32_t mb) -> uint32_t {
+#pragma unroll
+            for (int x = 1; x < 32; x <<= 1) {
+                const uint32_t t = __shfl_sync(FULL, lane >= x ? ma : mb, (lane + x) & 31);
+                const uint32_t tb = __shfl_down_sync(FULL, mb, x);
+                ma = min(ma, t);
+                mb = min(mb, tb);
+            }
+            return ma;
+        };
         // read start of the warm-up chunk's first position: the last boundary
         // bit at or before it, else the start of the read containing sbeg.
         int64_t rs;
@@ -280,6 +298,12 @@ find_superkmers_kernel(P1Params a) {
         // pipeline: A = p-mer keys of chunk c, B = of chunk c+1
         int cj = jstrip0 - 32;
         uint32_t A = pk_at(cj + lane), B = pk_at(cj + 32 + lane);
+        // W3: C = keys of chunk c+2, F = 32-wide minima of chunk c
+        uint32_t C = 0xFFFFFFFFu, F = 0xFFFFFFFFu;
+        if (W3) {
+            C = pk_at(cj + 64 + lane);
+            F = win32(A, B);
+        }
         uint32_t carried_key = 0xFFFFFFFFu;
         bool open = false;  // a superkmer of this warp whose end is not found yet
         int64_t o_pos = 0;
@@ -290,25 +314,40 @@ find_superkmers_kernel(P1Params a) {
             if (cont && !open) break;
             if (cj > jlimit || cj >= jtotal) break;
             // ---- window minimum over w p-mers for the k-mer at cj+lane ----
-            uint32_t ma = A, mb = B;
+            uint32_t key, Fn = 0xFFFFFFFFu;
+            if (W3) {
+                // [lane, lane + w) = [lane, lane + 32) u [lane + d, lane + d + 32)
+                Fn = win32(B, C);
+                const int d = w - 32;
+                const uint32_t t = __shfl_sync(FULL, lane >= d ? F : Fn, (lane + d) & 31);
+                key = min(F, t);
+            } else {
+                uint32_t ma = A, mb = B;
 #pragma unroll
-            for (int x = 1; x < L2; x <<= 1) {
-                uint32_t t = __shfl_sync(FULL, lane >= x ? ma : mb, (lane + x) & 31);
-                uint32_t tb = __shfl_down_sync(FULL, mb, x);
-                ma = min(ma, t);
-                mb = min(mb, tb);
-            }
-            uint32_t key = ma;
-            if (w > L2) {
-                int d = w - L2;
-                uint32_t t = __shfl_sync(FULL, lane >= d ? ma : mb, (lane + d) & 31);
-                key = min(ma, t);
+                for (int x = 1; x < L2; x <<= 1) {
+                    uint32_t t = __shfl_sync(FULL, lane >= x ? ma : mb, (lane + x) & 31);
+                    uint32_t tb = __shfl_down_sync(FULL, mb, x);
+                    ma = min(ma, t);
+                    mb = min(mb, tb);
+                }
+                key = ma;
+                if (w > L2) {
+                    int d = w - L2;
+                    uint32_t t = __shfl_sync(FULL, lane >= d ? ma : mb, (lane + d) & 31);
+                    key = min(ma, t);
+                }
             }
             const int j = cj + lane;
             uint32_t prevkey = __shfl_up_sync(FULL, key, 1);
             if (lane == 0) prevkey = carried_key;
             const uint32_t bits = bits_at(j);
-            const bool valid = j >= jmin && j <= jmaxk && ((bits >> 1) & vmask) == 0;
+            bool valid;
+            if (KW) {  // no read start at j+1 .. j+k-1 (k <= 64)
+                const uint64_t b64 = bits | ((uint64_t)bits_at(j + 32) << 32);
+                valid = j >= jmin && j <= jmaxk && ((b64 >> 1) & vmask64) == 0;
+            } else {
+                valid = j >= jmin && j <= jmaxk && ((bits >> 1) & vmask) == 0;
+            }
             const bool isrs = j >= jmin && (bits & 1u);
             const bool start = valid && (isrs || key != prevkey);
             const unsigned RSB = __ballot_sync(FULL, isrs);
@@ -364,8 +403,14 @@ find_superkmers_kernel(P1Params a) {
             if (RSB) rs = sbeg + cj + 31 - __clz(RSB);
             // advance
             cj += 32;
-            A = B;
-            B = (cj + 63 < P1_STAGE - 16) ? pk_at(cj + 32 + lane) : 0xFFFFFFFFu;
+            if (W3) {
+                F = Fn;
+                B = C;
+                C = (cj + 95 < P1_STAGE - 16) ? pk_at(cj + 64 + lane) : 0xFFFFFFFFu;
+            } else {
+                A = B;
+                B = (cj + 63 < P1_STAGE - 16) ? pk_at(cj + 32 + lane) : 0xFFFFFFFFu;
+            }
         }
         // superkmer running past the staged range: finish it from global memory
         if (open) {

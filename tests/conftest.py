@@ -31,6 +31,16 @@ def ref_oracle():
         pytest.skip(str(e))
 
 
+@pytest.fixture(scope="session")
+def ref_oracle_wide():
+    """The reference's 128-bit LONGERKMER build, for k > 32."""
+    from oracle.oracle import RefOracle
+    try:
+        return RefOracle(wide=True)
+    except FileNotFoundError as e:
+        pytest.skip(str(e))
+
+
 def golden_cases():
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
 
@@ -63,5 +73,10 @@ def partition_digest(stream):
 
 
 def sorted_table(kmers, counts):
-    o = np.argsort(kmers, kind="stable")
+    """The table in ascending k-mer order (u64 keys, or (n, 2) low/high pairs
+    ordered as 128-bit values for k > 32)."""
+    if kmers.ndim == 2:
+        o = np.lexsort((kmers[:, 0], kmers[:, 1]))
+    else:
+        o = np.argsort(kmers, kind="stable")
     return kmers[o], counts[o]

@@ -1,9 +1,12 @@
 """Regenerates the golden fixtures in this directory from the reference itself.
 
 Run where the reference source tree exists (the reference's own CPU path is
-compiled from it by oracle/Makefile into oracle/_ref/libgkc_ref.so):
+compiled from it by oracle/Makefile into oracle/_ref/libgkc_ref.so, and its
+128-bit LONGERKMER build, used for k > 32, into oracle/_ref/libgkc_ref_long.so):
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle && python tests/golden/make_golden.py [case ...]
+
+(no case names: every fixture).
 
 Fixtures (inputs and the reference's outputs, all seeded):
   skm_test_vector.json  the reference's own known answer (cpu_funcs.cpp:654-676):
@@ -11,7 +14,8 @@ Fixtures (inputs and the reference's outputs, all seeded):
   <case>.npz            reads (CSR), k, p, P, the reference's per-partition
                         bytes/superkmers/k-mers (SKMStoreNoncon counters), a
                         SHA-256 of each partition's sorted superkmer multiset,
-                        and the full sorted (k-mer, count) table (cmin = 1)
+                        and the full sorted (k-mer, count) table (cmin = 1);
+                        for k > 32 the k-mers are (n, 2) u64 (low, high) pairs
 """
 from __future__ import annotations
 
@@ -101,22 +105,38 @@ CASES = {
     "edge_k31_p11_P1": (lambda: edge_reads(15), 31, 11, 1),
     "lowcomp_k31_p11_P512": (lambda: rng_reads(16, 8_000, 800, (31, 400), 0.002, alphabet=b"AAAAAAACGTAT"), 31, 11, 512),
     "k32_p16_P97": (lambda: rng_reads(17, 10_000, 500, 150, 0.004), 32, 16, 97),
+    # k > 32: the reference's LONGERKMER build
+    "wide_k45_p11_P64": (lambda: rng_reads(18, 20_000, 1000, (40, 300), 0.004), 45, 11, 64),
+    "wide_k63_p9_P31": (lambda: rng_reads(19, 15_000, 600, 150, 0.003), 63, 9, 31),
+    "wide_k64_p16_P7": (lambda: rng_reads(20, 10_000, 400, (60, 200), 0.003), 64, 16, 7),
+    "wide_edge_k33_p5_P13": (lambda: edge_reads(21), 33, 5, 13),
 }
 
 
-def main():
-    ref = RefOracle()
-    read = b"AAAAAAAAACCCCCCCAAAAAAATGA"
-    offs, mm = ref.gen_skm_offs(read, 10, 5)
-    with open(os.path.join(HERE, "skm_test_vector.json"), "w") as f:
-        json.dump({"read": read.decode(), "k": 10, "p": 5, "offsets": offs.tolist(),
-                   "minimizers": mm.tolist(), "source": "cpu_funcs.cpp:654-676 (TEST main)"}, f, indent=1)
+def table_order(km):
+    """Ascending order of a k-mer table: u64 keys, or (low, high) pairs."""
+    if km.ndim == 2:
+        return np.lexsort((km[:, 0], km[:, 1]))
+    return np.argsort(km, kind="stable")
+
+
+def main(names):
+    refs = {False: RefOracle(), True: RefOracle(wide=True)}
+    if not names:
+        read = b"AAAAAAAAACCCCCCCAAAAAAATGA"
+        offs, mm = refs[False].gen_skm_offs(read, 10, 5)
+        with open(os.path.join(HERE, "skm_test_vector.json"), "w") as f:
+            json.dump({"read": read.decode(), "k": 10, "p": 5, "offsets": offs.tolist(),
+                       "minimizers": mm.tolist(), "source": "cpu_funcs.cpp:654-676 (TEST main)"}, f, indent=1)
     for name, (make, k, p, P) in CASES.items():
+        if names and name not in names:
+            continue
+        ref = refs[k > 32]
         reads, offs = make()
         pb, ps, pk, parts = ref.phase1(reads, offs, k, p, P)
         digests = [partition_digest(s) for s in parts]
         km, ct, dist, _ = ref.count_reads(reads, offs, k, p, P)
-        order = np.argsort(km, kind="stable")
+        order = table_order(km)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), reads=reads, offs=offs, k=k, p=p, P=P,
                             part_bytes=pb, part_skms=ps, part_kmers=pk, digests=np.array(digests),
                             kmers=km[order], counts=ct[order], n_distinct=dist)
@@ -125,4 +145,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

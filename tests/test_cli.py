@@ -105,3 +105,32 @@ def test_cli_fasta_records_longer_than_a_block(oracle, tmp_path):
     assert f"distinct k-mers {do}" in p_.stderr and f"bases {len(reads)}," in p_.stderr
     _, km, ct = _read_bin(out)
     assert np.array_equal(km, ko) and np.array_equal(ct, co)
+
+
+@pytest.mark.gpu
+def test_cli_wide_kmers(oracle, tmp_path):
+    """k = 47 (the reference's 128-bit build): binary records of low word,
+    high word and count, sorted as 128-bit values; text k-mers of 47 bases."""
+    k, p, P = 47, 11, 16
+    reads, offs = random_reads(92, 20_000, 1500, (50, 300), 0.005)
+    fq, fa = _write_inputs(str(tmp_path), reads, offs)
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P, 2, U32)
+    ko, co = sorted_table(ko, co)
+    out = str(tmp_path / "wide.bin")
+    p_ = _run("-k", str(k), "-p", str(p), "-skm", str(P), "-ci", "2", "-o", out, "-sorted", "-read", fq, fa)
+    assert f"distinct k-mers {do}" in p_.stderr
+    b = open(out, "rb").read()
+    assert b[:8] == b"GKCB1\0\0\0" and int(np.frombuffer(b[8:12], np.uint32)[0]) == k
+    n = int(np.frombuffer(b[16:24], np.uint64)[0])
+    rec = np.frombuffer(b[24:], dtype=np.dtype([("lo", "<u8"), ("hi", "<u8"), ("c", "<u4")]), count=n)
+    km = np.stack([rec["lo"], rec["hi"]], axis=1)
+    assert np.array_equal(km, ko) and np.array_equal(rec["c"], co)
+    out2 = str(tmp_path / "wide.txt")
+    _run("-k", str(k), "-p", str(p), "-skm", str(P), "-ci", "2", "-o", out2, "-of", "txt", "-read", fq, fa)
+    lines = open(out2).read().split()
+    code = {"A": 0, "C": 1, "G": 2, "T": 3}
+    vals = [int("".join(str(code[ch]) for ch in s), 4) for s in lines[0::2]]
+    assert all(len(s) == k for s in lines[0::2])
+    km2 = np.array([[v & (2**64 - 1), v >> 64] for v in vals], np.uint64)
+    km2, ct2 = sorted_table(km2, np.array(lines[1::2], np.uint32))
+    assert np.array_equal(km2, ko) and np.array_equal(ct2, co)

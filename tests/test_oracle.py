@@ -72,3 +72,51 @@ def test_oracle_matches_compiled_reference(oracle, ref_oracle, k, p, P, seed):
     kb, cb, db, _ = oracle.count_reads(reads, offs, k, p, P, cmin=2)
     assert da == db
     assert np.array_equal(ka, kb) and np.array_equal(ca, cb)
+
+
+@pytest.mark.parametrize("k,p,P,seed", [(33, 11, 64, 5), (48, 13, 31, 6), (64, 16, 7, 7), (57, 3, 5, 8)])
+def test_oracle_matches_compiled_reference_wide(oracle, ref_oracle_wide, k, p, P, seed):
+    """k > 32 against the reference's 128-bit LONGERKMER build (types.h:34-35)."""
+    from tests_util import random_reads
+    reads, offs = random_reads(seed, 20_000, 500, (k - 3, 300), 0.01)
+    a = ref_oracle_wide.phase1(reads, offs, k, p, P)
+    b = oracle.skmgen(reads, offs, k, p, P)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    ka, ca, da, _ = ref_oracle_wide.count_reads(reads, offs, k, p, P, cmin=2)
+    kb, cb, db, _ = oracle.count_reads(reads, offs, k, p, P, cmin=2)
+    assert da == db and ka.shape == kb.shape and ka.ndim == 2
+    assert np.array_equal(ka, kb) and np.array_equal(ca, cb)
+
+
+def test_oracle_wide_revcomp_and_order(oracle):
+    """128-bit keys: a k=64 k-mer and its reverse complement share one
+    canonical form, and the table is ordered by (high, low)."""
+    seq = np.frombuffer(b"ACGT" * 16, np.uint8)
+    # one superkmer of k=64 bases: first byte holds 3 bases (phase 0), then
+    # full bytes, then a terminal byte with 64 % 3 = 1 base
+    def pack(s):
+        codes = {65: 0, 67: 1, 71: 2, 84: 3}
+        c = [codes[x] for x in s]
+        out = [0xC0 | (c[0] << 4) | (c[1] << 2) | c[2]]
+        i = 3
+        while len(c) - i >= 3:
+            out.append(0xC0 | (c[i] << 4) | (c[i + 1] << 2) | c[i + 2])
+            i += 3
+        rem = len(c) - i
+        last = rem << 6
+        for t in range(rem):
+            last |= c[i + t] << (4 - 2 * t)
+        out.append(last)
+        return np.array(out, np.uint8)
+    a = oracle.extract(pack(bytes(seq)), 64)
+    comp = bytes(b"TGCA"[b"ACGT".index(x)] for x in bytes(seq)[::-1])
+    b = oracle.extract(pack(comp), 64)
+    assert a.shape == (1, 2) and np.array_equal(a, b)
+    # ACGT repeated is its own reverse complement: the value itself
+    v = 0
+    for x in bytes(seq):
+        v = (v << 2) | b"ACGT".index(x)
+    assert int(a[0, 0]) == v & (2**64 - 1) and int(a[0, 1]) == v >> 64
+    keys = np.array([[5, 1], [9, 0], [5, 1], [0, 2]], np.uint64)
+    km, ct, d = oracle.count(keys)
+    assert d == 3 and km.tolist() == [[9, 0], [5, 1], [0, 2]] and ct.tolist() == [1, 2, 1]
