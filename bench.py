@@ -122,7 +122,7 @@ def cpu_baseline(args, threads):
     """The reference's CPU path (oracle/_ref) on a bounded sample of the workload."""
     from oracle.oracle import RefOracle
     from rapidgkc_b200 import synth
-    ref = RefOracle()
+    ref = RefOracle(wide=args.k > 32)  # the reference's 128-bit LONGERKMER build for k > 32
     reads, offs = synth.make_workload(args.workload, read_fraction=args.cpu_fraction, threads=threads)
     t0 = time.perf_counter()
     d, t1, t2 = ref.run(reads, offs, args.k, args.p, args.partitions, threads)
@@ -150,7 +150,7 @@ def run_reference(args, rank, world):
     base["value"] = v
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Gbp/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "u128" if args.k > 32 else "u64", "data": "synthetic",
             "config": {"workload": args.workload, "k": args.k, "p": args.p, "partitions": args.partitions,
                        "threshold": ">=2", "sample_fraction": args.cpu_fraction},
             "cpu_baseline": base,
@@ -264,6 +264,8 @@ def main():
         """Order-independent digest of the (k-mer, count) result (of the
         whole job: every rank holds its partitions' k-mers)."""
         km, ct = c.result()
+        if km.ndim == 2:  # k > 32: (low, high) words folded into one u64 per k-mer
+            km = km[:, 0] ^ (km[:, 1] * np.uint64(0x9E3779B97F4A7C15))
         d = [int(np.bitwise_xor.reduce(km)) if len(km) else 0,
              int(np.sum(km * ct.astype(np.uint64), dtype=np.uint64)), int(ct.sum(dtype=np.uint64))]
         if world > 1:
@@ -347,7 +349,8 @@ def main():
             pos = int(offs[cuts[-1]])
         batch_reads = np.diff(np.concatenate([[0], cuts])).astype(np.uint64)
         cap = int(n_out * 1.05) + 1024
-        hk = torch.empty(cap, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+        kw = 2 if args.k > 32 else 1  # u64 words per k-mer
+        hk = torch.empty((cap, kw) if kw == 2 else cap, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
         hc = torch.empty(cap, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
 
         def step_batched():
@@ -380,7 +383,8 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ems = float(t.item())
         e2e = {"value": bases * world / (ems / 1e3) / 1e9, "unit": "Gbp/s",
-               "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)), "d2h_bytes_per_step": int(12 * (xinfo.get("local_kept", no) if exchange else no)),
+               "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)),
+               "d2h_bytes_per_step": int((8 * kw + 4) * (xinfo.get("local_kept", no) if exchange else no)),
                "ms_per_step": ems, "path": "gkc_add_reads_batches + gkc_count + gkc_result"}
         sizes = np.diff(offs[np.concatenate([[0], cuts])].astype(np.int64)) / (1 << 20)
         batching = {"batches_per_step": len(batch_reads), "batch_mb_min": float(sizes.min()),
@@ -390,7 +394,8 @@ def main():
                     "note": "latency = one batch's host-to-device copy start to its phase-1 end (CUDA events)"}
     elif not args.no_e2e:
         cap = int(n_out * 1.05) + 1024
-        hk = torch.empty(cap, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+        kw = 2 if args.k > 32 else 1  # u64 words per k-mer
+        hk = torch.empty((cap, kw) if kw == 2 else cap, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
         hc = torch.empty(cap, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
         def step_host():
             if exchange:
@@ -415,20 +420,23 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ems = float(t.item())
         e2e = {"value": bases * world / (ems / 1e3) / 1e9, "unit": "Gbp/s",
-               "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)), "d2h_bytes_per_step": int(12 * (xinfo.get("local_kept", no) if exchange else no)),
+               "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)),
+               "d2h_bytes_per_step": int((8 * kw + 4) * (xinfo.get("local_kept", no) if exchange else no)),
                "ms_per_step": ems}
 
     # ---- roofline of the dominant kernel class ----
     hbm, src = peaks()
     # counting phase (phase 2) against byte models: the compulsory traffic
-    # (superkmer bytes read once + 12-byte output records) and the LSD-sort
-    # path's (superkmers + 8 B key write + 16 B per k-mer per 8-bit digit pass
-    # over 2k bits + 8 B run-length read + output)
+    # (superkmer bytes read once + output records of a key and a u32 count)
+    # and the LSD-sort path's (superkmers + key write + a key read and write
+    # per k-mer per 8-bit digit pass over 2k bits + run-length read + output);
+    # keys are 8 B, 16 B for k > 32
     N, S = main_run["kmer_instances"], main_run["store_bytes"]
     p2 = tstats["phase2_ms"] / 1e3
     passes = -(-2 * args.k // 8)
-    comp = S + 12 * n_out
-    sort_model = S + 8 * N + 16 * N * passes + 8 * N + 12 * n_out
+    kbytes = 16 if args.k > 32 else 8
+    comp = S + (kbytes + 4) * n_out
+    sort_model = S + kbytes * N + 2 * kbytes * N * passes + kbytes * N + (kbytes + 4) * n_out
     counting = {"ms_per_step": tstats["phase2_ms"], "kmer_instances": N, "store_bytes": S,
                 "compulsory_bytes": comp, "compulsory_gbs": comp / p2 / 1e9,
                 "sort_model_bytes": sort_model, "sort_model_gbs": sort_model / p2 / 1e9,
@@ -450,7 +458,7 @@ def main():
 
     line = {"metric": METRIC, "value": value, "unit": "Gbp/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "u128" if args.k > 32 else "u64", "data": "synthetic",
             "config": {"workload": args.workload, "desc": WORKLOAD_DESC.get(args.workload, ""),
                        "bases_per_rank": bases, "reads_per_rank": len(offs) - 1, "k": args.k, "p": args.p,
                        "partitions": args.partitions, "counter": args.counter, "order": args.order,
