@@ -11,7 +11,9 @@
 //            superkmers and k-mers per sub-bucket (shared-memory aggregated),
 //            a scan, then a scatter of 16-byte entries {first byte address,
 //            k-mer count} into sub-bucket order;
-//   count    one CTA per sub-bucket: warps decode their superkmers 32 quads
+//   count    one CTA per sub-bucket: warps take groups of 32 superkmers from
+//            a shared-memory counter (groups differ in k-mers, so a fixed
+//            round robin left warps idle at the barrier), decode them 32 quads
 //            of consecutive k-mers at a time (warp_kmer_runs below), merge equal
 //            neighbouring k-mers into runs, and add the runs to a shared-memory table with
 //            shared-memory atomics; then the k-mers whose count lies in
@@ -112,11 +114,15 @@ __device__ __forceinline__ void warp_kmer_runs(const BEntry *ent, uint64_t b, ui
         // 48 bases, slot 0 in bits 95-94
         const unsigned __int128 v = ((unsigned __int128)pack6x8(lo) << 48) | pack6x8(hi);
         uint64_t x = (uint64_t)(v >> (96 - 2 * (s + (uint32_t)k))) & mask;
+        // the quad's KQ-1 entering bases (slots s+k .. s+k+KQ-2), the last in bits 1-0
+        const uint32_t nxt = (uint32_t)(v >> (96 - 2 * (s + (uint32_t)k + KQ - 1)));
         uint64_t r = rc64(x, k);
         uint64_t last = x < r ? x : r;
         uint32_t run = 1;
-        for (uint32_t t = 1; t < nk; t++) {
-            const uint32_t bt = (uint32_t)(v >> (94 - 2 * (s + (uint32_t)k + t - 1))) & 3u;  // the entering base
+#pragma unroll
+        for (uint32_t t = 1; t < (uint32_t)KQ; t++) {
+            if (t >= nk) break;
+            const uint32_t bt = (nxt >> (2 * (KQ - 1 - t))) & 3u;  // the entering base
             x = ((x << 2) | bt) & mask;
             r = (r >> 2) | ((uint64_t)(3u - bt) << (2 * k - 2));
             const uint64_t key = x < r ? x : r;
@@ -385,14 +391,21 @@ bucket_count_kernel(BCountParams a) {
         tk[t] = EMPTY_KEY;
         tc[t] = 0;
     }
-    if (threadIdx.x == 0) over = 0;
+    __shared__ uint32_t next_grp;  // the next group of 32 entries to take
+    if (threadIdx.x == 0) {
+        over = 0;
+        next_grp = BC_THREADS / 32;
+    }
     __syncthreads();
-    const int warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint64_t mask = kmask(a.k);
-    for (uint64_t bb = e0 + (uint64_t)warp * 32; bb < e1; bb += BC_THREADS) {
+    for (uint64_t bb = e0 + (uint64_t)warp * 32; bb < e1;) {
         if (__any_sync(FULL, over != 0)) break;  // a warp vote: the warp leaves together
         warp_kmer_runs(a.entries, bb, e1, a.k, mask,
                        [&](uint64_t key, uint32_t run) { smem_add<TS>(tk, tc, &over, key, run); });
+        uint32_t g = 0;
+        if (lane == 0) g = atomicAdd(&next_grp, 1u);
+        bb = e0 + 32ull * __shfl_sync(FULL, g, 0);
     }
     __syncthreads();
     if (over) {
