@@ -168,8 +168,9 @@ static_assert(sizeof(TileDesc) == 32, "tile layout");
 
 constexpr int RS_THREADS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
-constexpr int RS_ITEMS = 16;
-constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // 4096 keys
+// keys per thread: 16 u64, or 8 u128 (the scatter holds them in registers)
+template <class KT> constexpr int rs_items() { return sizeof(KT) == 16 ? 8 : 16; }
+template <class KT> constexpr int rs_tile() { return RS_THREADS * rs_items<KT>(); }
 
 template <int RB, class KT>
 __global__ void __launch_bounds__(RS_THREADS)
@@ -181,7 +182,7 @@ radix_hist_kernel(const KT *keys, const TileDesc *tiles, int shift, uint32_t *co
     __syncthreads();
     const uint64_t dmask = NB - 1;
 #pragma unroll 4
-    for (int i = 0; i < RS_ITEMS; i++) {
+    for (int i = 0; i < rs_items<KT>(); i++) {
         uint32_t j = (uint32_t)i * RS_THREADS + threadIdx.x;
         if (j < td.n) atomicAdd(&hist[(uint32_t)((keys[td.start + j] >> shift) & dmask)], 1u);
     }
@@ -201,12 +202,12 @@ radix_scatter_kernel(const KT *in, KT *out, const TileDesc *tiles, int shift, co
     for (int d = threadIdx.x; d < RS_WARPS * NB; d += RS_THREADS) (&wcnt[0][0])[d] = 0;
     __syncthreads();
     const uint64_t dmask = NB - 1;
-    KT key[RS_ITEMS];
-    uint32_t rank[RS_ITEMS];
+    KT key[rs_items<KT>()];
+    uint32_t rank[rs_items<KT>()];
     // warp-striped: warp w owns keys [w*32*ITEMS, (w+1)*32*ITEMS) of the tile
 #pragma unroll
-    for (int i = 0; i < RS_ITEMS; i++) {
-        uint32_t j = (uint32_t)warp * 32 * RS_ITEMS + (uint32_t)i * 32 + lane;
+    for (int i = 0; i < rs_items<KT>(); i++) {
+        uint32_t j = (uint32_t)warp * 32 * rs_items<KT>() + (uint32_t)i * 32 + lane;
         bool valid = j < td.n;
         key[i] = valid ? in[td.start + j] : KT(0);
         unsigned act = __ballot_sync(FULL, valid);
@@ -234,8 +235,8 @@ radix_scatter_kernel(const KT *in, KT *out, const TileDesc *tiles, int shift, co
     }
     __syncthreads();
 #pragma unroll
-    for (int i = 0; i < RS_ITEMS; i++) {
-        uint32_t j = (uint32_t)warp * 32 * RS_ITEMS + (uint32_t)i * 32 + lane;
+    for (int i = 0; i < rs_items<KT>(); i++) {
+        uint32_t j = (uint32_t)warp * 32 * rs_items<KT>() + (uint32_t)i * 32 + lane;
         if (j < td.n) {
             uint32_t dig = (uint32_t)((key[i] >> shift) & dmask);
             uint64_t pos = offsets[td.cnt_base + (uint64_t)dig * td.nt + td.t] + wcnt[warp][dig] + rank[i];

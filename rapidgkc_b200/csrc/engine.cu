@@ -1547,6 +1547,7 @@ int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t
     std::vector<TileDesc> td;
     uint64_t start = 0, cnt_base = 0;
     for (uint64_t sz : segs) {
+        constexpr uint64_t RS_TILE = rs_tile<KT>();
         uint32_t nt = (uint32_t)((sz + RS_TILE - 1) / RS_TILE);
         for (uint32_t t = 0; t < nt; t++) {
             TileDesc d;
