@@ -35,13 +35,13 @@ def _range_table(o, reads, offs, k, p, P, p0, p1, cmin):
     return o.count(o.extract(st[int(po[p0]):int(po[p1])], k), cmin)
 
 
-def oracle_exchange(rank, world, port, seed):
+def oracle_exchange(rank, world, port, seed, k=25):
     """Each rank packs the oracle's phase-1 output of its read shard (the
     partition streams, with an index tagging the source rank and keys naming
     each superkmer's partition), exchanges it with exchange_packed over gloo,
     and counts its range with the oracle: the result must equal the
     single-process oracle's for that range, and the distinct totals must add
-    up to the whole input's."""
+    up to the whole input's.  k > 32 gives 128-bit (low, high) k-mer tables."""
     import torch
     import torch.distributed as dist
 
@@ -51,7 +51,7 @@ def oracle_exchange(rank, world, port, seed):
         from rapidgkc_b200.exchange import exchange_packed, partition_ranges
 
         o = Oracle()
-        k, p, P = 25, 9, 24
+        p, P = 9, 24
         reads, offs = random_reads(seed, 20_000, 1500, (40, 200), 0.01)
         sr, so = _shard(reads, offs, rank, world)
         pb, ps, pk, _, stream = o.skmgen(sr, so, k, p, P)

@@ -34,6 +34,6 @@ def test_partition_ranges_edge_cases():
         partition_ranges([1, 2], 0)
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_exchange_over_gloo_matches_oracle(world):
-    mp.spawn(dist_workers.oracle_exchange, args=(world, dist_workers.free_port(), 31), nprocs=world, join=True)
+@pytest.mark.parametrize("world,k", [(2, 25), (3, 25), (2, 45)])
+def test_exchange_over_gloo_matches_oracle(world, k):
+    mp.spawn(dist_workers.oracle_exchange, args=(world, dist_workers.free_port(), 31, k), nprocs=world, join=True)
