@@ -339,6 +339,45 @@ int gkc_count_keys_noalloc(const uint64_t *keys, uint64_t n, uint32_t cmin, uint
                            uint32_t *out_counts, uint64_t out_cap, uint64_t *n_out, uint64_t *n_distinct,
                            void *stream);
 
+/* ---- the boundary in five calls ------------------------------------------
+ * One call per step of the reference's GPU interface, each a thin form of the
+ * calls above; every one returns a GKC_* status (the reference exits on
+ * errors instead, CUDA_CHECK in utilities.hpp).
+ *
+ * gkc_init: device setup, in place of GPUReset (gpu_skmgen.h:52), which
+ * resets the device; this one does not.  Same as gkc_create. */
+int gkc_init(int device, const gkc_options *config, gkc_ctx **out);
+
+/* gkc_skmgen_batch: one phase-1 batch, in place of GenSuperkmerGPU
+ * (gpu_skmgen.h:54-58): the batch's superkmers are appended to the
+ * context's partition store (gkc_add_reads), and part_bytes / part_skms /
+ * part_kmers (P entries each, may be NULL) receive the store's totals per
+ * partition, the counters GenSuperkmerGPU leaves in each SKMStoreNoncon
+ * (tot_size_bytes, skm_cnt, kmer_cnt; skmstore.hpp:85-87).  k, p and P must
+ * be the context's (GKC_EINVAL otherwise).  order_lut (4^p ranks, host
+ * memory) installs a minimizer order as gkc_set_order does; only while the
+ * store is empty (GKC_ESTATE otherwise), since one store holds one order. */
+int gkc_skmgen_batch(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads, int k, int p, int P,
+                     const uint32_t *order_lut, int mem, uint64_t *part_bytes, uint64_t *part_skms,
+                     uint64_t *part_kmers);
+
+/* gkc_count_partition: phase 2 of one partition, the per-store step of
+ * kmc_counting_GPU_streams (gpu_kmercounting.h:14-17): counts partition
+ * `part` (gkc_count_partitions with one id), keeps counts in [cmin, cmax],
+ * and copies its (k-mer, count) table to kmers / counts (cap entries, in
+ * `mem`; two words per k-mer for k > 32) when they are given; a table larger
+ * than cap is GKC_EINVAL with *n_out set.  *n_distinct = the partition's
+ * distinct k-mers (the reference's return value). */
+int gkc_count_partition(gkc_ctx *ctx, int part, uint32_t cmin, uint32_t cmax, uint64_t *kmers, uint32_t *counts,
+                        uint64_t cap, int mem, uint64_t *n_out, uint64_t *n_distinct);
+
+/* gkc_set_order_lut: gkc_set_order with a host table of 4^p ranks (NULL: the
+ * default order, minimizer_filter.h:20). */
+int gkc_set_order_lut(gkc_ctx *ctx, const uint32_t *lut);
+
+/* gkc_shutdown: releases the context (gkc_destroy). */
+int gkc_shutdown(gkc_ctx *ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,7 @@ EXPORTS = (
     "gkc_last_timings", "gkc_kernel_launches", "gkc_set_stream", "gkc_set_profiling", "gkc_kernel_stats",
     "gkc_mlp_param_count", "gkc_minimizer_loads", "gkc_mlp_grad", "gkc_mlp_train", "gkc_mlp_scores",
     "gkc_mlp_order", "gkc_count_keys_noalloc",
+    "gkc_init", "gkc_skmgen_batch", "gkc_count_partition", "gkc_set_order_lut", "gkc_shutdown",
 )
 KERNEL_CLASSES = ("find_superkmers", "scatter_superkmers", "hash_insert", "hash_collect", "sort_extract",
                   "radix_hist", "radix_scatter", "scan", "rle")
@@ -118,6 +119,11 @@ def load_library(path: str = LIB_PATH):
     L.gkc_mlp_scores.argtypes = [vp, vp, vp, i32]
     L.gkc_mlp_order.argtypes = [vp, vp, u64, vp]
     L.gkc_count_keys_noalloc.argtypes = [vp, u64, u32, u32, vp, vp, u64, C.POINTER(u64), C.POINTER(u64), vp]
+    L.gkc_init.argtypes = [i32, C.POINTER(Options), C.POINTER(vp)]
+    L.gkc_skmgen_batch.argtypes = [vp, vp, vp, u64, i32, i32, i32, vp, i32, vp, vp, vp]
+    L.gkc_count_partition.argtypes = [vp, i32, u32, u32, vp, vp, u64, i32, C.POINTER(u64), C.POINTER(u64)]
+    L.gkc_set_order_lut.argtypes = [vp, vp]
+    L.gkc_shutdown.argtypes = [vp]
     for name in EXPORTS:
         if name not in ("gkc_default_options", "gkc_last_error", "gkc_strerror", "gkc_kernel_launches",
                         "gkc_mlp_param_count"):

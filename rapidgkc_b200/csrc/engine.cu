@@ -2659,6 +2659,48 @@ int gkc_count_partitions(gkc_ctx *ctx, const int32_t *parts, uint64_t n, uint32_
     return GKC_OK;
 }
 
+// ---- the boundary in five calls (thin forms of the calls in this file) ----
+int gkc_init(int device, const gkc_options *config, gkc_ctx **out) { return gkc_create(device, config, out); }
+
+int gkc_skmgen_batch(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_t n_reads, int k, int p, int P,
+                     const uint32_t *order_lut, int mem, uint64_t *part_bytes, uint64_t *part_skms,
+                     uint64_t *part_kmers) {
+    if (!ctx) return GKC_EINVAL;
+    if (k != ctx->opt.k || p != ctx->opt.p || P != ctx->opt.partitions)
+        return ctx->fail(GKC_EINVAL, "k, p and P of a batch must be the context's (%d, %d, %d)", ctx->opt.k,
+                         ctx->opt.p, ctx->opt.partitions);
+    if (order_lut) {
+        if (!ctx->store.empty()) return ctx->fail(GKC_ESTATE, "the order of a non-empty store cannot change");
+        RET(gkc_set_order(ctx, order_lut, 1ull << (2 * p), GKC_MEM_HOST));
+    }
+    RET(gkc_add_reads(ctx, reads, offs, n_reads, mem));
+    return gkc_store_stats(ctx, part_bytes, part_skms, part_kmers);
+}
+
+int gkc_count_partition(gkc_ctx *ctx, int part, uint32_t cmin, uint32_t cmax, uint64_t *kmers, uint32_t *counts,
+                        uint64_t cap, int mem, uint64_t *n_out, uint64_t *n_distinct) {
+    if (!ctx) return GKC_EINVAL;
+    const int32_t id = part;
+    uint64_t no = 0, nd = 0;
+    RET(gkc_count_partitions(ctx, &id, 1, cmin, cmax, &no, &nd));
+    if (n_out) *n_out = no;
+    if (n_distinct) *n_distinct = nd;
+    if (kmers || counts) {
+        if (cap < no)
+            return ctx->fail(GKC_EINVAL, "output buffer too small (%llu < %llu)", (unsigned long long)cap,
+                             (unsigned long long)no);
+        RET(gkc_result(ctx, kmers, counts, cap, mem));
+    }
+    return GKC_OK;
+}
+
+int gkc_set_order_lut(gkc_ctx *ctx, const uint32_t *lut) {
+    if (!ctx) return GKC_EINVAL;
+    return gkc_set_order(ctx, lut, 1ull << (2 * ctx->opt.p), GKC_MEM_HOST);
+}
+
+int gkc_shutdown(gkc_ctx *ctx) { return gkc_destroy(ctx); }
+
 int gkc_result(gkc_ctx *ctx, uint64_t *kmers, uint32_t *counts, uint64_t cap, int mem) {
     if (!ctx) return GKC_EINVAL;
     if (!ctx->has_result) return ctx->fail(GKC_ESTATE, "no result: call gkc_count first");
