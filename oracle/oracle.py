@@ -156,6 +156,9 @@ class RefOracle:
         L.ref_phase1.argtypes = [_u8p, _u64p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int,
                                  _u64p, _u64p, _u64p]
         L.ref_phase1.restype = C.c_void_p
+        L.ref_phase1_hpc.argtypes = [_u8p, _u64p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                     _u64p, _u64p, _u64p]
+        L.ref_phase1_hpc.restype = C.c_void_p
         L.ref_part_bytes.argtypes = [C.c_void_p, C.c_int, _u8p]
         L.ref_part_bytes.restype = C.c_int64
         L.ref_count_bytes.argtypes = [_u8p, C.c_uint64, C.c_uint64, C.c_int, C.c_uint32, C.c_uint32,
@@ -173,12 +176,14 @@ class RefOracle:
         n = self.lib.ref_gen_skm_offs(read, len(read), k, p, offs, mm)
         return offs[: n + 1].copy(), mm[:n].copy()
 
-    def phase1(self, reads, offs, k, p, P, threads=1):
-        """Returns (part_bytes, part_skms, part_kmers, list of per-partition byte arrays)."""
+    def phase1(self, reads, offs, k, p, P, threads=1, hpc=False):
+        """Returns (part_bytes, part_skms, part_kmers, list of per-partition byte arrays).
+        hpc: the reference's CPU homopolymer compression (every read must stay
+        at least k + 1 bytes long after it)."""
         reads = np.ascontiguousarray(reads, np.uint8)
         offs = np.ascontiguousarray(offs, np.uint64)
         pb = np.zeros(P, np.uint64); ps = np.zeros(P, np.uint64); pk = np.zeros(P, np.uint64)
-        h = self.lib.ref_phase1(reads, offs, len(offs) - 1, k, p, P, threads, pb, ps, pk)
+        h = self.lib.ref_phase1_hpc(reads, offs, len(offs) - 1, k, p, P, threads, int(hpc), pb, ps, pk)
         try:
             parts = []
             for i in range(P):
@@ -203,9 +208,9 @@ class RefOracle:
             raise ValueError("reference extraction disagreed with the partition k-mer count")
         return ok[:w].copy(), oc[:w].copy(), int(d.value)
 
-    def count_reads(self, reads, offs, k, p, P, cmin=1, cmax=0xFFFFFFFF, threads=1):
+    def count_reads(self, reads, offs, k, p, P, cmin=1, cmax=0xFFFFFFFF, threads=1, hpc=False):
         """Whole reference path; output ordered by partition, ascending within."""
-        pb, ps, pk, parts = self.phase1(reads, offs, k, p, P, threads)
+        pb, ps, pk, parts = self.phase1(reads, offs, k, p, P, threads, hpc)
         ks, cs, dist = [], [], 0
         for i in range(P):
             a, b, d = self.count_bytes(parts[i], int(pk[i]), k, cmin, cmax)

@@ -62,7 +62,7 @@ std::vector<u_char> drain_store(SKMStoreNoncon *s) {
 // loader's thread pool, fileloader.hpp:492-525).  GenSuperkmerCPU packs each
 // read in place, so it is given a private copy of the reads.
 void run_phase1(std::vector<char> &buf, const uint64_t *offs, int64_t n_reads, int k, int p,
-                int P, int threads, int batch, std::vector<SKMStoreNoncon *> &stores) {
+                int P, int threads, int batch, std::vector<SKMStoreNoncon *> &stores, bool hpc = false) {
     std::atomic<int64_t> next{0};
     auto worker = [&](int tid) {
         for (;;) {
@@ -77,7 +77,7 @@ void run_phase1(std::vector<char> &buf, const uint64_t *offs, int64_t n_reads, i
                 reads.push_back(ReadPtr{buf.data() + offs[r], len});
             }
             if (!reads.empty())
-                GenSuperkmerCPU(reads, (T_kvalue)k, (T_kvalue)p, false, P, stores, tid);
+                GenSuperkmerCPU(reads, (T_kvalue)k, (T_kvalue)p, hpc, P, stores, tid);
         }
     };
     std::vector<std::thread> ts;
@@ -99,12 +99,25 @@ int ref_gen_skm_offs(const char *read, int len, int k, int p, int *offs, unsigne
 // Phase 1 of the reference over a CSR batch.  Fills per-partition bytes,
 // superkmer and k-mer counts, and returns an opaque handle holding the
 // partition stores.
+void *ref_phase1_hpc(const char *reads, const uint64_t *offs, int64_t n_reads, int k, int p, int P,
+                     int threads, int hpc, uint64_t *part_bytes, uint64_t *part_skms, uint64_t *part_kmers);
+
 void *ref_phase1(const char *reads, const uint64_t *offs, int64_t n_reads, int k, int p, int P,
                  int threads, uint64_t *part_bytes, uint64_t *part_skms, uint64_t *part_kmers) {
+    return ref_phase1_hpc(reads, offs, n_reads, k, p, P, threads, 0, part_bytes, part_skms, part_kmers);
+}
+
+// ref_phase1 with the reference's CPU homopolymer compression on or off
+// (GenSuperkmerCPU's HPC argument, cpu_funcs.cpp:253-275).  Every read must
+// stay at least k + 1 bytes long after compression: the reference's
+// _hpc_encoding returns the compressed length minus one (cpu_funcs.cpp:92-100),
+// and a read left shorter than k is read past its end (cpu_funcs.cpp:124-146).
+void *ref_phase1_hpc(const char *reads, const uint64_t *offs, int64_t n_reads, int k, int p, int P,
+                     int threads, int hpc, uint64_t *part_bytes, uint64_t *part_skms, uint64_t *part_kmers) {
     std::vector<char> buf(reads, reads + offs[n_reads]);
     auto *res = new Phase1Result();
     for (int i = 0; i < P; i++) res->stores.push_back(new SKMStoreNoncon(i, false));
-    run_phase1(buf, offs, n_reads, k, p, P, threads, 2000, res->stores);
+    run_phase1(buf, offs, n_reads, k, p, P, threads, 2000, res->stores, hpc != 0);
     for (int i = 0; i < P; i++) {
         part_bytes[i] = res->stores[i]->tot_size_bytes;
         part_skms[i] = res->stores[i]->skm_cnt;

@@ -18,6 +18,29 @@ def test_oracle_known_answers():
     assert ho.tolist() == [0, 4, 4, 5, 8, 9, 11]   # a read's first byte is kept even after an equal one
 
 
+@pytest.mark.parametrize("k,p,P", [(31, 11, 64), (21, 9, 7)])
+def test_oracle_pinned_to_the_reference_cpu_path(oracle, ref_oracle, k, p, P):
+    """The reference's CPU phase 1 with HPC on (GenSuperkmerCPU,
+    cpu_funcs.cpp:253-275) counts each compressed read without its last base:
+    its _hpc_encoding returns the last index, not the length
+    (cpu_funcs.cpp:92-100).  Its GPU path (GPU_HPCEncoding,
+    gpu_skmgen.cu:145-173), which the B200 path follows, keeps that base.
+    So the reference CPU table is the oracle's table of the compressed reads
+    with each read's last byte dropped."""
+    reads, offs = random_reads(31, 30_000, 800, (120, 300), 0.01)
+    hr, ho = hpc(reads, offs)
+    assert np.diff(ho.astype(np.int64)).min() > k  # the reference reads past shorter reads
+    keep = np.ones(len(hr), bool)
+    keep[ho[1:].astype(np.int64) - 1] = False
+    short_r = hr[keep]
+    short_o = (ho.astype(np.int64) - np.arange(len(ho))).astype(np.uint64)
+    ka, ca, da, pka = ref_oracle.count_reads(reads, offs, k, p, P, 1, hpc=True)
+    kb, cb, db, pkb = oracle.count_reads(short_r, short_o, k, p, P, 1)
+    assert da == db and np.array_equal(pka, pkb)
+    assert np.array_equal(ka, kb) and np.array_equal(ca, cb)
+    assert oracle.count_reads(hr, ho, k, p, P, 1)[2] != da  # the dropped bases matter
+
+
 def _reads_with_runs(seed):
     r = np.random.default_rng(seed)
     acgt = np.frombuffer(b"ACGT", np.uint8)
