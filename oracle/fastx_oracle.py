@@ -9,6 +9,11 @@ loader carries `is_read_line` from one buffer to the next.  A read line is
 kept whole except for '\\r' bytes (the reference keeps a trailing '\\r' in the
 read, where it becomes an invalid base; dropping it keeps CRLF files exact).
 
+Pinned to the compiled reference: tests/test_fastx.py runs the reference's
+own ReadLoader (as oracle/_ref/ref_load_reads) on multi-megabyte FASTQ and
+single-line FASTA files read in 1 MB buffers, and its reads equal these, in
+order (empty reads aside, which the loader skips and which hold no k-mer).
+
 FASTA: a record is a '>' header line and the sequence lines up to the next
 header, concatenated without '\\r'.  The reference loader instead takes every
 second line (`flag_mask = 0b1`, :203), which is right only for single-line

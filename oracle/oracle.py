@@ -224,3 +224,24 @@ class RefOracle:
         t1 = C.c_double(0); t2 = C.c_double(0)
         d = self.lib.ref_run(reads, offs, len(offs) - 1, k, p, P, threads, C.byref(t1), C.byref(t2))
         return int(d), t1.value, t2.value
+
+
+def ref_load_reads(path: str, buffer_mb: int = 1, timeout: float = 120.0) -> list:
+    """The reads of a FASTQ / FASTA file (FASTA when the name ends in 'a') as
+    the reference's ReadLoader extracts them (fileloader.hpp:51-545), run as
+    the program oracle/_ref/ref_load_reads in a process of its own."""
+    import subprocess
+    import tempfile
+    exe = os.path.join(HERE, "_ref", "ref_load_reads")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(f"{exe} missing: run `make -C oracle ref` where the reference tree exists")
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "reads.bin")
+        p = subprocess.run([exe, path, str(buffer_mb), out], capture_output=True, timeout=timeout)
+        if p.returncode != 0:
+            raise RuntimeError(f"reference loader failed ({p.returncode}): {p.stderr[-500:]!r}")
+        b = open(out, "rb").read()
+    n = int(np.frombuffer(b[:8], np.uint64)[0])
+    offs = np.frombuffer(b[8:8 + 8 * (n + 1)], np.uint64).astype(np.int64)
+    data = b[8 + 8 * (n + 1):]
+    return [data[offs[i]:offs[i + 1]] for i in range(n)]

@@ -12,12 +12,14 @@
 //   _h_process_bytes  cpu_funcs.cpp:437-515  (superkmer bytes -> canonical k-mers)
 //   sort_kmers        cpu_funcs.cpp:365-392  (in-tree MSD radix + std::sort)
 //   KmerCountingCPU   cpu_funcs.cpp:586-651  (phase 2 of one partition)
+//   ReadLoader        fileloader.hpp:51-545  (FASTQ / FASTA record extraction)
 //
 // oracle/Makefile builds it twice: libgkc_ref.so with the reference's default
 // 64-bit T_kmer (k <= 32) and libgkc_ref_long.so with -DLONGERKMER, the
 // reference's own 128-bit build for k <= 64 (types.h:34-35, CMakeLists.txt
 // target l_<name>).
 #include "cpu_funcs.h"
+#include "fileloader.hpp"
 #include "utilities.hpp"
 
 #include <atomic>
@@ -175,6 +177,37 @@ int64_t ref_count_bytes(const uint8_t *bytes, uint64_t nbytes, uint64_t n_kmers,
     }
     *n_distinct = d;
     return w;
+}
+
+// The reads of a FASTQ or FASTA file (FASTA when the name ends in 'a') as
+// the reference's loader extracts them (ReadLoader::work_while_loading,
+// fileloader.hpp:492-525; no length filter, one worker, buffers of
+// buffer_mb MB so that lines cross buffer boundaries).  The loader hands
+// reads over in batches; they are returned in the order the worker received
+// them.  Writes at most cap bytes to out and cap_reads + 1 offsets; returns
+// the number of reads, or -1 when out or offs is too small.
+int64_t ref_load_reads(const char *path, int buffer_mb, char *out, uint64_t cap, uint64_t *offs,
+                       uint64_t cap_reads) {
+    std::vector<std::string> files{path};
+    std::vector<std::string> got;
+    std::mutex mu;
+    ReadLoader::work_while_loading(
+        0,
+        [&](std::vector<ReadPtr> &batch, int) {
+            std::lock_guard<std::mutex> lk(mu);
+            for (const ReadPtr &r : batch) got.emplace_back(r.read, r.len);
+        },
+        1, files, 4096, 64, buffer_mb);
+    uint64_t o = 0;
+    if (got.size() > cap_reads) return -1;
+    offs[0] = 0;
+    for (size_t i = 0; i < got.size(); i++) {
+        if (o + got[i].size() > cap) return -1;
+        memcpy(out + o, got[i].data(), got[i].size());
+        o += got[i].size();
+        offs[i + 1] = o;
+    }
+    return (int64_t)got.size();
 }
 
 // Bits of the reference's T_kmer in this build (64, or 128 under LONGERKMER).

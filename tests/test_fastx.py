@@ -21,6 +21,32 @@ def test_oracle_known_answers():
     assert parse_fastx(b">1\nAAC\n>2\nGGT\n", "fasta")[0] == [b"AAC", b"GGT"]
 
 
+@pytest.mark.parametrize("fmt", ["fastq", "fasta"])
+def test_oracle_pinned_to_the_reference_loader(tmp_path, fmt):
+    """The reads the reference's own ReadLoader extracts (fileloader.hpp:51-545,
+    1 MB buffers, so records cross buffer boundaries) are the oracle's, in
+    order.  The loader skips empty reads, which hold no k-mer; the
+    comparison leaves them out.  FASTA is single-line here: the loader takes
+    every second line, which agrees with the oracle's records only then."""
+    from oracle.oracle import ref_load_reads
+    if fmt == "fastq":
+        text, _ = random_fastq(5, 9000, lens=(0, 400), crlf=0.0)
+        path = tmp_path / "reads.fq"
+    else:
+        r = np.random.default_rng(3)
+        acgt = np.frombuffer(b"ACGTN", np.uint8)
+        recs = [bytes(acgt[r.integers(0, 5, int(r.integers(1, 600)))]) for _ in range(6000)]
+        text = b"".join(b">r%d desc\n%s\n" % (i, x) for i, x in enumerate(recs))
+        path = tmp_path / "reads.fa"
+    assert len(text) > 1 << 20
+    path.write_bytes(text)
+    try:
+        got = ref_load_reads(str(path), 1)
+    except FileNotFoundError as e:
+        pytest.skip(str(e))
+    assert got == [x for x in parse_fastx(text, fmt)[0] if x]
+
+
 def random_fastq(seed, n, lens=(0, 400), crlf=0.1, long_every=0):
     r = np.random.default_rng(seed)
     alpha = np.frombuffer(b"ACGTNacgt", np.uint8)
