@@ -135,6 +135,58 @@ def cpu_baseline(args, threads):
                       f"(phase1 {t1:.1f} s, phase2 {t2:.1f} s); {d} distinct"}
 
 
+def write_fastq(path, reads, offs):
+    """The reads as FASTQ records (@<index>, the bases, +, a quality line)."""
+    n = len(offs) - 1
+    lens = np.diff(offs.astype(np.int64))
+    with open(path, "wb") as f:
+        if n and lens.min() == lens.max():  # one read length: records built as rows
+            L = int(lens[0])
+            ids = np.char.zfill(np.arange(n).astype("S12"), 12).view(np.uint8).reshape(n, 12)
+            rec = np.empty((n, 1 + 12 + 1 + L + 3 + L + 1), np.uint8)
+            rec[:, 0] = ord("@")
+            rec[:, 1:13] = ids
+            rec[:, 13] = 10
+            rec[:, 14:14 + L] = np.asarray(reads[:n * L]).reshape(n, L)
+            rec[:, 14 + L:17 + L] = np.frombuffer(b"\n+\n", np.uint8)
+            rec[:, 17 + L:17 + 2 * L] = ord("I")
+            rec[:, 17 + 2 * L] = 10
+            f.write(rec.tobytes())
+        else:
+            for i in range(n):
+                s = bytes(reads[int(offs[i]):int(offs[i + 1])])
+                f.write(b"@%d\n%s\n+\n%s\n" % (i, s, b"I" * len(s)))
+
+
+def reference_program(args, threads):
+    """The reference's own command-line program (its gkc_main.cpp and
+    cpu_funcs.cpp, built into oracle/_ref/rapidgkc_on_b200), run CPU-only as
+    `-cpuonly -ngpu 0 -im ... -read <FASTQ>` on the same bounded sample, timed
+    by the wall time it prints (gkc_main.cpp:433).  It includes the
+    reference's FASTQ loading, which the GPU path's e2e figure does not."""
+    import tempfile
+    from rapidgkc_b200 import synth
+    exe = os.path.join(ROOT, "oracle", "_ref", "rapidgkc_on_b200")
+    if not os.path.exists(exe) or args.k > 32:
+        return None
+    reads, offs = synth.make_workload(args.workload, read_fraction=args.cpu_fraction, threads=threads)
+    with tempfile.TemporaryDirectory() as d:
+        fq = os.path.join(d, "sample.fq")
+        write_fastq(fq, reads, offs)
+        cmd = [exe, "-cpuonly", "-ngpu", "0", "-im", "-k", str(args.k), "-p", str(args.p), "-skm",
+               str(args.partitions), "-t", str(threads), "-t2", str(threads), "-tsort", "1", "-read", fq]
+        p = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=900)
+    if p.returncode != 0:
+        return {"unavailable": f"exit {p.returncode}"}
+    wall = float(p.stdout.strip().split("\n")[-1])
+    m = [l for l in p.stderr.split("\n") if "Total number of distinct kmers:" in l]
+    bases = int(offs[-1])
+    return {"value": bases / wall / 1e9, "unit": "Gbp/s", "cores": threads, "wall_s": wall,
+            "distinct": int(m[-1].split(":")[-1]) if m else None,
+            "sample": f"{len(offs) - 1} reads ({bases / 1e6:.0f} Mbp) as FASTQ",
+            "cmd": "rapidgkc_on_b200 -cpuonly -ngpu 0 -im -k K -p P -skm SKM -t T -t2 T -tsort 1 -read sample.fq"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -154,7 +206,8 @@ def run_reference(args, rank, world):
             "config": {"workload": args.workload, "k": args.k, "p": args.p, "partitions": args.partitions,
                        "threshold": ">=2", "sample_fraction": args.cpu_fraction},
             "cpu_baseline": base,
-            "e2e": {"value": v, "unit": "Gbp/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": v, "unit": "Gbp/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "program": reference_program(args, threads)}
     print(json.dumps(line), flush=True)
 
 
