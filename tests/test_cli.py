@@ -30,6 +30,15 @@ def test_cli_rejects_bad_arguments(args, msg):
     assert p.returncode == 2 and msg in p.stderr
 
 
+def test_cli_rejects_k_beyond_64(tmp_path):
+    """k up to 64 is accepted (the reference's 128-bit build); 65 is refused
+    by the library before any device call."""
+    fq = tmp_path / "x.fq"
+    fq.write_bytes(b"@r\nACGT\n+\nIIII\n")
+    p = _run("-k", "65", "-p", "11", "-skm", "16", "-read", str(fq), check=False)
+    assert p.returncode == 1 and "invalid argument" in p.stderr
+
+
 def _write_inputs(tmp, reads, offs):
     seqs = [reads[int(offs[i]):int(offs[i + 1])].tobytes() for i in range(len(offs) - 1)]
     h = len(seqs) // 2
