@@ -14,10 +14,11 @@
 //   KmerCountingCPU   cpu_funcs.cpp:586-651  (phase 2 of one partition)
 //   ReadLoader        fileloader.hpp:51-545  (FASTQ / FASTA record extraction)
 //
-// oracle/Makefile builds it twice: libgkc_ref.so with the reference's default
-// 64-bit T_kmer (k <= 32) and libgkc_ref_long.so with -DLONGERKMER, the
+// oracle/Makefile builds it three times: libgkc_ref.so with the reference's
+// default 64-bit T_kmer (k <= 32), libgkc_ref_long.so with -DLONGERKMER, the
 // reference's own 128-bit build for k <= 64 (types.h:34-35, CMakeLists.txt
-// target l_<name>).
+// target l_<name>), and libgkc_ref_short.so with -DSHORTERKMER, its 32-bit
+// build for k <= 16 (types.h:36-37, target s_<name>).
 #include "cpu_funcs.h"
 #include "fileloader.hpp"
 #include "utilities.hpp"

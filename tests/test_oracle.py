@@ -120,3 +120,23 @@ def test_oracle_wide_revcomp_and_order(oracle):
     keys = np.array([[5, 1], [9, 0], [5, 1], [0, 2]], np.uint64)
     km, ct, d = oracle.count(keys)
     assert d == 3 and km.tolist() == [[9, 0], [5, 1], [0, 2]] and ct.tolist() == [1, 2, 1]
+
+
+@pytest.mark.parametrize("k,p,P,seed", [(12, 5, 7, 1), (16, 9, 31, 2), (9, 3, 3, 3)])
+def test_oracle_matches_compiled_reference_short(oracle, k, p, P, seed):
+    """k <= 16 against the reference's 32-bit SHORTERKMER build (types.h:36-37,
+    utilities.hpp:277-278): the same k-mer values, held in u32 there."""
+    import os
+    from conftest import ROOT
+    from oracle.oracle import RefOracle
+    from tests_util import random_reads
+    path = os.path.join(ROOT, "oracle", "_ref", "libgkc_ref_short.so")
+    if not os.path.exists(path):
+        pytest.skip(f"{path} missing")
+    ref = RefOracle(path=path)
+    assert ref.lib.ref_kmer_bits() == 32
+    reads, offs = random_reads(seed, 20_000, 800, (k, 300), 0.01)
+    ka, ca, da, pka = ref.count_reads(reads, offs, k, p, P, 2)
+    kb, cb, db, pkb = oracle.count_reads(reads, offs, k, p, P, 2)
+    assert da == db and np.array_equal(pka, pkb)
+    assert np.array_equal(ka, kb) and np.array_equal(ca, cb)
