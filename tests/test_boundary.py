@@ -87,3 +87,46 @@ def test_five_calls_match_the_oracle(oracle, counter, order):
         assert L.gkc_set_order_lut(h, None) == GKC_OK  # back to the default order
     finally:
         assert L.gkc_shutdown(h) == GKC_OK
+
+
+def _build_c_example(tmp_path):
+    """Compiles the plain-C example of the integration guide as C11 with
+    every warning an error; returns the program's path."""
+    import os
+    import subprocess
+    from conftest import ROOT
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    i = doc.index("```c\n/* five_calls.c")
+    j = doc.index("```", i + 4)
+    src = tmp_path / "five_calls.c"
+    src.write_text(doc[i + 5:j])
+    exe = tmp_path / "five_calls"
+    lib = os.path.join(ROOT, "rapidgkc_b200")
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"), "-o",
+                    str(exe), str(src), "-L", lib, "-lrapidgkc_b200", f"-Wl,-rpath,{lib}"], check=True,
+                   capture_output=True, timeout=120)
+    return str(exe)
+
+
+def test_c_example_compiles_as_c11(tmp_path):
+    import subprocess
+    import torch
+    exe = _build_c_example(tmp_path)
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: the GPU test runs the program")
+    p = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert p.returncode == 1 and "gkc_init" in p.stderr  # no device here: refused, no CPU fallback
+
+
+@pytest.mark.gpu
+def test_c_example_counts_match_the_oracle(oracle, tmp_path):
+    import subprocess
+    exe = _build_c_example(tmp_path)
+    p = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    r0 = b"ACGTTGCAAGGCTTACCGATGCATGCAAGTCCGATTAGCCGATAGGCTAACGTTAGC"
+    r1 = b"TTGACCGTAGGCATCGATCGGATCCAAGTTGCAGCATGCAACGTTGCAAGGCTTACCGATG"
+    reads = np.frombuffer(r0 + r1, np.uint8).copy()
+    offs = np.array([0, len(r0), len(r0) + len(r1)], np.uint64)
+    _, _, d, pk = oracle.count_reads(reads, offs, 31, 11, 4, 1)
+    assert p.stdout.split() == ["instances", str(int(pk.sum())), "distinct", str(d)]
