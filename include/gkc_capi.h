@@ -16,8 +16,23 @@
  *   gkc_count        kmc_counting_GPU_streams gpu_kmercounting.h:14-17, gpu_kmercounting.cu:343-548
  *   gkc_count_partitions  the same, on the store subset one call is given
  *   gkc_result       the kmc_result vectors   gkc_main.cpp:294, gpu_kmercounting.cu:505-508
+ *   gkc_store_clear  SKMStoreNoncon::clear_skm_data   skmstore.hpp:189-198
+ *   gkc_add_skm      SKMStoreNoncon::load_from_file   skmstore.hpp:102-114
+ *   gkc_add_fastx, gkc_parse_fastx  ReadLoader's record extraction  fileloader.hpp:201-232, 269-330
+ *   gkc_set_order    the fixed minimizer order        minimizer_filter.h:20
+ *   gkc_count_keys   the hash counter's insert_batch  gpu_hash_counter.cu:376-419 (its test, :693-708)
+ *   gkc_init, gkc_skmgen_batch, gkc_count_partition, gkc_set_order_lut, gkc_shutdown
+ *                    the same steps in five calls (end of this file)
  * and add what the reference declares but never does: the count threshold
  * [min, max] (utilities.hpp:190) and an output of the counted k-mers.
+ * The other entry points have no counterpart in the reference: context
+ * teardown (gkc_destroy), batching and its timings (gkc_add_reads_batches,
+ * gkc_batch_timings), device results (gkc_result_device), the one-call
+ * count (gkc_count_reads), the pinned spill arena (gkc_reserve_host), the
+ * multi-GPU exchange (gkc_store_pack, gkc_store_append), instrumentation
+ * (gkc_last_timings, gkc_kernel_launches, gkc_set_profiling,
+ * gkc_kernel_stats), streams (gkc_set_stream), the learned order
+ * (gkc_minimizer_loads, gkc_mlp_*) and gkc_count_keys_noalloc.
  */
 #ifndef GKC_CAPI_H
 #define GKC_CAPI_H
