@@ -343,12 +343,18 @@ int gkc_mlp_order(gkc_ctx *ctx, const float *params, uint64_t heavy, uint32_t *l
  *                count c satisfies cmin <= c <= cmax, unordered; if more than
  *                out_cap qualify, returns GKC_ELIMIT with *n_out = the number
  *   stream       a cudaStream_t of the current device (NULL: the default
- *                stream); the call returns after the stream's work is done
- * Runs on the current CUDA device.  The first call on a device looks up the
- * scratch's address (cudaGetSymbolAddress); make that first call outside any
- * stream capture.  All calls on one device share the one scratch table, so
- * two calls in flight at the same time (other host threads, other streams)
- * race and give wrong results: the caller serialises them. */
+ *                stream); the call copies its counters back to the host and
+ *                waits for the stream before it returns
+ * Runs on the current CUDA device.  The first call on a device (and the first
+ * after the device's context is reset, e.g. by cudaDeviceReset) looks up the
+ * scratch's address (cudaGetSymbolAddress); make that first call before any
+ * stream capture begins.  All calls on one device share the one scratch
+ * table and it keeps the last call's contents (each call clears it first),
+ * so two calls in flight at the same time (other host threads, other
+ * streams) race and give wrong results: the caller serialises them.
+ * GKC_ELIMIT is also returned, with no output, when more than 4096 of the
+ * keys hash onto one run of slots: the table is fixed, and the hash is
+ * invertible, so a key set can be built to do this. */
 enum { GKC_NOALLOC_SLOTS = 1 << 20, GKC_NOALLOC_MAX_KEYS = 1 << 19 };
 int gkc_count_keys_noalloc(const uint64_t *keys, uint64_t n, uint32_t cmin, uint32_t cmax, uint64_t *out_kmers,
                            uint32_t *out_counts, uint64_t out_cap, uint64_t *n_out, uint64_t *n_distinct,

@@ -169,6 +169,9 @@ class RefOracle:
         L.ref_run.argtypes = [_u8p, _u64p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int,
                               C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.ref_run.restype = C.c_int64
+        L.ref_digest.argtypes = [_u8p, _u64p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint32,
+                                 C.c_uint32, _u64p]
+        L.ref_digest.restype = C.c_int
 
     def gen_skm_offs(self, read: bytes, k: int, p: int):
         offs = np.zeros(len(read) + 2, np.int32)
@@ -216,6 +219,17 @@ class RefOracle:
             a, b, d = self.count_bytes(parts[i], int(pk[i]), k, cmin, cmax)
             ks.append(a); cs.append(b); dist += d
         return np.concatenate(ks), np.concatenate(cs), dist, pk
+
+    def digest(self, reads, offs, k, p, P, threads=1, cmin=1, cmax=0xFFFFFFFF) -> dict:
+        """Order-independent digest of the reference's thresholded table
+        (ref_digest): kept, distinct, xor, sum_kc, sum_c, instances.  A
+        128-bit k-mer enters as low ^ high * 0x9E3779B97F4A7C15."""
+        reads = np.ascontiguousarray(reads, np.uint8)
+        offs = np.ascontiguousarray(offs, np.uint64)
+        out = np.zeros(6, np.uint64)
+        if self.lib.ref_digest(reads, offs, len(offs) - 1, k, p, P, threads, cmin, cmax, out) != 0:
+            raise ValueError("reference extraction disagreed with the partition k-mer count")
+        return dict(zip(("kept", "distinct", "xor", "sum_kc", "sum_c", "instances"), (int(x) for x in out)))
 
     def run(self, reads, offs, k, p, P, threads):
         """Timed CPU-only reference pipeline.  Returns (distinct, t_phase1, t_phase2)."""

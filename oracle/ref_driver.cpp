@@ -23,6 +23,7 @@
 #include "fileloader.hpp"
 #include "utilities.hpp"
 
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cstdint>
@@ -213,6 +214,81 @@ int64_t ref_load_reads(const char *path, int buffer_mb, char *out, uint64_t cap,
 
 // Bits of the reference's T_kmer in this build (64, or 128 under LONGERKMER).
 int ref_kmer_bits() { return (int)(8 * sizeof(T_kmer)); }
+
+// Order-independent digest of the reference's thresholded (k-mer, count)
+// table for a CSR read set: the reference's phase 1 (GenSuperkmerCPU over
+// 2000-read batches, `threads` workers), then per partition its own
+// extraction (_h_process_bytes) and sort (sort_kmers), with the run-length
+// count of KmerCountingCPU (cpu_funcs.cpp:614-640) and [cmin, cmax] applied.
+// out[0] kept k-mers, out[1] distinct k-mers, out[2] XOR of the kept k-mers,
+// out[3] sum of k-mer * count (mod 2^64), out[4] sum of kept counts,
+// out[5] k-mer instances.  A 128-bit k-mer enters as low ^ high * 0x9E3779B97F4A7C15.
+// Returns 0, or -1 when a partition's extraction disagrees with its count.
+int ref_digest(const char *reads, const uint64_t *offs, int64_t n_reads, int k, int p, int P, int threads,
+               uint32_t cmin, uint32_t cmax, uint64_t *out) {
+    std::vector<char> buf(reads, reads + offs[n_reads]);
+    std::vector<SKMStoreNoncon *> stores;
+    for (int i = 0; i < P; i++) stores.push_back(new SKMStoreNoncon(i, false));
+    run_phase1(buf, offs, n_reads, k, p, P, threads, 2000, stores);
+    std::atomic<int> next{0};
+    std::atomic<int> bad{0};
+    std::vector<std::array<uint64_t, 6>> acc(threads, std::array<uint64_t, 6>{0, 0, 0, 0, 0, 0});
+    auto worker = [&](int tid) {
+        auto &a = acc[tid];
+        for (;;) {
+            int i = next.fetch_add(1);
+            if (i >= P) break;
+            SKMStoreNoncon *s = stores[i];
+            const size_t nk = s->kmer_cnt;
+            std::vector<u_char> b = drain_store(s);
+            s->clear_skm_data();
+            delete s;
+            if (nk == 0) continue;
+            std::vector<T_kmer> kmers(nk);
+            std::atomic<size_t> pos{0};
+            _h_process_bytes(0, b.size(), b.data(), kmers.data(), &pos, (T_kvalue)k);
+            if (pos.load() != nk) {
+                bad = 1;
+                continue;
+            }
+            sort_kmers(kmers.data(), nk, (T_kvalue)k, 0);
+            a[5] += nk;
+            size_t r = 0;
+            while (r < nk) {
+                size_t j = r + 1;
+                while (j < nk && kmers[j] == kmers[r]) j++;
+                const size_t run = j - r;
+                const uint32_t c = run > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)run;
+                a[1]++;
+                if (c >= cmin && c <= cmax) {
+#ifdef LONGERKMER
+                    const uint64_t key = (uint64_t)kmers[r] ^ ((uint64_t)(kmers[r] >> 64) * 0x9E3779B97F4A7C15ull);
+#else
+                    const uint64_t key = (uint64_t)kmers[r];
+#endif
+                    a[0]++;
+                    a[2] ^= key;
+                    a[3] += key * (uint64_t)c;
+                    a[4] += c;
+                }
+                r = j;
+            }
+        }
+    };
+    std::vector<std::thread> ts;
+    for (int t = 0; t < threads; t++) ts.emplace_back(worker, t);
+    for (auto &t : ts) t.join();
+    for (int f = 0; f < 6; f++) out[f] = 0;
+    for (auto &a : acc) {
+        out[0] += a[0];
+        out[1] += a[1];
+        out[2] ^= a[2];
+        out[3] += a[3];
+        out[4] += a[4];
+        out[5] += a[5];
+    }
+    return bad.load() ? -1 : 0;
+}
 
 void ref_free(void *h) {
     auto *res = (Phase1Result *)h;

@@ -70,21 +70,23 @@ def build_cli(force: bool = False) -> str:
     return out
 
 
-def build_oracle() -> None:
-    """The test oracles (oracle/Makefile); the reference part only where the
-    reference tree exists, otherwise the prebuilt library is used as is."""
+def build_oracle(ref_tree: str | None = None) -> None:
+    """The test oracles (oracle/Makefile).  The reference part is built only
+    when the reference source tree is given (`ref_tree`, or the environment
+    variable GKC_REFERENCE_TREE) and exists; otherwise the prebuilt
+    oracle/_ref files are used as they are."""
     oracle = os.path.join(ROOT, "oracle")
     _run(["make", "-s", "-C", oracle, "liboracle.so"])
-    ref_tree = os.environ.get("GKC_REFERENCE_TREE", "/root/reference")
-    if os.path.isdir(ref_tree):
+    ref_tree = ref_tree or os.environ.get("GKC_REFERENCE_TREE")
+    if ref_tree and os.path.isdir(ref_tree):
         _run(["make", "-s", "-C", oracle, "ref", f"REF={ref_tree}"])
 
 
-def build_all(ptxas: bool = False, force: bool = False) -> None:
+def build_all(ptxas: bool = False, force: bool = False, ref_tree: str | None = None) -> None:
     build_cuda(ptxas=ptxas, force=force)
     build_synth(force=force)
     build_cli(force=force)
-    build_oracle()
+    build_oracle(ref_tree)
 
 
 if __name__ == "__main__":

@@ -156,7 +156,7 @@ class KmerCounter:
     uint64 arrays of (low word, high word), ordered as 128-bit values."""
 
     def __init__(self, k: int = 31, p: int = 11, partitions: int = 512, counter: str = "hash",
-                 device: int = 0, radix_bits: int = 8, table_slots: float = 0.35,
+                 device: int = 0, radix_bits: int = 0, table_slots: float = 0.35,
                  batch_bases: int = 1 << 30, spill_host: bool = False, group_keys: int = 0,
                  hash_l2_only: bool = False, hpc: bool = False):
         L = load_library()
@@ -164,6 +164,7 @@ class KmerCounter:
         L.gkc_default_options(C.byref(o))
         o.k, o.p, o.partitions = k, p, partitions
         o.counter = {"hash": COUNTER_HASH, "sort": COUNTER_SORT}[counter]
+        default_bits = o.radix_bits
         o.radix_bits, o.table_slots, o.batch_bases = radix_bits, table_slots, batch_bases
         o.spill_host, o.group_keys, o.hash_l2_only = int(spill_host), group_keys, int(hash_l2_only)
         o.hpc = int(hpc)
@@ -173,6 +174,7 @@ class KmerCounter:
             raise GkcError(rc, L.gkc_strerror(rc).decode())
         self._L, self._h = L, h
         self.k, self.p, self.partitions, self.counter = k, p, partitions, counter
+        self.radix_bits = radix_bits or default_bits  # the sort counter's digit width
         self.device = device
         self._kw = 1  # u64 words per k-mer of the last result
 

@@ -28,9 +28,13 @@ struct __align__(16) HSlot {
 };
 static_assert(sizeof(HSlot) == 16, "slot layout");
 
+// Once any insert of the pass has given up (ERR_TABLE_FULL), the pass is
+// redone with a larger table or failed, so the others stop probing too: every
+// 64 probes a thread looks at the flag.
 __device__ __forceinline__ void table_add(HSlot *tab, uint64_t mask, uint64_t key, uint32_t c, uint32_t *err) {
     uint64_t h = hash64(key) & mask;
     for (uint32_t pr = 0; pr < H_MAX_PROBE; pr++) {
+        if ((pr & 63) == 63 && (__ldcg(err) & ERR_TABLE_FULL)) return;
         unsigned long long cur = __ldcg(&tab[h].key);
         if (cur == key) {
             atomicAdd(&tab[h].cnt, c);

@@ -40,6 +40,7 @@ from .capi import KmerCounter, load_library
 H = 64
 ORDERS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "orders")
 ORDER_MIX_KEY = 0x5BD1E995  # the tie-break mix of the learned order (gkc_device.cuh)
+ORDER_MAX_P = 15  # the learned order's rank levels need 32 - 2p >= 2 bits (order_mlp.cu)
 
 
 def param_count(p: int) -> int:

@@ -90,20 +90,16 @@ def test_five_calls_match_the_oracle(oracle, counter, order):
 
 
 def _build_c_example(tmp_path):
-    """Compiles the plain-C example of the integration guide as C11 with
-    every warning an error; returns the program's path."""
+    """Compiles the plain-C example (rapidgkc_b200/examples/five_calls.c) as
+    C11 with every warning an error; returns the program's path."""
     import os
     import subprocess
     from conftest import ROOT
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    i = doc.index("```c\n/* five_calls.c")
-    j = doc.index("```", i + 4)
-    src = tmp_path / "five_calls.c"
-    src.write_text(doc[i + 5:j])
+    src = os.path.join(ROOT, "rapidgkc_b200", "examples", "five_calls.c")
     exe = tmp_path / "five_calls"
     lib = os.path.join(ROOT, "rapidgkc_b200")
     subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"), "-o",
-                    str(exe), str(src), "-L", lib, "-lrapidgkc_b200", f"-Wl,-rpath,{lib}"], check=True,
+                    str(exe), src, "-L", lib, "-lrapidgkc_b200", f"-Wl,-rpath,{lib}"], check=True,
                    capture_output=True, timeout=120)
     return str(exe)
 

@@ -140,3 +140,18 @@ def test_oracle_matches_compiled_reference_short(oracle, k, p, P, seed):
     kb, cb, db, pkb = oracle.count_reads(reads, offs, k, p, P, 2)
     assert da == db and np.array_equal(pka, pkb)
     assert np.array_equal(ka, kb) and np.array_equal(ca, cb)
+
+
+def test_reference_digest_matches_oracle(oracle, ref_oracle):
+    """The digest bench.py compares against (the reference's phase 1, its
+    extraction and sort, run-length count, threshold) equals the digest of
+    the C restatement's table, on a sample of the skewed workload."""
+    from rapidgkc_b200 import synth
+    reads, offs = synth.make_workload("skewed_200m", scale=0.001, threads=4)
+    for k, cmin in ((31, 2), (25, 1)):
+        d = ref_oracle.digest(reads, offs, k, 11, 64, threads=4, cmin=cmin)
+        km, ct, dist, pk = oracle.count_reads(reads, offs, k, 11, 64, cmin)
+        assert d["kept"] == len(km) and d["distinct"] == dist and d["instances"] == int(pk.sum())
+        assert d["xor"] == int(np.bitwise_xor.reduce(km))
+        assert d["sum_kc"] == int(np.sum(km * ct.astype(np.uint64), dtype=np.uint64))
+        assert d["sum_c"] == int(ct.sum(dtype=np.uint64))

@@ -190,3 +190,41 @@ def test_learned_order_gain_on_held_out_skewed_genome():
     (s0, d0, k0, c0), (s1, d1, k1, c1) = res["default"], res["learned"]
     assert d0 == d1 and np.array_equal(k0, k1) and np.array_equal(c0, c1)
     assert s1["maxmean_kmers"] < 0.9 * s0["maxmean_kmers"], (s0, s1, log.iterations)
+
+
+@pytest.mark.gpu
+def test_trained_network_beats_its_untrained_order():
+    """What the trained network adds: the learned order against the same
+    order with no network levels (every p-mer ranked by the pseudo-random mix
+    alone), on a held-out skewed genome (seed 404, not among the training
+    seeds).  The network's levels lower the max/mean partition load in bytes
+    (the superkmer bytes phase 2 reads per partition) and the number of
+    sub-buckets that overflow shared memory, with identical counts.  The
+    max/mean load in k-mers is not asserted: its maximum is the partition of
+    the longest poly-A / (AT)n / (CAG)n runs, whose every window holds only the
+    run's own p-mers, so no order moves those k-mers."""
+    import torch
+    from rapidgkc_b200 import order, synth
+    params = order.load_order(order.default_order_path(11))[0]
+    reads, offs = synth.make_workload("skewed_200m", scale=0.02, seed=404)
+    d_reads = torch.from_numpy(reads).cuda()
+    d_offs = torch.from_numpy(offs.view(np.int64)).cuda()
+    res = {}
+    with _counter(k=31, p=11, partitions=512) as c:
+        for name in ("mix", "learned"):
+            if name == "mix":
+                c.set_order(order.mix_table(11))
+            else:
+                c.mlp_order(params)
+            c.store_clear()
+            c.add_reads(d_reads, d_offs)
+            st = order.partition_stats(c)
+            n, d = c.count(2, U32)
+            relisted = c.timings()["overflowed_sub_buckets"]
+            km, ct = c.result()
+            o = np.argsort(km)
+            res[name] = (st, relisted, d, km[o], ct[o])
+    (s0, r0, d0, k0, c0), (s1, r1, d1, k1, c1) = res["mix"], res["learned"]
+    assert d0 == d1 and np.array_equal(k0, k1) and np.array_equal(c0, c1)
+    assert s1["maxmean_bytes"] < 0.97 * s0["maxmean_bytes"], (s0, s1)
+    assert r1 < r0, (r0, r1, s0, s1)
