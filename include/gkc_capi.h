@@ -68,7 +68,7 @@ typedef struct gkc_options {
     int p;                  /* minimizer length, 3 <= p <= 16 (reference -p, utilities.hpp:188)   */
     int partitions;         /* superkmer partitions, 1..4096 (reference -skm, utilities.hpp:189)  */
     int counter;            /* GKC_COUNTER_SORT or GKC_COUNTER_HASH                               */
-    int radix_bits;         /* LSD digit width of the sort counter, 4..8 (0 = 8)                  */
+    int radix_bits;         /* LSD digit width of the sort counter, 4..11 (0 = 11)                */
     double table_slots;     /* hash slots per k-mer instance of a partition (0 = 0.35)            */
     uint64_t batch_bases;   /* bases per phase-1 batch, host and device input (0 = 1 GiB)         */
     int spill_host;         /* keep the partition store in pinned host memory (streamed input)    */
@@ -77,6 +77,9 @@ typedef struct gkc_options {
                             /* the ones that overflow; 1 = every partition through the L2 table   */
     int hpc;                /* 1: homopolymer compression of every read before phase 1: a run of  */
                             /* equal bytes counts as one base (reference -hpc, gpu_skmgen.cu:145) */
+    uint64_t sort_seg_max;  /* sort counter: partitions of more k-mer instances than this take    */
+                            /* the three-kernel radix sort, the others the one-pass-per-digit     */
+                            /* sort (0 = 2^30 - 1, its limit; lower values are for tests)         */
 } gkc_options;
 
 /* Fills defaults: k=31, p=11, partitions=512, hash counter. */
@@ -176,7 +179,9 @@ int gkc_store_pack(gkc_ctx *ctx, int p0, int p1, uint8_t *bytes, uint64_t cap_by
 /* Appends a packed range of partitions [p0, p1) (gkc_store_pack's layout, in
  * device or host memory; counts in host memory) to the store as one chunk
  * (SKMStoreNoncon::add_skms, skmstore.hpp:189-198, for a received range).
- * The buffers may be reused when the call returns. */
+ * None of [p0, p1) may have been counted yet (gkc_count_partitions); other
+ * partitions of the store may have been.  The buffers may be reused when the
+ * call returns. */
 int gkc_store_append(gkc_ctx *ctx, int p0, int p1, const uint8_t *bytes, const uint64_t *idx,
                      const uint32_t *keys, const uint64_t *counts);
 

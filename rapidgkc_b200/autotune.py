@@ -43,7 +43,7 @@ def _digest(c: KmerCounter):
 
 
 def autotune(reads: np.ndarray, offs: np.ndarray, k: int = 31, p: int = 11, cmin: int = 2, device: int = 0,
-             partitions=(256, 512, 1024), counters=("hash", "sort"), radix_bits=(6, 8), orders=("default", "learned"),
+             partitions=(256, 512, 1024), counters=("hash", "sort"), radix_bits=(8, 11), orders=("default", "learned"),
              batch_bases=(1 << 26, 1 << 28, 1 << 30), repeats: int = 2, verbose: bool = False) -> dict:
     """Measures every combination on (reads, offs) (a host CSR sample of the
     workload, ideally a few hundred Mbp) and returns the fastest:

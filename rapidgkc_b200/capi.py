@@ -54,6 +54,7 @@ class Options(C.Structure):
         ("group_keys", C.c_uint64),
         ("hash_l2_only", C.c_int),
         ("hpc", C.c_int),
+        ("sort_seg_max", C.c_uint64),
     ]
 
 
@@ -158,7 +159,7 @@ class KmerCounter:
     def __init__(self, k: int = 31, p: int = 11, partitions: int = 512, counter: str = "hash",
                  device: int = 0, radix_bits: int = 0, table_slots: float = 0.35,
                  batch_bases: int = 1 << 30, spill_host: bool = False, group_keys: int = 0,
-                 hash_l2_only: bool = False, hpc: bool = False):
+                 hash_l2_only: bool = False, hpc: bool = False, sort_seg_max: int = 0):
         L = load_library()
         o = Options()
         L.gkc_default_options(C.byref(o))
@@ -168,6 +169,7 @@ class KmerCounter:
         o.radix_bits, o.table_slots, o.batch_bases = radix_bits, table_slots, batch_bases
         o.spill_host, o.group_keys, o.hash_l2_only = int(spill_host), group_keys, int(hash_l2_only)
         o.hpc = int(hpc)
+        o.sort_seg_max = sort_seg_max
         h = C.c_void_p()
         rc = L.gkc_create(device, C.byref(o), C.byref(h))
         if rc != GKC_OK:

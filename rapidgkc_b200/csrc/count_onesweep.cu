@@ -1,0 +1,296 @@
+// count_onesweep.cu -- the sort counter's LSD radix sort, one pass over the
+// keys per digit.
+//
+// The reference sorts each partition's k-mers with thrust::sort
+// (gpu_kmercounting.cu:428).  Here every partition of a group is a segment of
+// one key buffer and all segments are sorted at once, least significant digit
+// first, over only the 2k meaningful bits:
+//
+//   os_hist_kernel   reads the keys once and counts, per segment, the keys of
+//                    every digit value of every pass (one histogram per pass);
+//   os_scan_kernel   turns those counts into each digit's first position in
+//                    its segment, for every pass;
+//   os_pass_kernel   one launch per digit: a CTA takes the next tile of keys
+//                    (tile ids from an atomic counter, so every tile before
+//                    it is already running), ranks them by digit in shared
+//                    memory (per-warp digit counters and __match_any_sync,
+//                    stable), publishes its per-digit counts, and reads the
+//                    earlier tiles' counts of its segment back to its own
+//                    offsets (decoupled look-back: each tile publishes its
+//                    count first and its inclusive prefix once known, and a
+//                    reader stops at the first inclusive prefix).  It then
+//                    writes its keys in digit order from shared memory, so
+//                    the keys of one digit leave as a contiguous run.
+//
+// Per pass the keys are read once and written once; the look-back statuses
+// add NB x 4 bytes per tile.  Digits are up to 11 bits (6 passes over the 62
+// bits of a 31-mer).  A status word holds a 2-bit flag and a 30-bit count,
+// so segments are limited to 2^30 - 1 keys (larger ones use the
+// three-kernel sort of count_sort.cu).  The flags cycle through three
+// (aggregate, inclusive) pairs, so statuses left by the previous pass never
+// read as the current pass's and the array is cleared once per sort.
+#include "gkc_device.cuh"
+
+namespace gkc {
+
+constexpr int OS_THREADS = 256;
+constexpr int OS_WARPS = OS_THREADS / 32;
+constexpr int OS_MAX_PASSES = 32;
+constexpr uint32_t OS_SEG_MAX = (1u << 30) - 1;
+constexpr uint32_t OS_SPIN_LIMIT = 1u << 22;  // look-back polls before giving up (~0.4 s)
+constexpr uint32_t ERR_LOOKBACK = 1u << 10;   // a look-back wait ran out
+
+// keys per thread: 16 u64 or 8 u128, so a tile's keys take 32 KB either way
+template <class KT> constexpr int os_items() { return sizeof(KT) == 16 ? 8 : 16; }
+template <class KT> constexpr int os_tile() { return OS_THREADS * os_items<KT>(); }
+
+struct OsTile {
+    uint64_t start;      // first key of the tile
+    uint64_t seg_start;  // first key of its segment
+    uint32_t n;          // keys in the tile
+    uint32_t t;          // tile index in its segment
+    uint32_t seg;        // segment index
+    uint32_t seg_n;      // keys in the segment
+};
+static_assert(sizeof(OsTile) == 32, "tile layout");
+
+struct OsPasses {
+    int n;                        // passes
+    int shift[OS_MAX_PASSES];     // lowest bit of each pass's digit
+    int width[OS_MAX_PASSES];     // bits of each pass's digit (<= RB)
+};
+
+template <class KT>
+__device__ __forceinline__ uint32_t os_digit(const KT &key, int shift, uint32_t mask) {
+    return (uint32_t)(key >> shift) & mask;
+}
+
+// ---------------------------------------------------------------------------
+// Per-segment histograms of every pass.  A CTA counts one chunk (a range of
+// one segment) in shared memory and adds the nonzero counts to
+// ghist[seg][pass][digit].
+struct OsChunk {
+    uint64_t start;
+    uint32_t n;
+    uint32_t seg;
+};
+
+template <int RB, class KT>
+__global__ void __launch_bounds__(OS_THREADS)
+os_hist_kernel(const KT *__restrict__ keys, const OsChunk *__restrict__ chunks, OsPasses ps, uint32_t *ghist) {
+    constexpr int NB = 1 << RB;
+    extern __shared__ uint32_t h[];  // [ps.n][NB]
+    const OsChunk ch = chunks[blockIdx.x];
+    for (int i = threadIdx.x; i < ps.n * NB; i += OS_THREADS) h[i] = 0;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < ch.n; j += OS_THREADS) {
+        const KT key = keys[ch.start + j];
+        for (int p = 0; p < ps.n; p++)
+            atomicAdd(&h[p * NB + os_digit(key, ps.shift[p], (1u << ps.width[p]) - 1)], 1u);
+    }
+    __syncthreads();
+    uint32_t *g = ghist + (uint64_t)ch.seg * ps.n * NB;
+    for (int i = threadIdx.x; i < ps.n * NB; i += OS_THREADS)
+        if (h[i]) atomicAdd(g + i, h[i]);
+}
+
+// Exclusive scan of one (segment, pass) histogram over its digits, in place:
+// the digit's first position in the segment's output.
+template <int RB>
+__global__ void __launch_bounds__(1024) os_scan_kernel(uint32_t *ghist) {
+    constexpr int NB = 1 << RB;
+    constexpr int PER = NB > 1024 ? NB / 1024 : 1;
+    __shared__ uint32_t ws[32];
+    uint32_t *g = ghist + (uint64_t)blockIdx.x * NB;
+    uint32_t v[PER], s = 0;
+    const int b0 = threadIdx.x * PER;
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        v[i] = b0 + i < NB ? g[b0 + i] : 0u;
+        s += v[i];
+    }
+    uint32_t tot;
+    uint32_t pre = block_exclusive_scan<1024>(s, &tot, ws);
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        if (b0 + i < NB) g[b0 + i] = pre;
+        pre += v[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t os_load_status(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void os_store_status(uint32_t *p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+struct OsPassParams {
+    const void *in;
+    void *out;
+    const OsTile *tiles;
+    uint32_t ntiles;
+    uint32_t *status;         // [ntiles][NB]
+    const uint32_t *gbase;    // [nseg][npass][NB] digit starts in the segment
+    int npass, pass, shift, width;
+    uint32_t agg, inc;        // this pass's flags (2 bits, shifted to 31..30)
+    uint32_t *tile_ctr;       // next tile of this pass
+    uint32_t *err;
+};
+
+template <int RB, class KT>
+__global__ void __launch_bounds__(OS_THREADS)
+os_pass_kernel(OsPassParams a) {
+    constexpr int NB = 1 << RB;
+    constexpr int ITEMS = os_items<KT>();
+    constexpr int T = os_tile<KT>();
+    static_assert(OS_WARPS * NB * 2 <= T * (int)sizeof(KT), "warp counters fit the key staging area");
+    extern __shared__ __align__(16) unsigned char os_smem[];
+    // the key staging area doubles as the per-warp digit counters (u16)
+    KT *skeys = reinterpret_cast<KT *>(os_smem);
+    uint16_t *wcnt = reinterpret_cast<uint16_t *>(os_smem);           // [OS_WARPS][NB]
+    uint32_t *bstart = reinterpret_cast<uint32_t *>(os_smem + T * sizeof(KT));  // [NB] tile-local run starts
+    int32_t *bdelta = reinterpret_cast<int32_t *>(bstart + NB);       // [NB] segment position - local index
+    uint16_t *tcount = reinterpret_cast<uint16_t *>(bdelta + NB);     // [NB] tile counts
+    __shared__ uint32_t ws[32];
+    __shared__ uint32_t s_tile;
+
+    const KT *in = static_cast<const KT *>(a.in);
+    KT *out = static_cast<KT *>(a.out);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1;
+    const uint32_t dmask = (1u << a.width) - 1;
+
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);
+        for (int i = threadIdx.x; i < OS_WARPS * NB / 2; i += OS_THREADS) reinterpret_cast<uint32_t *>(wcnt)[i] = 0;
+        __syncthreads();
+        const uint32_t tile = s_tile;
+        if (tile >= a.ntiles) break;
+        const OsTile td = a.tiles[tile];
+
+        // ---- load and rank (warp w owns keys [w * 32 * ITEMS, (w + 1) * 32 * ITEMS)) ----
+        KT key[ITEMS];
+        uint16_t rank[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
+            const bool valid = j < td.n;
+            key[i] = valid ? in[td.start + j] : KT(0);
+            const uint32_t dig = valid ? os_digit(key[i], a.shift, dmask) : (uint32_t)NB;
+            const unsigned grp = __match_any_sync(FULL, dig);
+            uint32_t pre = 0;
+            if (valid) pre = wcnt[warp * NB + dig];
+            rank[i] = (uint16_t)(pre + __popc(grp & lt));
+            __syncwarp();
+            if (valid && (grp & lt) == 0) wcnt[warp * NB + dig] = (uint16_t)(pre + __popc(grp));
+            __syncwarp();
+        }
+        __syncthreads();
+        // ---- per digit: exclusive prefix over warps, tile count ----
+        for (int b = threadIdx.x; b < NB; b += OS_THREADS) {
+            uint32_t s = 0;
+#pragma unroll
+            for (int w = 0; w < OS_WARPS; w++) {
+                const uint32_t c = wcnt[w * NB + b];
+                wcnt[w * NB + b] = (uint16_t)s;
+                s += c;
+            }
+            tcount[b] = (uint16_t)s;
+        }
+        __syncthreads();
+        // ---- tile-local run starts: exclusive scan of the counts over digits ----
+        {
+            constexpr int PER = NB / OS_THREADS > 0 ? NB / OS_THREADS : 1;
+            const int b0 = threadIdx.x * PER;
+            uint32_t s = 0;
+#pragma unroll
+            for (int i = 0; i < PER; i++) s += b0 + i < NB ? tcount[b0 + i] : 0u;
+            uint32_t tot;
+            uint32_t pre = block_exclusive_scan<OS_THREADS>(s, &tot, ws);
+#pragma unroll
+            for (int i = 0; i < PER; i++)
+                if (b0 + i < NB) {
+                    bstart[b0 + i] = pre;
+                    pre += tcount[b0 + i];
+                }
+        }
+        // ---- publish this tile's counts, then look back for its offsets ----
+        uint32_t *st = a.status + (uint64_t)tile * NB;
+        const uint32_t *gb = a.gbase + ((uint64_t)td.seg * a.npass + a.pass) * NB;
+        for (int b = threadIdx.x; b < NB; b += OS_THREADS)
+            os_store_status(st + b, (td.t == 0 ? a.inc : a.agg) | tcount[b]);
+        for (int b = threadIdx.x; b < NB; b += OS_THREADS) {
+            uint32_t excl = 0;
+            if (td.t != 0) {
+                // tiles tile-1 .. tile-t of the segment; its first tile publishes
+                // its inclusive prefix at once, so the walk ends there at the latest
+                uint32_t j = tile - 1, left = td.t;
+                uint32_t spins = 0;
+                for (;;) {
+                    const uint32_t s = os_load_status(a.status + (uint64_t)j * NB + b);
+                    const uint32_t f = s & 0xC0000000u;
+                    if (f == a.inc) {
+                        excl += s & 0x3FFFFFFFu;
+                        break;
+                    }
+                    if (f == a.agg && left > 1) {
+                        excl += s & 0x3FFFFFFFu;
+                        j--;
+                        left--;
+                        continue;
+                    }
+                    if (f == a.agg || ++spins > OS_SPIN_LIMIT) {  // never expected: record it, stop waiting
+                        atomicOr(a.err, ERR_LOOKBACK);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                os_store_status(st + b, a.inc | ((excl + tcount[b]) & 0x3FFFFFFFu));
+            }
+            bdelta[b] = (int32_t)(gb[b] + excl) - (int32_t)bstart[b];
+        }
+        __syncthreads();
+        // ---- tile-local positions, then stage the keys in digit order ----
+        uint16_t lpos[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
+            lpos[i] = 0;
+            if (j < td.n) {
+                const uint32_t dig = os_digit(key[i], a.shift, dmask);
+                lpos[i] = (uint16_t)(bstart[dig] + wcnt[warp * NB + dig] + rank[i]);
+            }
+        }
+        __syncthreads();  // the counters are read: the area now takes the keys
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
+            if (j < td.n) skeys[lpos[i]] = key[i];
+        }
+        __syncthreads();
+        // ---- write: consecutive threads, consecutive keys of one digit run ----
+        KT *o = out + td.seg_start;
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t idx = (uint32_t)i * OS_THREADS + threadIdx.x;
+            if (idx < td.n) {
+                const KT k = skeys[idx];
+                const int64_t q = (int64_t)bdelta[os_digit(k, a.shift, dmask)] + idx;
+                if (q >= 0 && q < (int64_t)td.seg_n) o[q] = k;  // always true unless a look-back failed
+                else atomicOr(a.err, ERR_LOOKBACK);
+            }
+        }
+        __syncthreads();  // the staging area is cleared for the next tile
+    }
+}
+
+template <int RB, class KT>
+constexpr size_t os_pass_smem() {
+    return (size_t)os_tile<KT>() * sizeof(KT) + (size_t)(1 << RB) * (4 + 4 + 2);
+}
+
+}  // namespace gkc

@@ -27,6 +27,7 @@
 
 #include "count_records.cu"
 #include "count_sort.cu"
+#include "count_onesweep.cu"
 #include "order_mlp.cu"
 #include "skmgen.cu"
 #include "store_pack.cu"
@@ -325,6 +326,7 @@ struct gkc_ctx {
     std::vector<cudaEvent_t> batch_ev;  // start / end of each batch of the last gkc_add_reads
     std::vector<double> batch_ms;       // latency of each batch: its copy start to its phase-1 end
     DevBuf keysA, keysB, tiles, counts, offsets, blocksums, heads_pos, heads_key, tilecnt, tileoff;
+    DevBuf os_status, os_hist, os_chunks, os_ctr;  // one-pass-per-digit radix sort
     DevBuf segoff, segcur, part_err, scal;
     DevBuf stage_bytes, stage_idx;
     DevBuf spill_bytes[2], spill_idx[2], spill_keys[2];  // device staging of chunks being spilled
@@ -1535,61 +1537,12 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     return GKC_OK;
 }
 
-// ---------------------------------------------------------------------------
-// phase 2, sort counter: sorts `n` keys (KT: u64, or u128 for k > 32) already
-// in keysA split into segments segs (sizes), then RLE + threshold, appending
-// to the output.
-template <int RB, class KT>
-int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, int nbits, uint32_t cmin,
-                       uint32_t cmax, float *sort_ms) {
+// Run-length count + threshold of the sorted keys `src` (n), appending to the
+// output; adds the sort's time (events e2..e3, recorded by the caller) to
+// *sort_ms.
+template <class KT>
+int reduce_sorted(gkc_ctx *ctx, const KT *src, uint64_t n, uint32_t cmin, uint32_t cmax, float *sort_ms) {
     constexpr double KB = sizeof(KT);
-    // tiles
-    std::vector<TileDesc> td;
-    uint64_t start = 0, cnt_base = 0;
-    for (uint64_t sz : segs) {
-        constexpr uint64_t RS_TILE = rs_tile<KT>();
-        uint32_t nt = (uint32_t)((sz + RS_TILE - 1) / RS_TILE);
-        for (uint32_t t = 0; t < nt; t++) {
-            TileDesc d;
-            d.start = start + (uint64_t)t * RS_TILE;
-            d.cnt_base = cnt_base;
-            d.n = (uint32_t)std::min<uint64_t>(RS_TILE, sz - (uint64_t)t * RS_TILE);
-            d.t = t;
-            d.nt = nt;
-            d.pad = 0;
-            td.push_back(d);
-        }
-        start += sz;
-        cnt_base += (uint64_t)nt << RB;
-    }
-    const uint64_t ntiles = td.size();
-    const uint64_t ncounts = cnt_base;
-    if (ntiles) {
-        CK(ctx->tiles.ensure(ntiles * sizeof(TileDesc)));
-        CK(ctx->counts.ensure(ncounts * 4));
-        CK(ctx->offsets.ensure(ncounts * 8));
-        CK(cudaMemcpyAsync(ctx->tiles.p, td.data(), ntiles * sizeof(TileDesc), cudaMemcpyHostToDevice, ctx->s));
-        CK(cudaStreamSynchronize(ctx->s));  // td is host memory about to go out of scope
-    }
-    KT *src = ctx->keysA.as<KT>(), *dst = ctx->keysB.as<KT>();
-    CK(cudaEventRecord(ctx->e2, ctx->s));
-    for (int shift = 0; shift < nbits && ntiles; shift += RB) {
-        {
-            KScope ks(ctx, GKC_K_RADIX_HIST, KB * n + 4.0 * ncounts);
-            radix_hist_kernel<RB, KT><<<(unsigned)ntiles, RS_THREADS, 0, ctx->s>>>(
-                src, ctx->tiles.as<TileDesc>(), shift, ctx->counts.as<uint32_t>());
-            LAUNCHED();
-        }
-        RET(scan_u32(ctx, ctx->counts.as<uint32_t>(), ncounts, ctx->offsets.as<uint64_t>(), nullptr));
-        {
-            KScope ks(ctx, GKC_K_RADIX_SCATTER, 2 * KB * n + 8.0 * ncounts);
-            radix_scatter_kernel<RB, KT><<<(unsigned)ntiles, RS_THREADS, 0, ctx->s>>>(
-                src, dst, ctx->tiles.as<TileDesc>(), shift, ctx->offsets.as<uint64_t>());
-            LAUNCHED();
-        }
-        std::swap(src, dst);
-    }
-    CK(cudaEventRecord(ctx->e3, ctx->s));
     // ---- RLE ----
     const uint64_t rt = (n + RL_TILE - 1) / RL_TILE;
     CK(ctx->tilecnt.ensure(std::max<uint64_t>(rt, 1) * 4));
@@ -1647,6 +1600,185 @@ int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t
     return GKC_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// phase 2, sort counter: the radix sort of count_onesweep.cu over segments
+// `segs` of the n keys in keysA (every segment < 2^30 keys).  Digits of at
+// most RB bits, spread evenly over nbits; *sorted receives the buffer that
+// holds the result (keysA or keysB).
+template <int RB, class KT>
+int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, int nbits, KT **sorted) {
+    constexpr double KB = sizeof(KT);
+    constexpr uint64_t T = os_tile<KT>();
+    constexpr uint64_t HCHUNK = 1u << 16;  // keys per histogram CTA
+    constexpr int NB = 1 << RB;
+    OsPasses ps{};
+    ps.n = (nbits + RB - 1) / RB;
+    if (ps.n > OS_MAX_PASSES) return ctx->fail(GKC_EINTERNAL, "too many radix passes");
+    for (int p = 0, sh = 0; p < ps.n; p++) {  // widths differ by at most one bit
+        ps.width[p] = nbits / ps.n + (p < nbits % ps.n ? 1 : 0);
+        ps.shift[p] = sh;
+        sh += ps.width[p];
+    }
+    std::vector<OsTile> td;
+    std::vector<OsChunk> ch;
+    uint64_t start = 0;
+    for (uint32_t sgi = 0; sgi < (uint32_t)segs.size(); sgi++) {
+        const uint64_t sz = segs[sgi];
+        for (uint64_t t = 0; t * T < sz; t++)
+            td.push_back({start + t * T, start, (uint32_t)std::min<uint64_t>(T, sz - t * T), (uint32_t)t, sgi,
+                          (uint32_t)sz});
+        for (uint64_t c = 0; c < sz; c += HCHUNK)
+            ch.push_back({start + c, (uint32_t)std::min<uint64_t>(HCHUNK, sz - c), sgi});
+        start += sz;
+    }
+    KT *src = ctx->keysA.as<KT>(), *dst = ctx->keysB.as<KT>();
+    *sorted = src;
+    const uint64_t ntiles = td.size();
+    if (!ntiles) return GKC_OK;
+    const uint64_t nhist = segs.size() * (uint64_t)ps.n * NB;
+    CK(ctx->tiles.ensure(ntiles * sizeof(OsTile)));
+    CK(ctx->os_chunks.ensure(ch.size() * sizeof(OsChunk)));
+    CK(ctx->os_hist.ensure(nhist * 4));
+    CK(ctx->os_status.ensure(ntiles * NB * 4));
+    CK(ctx->os_ctr.ensure(64 * 4));
+    CK(ctx->part_err.ensure(64));
+    CK(cudaMemcpyAsync(ctx->tiles.p, td.data(), ntiles * sizeof(OsTile), cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemcpyAsync(ctx->os_chunks.p, ch.data(), ch.size() * sizeof(OsChunk), cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemsetAsync(ctx->os_hist.p, 0, nhist * 4, ctx->s));
+    CK(cudaMemsetAsync(ctx->os_status.p, 0, ntiles * NB * 4, ctx->s));
+    CK(cudaMemsetAsync(ctx->os_ctr.p, 0, 64 * 4, ctx->s));
+    CK(cudaMemsetAsync(ctx->part_err.p, 0, 4, ctx->s));
+    const size_t hsm = (size_t)ps.n * NB * 4;
+    {
+        static bool attr = false;  // per template instance
+        if (!attr) {
+            CK(cudaFuncSetAttribute(os_hist_kernel<RB, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)((size_t)((8 * sizeof(KT) + RB - 1) / RB) * NB * 4)));
+            CK(cudaFuncSetAttribute(os_pass_kernel<RB, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)os_pass_smem<RB, KT>()));
+            attr = true;
+        }
+    }
+    {
+        KScope ks(ctx, GKC_K_RADIX_HIST, KB * n + 4.0 * nhist);
+        os_hist_kernel<RB, KT><<<(unsigned)ch.size(), OS_THREADS, hsm, ctx->s>>>(
+            src, ctx->os_chunks.as<OsChunk>(), ps, ctx->os_hist.as<uint32_t>());
+        LAUNCHED();
+    }
+    {
+        KScope ks(ctx, GKC_K_SCAN, 8.0 * nhist);
+        os_scan_kernel<RB><<<(unsigned)(segs.size() * ps.n), 1024, 0, ctx->s>>>(ctx->os_hist.as<uint32_t>());
+        LAUNCHED();
+    }
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, os_pass_kernel<RB, KT>, OS_THREADS,
+                                                     os_pass_smem<RB, KT>()));
+    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)ctx->sms * std::max(per_sm, 1));
+    static const uint32_t flags[3][2] = {{1u << 30, 2u << 30}, {3u << 30, 1u << 30}, {2u << 30, 3u << 30}};
+    for (int p = 0; p < ps.n; p++) {
+        OsPassParams q;
+        q.in = src;
+        q.out = dst;
+        q.tiles = ctx->tiles.as<OsTile>();
+        q.ntiles = (uint32_t)ntiles;
+        q.status = ctx->os_status.as<uint32_t>();
+        q.gbase = ctx->os_hist.as<uint32_t>();
+        q.npass = ps.n;
+        q.pass = p;
+        q.shift = ps.shift[p];
+        q.width = ps.width[p];
+        q.agg = flags[p % 3][0];
+        q.inc = flags[p % 3][1];
+        q.tile_ctr = ctx->os_ctr.as<uint32_t>() + p;
+        q.err = ctx->part_err.as<uint32_t>();
+        {
+            KScope ks(ctx, GKC_K_RADIX_SCATTER, 2 * KB * n + 8.0 * ntiles * NB);
+            os_pass_kernel<RB, KT><<<grid, OS_THREADS, os_pass_smem<RB, KT>(), ctx->s>>>(q);
+            LAUNCHED();
+        }
+        std::swap(src, dst);
+    }
+    uint32_t e = 0;
+    CK(cudaMemcpyAsync(&e, ctx->part_err.p, 4, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    if (e & ERR_LOOKBACK) return ctx->fail(GKC_EINTERNAL, "radix sort: a look-back wait ran out");
+    *sorted = src;
+    return GKC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// phase 2, sort counter: sorts `n` keys (KT: u64, or u128 for k > 32) already
+// in keysA split into segments segs (sizes), then RLE + threshold, appending
+// to the output.  Digits of RB bits; segments of 2^30 keys or more take the
+// three-kernel sort (a histogram, a scan and a scatter per digit).
+template <int RB, class KT>
+int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, int nbits, uint32_t cmin,
+                       uint32_t cmax, float *sort_ms) {
+    constexpr double KB = sizeof(KT);
+    const uint64_t seg_max = ctx->opt.sort_seg_max && ctx->opt.sort_seg_max < OS_SEG_MAX ? ctx->opt.sort_seg_max
+                                                                                          : OS_SEG_MAX;
+    bool small_segs = true;
+    for (uint64_t sz : segs) small_segs &= sz <= seg_max;
+    if (small_segs) {
+        KT *sorted = nullptr;
+        CK(cudaEventRecord(ctx->e2, ctx->s));
+        const int rc = onesweep_sort<RB, KT>(ctx, segs, n, nbits, &sorted);
+        if (rc != GKC_OK) return rc;
+        CK(cudaEventRecord(ctx->e3, ctx->s));
+        return reduce_sorted<KT>(ctx, sorted, n, cmin, cmax, sort_ms);
+    }
+    constexpr int RB8 = RB > 8 ? 8 : RB;  // the three-kernel sort keeps per-warp u32 counters of 2^RB digits
+    // tiles
+    std::vector<TileDesc> td;
+    uint64_t start = 0, cnt_base = 0;
+    for (uint64_t sz : segs) {
+        constexpr uint64_t RS_TILE = rs_tile<KT>();
+        uint32_t nt = (uint32_t)((sz + RS_TILE - 1) / RS_TILE);
+        for (uint32_t t = 0; t < nt; t++) {
+            TileDesc d;
+            d.start = start + (uint64_t)t * RS_TILE;
+            d.cnt_base = cnt_base;
+            d.n = (uint32_t)std::min<uint64_t>(RS_TILE, sz - (uint64_t)t * RS_TILE);
+            d.t = t;
+            d.nt = nt;
+            d.pad = 0;
+            td.push_back(d);
+        }
+        start += sz;
+        cnt_base += (uint64_t)nt << RB8;
+    }
+    const uint64_t ntiles = td.size();
+    const uint64_t ncounts = cnt_base;
+    if (ntiles) {
+        CK(ctx->tiles.ensure(ntiles * sizeof(TileDesc)));
+        CK(ctx->counts.ensure(ncounts * 4));
+        CK(ctx->offsets.ensure(ncounts * 8));
+        CK(cudaMemcpyAsync(ctx->tiles.p, td.data(), ntiles * sizeof(TileDesc), cudaMemcpyHostToDevice, ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));  // td is host memory about to go out of scope
+    }
+    KT *src = ctx->keysA.as<KT>(), *dst = ctx->keysB.as<KT>();
+    CK(cudaEventRecord(ctx->e2, ctx->s));
+    for (int shift = 0; shift < nbits && ntiles; shift += RB8) {
+        {
+            KScope ks(ctx, GKC_K_RADIX_HIST, KB * n + 4.0 * ncounts);
+            radix_hist_kernel<RB8, KT><<<(unsigned)ntiles, RS_THREADS, 0, ctx->s>>>(
+                src, ctx->tiles.as<TileDesc>(), shift, ctx->counts.as<uint32_t>());
+            LAUNCHED();
+        }
+        RET(scan_u32(ctx, ctx->counts.as<uint32_t>(), ncounts, ctx->offsets.as<uint64_t>(), nullptr));
+        {
+            KScope ks(ctx, GKC_K_RADIX_SCATTER, 2 * KB * n + 8.0 * ncounts);
+            radix_scatter_kernel<RB8, KT><<<(unsigned)ntiles, RS_THREADS, 0, ctx->s>>>(
+                src, dst, ctx->tiles.as<TileDesc>(), shift, ctx->offsets.as<uint64_t>());
+            LAUNCHED();
+        }
+        std::swap(src, dst);
+    }
+    CK(cudaEventRecord(ctx->e3, ctx->s));
+    return reduce_sorted<KT>(ctx, src, n, cmin, cmax, sort_ms);
+}
+
 template <class KT = uint64_t>
 int sort_and_reduce(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, int nbits, uint32_t cmin,
                     uint32_t cmax, float *sort_ms) {
@@ -1655,7 +1787,10 @@ int sort_and_reduce(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n,
         case 5: return sort_and_reduce_rb<5, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
         case 6: return sort_and_reduce_rb<6, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
         case 7: return sort_and_reduce_rb<7, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
-        default: return sort_and_reduce_rb<8, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        case 8: return sort_and_reduce_rb<8, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        case 9: return sort_and_reduce_rb<9, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        case 10: return sort_and_reduce_rb<10, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
+        default: return sort_and_reduce_rb<11, KT>(ctx, segs, n, nbits, cmin, cmax, sort_ms);
     }
 }
 
@@ -1777,13 +1912,14 @@ void gkc_default_options(gkc_options *o) {
     o->p = 11;
     o->partitions = 512;
     o->counter = GKC_COUNTER_HASH;
-    o->radix_bits = 8;
+    o->radix_bits = 11;
     o->table_slots = 0.35;
     o->batch_bases = 1ull << 30;
     o->spill_host = 0;
     o->group_keys = 0;
     o->hash_l2_only = 0;
     o->hpc = 0;
+    o->sort_seg_max = 0;
 }
 
 const char *gkc_strerror(int code) {
@@ -1810,10 +1946,10 @@ int gkc_create(int device, const gkc_options *opt, gkc_ctx **out) {
     gkc_default_options(&o);
     if (opt) o = *opt;
     if (o.p < 3 || o.p > 16 || o.k < o.p || o.k > 64 || o.partitions < 1 || o.partitions > 4096 ||
-        (o.counter != GKC_COUNTER_SORT && o.counter != GKC_COUNTER_HASH) || o.radix_bits < 0 || o.radix_bits > 8 ||
+        (o.counter != GKC_COUNTER_SORT && o.counter != GKC_COUNTER_HASH) || o.radix_bits < 0 || o.radix_bits > 11 ||
         (o.radix_bits != 0 && o.radix_bits < 4))
         return GKC_EINVAL;
-    if (!o.radix_bits) o.radix_bits = 8;
+    if (!o.radix_bits) o.radix_bits = 11;
     if (!o.batch_bases) o.batch_bases = 1ull << 30;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return GKC_ECUDA;
@@ -2506,8 +2642,8 @@ int gkc_store_append(gkc_ctx *ctx, int p0, int p1, const uint8_t *bytes, const u
                      const uint64_t *counts) {
     if (!ctx || p0 < 0 || p1 < p0 || p1 > ctx->opt.partitions || !counts) return GKC_EINVAL;
     CK(cudaSetDevice(ctx->device));
-    for (char cn : ctx->counted)
-        if (cn) return ctx->fail(GKC_ESTATE, "the store is partly counted; clear it before appending");
+    for (int p = p0; p < p1 && !ctx->counted.empty(); p++)  // partitions not yet counted may still grow
+        if (ctx->counted[p]) return ctx->fail(GKC_ESTATE, "partition %d was counted already", p);
     const uint32_t P = (uint32_t)ctx->opt.partitions, n = (uint32_t)(p1 - p0);
     uint64_t nb = 0, ns = 0;
     for (uint32_t j = 0; j < n; j++) nb += counts[j], ns += counts[n + j];

@@ -85,3 +85,28 @@ def test_pack_rejects_bad_arguments():
 def test_count_exchanged_ranks(backend, world, kind, spill):
     mp.spawn(dist_workers.gpu_exchange, args=(world, dist_workers.free_port(), 43, backend, kind, spill),
              nprocs=world, join=True)
+
+
+def test_append_to_a_partly_counted_store(oracle):
+    """Partition groups arrive one at a time (the reference's phase-2 worker
+    counts group after group on its device): a group may be appended after
+    other groups were counted, but a counted partition takes no more."""
+    from rapidgkc_b200 import KmerCounter
+    k, p, P = 31, 11, 16
+    reads, offs = random_reads(45, 30_000, 3000, (80, 250), 0.01)
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P, 1, U32)
+    ko, co = sorted_table(ko, co)
+    with KmerCounter(k=k, p=p, partitions=P) as src, KmerCounter(k=k, p=p, partitions=P) as dst:
+        src.add_reads(reads, offs)
+        tables, tot = [], 0
+        for p0, p1 in ((0, 5), (5, 11), (11, 16)):
+            b, i, kk, cnt = src.store_pack(p0, p1)
+            dst.store_append(p0, p1, b, i, kk, cnt)
+            n_, d = dst.count_partitions(list(range(p0, p1)), 1, U32)
+            tables.append(dst.result())
+            tot += d
+            if p0 == 0:
+                with pytest.raises(Exception):
+                    dst.store_append(p0, p1, b, i, kk, cnt)  # counted already
+        km, ct = sorted_table(np.concatenate([t[0] for t in tables]), np.concatenate([t[1] for t in tables]))
+        assert tot == do and np.array_equal(km, ko) and np.array_equal(ct, co)

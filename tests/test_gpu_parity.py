@@ -212,7 +212,9 @@ def test_retries_spill_and_groups(oracle):
                      (dict(spill_host=True, batch_bases=500_000), "hash"),  # many spilled chunks staged together
                      (dict(spill_host=True, batch_bases=500_000), "sort"),
                      (dict(spill_host=True, group_keys=50_000), "sort"), (dict(group_keys=1), "sort"),
-                     (dict(radix_bits=5), "sort")]:
+                     (dict(radix_bits=5), "sort"), (dict(radix_bits=8), "sort"), (dict(radix_bits=10), "sort"),
+                     # partitions above sort_seg_max keys take the three-kernel sort (some do, some not)
+                     (dict(sort_seg_max=20_000), "sort"), (dict(sort_seg_max=1, radix_bits=11), "sort")]:
         with counter(k, p, P, kind, **kw) as c:
             c.add_reads(reads, offs)
             n, d = c.count(2, U32)

@@ -78,7 +78,7 @@ def test_wide_device_input_batches_spill_and_learned_order(oracle):
     lut = np.random.default_rng(13).permutation(4 ** p).astype(np.uint32)
     pbl, psl, pkl, _, _ = oracle.skmgen(reads, offs, k, p, P, lut)
     runs = [dict(batch_bases=20_000), dict(batch_bases=50_000, spill_host=True), dict(kind="hash"),
-            dict(order=True), dict(group_keys=5000)]
+            dict(order=True), dict(group_keys=5000), dict(sort_seg_max=1000), dict(radix_bits=8)]
     for kw in runs:
         order = kw.pop("order", False)
         with counter(k, p, P, **kw) as c:
