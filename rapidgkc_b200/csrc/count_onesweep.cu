@@ -164,6 +164,8 @@ os_pass_kernel(OsPassParams a) {
     const unsigned lt = (1u << lane) - 1;
     const uint32_t dmask = (1u << a.width) - 1;
 
+    constexpr int BPT = NB >= OS_THREADS ? NB / OS_THREADS : 1;  // digits per thread in the look-back
+    constexpr int LB_ROWS = 4;  // earlier tiles read at once per digit
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);
         for (int i = threadIdx.x; i < OS_WARPS * NB / 2; i += OS_THREADS) reinterpret_cast<uint32_t *>(wcnt)[i] = 0;
@@ -172,14 +174,19 @@ os_pass_kernel(OsPassParams a) {
         if (tile >= a.ntiles) break;
         const OsTile td = a.tiles[tile];
 
-        // ---- load and rank (warp w owns keys [w * 32 * ITEMS, (w + 1) * 32 * ITEMS)) ----
+        // ---- load (all loads in flight first), then rank; warp w owns keys
+        //      [w * 32 * ITEMS, (w + 1) * 32 * ITEMS) ----
         KT key[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
+            key[i] = j < td.n ? in[td.start + j] : KT(0);
+        }
         uint16_t rank[ITEMS];
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
             const bool valid = j < td.n;
-            key[i] = valid ? in[td.start + j] : KT(0);
             const uint32_t dig = valid ? os_digit(key[i], a.shift, dmask) : (uint32_t)NB;
             const unsigned grp = __match_any_sync(FULL, dig);
             uint32_t pre = 0;
@@ -190,7 +197,8 @@ os_pass_kernel(OsPassParams a) {
             __syncwarp();
         }
         __syncthreads();
-        // ---- per digit: exclusive prefix over warps, tile count ----
+        // ---- per digit: exclusive prefix over warps, tile count, published at once ----
+        uint32_t *st = a.status + (uint64_t)tile * NB;
         for (int b = threadIdx.x; b < NB; b += OS_THREADS) {
             uint32_t s = 0;
 #pragma unroll
@@ -200,6 +208,7 @@ os_pass_kernel(OsPassParams a) {
                 s += c;
             }
             tcount[b] = (uint16_t)s;
+            os_store_status(st + b, (td.t == 0 ? a.inc : a.agg) | s);
         }
         __syncthreads();
         // ---- tile-local run starts: exclusive scan of the counts over digits ----
@@ -218,58 +227,98 @@ os_pass_kernel(OsPassParams a) {
                     pre += tcount[b0 + i];
                 }
         }
-        // ---- publish this tile's counts, then look back for its offsets ----
-        uint32_t *st = a.status + (uint64_t)tile * NB;
-        const uint32_t *gb = a.gbase + ((uint64_t)td.seg * a.npass + a.pass) * NB;
-        for (int b = threadIdx.x; b < NB; b += OS_THREADS)
-            os_store_status(st + b, (td.t == 0 ? a.inc : a.agg) | tcount[b]);
-        for (int b = threadIdx.x; b < NB; b += OS_THREADS) {
-            uint32_t excl = 0;
-            if (td.t != 0) {
-                // tiles tile-1 .. tile-t of the segment; its first tile publishes
-                // its inclusive prefix at once, so the walk ends there at the latest
-                uint32_t j = tile - 1, left = td.t;
-                uint32_t spins = 0;
-                for (;;) {
-                    const uint32_t s = os_load_status(a.status + (uint64_t)j * NB + b);
-                    const uint32_t f = s & 0xC0000000u;
-                    if (f == a.inc) {
-                        excl += s & 0x3FFFFFFFu;
-                        break;
+        __syncthreads();
+        // ---- stage the keys in digit order (the counters' area takes the keys) ----
+        {
+            uint16_t lpos[ITEMS];
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
+                lpos[i] = 0;
+                if (j < td.n) {
+                    const uint32_t dig = os_digit(key[i], a.shift, dmask);
+                    lpos[i] = (uint16_t)(bstart[dig] + wcnt[warp * NB + dig] + rank[i]);
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
+                if (j < td.n) skeys[lpos[i]] = key[i];
+            }
+        }
+        // ---- look back: each thread's digits together, LB_ROWS earlier tiles a step ----
+        {
+            const uint32_t *gb = a.gbase + ((uint64_t)td.seg * a.npass + a.pass) * NB;
+            uint32_t excl[BPT], jn[BPT], left[BPT];
+            uint32_t pending = 0;  // digits still looking back
+#pragma unroll
+            for (int x = 0; x < BPT; x++) {
+                excl[x] = 0;
+                jn[x] = tile - 1;
+                left[x] = td.t;  // earlier tiles of the segment
+                if (td.t != 0 && x * OS_THREADS + (int)threadIdx.x < NB) pending |= 1u << x;
+            }
+            uint32_t spins = 0;
+            while (pending) {
+                uint32_t v[BPT][LB_ROWS];
+#pragma unroll
+                for (int x = 0; x < BPT; x++)
+#pragma unroll
+                    for (int r = 0; r < LB_ROWS; r++)
+                        v[x][r] = ((pending >> x) & 1) && (uint32_t)r < left[x]
+                                      ? os_load_status(a.status + (uint64_t)(jn[x] - r) * NB + x * OS_THREADS +
+                                                       threadIdx.x)
+                                      : 0u;
+                bool waited = false;
+#pragma unroll
+                for (int x = 0; x < BPT; x++) {
+                    if (!((pending >> x) & 1)) continue;
+                    const uint32_t nr = left[x] < (uint32_t)LB_ROWS ? left[x] : (uint32_t)LB_ROWS;
+                    uint32_t r = 0;  // rows consumed
+#pragma unroll
+                    for (int rr = 0; rr < LB_ROWS; rr++) {
+                        if ((uint32_t)rr >= nr) break;
+                        const uint32_t f = v[x][rr] & 0xC0000000u;
+                        if (f == a.inc) {
+                            excl[x] += v[x][rr] & 0x3FFFFFFFu;
+                            pending &= ~(1u << x);
+                            break;
+                        }
+                        if (f != a.agg) {  // not published yet: this row is read again next step
+                            waited = true;
+                            break;
+                        }
+                        excl[x] += v[x][rr] & 0x3FFFFFFFu;
+                        r++;
                     }
-                    if (f == a.agg && left > 1) {
-                        excl += s & 0x3FFFFFFFu;
-                        j--;
-                        left--;
-                        continue;
+                    if ((pending >> x) & 1) {
+                        jn[x] -= r;
+                        left[x] -= r;
+                        // the segment's first tile publishes its inclusive prefix at once,
+                        // so the walk cannot run past it
+                        if (left[x] == 0) {
+                            atomicOr(a.err, ERR_LOOKBACK);
+                            pending &= ~(1u << x);
+                        }
                     }
-                    if (f == a.agg || ++spins > OS_SPIN_LIMIT) {  // never expected: record it, stop waiting
+                }
+                if (waited) {
+                    if (++spins > OS_SPIN_LIMIT) {  // never expected: record it and stop waiting
                         atomicOr(a.err, ERR_LOOKBACK);
                         break;
                     }
-                    __nanosleep(64);
+                    __nanosleep(32);
                 }
-                os_store_status(st + b, a.inc | ((excl + tcount[b]) & 0x3FFFFFFFu));
             }
-            bdelta[b] = (int32_t)(gb[b] + excl) - (int32_t)bstart[b];
-        }
-        __syncthreads();
-        // ---- tile-local positions, then stage the keys in digit order ----
-        uint16_t lpos[ITEMS];
 #pragma unroll
-        for (int i = 0; i < ITEMS; i++) {
-            const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
-            lpos[i] = 0;
-            if (j < td.n) {
-                const uint32_t dig = os_digit(key[i], a.shift, dmask);
-                lpos[i] = (uint16_t)(bstart[dig] + wcnt[warp * NB + dig] + rank[i]);
+            for (int x = 0; x < BPT; x++) {
+                const int b = x * OS_THREADS + threadIdx.x;
+                if (b < NB) {
+                    if (td.t != 0) os_store_status(st + b, a.inc | ((excl[x] + tcount[b]) & 0x3FFFFFFFu));
+                    bdelta[b] = (int32_t)(gb[b] + excl[x]) - (int32_t)bstart[b];
+                }
             }
-        }
-        __syncthreads();  // the counters are read: the area now takes the keys
-#pragma unroll
-        for (int i = 0; i < ITEMS; i++) {
-            const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
-            if (j < td.n) skeys[lpos[i]] = key[i];
         }
         __syncthreads();
         // ---- write: consecutive threads, consecutive keys of one digit run ----

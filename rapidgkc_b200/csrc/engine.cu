@@ -532,21 +532,10 @@ struct P1Plan {
 int p1_plan(gkc_ctx *ctx, uint64_t total, P1Plan *pl) {
     const uint32_t P = (uint32_t)ctx->opt.partitions;
     pl->ntiles = (total + P1_TILE - 1) / P1_TILE;
-    // the window-minimum doubling is unrolled per level count
-    const int w = ctx->opt.k - ctx->opt.p + 1;
-    int lg = 0;
-    while ((2 << lg) <= w) lg++;
-    if (ctx->opt.k > 32)  // w >= 33 - 16 + 1 = 18: four or five levels
-        pl->kfind = ctx->has_lut ? (lg >= 5 ? find_superkmers_kernel<5, true, true> : find_superkmers_kernel<4, true, true>)
-                                 : (lg >= 5 ? find_superkmers_kernel<5, false, true> : find_superkmers_kernel<4, false, true>);
-    else if (ctx->has_lut)
-        pl->kfind = lg == 0 ? find_superkmers_kernel<0, true, false> : lg == 1 ? find_superkmers_kernel<1, true, false>
-                  : lg == 2 ? find_superkmers_kernel<2, true, false> : lg == 3 ? find_superkmers_kernel<3, true, false>
-                                                                               : find_superkmers_kernel<4, true, false>;
+    if (ctx->opt.k > 32)
+        pl->kfind = ctx->has_lut ? find_superkmers_kernel<true, true> : find_superkmers_kernel<false, true>;
     else
-        pl->kfind = lg == 0 ? find_superkmers_kernel<0, false, false> : lg == 1 ? find_superkmers_kernel<1, false, false>
-                  : lg == 2 ? find_superkmers_kernel<2, false, false> : lg == 3 ? find_superkmers_kernel<3, false, false>
-                                                                                : find_superkmers_kernel<4, false, false>;
+        pl->kfind = ctx->has_lut ? find_superkmers_kernel<true, false> : find_superkmers_kernel<false, false>;
     pl->dyn = 3ull * P * sizeof(uint32_t);
     CK(cudaFuncSetAttribute(pl->kfind, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl->dyn));
     int per_sm = 0;

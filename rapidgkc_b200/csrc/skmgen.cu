@@ -10,21 +10,24 @@
 //
 // Kernel 1 (find_superkmers) walks the concatenated read bases tile by tile.
 // A CTA stages its tile's ASCII bytes in shared memory as 2-bit codes (16-byte
-// vector loads) and a bitmap of read boundaries, and writes the tile's codes
-// back to global memory packed 16 bases per word.  Each warp then walks a
-// strip of the tile 32 positions at a time: lane l evaluates the canonical
-// p-mer key at position c0+l; the minimum over the window of w = k-p+1 p-mers
-// is a sparse-table doubling over a 64-wide register window (this chunk and
-// the next) built from shuffles.  A superkmer starts at a valid k-mer that
-// begins a read or whose key differs from its predecessor's, and ends at the
-// next start or invalid position; both are ballots over the chunk.  The
-// lanes where a superkmer ends build its record (begin, k-mer count, key,
-// packing phase, trailing bases) in the warp's shared-memory queue; every 32
-// queued records the warp's lanes emit one each into a per-CTA region and add
-// it to per-partition byte/superkmer/k-mer counts in shared memory, which the
-// CTA also writes out (cta_hist).  Emitting 32 at a time keeps every lane busy
-// (a chunk ends about 3 superkmers): find took 11% less time than emitting
-// each record in the chunk where it ends.
+// vector loads) and a bitmap of read boundaries, writes the tile's codes back
+// to global memory packed 16 bases per word, and puts the p-mer key of every
+// staged position in shared memory.  Each lane then owns 32 consecutive k-mer
+// starts and works through them serially: the minimum over each window of
+// w = k-p+1 keys from block suffix and prefix minima (van Herk / Gil-Werman),
+// and 32-bit masks of valid k-mers, superkmer starts (a valid k-mer that
+// begins a read or whose key differs from its predecessor's) and end events
+// (a start or an invalid k-mer).  A superkmer ends at the next end event after
+// its start, found in the lane's mask, the later lanes' (a suffix minimum over
+// the warp), the later strips' (published per warp) or, past the tile, in the
+// staged halo.  Each lane writes the records (begin, k-mer count, key, packing
+// phase, trailing bases) of the superkmers that start in it into a per-CTA
+// region and adds them to per-partition byte/superkmer/k-mer counts in shared
+// memory, which the CTA also writes out (cta_hist).  Against one position per
+// lane per step (a shuffle doubling for the window and ballots for the
+// boundaries every 32 positions), this cuts the instructions per base about
+// tenfold: the window, boundary and record work is done once per position
+// instead of once per lane per step.
 //
 // cta_offsets_kernel lays out, from those counts, each CTA's contiguous range
 // of every partition's byte and index buffers (CTA order: deterministic).
@@ -34,6 +37,8 @@
 // (cpu_funcs.cpp:200-250): a copy of the packed read whose first byte's
 // header says 3-beg%3 valid bases and whose last byte's header says
 // (end-1+k)%3, so the bytes are bit-identical to the reference's.
+#include <type_traits>
+
 #include "gkc_device.cuh"
 
 namespace gkc {
@@ -190,29 +195,50 @@ __device__ __forceinline__ void emit_packed(const P1Params &a, uint32_t *h, uint
     else atomicOr(a.err, ERR_RECORD_OVERFLOW);
 }
 
-// LOG = log2 of the largest power of two <= w (the doubling levels); LUT: the
-// key of a position is a.lut[p-mer] (an order table, already canonical), else
-// the default order over both strands.  KW: k > 32 (the reference's 128-bit
-// LONGERKMER build, k <= 64): a k-mer's read-boundary test spans 64 bits, and
-// LOG = 5 takes windows of 32 < w <= 62 p-mers over three chunks in
-// registers: the 32-wide minimum of this chunk and of the next, combined at
-// offset w - 32.
-template <int LOG, bool LUT, bool KW>
-__global__ void __launch_bounds__(P1_THREADS, 6)  // 6 CTAs (48 warps) per SM
+// Skewed shared-memory index of staged position j: lane l of a warp reads
+// positions 32 l + t in step t, and the skew puts them in 32 different banks.
+__device__ __forceinline__ int p1_sk(int j) { return j + (j >> 5); }
+constexpr int P1_NKEYS = P1_STAGE - 16;                 // staged positions with a p-mer key
+constexpr int P1_KEY_SLOTS = P1_NKEYS + P1_NKEYS / 32 + 2;
+constexpr int P1_INF = 0x7FFFFFFF;
+
+// LUT: the key of a position is a.lut[p-mer] (an order table, already
+// canonical), else the default order over both strands.  KW: k > 32 (the
+// reference's 128-bit LONGERKMER build, k <= 64): read-boundary windows of up
+// to 63 bits and minimizer windows of up to 62 p-mers.
+//
+// Per tile: (A) every staged position's p-mer key into shared memory; (B)
+// lane l of warp w owns the 32 k-mer starts [32 l, 32 l + 32) of strip w and
+// computes their window minima serially -- blocks of w keys from the lane's
+// first position, suffix minima backwards, prefix minima forwards, window =
+// min(suffix at its first key, prefix at its last key) (van Herk / Gil-Werman)
+// -- then its superkmer starts and ends as 32-bit masks: valid (no read start
+// inside the k-mer), start = valid and (read start or key change), end event =
+// start or invalid.  Each start's end is the next end event: in the lane, in
+// a later lane (a suffix minimum over lanes), in a later strip (published per
+// warp), or past the tile (the owning warp scans the staged halo, then global
+// memory).  Each lane then writes its records.
+template <bool LUT, bool KW>
+__global__ void __launch_bounds__(P1_THREADS)
 find_superkmers_kernel(P1Params a) {
     extern __shared__ uint32_t hist[];  // [3P]: bytes, superkmers, k-mers per partition
     __shared__ P1Smem sm;
-    // per warp: records found but not yet emitted; emitted 32 at a time, one
-    // per lane (a chunk ends ~3 superkmers, so emitting them where they end
-    // would run the emission with most lanes idle)
-    __shared__ SkmRecord pend[P1_WARPS][64];
-    static_assert(LOG < 5 || KW, "windows of more than 31 p-mers need k > 32");
-    constexpr bool W3 = LOG == 5;  // three-chunk window
-    constexpr int L2 = 1 << (W3 ? 4 : LOG);
+    __shared__ uint32_t skey[P1_KEY_SLOTS];  // keys, then (tile positions) window minima
+    __shared__ int fe_warp[P1_WARPS];        // first end event of each strip (staged index)
+    using BM = typename std::conditional<KW, u128, uint64_t>::type;
+    constexpr int TMAX = KW ? 96 : 64;  // > the last local index the backward pass reads, for any w
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int k = a.k, p = a.p, w = k - p + 1;
     const uint32_t pmask = 0xFFFFFFFFu >> (32 - 2 * p);
-    const unsigned lt_mask = (1u << lane) - 1;
+    const int shp = 32 - 2 * p;
+    // blocks of w keys from the lane's local index 0 (its first k-mer's predecessor)
+    BM bend = 0;  // bit t: local index t ends a block
+    for (int t = w - 1; t < TMAX; t += w) bend |= (BM)1 << t;
+    uint64_t bfirst = 0;  // bit i (1..32): local index i + w - 1 starts a block
+    for (int i = 1; i < 33; i += w) bfirst |= 1ull << i;
+    const int top = (32 / w + 1) * w - 1;  // end of the block that holds local index 32
+    const uint32_t vmask = (1u << ((k - 1) & 31)) - 1;      // k <= 32
+    const uint64_t vmask64 = (1ull << ((k - 1) & 63)) - 1;  // KW: k <= 64
 
     for (uint32_t i = threadIdx.x; i < 3 * a.P; i += blockDim.x) hist[i] = 0;
     if (threadIdx.x == 0) sm.region_n = 0;
@@ -254,21 +280,6 @@ find_superkmers_kernel(P1Params a) {
                 if (o >= sbeg) atomicOr(&sm.bm[(o - sbeg) >> 5], 1u << ((o - sbeg) & 31));
             }
         }
-        __syncthreads();
-        // ---- each warp walks its strip ----
-        const int64_t strip0 = t0 + (int64_t)warp * P1_STRIP;
-        if (strip0 >= (int64_t)a.total) continue;
-        // staged-relative limits
-        const int jstrip0 = (int)(strip0 - sbeg), jstrip1 = jstrip0 + P1_STRIP;
-        const int jmin = sbeg < 0 ? (int)(-sbeg) : 0;                     // first position >= 0
-        const int64_t jk64 = (int64_t)a.total - k - sbeg;                 // last valid k-mer start
-        const int jmaxk = jk64 > (int64_t)P1_STAGE ? P1_STAGE : (int)jk64;
-        const int64_t jt64 = (int64_t)a.total - sbeg;
-        const int jtotal = jt64 > (int64_t)P1_STAGE ? P1_STAGE : (int)jt64;
-        // last chunk start whose next chunk's p-mers and boundary bits are staged
-        const int jlimit = P1_STAGE - (128 + k);
-        const int shp = 32 - 2 * p;
-
         auto pk_at = [&](int j) -> uint32_t {  // canonical p-mer key at staged position j
             int i = j >> 4, o = j & 15;
             uint32_t f = __funnelshift_l(sm.codes[i + 1], sm.codes[i], 2 * o) >> shp;
@@ -282,187 +293,209 @@ find_superkmers_kernel(P1Params a) {
         auto bits_at = [&](int j) -> uint32_t {  // 32 boundary bits from staged position j
             return __funnelshift_r(sm.bm[j >> 5], sm.bm[(j >> 5) + 1], j & 31);
         };
-        const uint32_t vmask = (1u << ((k - 1) & 31)) - 1;  // k <= 32
-        const uint64_t vmask64 = (1ull << ((k - 1) & 63)) - 1;  // KW: k <= 64
-        // minimum over [lane, lane + 32) of the 64 keys of two chunks (W3)
-        auto win32 = [&](uint32_t ma, uint32_t mb) -> uint32_t {
+        // ---- (A) the p-mer key of every staged position ----
+        // (unrolled: the table reads of one thread are in flight together)
+        constexpr int NA = (P1_NKEYS + P1_THREADS - 1) / P1_THREADS;
 #pragma unroll
-            for (int x = 1; x < 32; x <<= 1) {
-                const uint32_t t = __shfl_sync(FULL, lane >= x ? ma : mb, (lane + x) & 31);
-                const uint32_t tb = __shfl_down_sync(FULL, mb, x);
-                ma = min(ma, t);
-                mb = min(mb, tb);
-            }
-            return ma;
-        };
-        // read start of the warm-up chunk's first position: the last boundary
-        // bit at or before it, else the start of the read containing sbeg.
-        int64_t rs;
+        for (int r = 0; r < NA; r++) {
+            const int j = threadIdx.x + r * P1_THREADS;
+            if (j < P1_NKEYS) skey[p1_sk(j)] = pk_at(j);
+        }
+        __syncthreads();
+
+        // ---- (B) lane-serial window minima over the lane's 32 k-mer starts ----
+        const int jstrip0 = 32 + warp * P1_STRIP;            // staged index of the strip's first k-mer
+        const int jb = jstrip0 + 32 * lane;                  // the lane's first k-mer (multiple of 32)
+        const int64_t q0 = sbeg + jb;
+        const int64_t jk64 = (int64_t)a.total - k - sbeg;    // last valid k-mer start
+        const int jmaxk = jk64 > (int64_t)P1_STAGE ? P1_STAGE : (int)jk64;
+        uint32_t M[33];  // M[i]: minimum over local keys [i, i + w), the k-mer at jb - 1 + i
         {
-            const int j = jstrip0 - 32;  // multiple of 32
+            uint32_t suf = 0xFFFFFFFFu;
+#pragma unroll
+            for (int t = TMAX - 1; t >= 0; t--) {
+                if (t <= top) {
+                    const uint32_t kk = skey[p1_sk(jb - 1 + t)];
+                    suf = ((bend >> t) & 1) ? kk : min(suf, kk);
+                    if (t < 33) M[t] = suf;
+                }
+            }
+            uint32_t pre = M[0];  // local keys [0, w) are block 0
+#pragma unroll
+            for (int i = 1; i < 33; i++) {
+                const uint32_t kk = skey[p1_sk(jb + i + w - 2)];
+                pre = ((bfirst >> i) & 1) ? kk : min(pre, kk);
+                M[i] = min(M[i], pre);
+            }
+        }
+        uint32_t D = 0;  // bit i: the key of k-mer jb + i differs from its predecessor's
+#pragma unroll
+        for (int i = 0; i < 32; i++) D |= (uint32_t)(M[i + 1] != M[i]) << i;
+        // validity: no read start at jb + i + 1 .. jb + i + k - 1, and a k-mer inside the input
+        const int wb = jb >> 5;
+        const uint32_t RS = sm.bm[wb];  // read starts at jb .. jb + 31
+        BM X;
+        if (KW) {
+            const u128 lo = (u128)sm.bm[wb] | ((u128)sm.bm[wb + 1] << 32) | ((u128)sm.bm[wb + 2] << 64) |
+                            ((u128)sm.bm[wb + 3] << 96);
+            X = (BM)(lo >> 1);
+        } else {
+            const uint64_t lo = (uint64_t)sm.bm[wb] | ((uint64_t)sm.bm[wb + 1] << 32);
+            X = (BM)((lo >> 1) | ((uint64_t)sm.bm[wb + 2] << 63));
+        }
+        {  // X bit i = OR of read-start bits i .. i + k - 2 (from jb + 1)
+            const int n = k - 1;
+            int s = 1;
+            while (2 * s <= n) {
+                X |= X >> s;
+                s *= 2;
+            }
+            if (n > s) X |= X >> (n - s);
+        }
+        const int lim = jmaxk - jb;
+        uint32_t V = ~(uint32_t)X;
+        V &= lim >= 31 ? 0xFFFFFFFFu : lim < 0 ? 0u : ((2u << lim) - 1);
+        const uint32_t S = V & (RS | D);
+        const uint32_t E = S | ~V;
+        // the first end event after this lane: a suffix minimum over lanes
+        const int fe = E ? jb + __ffs(E) - 1 : P1_INF;
+        int sfx = fe;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_down_sync(FULL, sfx, d);
+            if (lane + d < 32) sfx = min(sfx, o);
+        }
+        int after = __shfl_down_sync(FULL, sfx, 1);
+        if (lane == 31) after = P1_INF;
+        if (lane == 0) fe_warp[warp] = sfx;
+        // last read start before the strip (its base may lie before the staged range)
+        int64_t rs_before;
+        {
             int64_t found = -1;
-            for (int base = (j >> 5); found < 0 && base >= 0; base -= 32) {
-                int idx = base - lane;
-                uint32_t v = idx >= 0 ? sm.bm[idx] : 0u;
-                if (idx == (j >> 5)) v &= 1u;  // only position j itself in its own word
-                unsigned bal = __ballot_sync(FULL, v != 0);
+            for (int base = (jstrip0 >> 5) - 1; found < 0 && base >= 0; base -= 32) {
+                const int idx = base - lane;
+                const uint32_t v = idx >= 0 ? sm.bm[idx] : 0u;
+                const unsigned bal = __ballot_sync(FULL, v != 0);
                 if (bal) {
-                    int src = __ffs(bal) - 1;  // lowest lane = highest word index
-                    uint32_t vv = __shfl_sync(FULL, v, src);
+                    const int src = __ffs(bal) - 1;  // lowest lane = highest word index
+                    const uint32_t vv = __shfl_sync(FULL, v, src);
                     found = sbeg + ((int64_t)(base - src) << 5) + (31 - __clz(vv));
                 }
             }
-            rs = found >= 0 ? found : (int64_t)sm.rs0;
-        }
-
-        // pipeline: A = p-mer keys of chunk c, B = of chunk c+1
-        int cj = jstrip0 - 32;
-        uint32_t A = pk_at(cj + lane), B = pk_at(cj + 32 + lane);
-        // W3: C = keys of chunk c+2, F = 32-wide minima of chunk c
-        uint32_t C = 0xFFFFFFFFu, F = 0xFFFFFFFFu;
-        if (W3) {
-            C = pk_at(cj + 64 + lane);
-            F = win32(A, B);
-        }
-        uint32_t carried_key = 0xFFFFFFFFu;
-        uint32_t npend = 0;  // records in pend[warp] (warp-uniform)
-        SkmRecord *wp = pend[warp];
-        // emits pend[warp][0, n), n <= 32, one per lane
-        auto flush = [&](uint32_t n) {
-            __syncwarp();
-            uint32_t base = 0;
-            if (lane == 0) base = atomicAdd(&sm.region_n, n);
-            base = __shfl_sync(FULL, base, 0);
-            if ((uint32_t)lane < n) emit_packed(a, hist, base + lane, wp[lane]);
-            __syncwarp();
-        };
-        bool open = false;  // a superkmer of this warp whose end is not found yet
-        int64_t o_pos = 0;
-        uint32_t o_key = 0, o_phase = 0;
-        for (;;) {
-            const bool warm = cj < jstrip0;
-            const bool cont = cj >= jstrip1;
-            if (cont && !open) break;
-            if (cj > jlimit || cj >= jtotal) break;
-            // ---- window minimum over w p-mers for the k-mer at cj+lane ----
-            uint32_t key, Fn = 0xFFFFFFFFu;
-            if (W3) {
-                // [lane, lane + w) = [lane, lane + 32) u [lane + d, lane + d + 32)
-                Fn = win32(B, C);
-                const int d = w - 32;
-                const uint32_t t = __shfl_sync(FULL, lane >= d ? F : Fn, (lane + d) & 31);
-                key = min(F, t);
-            } else {
-                uint32_t ma = A, mb = B;
+            const int64_t rs_strip = found >= 0 ? found : (int64_t)sm.rs0;
+            // ... then before each lane: the last read start of the lanes below
+            int64_t incl = RS ? q0 + 31 - __clz(RS) : -1;
 #pragma unroll
-                for (int x = 1; x < L2; x <<= 1) {
-                    uint32_t t = __shfl_sync(FULL, lane >= x ? ma : mb, (lane + x) & 31);
-                    uint32_t tb = __shfl_down_sync(FULL, mb, x);
-                    ma = min(ma, t);
-                    mb = min(mb, tb);
-                }
-                key = ma;
-                if (w > L2) {
-                    int d = w - L2;
-                    uint32_t t = __shfl_sync(FULL, lane >= d ? ma : mb, (lane + d) & 31);
-                    key = min(ma, t);
-                }
+            for (int d = 1; d < 32; d <<= 1) {
+                const int64_t o = __shfl_up_sync(FULL, incl, d);
+                if (lane >= d) incl = max(incl, o);
             }
-            const int j = cj + lane;
-            uint32_t prevkey = __shfl_up_sync(FULL, key, 1);
-            if (lane == 0) prevkey = carried_key;
-            const uint32_t bits = bits_at(j);
-            bool valid;
-            if (KW) {  // no read start at j+1 .. j+k-1 (k <= 64)
-                const uint64_t b64 = bits | ((uint64_t)bits_at(j + 32) << 32);
-                valid = j >= jmin && j <= jmaxk && ((b64 >> 1) & vmask64) == 0;
-            } else {
-                valid = j >= jmin && j <= jmaxk && ((bits >> 1) & vmask) == 0;
-            }
-            const bool isrs = j >= jmin && (bits & 1u);
-            const bool start = valid && (isrs || key != prevkey);
-            const unsigned RSB = __ballot_sync(FULL, isrs);
-            const unsigned E = __ballot_sync(FULL, start || !valid);
-            const unsigned S = __ballot_sync(FULL, start);
-
-            if (!warm) {
-                // a superkmer ends at each E lane whose nearest E bit below is
-                // an owned start, or (none below) at the first E lane if one
-                // is open from an earlier chunk
-                const unsigned below = E & lt_mask;
-                const int src = below ? 31 - __clz(below) : 0;
-                const uint32_t skey = __shfl_sync(FULL, key, src);
-                const bool isE = (E >> lane) & 1u;
-                const bool emit = isE && (below ? (((S >> src) & 1u) && !cont) : open);
-                const unsigned EM = __ballot_sync(FULL, emit);
-                if (EM) {
-                    if (emit) {
-                        const int64_t e = sbeg + j;  // exclusive end (k-mer index)
-                        int64_t b = o_pos;
-                        uint32_t phase = o_phase, skey2 = o_key;
-                        if (below) {
-                            // read start at or before src: last boundary bit in
-                            // the chunk up to src, else the carried one
-                            const unsigned rsb = RSB & ((2u << src) - 1);
-                            const int64_t rss = rsb ? sbeg + cj + 31 - __clz(rsb) : rs;
-                            b = sbeg + cj + src;
-                            phase = (uint32_t)(b - rss) % 3u;
-                            skey2 = skey;
-                        }
-                        const uint32_t tail = tail_of(bits_at(j + k - 1) & 7u);
-                        SkmRecord r;
-                        r.pos = rec_pack_pos((uint64_t)b, phase, tail);
-                        r.len = (uint32_t)(e - b);
-                        r.key = skey2;
-                        wp[npend + __popc(EM & lt_mask)] = r;
-                    }
-                    npend += __popc(EM);
-                    if (npend >= 32) {  // emit the first 32, keep the rest
-                        flush(32);
-                        npend -= 32;
-                        if ((uint32_t)lane < npend) wp[lane] = wp[32 + lane];
-                        __syncwarp();
-                    }
-                }
-                // the last start with no end in this chunk stays open
-                if (E) {
-                    const int last = 31 - __clz(E);
-                    open = ((S >> last) & 1u) && !cont;
-                    if (open) {
-                        const unsigned rsb = RSB & ((2u << last) - 1);
-                        const int64_t rsl = rsb ? sbeg + cj + 31 - __clz(rsb) : rs;
-                        o_pos = sbeg + cj + last;
-                        o_key = __shfl_sync(FULL, key, last);
-                        o_phase = (uint32_t)(o_pos - rsl) % 3u;
-                    }
-                }
-            }
-            carried_key = __shfl_sync(FULL, key, 31);
-            if (RSB) rs = sbeg + cj + 31 - __clz(RSB);
-            // advance
-            cj += 32;
-            if (W3) {
-                F = Fn;
-                B = C;
-                C = (cj + 95 < P1_STAGE - 16) ? pk_at(cj + 64 + lane) : 0xFFFFFFFFu;
-            } else {
-                A = B;
-                B = (cj + 63 < P1_STAGE - 16) ? pk_at(cj + 32 + lane) : 0xFFFFFFFFu;
-            }
+            rs_before = __shfl_up_sync(FULL, incl, 1);
+            if (lane == 0) rs_before = -1;
+            rs_before = max(rs_before, rs_strip);
         }
-        if (npend) flush(npend);
-        // superkmer running past the staged range: finish it from global memory
-        if (open) {
-            if (lane == 0) {
-                const int64_t c0 = sbeg + cj;
-                int64_t r = read_of(a.offs, a.n_reads, (uint64_t)o_pos);
-                int64_t re = (int64_t)a.offs[r + 1];
-                int64_t e = c0 > o_pos + 1 ? c0 : o_pos + 1;
-                while (e + k <= re && kmer_key_global<LUT>(a, (uint64_t)e) == o_key) e++;
-                int64_t after = re - (e + k - 1);
-                uint32_t tail = after >= 3 ? 3 : (uint32_t)after;
-                uint32_t slot = atomicAdd(&sm.region_n, 1u);
-                emit_record(a, hist, slot, (uint64_t)o_pos, (uint32_t)(e - o_pos), o_key, o_phase, tail);
+        __syncthreads();  // keys read by every lane; strip end events published
+#pragma unroll
+        for (int i = 0; i < 32; i++) skey[p1_sk(jb + i)] = M[i + 1];  // window minimum of k-mer jb + i
+        __syncwarp();
+        // ---- records: each lane writes those that start in it ----
+        const uint32_t cnt = __popc(S);
+        uint32_t pre = cnt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(FULL, pre, d);
+            if (lane >= d) pre += o;
+        }
+        const uint32_t wtot = __shfl_sync(FULL, pre, 31);
+        uint32_t base = 0;
+        if (lane == 0 && wtot) base = atomicAdd(&sm.region_n, wtot);
+        uint32_t slot = __shfl_sync(FULL, base, 0) + pre - cnt;
+        bool open = false;  // this lane's last superkmer runs past the tile
+        int64_t o_pos = 0;
+        uint32_t o_key = 0, o_phase = 0, o_slot = 0;
+        uint32_t s = S;
+        while (s) {
+            const int i = __ffs(s) - 1;
+            s &= s - 1;
+            const int bj = jb + i;
+            const uint32_t above = i == 31 ? 0u : (E >> (i + 1));
+            int ej;
+            if (above) {
+                ej = bj + __ffs(above);
+            } else if (after != P1_INF) {
+                ej = after;
+            } else {
+                ej = P1_INF;
+                for (int w2 = warp + 1; w2 < P1_WARPS; w2++)
+                    if (fe_warp[w2] != P1_INF) {
+                        ej = fe_warp[w2];
+                        break;
+                    }
+            }
+            const uint32_t key = skey[p1_sk(bj)];
+            const int64_t b = sbeg + bj;
+            const uint32_t rsb = RS & (i == 31 ? 0xFFFFFFFFu : ((2u << i) - 1));
+            const int64_t rs = rsb ? q0 + 31 - __clz(rsb) : rs_before;
+            const uint32_t phase = (uint32_t)(b - rs) % 3u;
+            if (ej == P1_INF) {  // ends past the tile: the warp finds its end below
+                open = true;
+                o_pos = b;
+                o_key = key;
+                o_phase = phase;
+                o_slot = slot++;
+                continue;
+            }
+            SkmRecord r;
+            r.pos = rec_pack_pos((uint64_t)b, phase, tail_of(bits_at(ej + k - 1) & 7u));
+            r.len = (uint32_t)(ej - bj);
+            r.key = key;
+            emit_packed(a, hist, slot++, r);
+        }
+        // ---- the superkmer that runs past the tile: its end in the staged halo ----
+        const unsigned op = __ballot_sync(FULL, open);
+        if (op) {
+            const int src = __ffs(op) - 1;
+            o_pos = __shfl_sync(FULL, o_pos, src);
+            o_key = __shfl_sync(FULL, o_key, src);
+            o_phase = __shfl_sync(FULL, o_phase, src);
+            o_slot = __shfl_sync(FULL, o_slot, src);
+            const int jlimit = P1_STAGE - (128 + k);  // last chunk start whose keys and bits are staged
+            int cj = 32 + P1_TILE, ej = P1_INF;
+            for (; cj <= jlimit; cj += 32) {
+                const int j = cj + lane;
+                uint32_t m = 0xFFFFFFFFu;
+                for (int x = 0; x < w; x++) m = min(m, skey[p1_sk(j + x)]);
+                const uint32_t bits = bits_at(j);
+                bool valid;
+                if (KW) {
+                    const uint64_t b64 = bits | ((uint64_t)bits_at(j + 32) << 32);
+                    valid = j <= jmaxk && ((b64 >> 1) & vmask64) == 0;
+                } else {
+                    valid = j <= jmaxk && ((bits >> 1) & vmask) == 0;
+                }
+                const unsigned eb = __ballot_sync(FULL, !valid || (bits & 1u) || m != o_key);
+                if (eb) {
+                    ej = cj + __ffs(eb) - 1;
+                    break;
+                }
+            }
+            if (lane == src) {
+                if (ej != P1_INF) {
+                    SkmRecord r;
+                    r.pos = rec_pack_pos((uint64_t)o_pos, o_phase, tail_of(bits_at(ej + k - 1) & 7u));
+                    r.len = (uint32_t)(sbeg + ej - o_pos);
+                    r.key = o_key;
+                    emit_packed(a, hist, o_slot, r);
+                } else {  // past the staged range too: from global memory
+                    const int64_t c0 = sbeg + cj;
+                    const int64_t rr = read_of(a.offs, a.n_reads, (uint64_t)o_pos);
+                    const int64_t re = (int64_t)a.offs[rr + 1];
+                    int64_t e = c0 > o_pos + 1 ? c0 : o_pos + 1;
+                    while (e + k <= re && kmer_key_global<LUT>(a, (uint64_t)e) == o_key) e++;
+                    const int64_t rest = re - (e + k - 1);
+                    emit_record(a, hist, o_slot, (uint64_t)o_pos, (uint32_t)(e - o_pos), o_key, o_phase,
+                                rest >= 3 ? 3u : (uint32_t)rest);
+                }
             }
             __syncwarp();
         }
