@@ -276,7 +276,8 @@ enum {
     GKC_K_RADIX_SCATTER = 6,    /* phase 2 sort: stable scatter            */
     GKC_K_SCAN = 7,             /* device-wide scans                       */
     GKC_K_RLE = 8,              /* run-length encoding + threshold         */
-    GKC_K_CLASSES = 9
+    GKC_K_BUCKET_SPLIT = 9,     /* phase 2 hash: superkmers -> sub-buckets */
+    GKC_K_CLASSES = 10
 };
 
 /* With profiling on, every kernel launch is bracketed by CUDA events on the

@@ -38,7 +38,7 @@ EXPORTS = (
     "gkc_init", "gkc_skmgen_batch", "gkc_count_partition", "gkc_set_order_lut", "gkc_shutdown",
 )
 KERNEL_CLASSES = ("find_superkmers", "scatter_superkmers", "hash_insert", "hash_collect", "sort_extract",
-                  "radix_hist", "radix_scatter", "scan", "rle")
+                  "radix_hist", "radix_scatter", "scan", "rle", "bucket_split")
 
 
 class Options(C.Structure):

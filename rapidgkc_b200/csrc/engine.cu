@@ -306,7 +306,7 @@ struct gkc_ctx {
     // FASTQ / FASTA scanning: staged text, tile transforms and carries, the CSR
     DevBuf fx_text, fx_tiles, fx_state, fx_kept, fx_reads, fx_res, fx_out, fx_offs;
     // .skm loading: tile transforms and carries, superkmer starts, k-mer counts
-    DevBuf sk_tiles, sk_state, sk_tstarts, sk_res, sk_starts, sk_k32;
+    DevBuf sk_tiles, sk_state, sk_tstarts, sk_res, sk_starts, sk_k32, sk_po;
     DevBuf hpc_tiles, hpc_tbase, hpc_reads, hpc_offs;  // homopolymer-compressed batch
     std::vector<StoreChunk *> store;
 
@@ -328,7 +328,7 @@ struct gkc_ctx {
     DevBuf keysA, keysB, tiles, counts, offsets, blocksums, heads_pos, heads_key, tilecnt, tileoff;
     DevBuf os_status, os_hist, os_chunks, os_ctr;  // one-pass-per-digit radix sort
     DevBuf segoff, segcur, part_err, scal;
-    DevBuf stage_bytes, stage_idx;
+    DevBuf stage_bytes, stage_idx, stage_keys;
     DevBuf spill_bytes[2], spill_idx[2], spill_keys[2];  // device staging of chunks being spilled
     // shared-memory bucket counter
     DevBuf bk_skms, bk_kmers, bk_off, bk_cur, bk_entries, bk_failed, bk_arena, bk_part, bk_desc;
@@ -655,29 +655,94 @@ int spill_slot(gkc_ctx *ctx, uint64_t nbytes, uint64_t nskm, DevBuf **db, DevBuf
 // Copies a chunk from the current device staging slot (c->bytes, idx, keys,
 // written on ctx->s) to pinned host memory of the context's arena, on the
 // spill stream; the slot is released by spill_done when the copy ends.
+// Only the superkmer bytes are kept: a spilled chunk's index entries and
+// minimizer keys follow from its bytes and partition offsets, and are rebuilt
+// on the device when a range of it is staged back (stage_spilled).  That
+// halves the pinned memory and the PCIe traffic of a spilled store.
 int spill_chunk(gkc_ctx *ctx, StoreChunk *c) {
-    // three regions, so slabs pack tightly
-    const uint64_t ni = std::max<uint64_t>(c->nskm, 1);
-    uint8_t *hb = nullptr, *hi8 = nullptr, *hk8 = nullptr;
+    uint8_t *hb = nullptr;
     cudaError_t ea = ctx->arena.take(c->nbytes + 16, &hb);
-    if (ea == cudaSuccess) ea = ctx->arena.take(ni * 8, &hi8);
-    if (ea == cudaSuccess) ea = ctx->arena.take(ni * 4, &hk8);
     if (ea != cudaSuccess) return ctx->fail(GKC_ENOMEM, "pinned spill allocation: %s", cudaGetErrorString(ea));
-    uint64_t *hi = reinterpret_cast<uint64_t *>(hi8);
-    uint32_t *hk = reinterpret_cast<uint32_t *>(hk8);
-    // the copies wait for the chunk's kernels, not the other way round:
+    // the copy waits for the chunk's kernels, not the other way round:
     // readers of spilled chunks call spill_sync first
     CK(cudaEventRecord(ctx->spill_ready, ctx->s));
     CK(cudaStreamWaitEvent(ctx->ss, ctx->spill_ready, 0));
     CK(cudaMemcpyAsync(hb, c->bytes, c->nbytes, cudaMemcpyDeviceToHost, ctx->ss));
-    CK(cudaMemcpyAsync(hi, c->idx, c->nskm * 8, cudaMemcpyDeviceToHost, ctx->ss));
-    CK(cudaMemcpyAsync(hk, c->keys, c->nskm * 4, cudaMemcpyDeviceToHost, ctx->ss));
     CK(cudaEventRecord(ctx->spill_done[ctx->spill_slot], ctx->ss));
     ctx->spill_slot ^= 1;
     c->bytes = hb;
-    c->idx = hi;
-    c->keys = hk;
+    c->idx = nullptr;
+    c->keys = nullptr;
     c->on_host = true;
+    return GKC_OK;
+}
+
+// Stages partitions [p0, p1) of spilled chunk c on stream st: its bytes to pb
+// (then 32 zero bytes of padding), and its index entries and minimizer keys,
+// rebuilt from the bytes by the .skm parse (skm_load.cu) under the context's
+// order, to pi / pk (one per superkmer of the range, in byte order; the
+// order of a partition's entries does not matter to any reader).
+int stage_spilled(gkc_ctx *ctx, StoreChunk *c, uint32_t p0, uint32_t p1, uint8_t *pb, uint64_t *pi, uint32_t *pk,
+                  cudaStream_t st) {
+    const uint64_t b0 = c->byte_off[p0], b1 = c->byte_off[p1], s0 = c->skm_off[p0], s1 = c->skm_off[p1];
+    const uint64_t n = b1 - b0, nskm = s1 - s0;
+    CK(cudaMemcpyAsync(pb, c->bytes + b0, n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(pb + n, 0, 32, st));
+    if (!nskm) return GKC_OK;
+    const uint32_t np = p1 - p0;
+    const uint64_t ntiles = (n + gkc::SL_TILE - 1) / gkc::SL_TILE;
+    CK(ctx->sk_po.ensure((np + 1) * 8ull));
+    CK(ctx->sk_tiles.ensure(ntiles * sizeof(gkc::SlT)));
+    CK(ctx->sk_state.ensure(ntiles));
+    CK(ctx->sk_tstarts.ensure(ntiles * 8));
+    CK(ctx->sk_res.ensure(64));
+    CK(ctx->sk_starts.ensure(nskm * 8));
+    CK(ctx->sk_k32.ensure(nskm * 4));
+    // the partition offsets, rebased to the staged range (a pageable copy: the
+    // call returns once the source is consumed)
+    std::vector<unsigned long long> po(np + 1);
+    for (uint32_t j = 0; j <= np; j++) po[j] = c->byte_off[p0 + j] - b0;
+    CK(cudaMemcpyAsync(ctx->sk_po.p, po.data(), (np + 1) * 8ull, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(ctx->sk_res.p, 0, 64, st));
+    gkc::SlParams a;
+    a.bytes = pb;
+    a.n = n;
+    a.part_off = ctx->sk_po.as<unsigned long long>();
+    a.P = np;
+    a.tiles = ctx->sk_tiles.as<gkc::SlT>();
+    a.ntiles = ntiles;
+    a.tile_state = ctx->sk_state.as<uint8_t>();
+    a.tile_starts = ctx->sk_tstarts.as<uint64_t>();
+    a.result = ctx->sk_res.as<uint64_t>();
+    a.err = reinterpret_cast<uint32_t *>(ctx->sk_res.as<uint64_t>() + 1);
+    a.starts = ctx->sk_starts.as<uint64_t>();
+    gkc::skm_tile_kernel<<<(uint32_t)ntiles, gkc::SL_THREADS, 0, st>>>(a);
+    LAUNCHED();
+    gkc::skm_carry_kernel<<<1, gkc::SL_CARRY_THREADS, 0, st>>>(a);
+    LAUNCHED();
+    gkc::skm_starts_kernel<<<(uint32_t)ntiles, gkc::SL_THREADS, 0, st>>>(a);
+    LAUNCHED();
+    gkc::SiParams x;
+    x.bytes = pb;
+    x.n = n;
+    x.part_off = a.part_off;
+    x.P = np;
+    x.part0 = p0;
+    x.P_store = (uint32_t)ctx->opt.partitions;
+    x.pmod = gkc::fastmod_m(x.P_store);
+    x.k = ctx->opt.k;
+    x.p = ctx->opt.p;
+    x.lut = ctx->has_lut ? ctx->lut.as<uint32_t>() : nullptr;
+    x.starts = a.starts;
+    x.nskm = nskm;
+    x.idx = pi;
+    x.keys = pk;
+    x.part_kmers32 = ctx->sk_k32.as<uint32_t>();
+    x.err = a.err;
+    const uint32_t g = (uint32_t)std::min<uint64_t>((nskm + 255) / 256, (uint64_t)ctx->sms * 8);
+    if (x.lut) gkc::skm_index_kernel<true><<<g, 256, 0, st>>>(x);
+    else gkc::skm_index_kernel<false><<<g, 256, 0, st>>>(x);
+    LAUNCHED();
     return GKC_OK;
 }
 
@@ -922,9 +987,7 @@ int chunk_range(gkc_ctx *ctx, StoreChunk *c, uint32_t p0, uint32_t p1, DevBuf &a
     uint8_t *pb = base;
     uint64_t *pi = reinterpret_cast<uint64_t *>(base + nbb);
     uint32_t *pk = reinterpret_cast<uint32_t *>(base + nbb + nib);
-    CK(cudaMemcpyAsync(pb, c->bytes + b0, b1 - b0, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(pi, c->idx + s0, (s1 - s0) * 8, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(pk, c->keys + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, st));
+    RET(stage_spilled(ctx, c, p0, p1, pb, pi, pk, st));
     *arena_used += need;
     // the kernels index with the chunk's absolute offsets: rebase
     *bytes = pb - b0;
@@ -1403,7 +1466,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
             sp.bucket_cursor = ctx->bk_cur.as<unsigned long long>();
             sp.entries = ctx->bk_entries.as<BEntry>();
             sp.pass = pass;
-            KScope ks(ctx, GKC_K_SCAN, pass ? 28.0 * gs : 12.0 * gs);
+            KScope ks(ctx, GKC_K_BUCKET_SPLIT, pass ? 28.0 * gs : 12.0 * gs);
             bucket_split_kernel<<<ncta, BS_THREADS, BS_SMEM, ctx->s>>>(sp);
             LAUNCHED();
         }
@@ -1828,8 +1891,9 @@ int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
                     CK(cudaStreamSynchronize(ctx->s));
                     CK(ctx->stage_bytes.ensure(b1 - b0 + 32));
                     CK(ctx->stage_idx.ensure((i1 - i0) * 8 + 8));
-                    CK(cudaMemcpyAsync(ctx->stage_bytes.p, c->bytes + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->s));
-                    CK(cudaMemcpyAsync(ctx->stage_idx.p, c->idx + i0, (i1 - i0) * 8, cudaMemcpyHostToDevice, ctx->s));
+                    CK(ctx->stage_keys.ensure((i1 - i0) * 4 + 4));
+                    RET(stage_spilled(ctx, c, p0, p1, ctx->stage_bytes.as<uint8_t>(), ctx->stage_idx.as<uint64_t>(),
+                                      ctx->stage_keys.as<uint32_t>(), ctx->s));
                     // kernel indexes bytes by partition offsets: rebase the pointers
                     bytes = ctx->stage_bytes.as<uint8_t>() - b0;
                     idx = ctx->stage_idx.as<uint64_t>() - i0;
@@ -2447,6 +2511,8 @@ int gkc_add_skm(gkc_ctx *ctx, const uint8_t *bytes, const uint64_t *part_off, in
     x.n = n;
     x.part_off = a.part_off;
     x.P = P;
+    x.part0 = 0;
+    x.P_store = P;
     x.pmod = gkc::fastmod_m(P);
     x.k = ctx->opt.k;
     x.p = ctx->opt.p;
@@ -3011,13 +3077,14 @@ int gkc_minimizer_loads(gkc_ctx *ctx, uint64_t *loads, uint64_t n, int mem) {
         if (!c->nskm) continue;
         const uint64_t *idx = c->idx;
         const uint32_t *keys = c->keys;
-        if (c->on_host) {  // a spilled chunk: stage its index and keys
-            CK(ctx->ord_stage.ensure(c->nskm * 12));
-            CK(cudaMemcpyAsync(ctx->ord_stage.p, c->idx, c->nskm * 8, cudaMemcpyHostToDevice, ctx->s));
-            CK(cudaMemcpyAsync(ctx->ord_stage.as<uint8_t>() + c->nskm * 8, c->keys, c->nskm * 4,
-                               cudaMemcpyHostToDevice, ctx->s));
-            idx = ctx->ord_stage.as<uint64_t>();
-            keys = reinterpret_cast<const uint32_t *>(ctx->ord_stage.as<uint8_t>() + c->nskm * 8);
+        if (c->on_host) {  // a spilled chunk: stage it, its index and keys rebuilt
+            const uint64_t nbb = (c->nbytes + 32 + 15) / 16 * 16;
+            CK(ctx->ord_stage.ensure(nbb + c->nskm * 12));
+            uint8_t *sb = ctx->ord_stage.as<uint8_t>();
+            RET(stage_spilled(ctx, c, 0, (uint32_t)ctx->opt.partitions, sb, reinterpret_cast<uint64_t *>(sb + nbb),
+                              reinterpret_cast<uint32_t *>(sb + nbb + c->nskm * 8), ctx->s));
+            idx = reinterpret_cast<const uint64_t *>(sb + nbb);
+            keys = reinterpret_cast<const uint32_t *>(sb + nbb + c->nskm * 8);
         }
         const uint32_t g = (uint32_t)std::min<uint64_t>((c->nskm + 255) / 256, (uint64_t)ctx->sms * 8);
         minimizer_loads_kernel<<<g, 256, 0, ctx->s>>>(idx, keys, c->nskm, (uint32_t)(np - 1),

@@ -40,8 +40,11 @@
 
 namespace {
 
+// Defaults are the reference's (utilities.hpp:187-189): k=21, p=7, 31
+// partitions.  Its count threshold [1, 1000] (utilities.hpp:190) is never
+// applied by the reference, so the default here keeps every k-mer.
 struct Args {
-    int k = 31, p = 11, partitions = 512, device = 0;
+    int k = 21, p = 7, partitions = 31, device = 0;
     uint32_t cmin = 1, cmax = 0xFFFFFFFFu;
     std::string out, fmt = "bin", counter = "hash", order = "default";
     bool sorted = false, hpc = false;
@@ -51,7 +54,7 @@ struct Args {
 
 [[noreturn]] void usage(const char *prog, const char *why) {
     std::fprintf(stderr,
-                 "%s\nUsage: %s -k <K> -p <P> -skm <partitions> [-ci <min count>] [-cx <max count>]\n"
+                 "%s\nUsage: %s [-k <K> (21)] [-p <P> (7)] [-skm <partitions> (31)] [-ci <min count>] [-cx <max count>]\n"
                  "       [-o <output>] [-of bin|txt] [-sorted] [-counter hash|sort]\n"
                  "       [-order default|learned|<params.f32>] [-gpu <device>] [-bb <batch MB>] [-hpc 0|1]\n"
                  "       -read <files...>\n"
@@ -391,6 +394,12 @@ int main(int argc, char **argv) {
     parser.join();
     const double t1 = secs();
     // ---- phase 2
+    uint64_t kmer_instances = 0;
+    {
+        std::vector<uint64_t> pb(a.partitions), ps(a.partitions), pk(a.partitions);
+        check(gkc_store_stats(ctx, pb.data(), ps.data(), pk.data()), ctx, "store stats");
+        for (uint64_t v : pk) kmer_instances += v;
+    }
     uint64_t n_out = 0, n_distinct = 0;
     check(gkc_count(ctx, a.cmin, a.cmax, &n_out, &n_distinct), ctx, "phase 2");
     const double t2 = secs();
@@ -425,11 +434,16 @@ int main(int argc, char **argv) {
         cudaFreeHost(ct);
     }
     const double t3 = secs();
+    // the reference's report: its log lines on stderr (gkc_main.cpp:385 and
+    // the phase-1 k-mer total), the wall seconds alone on stdout (:433)
+    std::fprintf(stderr, "P0 [INFO]\tKMER TOT CNT = %llu\n", (unsigned long long)kmer_instances);
+    std::fprintf(stderr, "P0 [NOTICE]\tTotal number of distinct kmers: %llu\n", (unsigned long long)n_distinct);
     std::fprintf(stderr,
                  "reads %llu, bases %llu, distinct k-mers %llu, written %llu (count in [%u, %u])\n"
                  "phase 1 %.3f s, phase 2 %.3f s, output %.3f s, total %.3f s (%.2f Gbp/s)\n",
                  (unsigned long long)n_reads, (unsigned long long)n_bases, (unsigned long long)n_distinct,
                  (unsigned long long)n_out, a.cmin, a.cmax, t1, t2 - t1, t3 - t2, t3, n_bases / t3 / 1e9);
+    std::printf("%g\n", t3);
     gkc_destroy(ctx);
     return 0;
 }

@@ -177,9 +177,11 @@ __global__ void __launch_bounds__(SL_THREADS) skm_starts_kernel(SlParams a) {
 struct SiParams {
     const uint8_t *bytes;
     uint64_t n;
-    const unsigned long long *part_off;
+    const unsigned long long *part_off;  // [P+1] starts of partitions part0 .. part0 + P in bytes
     uint32_t P;
-    uint64_t pmod;
+    uint32_t part0;             // the store partition of part_off[0]
+    uint32_t P_store;           // the store's partitions (the key -> partition map)
+    uint64_t pmod;              // fastmod multiplier of P_store
     int k, p;
     const uint32_t *lut;        // canonical order table, or null for the default order
     const uint64_t *starts;
@@ -230,7 +232,7 @@ __global__ void __launch_bounds__(256) skm_index_kernel(SiParams a) {
                 }
             }
         }
-        if (kmers && fastmod(~best, a.pmod, a.P) != part) atomicOr(a.err, SKM_ERR_PARTITION);
+        if (kmers && fastmod(~best, a.pmod, a.P_store) != a.part0 + part) atomicOr(a.err, SKM_ERR_PARTITION);
         a.idx[i] = idx_pack(s - a.part_off[part], kmers);
         a.keys[i] = best;
         a.part_kmers32[i] = kmers;

@@ -26,7 +26,7 @@ from . import synth
 from .capi import KmerCounter
 
 
-STORE_BYTES_PER_BASE = 2.4
+STORE_BYTES_PER_BASE = 1.35  # a spilled chunk keeps its superkmer bytes only
 
 
 def _mem_available() -> int:
@@ -67,8 +67,9 @@ def stream_count(workload: str = "human_3g", scale: float = 1.0, batch_gb: float
             q.put(item)
         q.put(None)
 
-    # the spilled store takes ~2.3 bytes per base (superkmer bytes 1.2, index
-    # and keys 12 per superkmer); it must fit host memory beside two batches
+    # the spilled store takes ~1.3 bytes per base (superkmer bytes; index
+    # entries and keys are rebuilt on the device when a range is staged back);
+    # it must fit host memory beside two batches
     est_store = int(STORE_BYTES_PER_BASE * n_reads * read_len) if spill else 0
     avail = _mem_available()
     if spill and avail and est_store > 0.8 * avail - 4 * batch_gb * 1e9:

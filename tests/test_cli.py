@@ -74,6 +74,9 @@ def test_cli_counts_match_oracle(oracle, tmp_path):
     p_ = _run("-k", str(k), "-p", str(p), "-skm", str(P), "-ci", "2", "-o", out, "-sorted", "-t", "8",
               "-read", fq, fa)
     assert f"distinct k-mers {do}" in p_.stderr
+    # the reference's own report lines (gkc_main.cpp:385, 433)
+    assert f"Total number of distinct kmers: {do}" in p_.stderr
+    assert float(p_.stdout.strip().splitlines()[-1]) > 0
     kk, km, ct = _read_bin(out)
     assert kk == k and np.all(np.diff(km.astype(np.int64)) > 0)
     assert np.array_equal(km, ko) and np.array_equal(ct, co)
@@ -143,3 +146,19 @@ def test_cli_wide_kmers(oracle, tmp_path):
     km2 = np.array([[v & (2**64 - 1), v >> 64] for v in vals], np.uint64)
     km2, ct2 = sorted_table(km2, np.array(lines[1::2], np.uint32))
     assert np.array_equal(km2, ko) and np.array_equal(ct2, co)
+
+
+@pytest.mark.gpu
+def test_cli_reference_defaults(oracle, tmp_path):
+    """No -k / -p / -skm: the reference's defaults (k=21, p=7, 31 partitions,
+    utilities.hpp:187-189) and its report lines."""
+    reads, offs = random_reads(93, 8_000, 2000, (40, 300), 0.005)
+    fq, _ = _write_inputs(str(tmp_path), reads, offs)
+    ko, co, do, pk = oracle.count_reads(reads, offs, 21, 7, 31, 1, U32)
+    out = str(tmp_path / "counts.bin")
+    p_ = _run("-o", out, "-sorted", "-read", fq)
+    assert f"Total number of distinct kmers: {do}" in p_.stderr
+    assert f"KMER TOT CNT = {int(pk.sum())}" in p_.stderr
+    kk, km, ct = _read_bin(out)
+    ko, co = sorted_table(ko, co)
+    assert kk == 21 and np.array_equal(km, ko) and np.array_equal(ct, co)
