@@ -68,7 +68,7 @@ typedef struct gkc_options {
     int p;                  /* minimizer length, 3 <= p <= 16 (reference -p, utilities.hpp:188)   */
     int partitions;         /* superkmer partitions, 1..4096 (reference -skm, utilities.hpp:189)  */
     int counter;            /* GKC_COUNTER_SORT or GKC_COUNTER_HASH                               */
-    int radix_bits;         /* LSD digit width of the sort counter, 4..11 (0 = 11)                */
+    int radix_bits;         /* LSD digit width of the sort counter, 4..11 (0 = 8)                 */
     double table_slots;     /* hash slots per k-mer instance of a partition (0 = 0.35)            */
     uint64_t batch_bases;   /* bases per phase-1 batch, host and device input (0 = 1 GiB)         */
     int spill_host;         /* keep the partition store in pinned host memory (streamed input)    */

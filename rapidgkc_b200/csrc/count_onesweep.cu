@@ -24,7 +24,10 @@
 //
 // Per pass the keys are read once and written once; the look-back statuses
 // add NB x 4 bytes per tile.  Digits are up to 11 bits (6 passes over the 62
-// bits of a 31-mer).  A status word holds a 2-bit flag and a 30-bit count,
+// bits of a 31-mer); 8 bits is the default (8 passes): a thread then owns one
+// digit in the look-back and reads 32 earlier tiles' statuses per step, where
+// with 2048 digits it owns eight and can read only four, and the look-back's
+// progress (tiles per L2 round trip) bounds the pass.  A status word holds a 2-bit flag and a 30-bit count,
 // so segments are limited to 2^30 - 1 keys (larger ones use the
 // three-kernel sort of count_sort.cu).  The flags cycle through three
 // (aggregate, inclusive) pairs, so statuses left by the previous pass never
@@ -37,7 +40,7 @@ constexpr int OS_THREADS = 256;
 constexpr int OS_WARPS = OS_THREADS / 32;
 constexpr int OS_MAX_PASSES = 32;
 constexpr uint32_t OS_SEG_MAX = (1u << 30) - 1;
-constexpr uint32_t OS_SPIN_LIMIT = 1u << 22;  // look-back polls before giving up (~0.4 s)
+constexpr uint64_t OS_WAIT_NS = 100000000ull;  // a look-back gives up after 0.1 s of waiting
 constexpr uint32_t ERR_LOOKBACK = 1u << 10;   // a look-back wait ran out
 
 // keys per thread: 16 u64 or 8 u128, so a tile's keys take 32 KB either way
@@ -119,6 +122,11 @@ __global__ void __launch_bounds__(1024) os_scan_kernel(uint32_t *ghist) {
 }
 
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t os_now_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 __device__ __forceinline__ uint32_t os_load_status(const uint32_t *p) {
     uint32_t v;
     asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -165,7 +173,10 @@ os_pass_kernel(OsPassParams a) {
     const uint32_t dmask = (1u << a.width) - 1;
 
     constexpr int BPT = NB >= OS_THREADS ? NB / OS_THREADS : 1;  // digits per thread in the look-back
-    constexpr int LB_ROWS = 4;  // earlier tiles read at once per digit
+    // earlier tiles read at once per digit: the look-back frontier advances
+    // at most this many tiles per L2 round trip, so a thread with one digit
+    // reads 32 rows a step (32 status loads in flight either way)
+    constexpr int LB_ROWS = BPT >= 8 ? 4 : 32 / BPT;
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);
         for (int i = threadIdx.x; i < OS_WARPS * NB / 2; i += OS_THREADS) reinterpret_cast<uint32_t *>(wcnt)[i] = 0;
@@ -259,7 +270,7 @@ os_pass_kernel(OsPassParams a) {
                 left[x] = td.t;  // earlier tiles of the segment
                 if (td.t != 0 && x * OS_THREADS + (int)threadIdx.x < NB) pending |= 1u << x;
             }
-            uint32_t spins = 0;
+            uint64_t t_wait = 0;  // when this thread first waited
             while (pending) {
                 uint32_t v[BPT][LB_ROWS];
 #pragma unroll
@@ -304,8 +315,17 @@ os_pass_kernel(OsPassParams a) {
                     }
                 }
                 if (waited) {
-                    if (++spins > OS_SPIN_LIMIT) {  // never expected: record it and stop waiting
-                        atomicOr(a.err, ERR_LOOKBACK);
+                    // never expected: an earlier tile that does not publish.  Give
+                    // up after OS_WAIT_NS, or at once when another tile gave up,
+                    // record it and go on (the host then fails the call)
+                    const uint64_t now = os_now_ns();
+                    if (!t_wait) t_wait = now;
+                    if (now - t_wait > OS_WAIT_NS || (os_load_status(a.err) & ERR_LOOKBACK)) {
+                        if (!(atomicOr(a.err, ERR_LOOKBACK) & ERR_LOOKBACK)) {  // the first to give up
+                            a.err[1] = tile;
+                            a.err[2] = (uint32_t)__ffs(pending) - 1 + 0;  // the digit slot still waiting
+                            a.err[3] = td.t;
+                        }
                         break;
                     }
                     __nanosleep(32);

@@ -120,14 +120,18 @@ sort_extract_kernel(SExtractParams a) {
             const uint64_t d0 = __shfl_sync(FULL, delta, 0);
             for (uint32_t x = lane; x < n_st; x += 32) keys[d0 + x] = sw[x];
         } else {
-            for (uint32_t x = lane; x < n_st; x += 32) {
+            // every lane takes every step (the owner search shuffles), the
+            // store is predicated
+            for (uint32_t x0 = 0; x0 < n_st; x0 += 32) {
+                const uint32_t x = x0 + lane;
                 int own = 0;  // the last lane whose range starts at or before x
 #pragma unroll
                 for (int st = 16; st; st >>= 1) {
                     const int cand = own + st;
                     if (__shfl_sync(FULL, excl, cand) <= x) own = cand;
                 }
-                keys[__shfl_sync(FULL, delta, own) + x] = sw[x];
+                const uint64_t dl = __shfl_sync(FULL, delta, own);
+                if (x < n_st) keys[dl + x] = sw[x];
             }
         }
         __syncwarp();

@@ -1700,7 +1700,7 @@ int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, i
     CK(cudaMemsetAsync(ctx->os_hist.p, 0, nhist * 4, ctx->s));
     CK(cudaMemsetAsync(ctx->os_status.p, 0, ntiles * NB * 4, ctx->s));
     CK(cudaMemsetAsync(ctx->os_ctr.p, 0, 64 * 4, ctx->s));
-    CK(cudaMemsetAsync(ctx->part_err.p, 0, 4, ctx->s));
+    CK(cudaMemsetAsync(ctx->part_err.p, 0, 16, ctx->s));
     const size_t hsm = (size_t)ps.n * NB * 4;
     {
         static bool attr = false;  // per template instance
@@ -1751,10 +1751,12 @@ int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, i
         }
         std::swap(src, dst);
     }
-    uint32_t e = 0;
-    CK(cudaMemcpyAsync(&e, ctx->part_err.p, 4, cudaMemcpyDeviceToHost, ctx->s));
+    uint32_t e[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(e, ctx->part_err.p, 16, cudaMemcpyDeviceToHost, ctx->s));
     CK(cudaStreamSynchronize(ctx->s));
-    if (e & ERR_LOOKBACK) return ctx->fail(GKC_EINTERNAL, "radix sort: a look-back wait ran out");
+    if (e[0] & ERR_LOOKBACK)
+        return ctx->fail(GKC_EINTERNAL, "radix sort: a look-back wait ran out (tile %u of %llu, %u of its segment, "
+                                        "digit slot %u)", e[1], (unsigned long long)ntiles, e[3], e[2]);
     *sorted = src;
     return GKC_OK;
 }
@@ -1965,7 +1967,7 @@ void gkc_default_options(gkc_options *o) {
     o->p = 11;
     o->partitions = 512;
     o->counter = GKC_COUNTER_HASH;
-    o->radix_bits = 11;
+    o->radix_bits = 8;
     o->table_slots = 0.35;
     o->batch_bases = 1ull << 30;
     o->spill_host = 0;
@@ -2002,7 +2004,7 @@ int gkc_create(int device, const gkc_options *opt, gkc_ctx **out) {
         (o.counter != GKC_COUNTER_SORT && o.counter != GKC_COUNTER_HASH) || o.radix_bits < 0 || o.radix_bits > 11 ||
         (o.radix_bits != 0 && o.radix_bits < 4))
         return GKC_EINVAL;
-    if (!o.radix_bits) o.radix_bits = 11;
+    if (!o.radix_bits) o.radix_bits = 8;
     if (!o.batch_bases) o.batch_bases = 1ull << 30;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return GKC_ECUDA;
