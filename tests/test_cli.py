@@ -153,10 +153,10 @@ def test_cli_reference_defaults(oracle, tmp_path):
     """No -k / -p / -skm: the reference's defaults (k=21, p=7, 31 partitions,
     utilities.hpp:187-189) and its report lines."""
     reads, offs = random_reads(93, 8_000, 2000, (40, 300), 0.005)
-    fq, _ = _write_inputs(str(tmp_path), reads, offs)
+    fq, fa = _write_inputs(str(tmp_path), reads, offs)  # half the reads in each file
     ko, co, do, pk = oracle.count_reads(reads, offs, 21, 7, 31, 1, U32)
     out = str(tmp_path / "counts.bin")
-    p_ = _run("-o", out, "-sorted", "-read", fq)
+    p_ = _run("-o", out, "-sorted", "-read", fq, fa)
     assert f"Total number of distinct kmers: {do}" in p_.stderr
     assert f"KMER TOT CNT = {int(pk.sum())}" in p_.stderr
     kk, km, ct = _read_bin(out)
