@@ -24,10 +24,13 @@
 //
 // Per pass the keys are read once and written once; the look-back statuses
 // add NB x 4 bytes per tile.  Digits are up to 11 bits (6 passes over the 62
-// bits of a 31-mer); 8 bits is the default (8 passes): a thread then owns one
-// digit in the look-back and reads 32 earlier tiles' statuses per step, where
-// with 2048 digits it owns eight and can read only four, and the look-back's
-// progress (tiles per L2 round trip) bounds the pass.  A status word holds a 2-bit flag and a 30-bit count,
+// bits of a 31-mer); 8 bits is the default (8 passes): with 8-bit digits a
+// tile's runs average 16 keys (128 bytes, whole sectors), where 11-bit digits
+// leave 2-key runs and partial sectors.  A thread owns one digit (8 bits) in
+// the look-back and reads four earlier tiles' statuses per step; the pass is
+// latency-bound unless three CTAs share an SM, so the look-back keeps its
+// loads few (one base address, constant row offsets) and the register count
+// under the three-CTA bound.  A status word holds a 2-bit flag and a 30-bit count,
 // so segments are limited to 2^30 - 1 keys (larger ones use the
 // three-kernel sort of count_sort.cu).  The flags cycle through three
 // (aggregate, inclusive) pairs, so statuses left by the previous pass never
@@ -149,8 +152,12 @@ struct OsPassParams {
     uint32_t *err;
 };
 
+// CTAs per SM the register budget must allow: three with 16 u64 keys a thread
+// (80 registers, no spills; four would spill), four with 8 u128 keys
+template <class KT> constexpr int os_min_ctas() { return sizeof(KT) == 16 ? 4 : 3; }
+
 template <int RB, class KT>
-__global__ void __launch_bounds__(OS_THREADS)
+__global__ void __launch_bounds__(OS_THREADS, os_min_ctas<KT>())
 os_pass_kernel(OsPassParams a) {
     constexpr int NB = 1 << RB;
     constexpr int ITEMS = os_items<KT>();
@@ -173,10 +180,10 @@ os_pass_kernel(OsPassParams a) {
     const uint32_t dmask = (1u << a.width) - 1;
 
     constexpr int BPT = NB >= OS_THREADS ? NB / OS_THREADS : 1;  // digits per thread in the look-back
-    // earlier tiles read at once per digit: the look-back frontier advances
-    // at most this many tiles per L2 round trip, so a thread with one digit
-    // reads 32 rows a step (32 status loads in flight either way)
-    constexpr int LB_ROWS = BPT >= 8 ? 4 : 32 / BPT;
+    // earlier tiles read at once per digit: the frontier advances at most
+    // this many tiles per L2 round trip; tiles start in order, so the tile
+    // before is usually already inclusive or nearly so
+    constexpr int LB_ROWS = BPT >= 4 ? 1 : 4 / BPT;
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);
         for (int i = threadIdx.x; i < OS_WARPS * NB / 2; i += OS_THREADS) reinterpret_cast<uint32_t *>(wcnt)[i] = 0;
@@ -193,7 +200,7 @@ os_pass_kernel(OsPassParams a) {
             const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
             key[i] = j < td.n ? in[td.start + j] : KT(0);
         }
-        uint16_t rank[ITEMS];
+        uint32_t rank[(ITEMS + 1) / 2];  // 16-bit ranks, two to a register
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
@@ -202,7 +209,8 @@ os_pass_kernel(OsPassParams a) {
             const unsigned grp = __match_any_sync(FULL, dig);
             uint32_t pre = 0;
             if (valid) pre = wcnt[warp * NB + dig];
-            rank[i] = (uint16_t)(pre + __popc(grp & lt));
+            const uint32_t rk = pre + __popc(grp & lt);
+            if (i & 1) rank[i >> 1] |= rk << 16; else rank[i >> 1] = rk;
             __syncwarp();
             if (valid && (grp & lt) == 0) wcnt[warp * NB + dig] = (uint16_t)(pre + __popc(grp));
             __syncwarp();
@@ -241,21 +249,22 @@ os_pass_kernel(OsPassParams a) {
         __syncthreads();
         // ---- stage the keys in digit order (the counters' area takes the keys) ----
         {
-            uint16_t lpos[ITEMS];
+            // each key's place in the tile, written over its rank (16 bits each)
 #pragma unroll
             for (int i = 0; i < ITEMS; i++) {
                 const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
-                lpos[i] = 0;
+                uint32_t lp = 0;
                 if (j < td.n) {
                     const uint32_t dig = os_digit(key[i], a.shift, dmask);
-                    lpos[i] = (uint16_t)(bstart[dig] + wcnt[warp * NB + dig] + rank[i]);
+                    lp = bstart[dig] + wcnt[warp * NB + dig] + ((rank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
                 }
+                rank[i >> 1] = (i & 1) ? (rank[i >> 1] & 0xFFFFu) | (lp << 16) : (rank[i >> 1] & 0xFFFF0000u) | lp;
             }
             __syncthreads();
 #pragma unroll
             for (int i = 0; i < ITEMS; i++) {
                 const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
-                if (j < td.n) skeys[lpos[i]] = key[i];
+                if (j < td.n) skeys[(rank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu] = key[i];
             }
         }
         // ---- look back: each thread's digits together, LB_ROWS earlier tiles a step ----
@@ -274,13 +283,13 @@ os_pass_kernel(OsPassParams a) {
             while (pending) {
                 uint32_t v[BPT][LB_ROWS];
 #pragma unroll
-                for (int x = 0; x < BPT; x++)
+                for (int x = 0; x < BPT; x++) {
+                    // row jn - r of digit slot x: one base, constant offsets
+                    const uint32_t *row = a.status + (uint64_t)jn[x] * NB + x * OS_THREADS + threadIdx.x;
 #pragma unroll
                     for (int r = 0; r < LB_ROWS; r++)
-                        v[x][r] = ((pending >> x) & 1) && (uint32_t)r < left[x]
-                                      ? os_load_status(a.status + (uint64_t)(jn[x] - r) * NB + x * OS_THREADS +
-                                                       threadIdx.x)
-                                      : 0u;
+                        v[x][r] = ((pending >> x) & 1) && (uint32_t)r < left[x] ? os_load_status(row - r * NB) : 0u;
+                }
                 bool waited = false;
 #pragma unroll
                 for (int x = 0; x < BPT; x++) {

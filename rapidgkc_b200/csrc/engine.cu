@@ -1709,6 +1709,9 @@ int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, i
                                     (int)((size_t)((8 * sizeof(KT) + RB - 1) / RB) * NB * 4)));
             CK(cudaFuncSetAttribute(os_pass_kernel<RB, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)os_pass_smem<RB, KT>()));
+            // all of the unified L1 that may be shared memory: several CTAs per SM
+            CK(cudaFuncSetAttribute(os_pass_kernel<RB, KT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared));
             attr = true;
         }
     }

@@ -6,8 +6,10 @@ serialises every launch ends quickly).
     python -m rapidgkc_b200.profcase [--workload skewed_200m] [--scale 0.05]
         [--counter hash|sort] [--order learned|mix|default] [--reps 2] [--k 31]
 
-Prints one JSON line: bases, kept and distinct k-mers, and the device time
-of the last count (CUDA events).
+Prints one JSON line: bases, kept and distinct k-mers, the device time of
+the last count (CUDA events), free device memory before the counts, and,
+with --classes, each kernel class's time, launches and algorithmic bytes over
+one more count with every launch bracketed by events.
 """
 from __future__ import annotations
 
@@ -30,6 +32,7 @@ def main():
     ap.add_argument("--partitions", type=int, default=512)
     ap.add_argument("--radix-bits", type=int, default=0)
     ap.add_argument("--batch-mb", type=int, default=256)
+    ap.add_argument("--classes", action="store_true", help="also time every kernel class (one more count)")
     args = ap.parse_args()
 
     import torch
@@ -55,9 +58,21 @@ def main():
             e1.record(stream)
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1)
-        print(json.dumps({"workload": args.workload, "scale": args.scale, "bases": int(offs[-1]),
-                          "counter": args.counter, "order": args.order, "kept": n_out, "distinct": n_dist,
-                          "ms_last": ms, "launches": c.kernel_launches()}), flush=True)
+        free_b, total_b = torch.cuda.mem_get_info()
+        line = {"workload": args.workload, "scale": args.scale, "bases": int(offs[-1]),
+                "counter": args.counter, "order": args.order, "kept": n_out, "distinct": n_dist,
+                "ms_last": ms, "gbps_last": int(offs[-1]) / ms / 1e6, "launches": c.kernel_launches(),
+                "free_gb_after": free_b / 1e9, "timings": c.timings()}
+        if args.classes:
+            c.set_profiling(True)
+            c.kernel_stats(reset=True)
+            c.count_reads(d_reads, d_offs, 2)
+            torch.cuda.synchronize()
+            line["classes"] = {k: {"ms": round(v[0], 3), "launches": v[1],
+                                   "gbs": round(v[2] / (v[0] / 1e3) / 1e9, 1) if v[0] else 0.0}
+                               for k, v in c.kernel_stats(reset=True).items() if v[1]}
+            c.set_profiling(False)
+        print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":
