@@ -50,6 +50,28 @@ constexpr uint32_t ERR_LOOKBACK = 1u << 10;   // a look-back wait ran out
 template <class KT> constexpr int os_items() { return sizeof(KT) == 16 ? 8 : 16; }
 template <class KT> constexpr int os_tile() { return OS_THREADS * os_items<KT>(); }
 
+// The segments of one sort: segment s holds keys [key0[s], key0[s+1]) of the
+// key buffer, pass tiles [tile0[s], tile0[s+1]) and histogram chunks
+// [chunk0[s], chunk0[s+1]).  Kernels find a tile's or chunk's segment by a
+// binary search, so no per-tile descriptor is built on the host.
+struct OsSegs {
+    const unsigned long long *key0;  // [nseg + 1]
+    const uint32_t *tile0;           // [nseg + 1]
+    const uint32_t *chunk0;          // [nseg + 1]
+    uint32_t nseg;
+};
+
+// The segment holding item x: the largest s with first[s] <= x (first[0] = 0,
+// first[nseg] > x; empty segments repeat a value and are skipped).
+__device__ __forceinline__ uint32_t os_seg_of(const uint32_t *first, uint32_t nseg, uint32_t x) {
+    uint32_t lo = 0, hi = nseg;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(first + mid) <= x) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 struct OsTile {
     uint64_t start;      // first key of the tile
     uint64_t seg_start;  // first key of its segment
@@ -58,7 +80,6 @@ struct OsTile {
     uint32_t seg;        // segment index
     uint32_t seg_n;      // keys in the segment
 };
-static_assert(sizeof(OsTile) == 32, "tile layout");
 
 struct OsPasses {
     int n;                        // passes
@@ -72,30 +93,29 @@ __device__ __forceinline__ uint32_t os_digit(const KT &key, int shift, uint32_t 
 }
 
 // ---------------------------------------------------------------------------
-// Per-segment histograms of every pass.  A CTA counts one chunk (a range of
-// one segment) in shared memory and adds the nonzero counts to
+// Per-segment histograms of every pass.  A CTA counts one chunk (OS_HCHUNK
+// keys of one segment) in shared memory and adds the nonzero counts to
 // ghist[seg][pass][digit].
-struct OsChunk {
-    uint64_t start;
-    uint32_t n;
-    uint32_t seg;
-};
+constexpr uint32_t OS_HCHUNK = 1u << 16;
 
 template <int RB, class KT>
 __global__ void __launch_bounds__(OS_THREADS)
-os_hist_kernel(const KT *__restrict__ keys, const OsChunk *__restrict__ chunks, OsPasses ps, uint32_t *ghist) {
+os_hist_kernel(const KT *__restrict__ keys, OsSegs sg, OsPasses ps, uint32_t *ghist) {
     constexpr int NB = 1 << RB;
     extern __shared__ uint32_t h[];  // [ps.n][NB]
-    const OsChunk ch = chunks[blockIdx.x];
+    const uint32_t seg = os_seg_of(sg.chunk0, sg.nseg, blockIdx.x);
+    const uint64_t s0 = sg.key0[seg], s1 = sg.key0[seg + 1];
+    const uint64_t c0 = s0 + (uint64_t)(blockIdx.x - sg.chunk0[seg]) * OS_HCHUNK;
+    const uint32_t n = (uint32_t)(s1 - c0 < OS_HCHUNK ? s1 - c0 : OS_HCHUNK);
     for (int i = threadIdx.x; i < ps.n * NB; i += OS_THREADS) h[i] = 0;
     __syncthreads();
-    for (uint32_t j = threadIdx.x; j < ch.n; j += OS_THREADS) {
-        const KT key = keys[ch.start + j];
+    for (uint32_t j = threadIdx.x; j < n; j += OS_THREADS) {
+        const KT key = keys[c0 + j];
         for (int p = 0; p < ps.n; p++)
             atomicAdd(&h[p * NB + os_digit(key, ps.shift[p], (1u << ps.width[p]) - 1)], 1u);
     }
     __syncthreads();
-    uint32_t *g = ghist + (uint64_t)ch.seg * ps.n * NB;
+    uint32_t *g = ghist + (uint64_t)seg * ps.n * NB;
     for (int i = threadIdx.x; i < ps.n * NB; i += OS_THREADS)
         if (h[i]) atomicAdd(g + i, h[i]);
 }
@@ -142,7 +162,7 @@ __device__ __forceinline__ void os_store_status(uint32_t *p, uint32_t v) {
 struct OsPassParams {
     const void *in;
     void *out;
-    const OsTile *tiles;
+    OsSegs seg;
     uint32_t ntiles;
     uint32_t *status;         // [ntiles][NB]
     const uint32_t *gbase;    // [nseg][npass][NB] digit starts in the segment
@@ -156,13 +176,21 @@ struct OsPassParams {
 // (80 registers, no spills; four would spill), four with 8 u128 keys
 template <class KT> constexpr int os_min_ctas() { return sizeof(KT) == 16 ? 4 : 3; }
 
-template <int RB, class KT>
-__global__ void __launch_bounds__(OS_THREADS, os_min_ctas<KT>())
-os_pass_kernel(OsPassParams a) {
+// Shared memory of a pass CTA besides the dynamic key / counter area.
+struct OsShared {
+    uint32_t ws[32];
+    OsTile td;
+    uint32_t tile;
+    uint32_t lb_fail;  // a look-back of this tile gave up: its keys are not written
+};
+
+// One tile of a pass.  WHOLE: the tile holds os_tile<KT>() keys (every tile
+// but a segment's last), so no key needs a bounds check.
+template <int RB, class KT, bool WHOLE>
+__device__ __forceinline__ void os_pass_tile(const OsPassParams &a, OsShared &sh) {
     constexpr int NB = 1 << RB;
     constexpr int ITEMS = os_items<KT>();
     constexpr int T = os_tile<KT>();
-    static_assert(OS_WARPS * NB * 2 <= T * (int)sizeof(KT), "warp counters fit the key staging area");
     extern __shared__ __align__(16) unsigned char os_smem[];
     // the key staging area doubles as the per-warp digit counters (u16)
     KT *skeys = reinterpret_cast<KT *>(os_smem);
@@ -170,198 +198,238 @@ os_pass_kernel(OsPassParams a) {
     uint32_t *bstart = reinterpret_cast<uint32_t *>(os_smem + T * sizeof(KT));  // [NB] tile-local run starts
     int32_t *bdelta = reinterpret_cast<int32_t *>(bstart + NB);       // [NB] segment position - local index
     uint16_t *tcount = reinterpret_cast<uint16_t *>(bdelta + NB);     // [NB] tile counts
-    __shared__ uint32_t ws[32];
-    __shared__ uint32_t s_tile;
-
     const KT *in = static_cast<const KT *>(a.in);
     KT *out = static_cast<KT *>(a.out);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1;
     const uint32_t dmask = (1u << a.width) - 1;
-
+    const uint32_t tile = sh.tile;
+    const OsTile td = sh.td;
     constexpr int BPT = NB >= OS_THREADS ? NB / OS_THREADS : 1;  // digits per thread in the look-back
     // earlier tiles read at once per digit: the frontier advances at most
     // this many tiles per L2 round trip; tiles start in order, so the tile
     // before is usually already inclusive or nearly so
     constexpr int LB_ROWS = BPT >= 4 ? 1 : 4 / BPT;
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);
-        for (int i = threadIdx.x; i < OS_WARPS * NB / 2; i += OS_THREADS) reinterpret_cast<uint32_t *>(wcnt)[i] = 0;
-        __syncthreads();
-        const uint32_t tile = s_tile;
-        if (tile >= a.ntiles) break;
-        const OsTile td = a.tiles[tile];
+    auto has = [&](uint32_t j) { return WHOLE || j < td.n; };
 
-        // ---- load (all loads in flight first), then rank; warp w owns keys
-        //      [w * 32 * ITEMS, (w + 1) * 32 * ITEMS) ----
-        KT key[ITEMS];
+    // ---- load (all loads in flight first), then rank; warp w owns keys
+    //      [w * 32 * ITEMS, (w + 1) * 32 * ITEMS) ----
+    KT key[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
+        key[i] = has(j) ? in[td.start + j] : KT(0);
+    }
+    uint32_t rank[(ITEMS + 1) / 2];  // 16-bit ranks, two to a register
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
+        const bool valid = has(j);
+        const uint32_t dig = valid ? os_digit(key[i], a.shift, dmask) : (uint32_t)NB;
+        const unsigned grp = __match_any_sync(FULL, dig);
+        uint32_t pre = 0;
+        if (valid) pre = wcnt[warp * NB + dig];
+        const uint32_t rk = pre + __popc(grp & lt);
+        if (i & 1) rank[i >> 1] |= rk << 16; else rank[i >> 1] = rk;
+        __syncwarp();
+        if (valid && (grp & lt) == 0) wcnt[warp * NB + dig] = (uint16_t)(pre + __popc(grp));
+        __syncwarp();
+    }
+    __syncthreads();
+    // ---- per digit: exclusive prefix over warps, tile count, published at once ----
+    uint32_t *st = a.status + (uint64_t)tile * NB;
+    for (int b = threadIdx.x; b < NB; b += OS_THREADS) {
+        uint32_t s = 0;
+#pragma unroll
+        for (int w = 0; w < OS_WARPS; w++) {
+            const uint32_t c = wcnt[w * NB + b];
+            wcnt[w * NB + b] = (uint16_t)s;
+            s += c;
+        }
+        tcount[b] = (uint16_t)s;
+        os_store_status(st + b, (td.t == 0 ? a.inc : a.agg) | s);
+    }
+    __syncthreads();
+    // ---- tile-local run starts: exclusive scan of the counts over digits ----
+    {
+        constexpr int PER = NB / OS_THREADS > 0 ? NB / OS_THREADS : 1;
+        const int b0 = threadIdx.x * PER;
+        uint32_t s = 0;
+#pragma unroll
+        for (int i = 0; i < PER; i++) s += b0 + i < NB ? tcount[b0 + i] : 0u;
+        uint32_t tot;
+        uint32_t pre = block_exclusive_scan<OS_THREADS>(s, &tot, sh.ws);
+#pragma unroll
+        for (int i = 0; i < PER; i++)
+            if (b0 + i < NB) {
+                bstart[b0 + i] = pre;
+                pre += tcount[b0 + i];
+            }
+    }
+    __syncthreads();
+    // ---- stage the keys in digit order (the counters' area takes the keys) ----
+    {
+        // each key's place in the tile, written over its rank (16 bits each)
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
-            key[i] = j < td.n ? in[td.start + j] : KT(0);
+            uint32_t lp = 0;
+            if (has(j)) {
+                const uint32_t dig = os_digit(key[i], a.shift, dmask);
+                lp = bstart[dig] + wcnt[warp * NB + dig] + ((rank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
+            }
+            rank[i >> 1] = (i & 1) ? (rank[i >> 1] & 0xFFFFu) | (lp << 16) : (rank[i >> 1] & 0xFFFF0000u) | lp;
         }
-        uint32_t rank[(ITEMS + 1) / 2];  // 16-bit ranks, two to a register
+        __syncthreads();
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
-            const bool valid = j < td.n;
-            const uint32_t dig = valid ? os_digit(key[i], a.shift, dmask) : (uint32_t)NB;
-            const unsigned grp = __match_any_sync(FULL, dig);
-            uint32_t pre = 0;
-            if (valid) pre = wcnt[warp * NB + dig];
-            const uint32_t rk = pre + __popc(grp & lt);
-            if (i & 1) rank[i >> 1] |= rk << 16; else rank[i >> 1] = rk;
-            __syncwarp();
-            if (valid && (grp & lt) == 0) wcnt[warp * NB + dig] = (uint16_t)(pre + __popc(grp));
-            __syncwarp();
+            if (has(j)) skeys[(rank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu] = key[i];
         }
-        __syncthreads();
-        // ---- per digit: exclusive prefix over warps, tile count, published at once ----
-        uint32_t *st = a.status + (uint64_t)tile * NB;
-        for (int b = threadIdx.x; b < NB; b += OS_THREADS) {
-            uint32_t s = 0;
+    }
+    // ---- look back: each thread's digits together, LB_ROWS earlier tiles a step ----
+    {
+        const uint32_t *gb = a.gbase + ((uint64_t)td.seg * a.npass + a.pass) * NB;
+        uint32_t excl[BPT], jn[BPT], left[BPT];
+        uint32_t pending = 0;  // digits still looking back
 #pragma unroll
-            for (int w = 0; w < OS_WARPS; w++) {
-                const uint32_t c = wcnt[w * NB + b];
-                wcnt[w * NB + b] = (uint16_t)s;
-                s += c;
-            }
-            tcount[b] = (uint16_t)s;
-            os_store_status(st + b, (td.t == 0 ? a.inc : a.agg) | s);
+        for (int x = 0; x < BPT; x++) {
+            excl[x] = 0;
+            jn[x] = tile - 1;
+            left[x] = td.t;  // earlier tiles of the segment
+            if (td.t != 0 && x * OS_THREADS + (int)threadIdx.x < NB) pending |= 1u << x;
         }
-        __syncthreads();
-        // ---- tile-local run starts: exclusive scan of the counts over digits ----
-        {
-            constexpr int PER = NB / OS_THREADS > 0 ? NB / OS_THREADS : 1;
-            const int b0 = threadIdx.x * PER;
-            uint32_t s = 0;
-#pragma unroll
-            for (int i = 0; i < PER; i++) s += b0 + i < NB ? tcount[b0 + i] : 0u;
-            uint32_t tot;
-            uint32_t pre = block_exclusive_scan<OS_THREADS>(s, &tot, ws);
-#pragma unroll
-            for (int i = 0; i < PER; i++)
-                if (b0 + i < NB) {
-                    bstart[b0 + i] = pre;
-                    pre += tcount[b0 + i];
-                }
-        }
-        __syncthreads();
-        // ---- stage the keys in digit order (the counters' area takes the keys) ----
-        {
-            // each key's place in the tile, written over its rank (16 bits each)
-#pragma unroll
-            for (int i = 0; i < ITEMS; i++) {
-                const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
-                uint32_t lp = 0;
-                if (j < td.n) {
-                    const uint32_t dig = os_digit(key[i], a.shift, dmask);
-                    lp = bstart[dig] + wcnt[warp * NB + dig] + ((rank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
-                }
-                rank[i >> 1] = (i & 1) ? (rank[i >> 1] & 0xFFFFu) | (lp << 16) : (rank[i >> 1] & 0xFFFF0000u) | lp;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int i = 0; i < ITEMS; i++) {
-                const uint32_t j = (uint32_t)warp * 32 * ITEMS + (uint32_t)i * 32 + lane;
-                if (j < td.n) skeys[(rank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu] = key[i];
-            }
-        }
-        // ---- look back: each thread's digits together, LB_ROWS earlier tiles a step ----
-        {
-            const uint32_t *gb = a.gbase + ((uint64_t)td.seg * a.npass + a.pass) * NB;
-            uint32_t excl[BPT], jn[BPT], left[BPT];
-            uint32_t pending = 0;  // digits still looking back
+        uint64_t t_wait = 0;  // when this thread first waited
+        bool failed = false;
+        while (pending) {
+            uint32_t v[BPT][LB_ROWS];
 #pragma unroll
             for (int x = 0; x < BPT; x++) {
-                excl[x] = 0;
-                jn[x] = tile - 1;
-                left[x] = td.t;  // earlier tiles of the segment
-                if (td.t != 0 && x * OS_THREADS + (int)threadIdx.x < NB) pending |= 1u << x;
+                // row jn - r of digit slot x: one base, constant offsets
+                const uint32_t *row = a.status + (uint64_t)jn[x] * NB + x * OS_THREADS + threadIdx.x;
+#pragma unroll
+                for (int r = 0; r < LB_ROWS; r++)
+                    v[x][r] = ((pending >> x) & 1) && (uint32_t)r < left[x] ? os_load_status(row - r * NB) : 0u;
             }
-            uint64_t t_wait = 0;  // when this thread first waited
-            while (pending) {
-                uint32_t v[BPT][LB_ROWS];
+            bool waited = false;
 #pragma unroll
-                for (int x = 0; x < BPT; x++) {
-                    // row jn - r of digit slot x: one base, constant offsets
-                    const uint32_t *row = a.status + (uint64_t)jn[x] * NB + x * OS_THREADS + threadIdx.x;
+            for (int x = 0; x < BPT; x++) {
+                if (!((pending >> x) & 1)) continue;
+                const uint32_t nr = left[x] < (uint32_t)LB_ROWS ? left[x] : (uint32_t)LB_ROWS;
+                uint32_t r = 0;  // rows consumed
 #pragma unroll
-                    for (int r = 0; r < LB_ROWS; r++)
-                        v[x][r] = ((pending >> x) & 1) && (uint32_t)r < left[x] ? os_load_status(row - r * NB) : 0u;
-                }
-                bool waited = false;
-#pragma unroll
-                for (int x = 0; x < BPT; x++) {
-                    if (!((pending >> x) & 1)) continue;
-                    const uint32_t nr = left[x] < (uint32_t)LB_ROWS ? left[x] : (uint32_t)LB_ROWS;
-                    uint32_t r = 0;  // rows consumed
-#pragma unroll
-                    for (int rr = 0; rr < LB_ROWS; rr++) {
-                        if ((uint32_t)rr >= nr) break;
-                        const uint32_t f = v[x][rr] & 0xC0000000u;
-                        if (f == a.inc) {
-                            excl[x] += v[x][rr] & 0x3FFFFFFFu;
-                            pending &= ~(1u << x);
-                            break;
-                        }
-                        if (f != a.agg) {  // not published yet: this row is read again next step
-                            waited = true;
-                            break;
-                        }
+                for (int rr = 0; rr < LB_ROWS; rr++) {
+                    if ((uint32_t)rr >= nr) break;
+                    const uint32_t f = v[x][rr] & 0xC0000000u;
+                    if (f == a.inc) {
                         excl[x] += v[x][rr] & 0x3FFFFFFFu;
-                        r++;
-                    }
-                    if ((pending >> x) & 1) {
-                        jn[x] -= r;
-                        left[x] -= r;
-                        // the segment's first tile publishes its inclusive prefix at once,
-                        // so the walk cannot run past it
-                        if (left[x] == 0) {
-                            atomicOr(a.err, ERR_LOOKBACK);
-                            pending &= ~(1u << x);
-                        }
-                    }
-                }
-                if (waited) {
-                    // never expected: an earlier tile that does not publish.  Give
-                    // up after OS_WAIT_NS, or at once when another tile gave up,
-                    // record it and go on (the host then fails the call)
-                    const uint64_t now = os_now_ns();
-                    if (!t_wait) t_wait = now;
-                    if (now - t_wait > OS_WAIT_NS || (os_load_status(a.err) & ERR_LOOKBACK)) {
-                        if (!(atomicOr(a.err, ERR_LOOKBACK) & ERR_LOOKBACK)) {  // the first to give up
-                            a.err[1] = tile;
-                            a.err[2] = (uint32_t)__ffs(pending) - 1 + 0;  // the digit slot still waiting
-                            a.err[3] = td.t;
-                        }
+                        pending &= ~(1u << x);
                         break;
                     }
-                    __nanosleep(32);
+                    if (f != a.agg) {  // not published yet: this row is read again next step
+                        waited = true;
+                        break;
+                    }
+                    excl[x] += v[x][rr] & 0x3FFFFFFFu;
+                    r++;
+                }
+                if ((pending >> x) & 1) {
+                    jn[x] -= r;
+                    left[x] -= r;
+                    // the segment's first tile publishes its inclusive prefix at once,
+                    // so the walk cannot run past it
+                    if (left[x] == 0) {
+                        atomicOr(a.err, ERR_LOOKBACK);
+                        failed = true;
+                        pending &= ~(1u << x);
+                    }
                 }
             }
-#pragma unroll
-            for (int x = 0; x < BPT; x++) {
-                const int b = x * OS_THREADS + threadIdx.x;
-                if (b < NB) {
-                    if (td.t != 0) os_store_status(st + b, a.inc | ((excl[x] + tcount[b]) & 0x3FFFFFFFu));
-                    bdelta[b] = (int32_t)(gb[b] + excl[x]) - (int32_t)bstart[b];
+            if (waited) {
+                // never expected: an earlier tile that does not publish.  Give
+                // up after OS_WAIT_NS, or at once when another tile gave up,
+                // record it and go on (the host then fails the call)
+                const uint64_t now = os_now_ns();
+                if (!t_wait) t_wait = now;
+                if (now - t_wait > OS_WAIT_NS || (os_load_status(a.err) & ERR_LOOKBACK)) {
+                    if (!(atomicOr(a.err, ERR_LOOKBACK) & ERR_LOOKBACK)) {  // the first to give up
+                        a.err[1] = tile;
+                        a.err[2] = (uint32_t)__ffs(pending) - 1 + 0;  // the digit slot still waiting
+                        a.err[3] = td.t;
+                    }
+                    failed = true;
+                    break;
                 }
+                __nanosleep(32);
             }
         }
-        __syncthreads();
-        // ---- write: consecutive threads, consecutive keys of one digit run ----
+        if (failed) sh.lb_fail = 1;
+#pragma unroll
+        for (int x = 0; x < BPT; x++) {
+            const int b = x * OS_THREADS + threadIdx.x;
+            if (b < NB) {
+                if (td.t != 0) os_store_status(st + b, a.inc | ((excl[x] + tcount[b]) & 0x3FFFFFFFu));
+                bdelta[b] = (int32_t)(gb[b] + excl[x]) - (int32_t)bstart[b];
+            }
+        }
+    }
+    __syncthreads();
+    // ---- write: consecutive threads, consecutive keys of one digit run.
+    //      Every position is inside the segment by construction (the
+    //      segment's histogram counts exactly its keys); a tile whose
+    //      look-back gave up writes nothing (the host fails the call). ----
+    if (!sh.lb_fail) {
         KT *o = out + td.seg_start;
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t idx = (uint32_t)i * OS_THREADS + threadIdx.x;
-            if (idx < td.n) {
+            if (has(idx)) {
                 const KT k = skeys[idx];
-                const int64_t q = (int64_t)bdelta[os_digit(k, a.shift, dmask)] + idx;
-                if (q >= 0 && q < (int64_t)td.seg_n) o[q] = k;  // always true unless a look-back failed
-                else atomicOr(a.err, ERR_LOOKBACK);
+                o[(int64_t)bdelta[os_digit(k, a.shift, dmask)] + idx] = k;
             }
         }
+    }
+}
+
+template <int RB, class KT>
+__global__ void __launch_bounds__(OS_THREADS, os_min_ctas<KT>())
+os_pass_kernel(OsPassParams a) {
+    constexpr int NB = 1 << RB;
+    constexpr int T = os_tile<KT>();
+    static_assert(OS_WARPS * NB * 2 <= T * (int)sizeof(KT), "warp counters fit the key staging area");
+    extern __shared__ __align__(16) unsigned char os_smem[];
+    uint16_t *wcnt = reinterpret_cast<uint16_t *>(os_smem);
+    __shared__ OsShared sh;
+    // The next tile's id is taken while the current tile runs, so the atomic's
+    // round trip is off the critical path.  A CTA's next tile is always later
+    // than its current one, so the earliest unfinished tile is always running
+    // and every look-back ends.
+    uint32_t next = 0;
+    if (threadIdx.x == 0) next = atomicAdd(a.tile_ctr, 1u);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint32_t tile = next;
+            if (tile < a.ntiles) next = atomicAdd(a.tile_ctr, 1u);
+            sh.tile = tile;
+            sh.lb_fail = 0;
+            if (tile < a.ntiles) {
+                const uint32_t s = os_seg_of(a.seg.tile0, a.seg.nseg, tile);
+                const uint64_t s0 = a.seg.key0[s], sn = a.seg.key0[s + 1] - s0;
+                OsTile td;
+                td.t = tile - a.seg.tile0[s];
+                td.seg = s;
+                td.seg_start = s0;
+                td.seg_n = (uint32_t)sn;
+                td.start = s0 + (uint64_t)td.t * T;
+                td.n = (uint32_t)(sn - (uint64_t)td.t * T < (uint64_t)T ? sn - (uint64_t)td.t * T : (uint64_t)T);
+                sh.td = td;
+            }
+        }
+        for (int i = threadIdx.x; i < OS_WARPS * NB / 2; i += OS_THREADS) reinterpret_cast<uint32_t *>(wcnt)[i] = 0;
+        __syncthreads();
+        if (sh.tile >= a.ntiles) break;
+        if (sh.td.n == (uint32_t)T) os_pass_tile<RB, KT, true>(a, sh);
+        else os_pass_tile<RB, KT, false>(a, sh);
         __syncthreads();  // the staging area is cleared for the next tile
     }
 }

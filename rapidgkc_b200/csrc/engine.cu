@@ -326,7 +326,8 @@ struct gkc_ctx {
     std::vector<cudaEvent_t> batch_ev;  // start / end of each batch of the last gkc_add_reads
     std::vector<double> batch_ms;       // latency of each batch: its copy start to its phase-1 end
     DevBuf keysA, keysB, tiles, counts, offsets, blocksums, heads_pos, heads_key, tilecnt, tileoff;
-    DevBuf os_status, os_hist, os_chunks, os_ctr;  // one-pass-per-digit radix sort
+    DevBuf os_status, os_hist, os_segs, os_ctr;  // one-pass-per-digit radix sort
+    PinBuf h_segs;                               // its segment tables, staged for the copy
     DevBuf segoff, segcur, part_err, scal;
     DevBuf stage_bytes, stage_idx, stage_keys;
     DevBuf spill_bytes[2], spill_idx[2], spill_keys[2];  // device staging of chunks being spilled
@@ -375,10 +376,11 @@ struct gkc_ctx {
                         &r_woff, &r_wrec, &ord_loads, &ord_stage, &ord_list, &mlp_p, &mlp_m, &mlp_v, &mlp_g, &mlp_t,
                         &mlp_w, &mlp_s, &mlp_scalar, &fx_text, &fx_tiles, &fx_state, &fx_kept,
                         &fx_reads, &fx_res, &fx_out, &fx_offs, &sk_tiles, &sk_state, &sk_tstarts, &sk_res,
-                        &sk_starts, &sk_k32, &hpc_tiles, &hpc_tbase, &hpc_reads, &hpc_offs};
+                        &sk_starts, &sk_k32, &hpc_tiles, &hpc_tbase, &hpc_reads, &hpc_offs, &os_status, &os_hist,
+                        &os_segs, &os_ctr};
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work,
-                        &h_desc, &h_cur};
+                        &h_desc, &h_cur, &h_segs};
         for (auto *p : ps) p->release();
         arena.release();
         cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_ready[0], buf_ready[1], spill_ready,
@@ -494,15 +496,43 @@ int ensure_table(gkc_ctx *ctx, uint64_t C) {
     return GKC_OK;
 }
 
+// Releases the pooled scratch that no counting group holds between groups:
+// phase-1 batch buffers, spill staging, the record path's slices, the L2
+// table, and (hash counter) the sort buffers.  Called when an allocation of
+// the output fails; the buffers are allocated again when next needed.
+void trim_scratch(gkc_ctx *ctx) {
+    cudaStreamSynchronize(ctx->s);
+    DevBuf *ds[] = {&ctx->reads[0], &ctx->reads[1], &ctx->offs[0], &ctx->offs[1], &ctx->records, &ctx->codes,
+                    &ctx->tile_read, &ctx->cta_hist, &ctx->cta_base, &ctx->spill_bytes[0], &ctx->spill_bytes[1],
+                    &ctx->spill_idx[0], &ctx->spill_idx[1], &ctx->spill_keys[0], &ctx->spill_keys[1],
+                    &ctx->stage_bytes, &ctx->stage_idx, &ctx->stage_keys, &ctx->r_work, &ctx->r_count, &ctx->r_off,
+                    &ctx->r_cur, &ctx->r_recs, &ctx->r_failed, &ctx->r_stage, &ctx->r_winst, &ctx->r_woff,
+                    &ctx->r_wrec, &ctx->fx_text, &ctx->fx_reads, &ctx->fx_out, &ctx->hpc_reads};
+    for (auto *d : ds) d->release();
+    ctx->table.release();
+    ctx->tcap = 0;
+    if (ctx->opt.counter == GKC_COUNTER_HASH && ctx->opt.k <= 32) {
+        DevBuf *sb[] = {&ctx->keysA, &ctx->keysB, &ctx->heads_pos, &ctx->heads_key, &ctx->os_status};
+        for (auto *d : sb) d->release();
+    }
+}
+
 // Output capacity of at least `need` entries; a new buffer keeps the first
-// `keep` entries of the old one.
+// `keep` entries of the old one.  If the device is short of memory, the
+// pooled scratch is released (trim_scratch) and the allocation tried again.
 int ensure_out(gkc_ctx *ctx, uint64_t need, uint64_t keep) {
     if (need <= ctx->out_cap && ctx->out_k.p) return GKC_OK;
     const uint64_t kb = ctx->opt.k > 32 ? 16 : 8;  // key bytes per entry
     uint64_t cap = std::max<uint64_t>(need, 1024);
     DevBuf nk, nc;
-    CK(nk.ensure(cap * kb));
-    CK(nc.ensure(cap * 4));
+    if (nk.ensure(cap * kb) != cudaSuccess || nc.ensure(cap * 4) != cudaSuccess) {
+        cudaGetLastError();  // the failed allocation's error, not sticky
+        nk.release();
+        nc.release();
+        trim_scratch(ctx);
+        CK(nk.ensure(cap * kb));
+        CK(nc.ensure(cap * 4));
+    }
     keep = std::min<uint64_t>(keep, ctx->out_cap);
     if (keep && ctx->out_k.p) {
         CK(cudaMemcpyAsync(nk.p, ctx->out_k.p, keep * kb, cudaMemcpyDeviceToDevice, ctx->s));
@@ -1592,8 +1622,12 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
 // Run-length count + threshold of the sorted keys `src` (n), appending to the
 // output; adds the sort's time (events e2..e3, recorded by the caller) to
 // *sort_ms.
+// RLE + threshold of n sorted keys, appended to the output.  sort_err: the
+// radix sort's device error words (onesweep_sort, read here at the first
+// synchronisation), or null.
 template <class KT>
-int reduce_sorted(gkc_ctx *ctx, const KT *src, uint64_t n, uint32_t cmin, uint32_t cmax, float *sort_ms) {
+int reduce_sorted(gkc_ctx *ctx, const KT *src, uint64_t n, uint32_t cmin, uint32_t cmax, float *sort_ms,
+                  const uint32_t *sort_err = nullptr) {
     constexpr double KB = sizeof(KT);
     // ---- RLE ----
     const uint64_t rt = (n + RL_TILE - 1) / RL_TILE;
@@ -1611,7 +1645,14 @@ int reduce_sorted(gkc_ctx *ctx, const KT *src, uint64_t n, uint32_t cmin, uint32
         }
         RET(scan_u32(ctx, ctx->tilecnt.as<uint32_t>(), rt, ctx->tileoff.as<uint64_t>(), sc));
         CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 8, cudaMemcpyDeviceToHost, ctx->s));
+        if (sort_err) CK(cudaMemcpyAsync(ctx->h_scal.as<uint32_t>() + 8, sort_err, 16, cudaMemcpyDeviceToHost, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
+        if (sort_err) {
+            const uint32_t *e = ctx->h_scal.as<uint32_t>() + 8;
+            if (e[0] & ERR_LOOKBACK)
+                return ctx->fail(GKC_EINTERNAL, "radix sort: a look-back wait ran out (tile %u, %u of its segment, "
+                                                "digit slot %u)", e[1], e[3], e[2]);
+        }
         d = ctx->h_scal.as<unsigned long long>()[0];
         CK(ctx->heads_pos.ensure(std::max<uint64_t>(d, 1) * 8));
         CK(ctx->heads_key.ensure(std::max<uint64_t>(d, 1) * sizeof(KT)));
@@ -1657,12 +1698,13 @@ int reduce_sorted(gkc_ctx *ctx, const KT *src, uint64_t n, uint32_t cmin, uint32
 // phase 2, sort counter: the radix sort of count_onesweep.cu over segments
 // `segs` of the n keys in keysA (every segment < 2^30 keys).  Digits of at
 // most RB bits, spread evenly over nbits; *sorted receives the buffer that
-// holds the result (keysA or keysB).
+// holds the result (keysA or keysB).  Nothing here waits for the device: the
+// look-back error flags (part_err) are read at the reduction's first
+// synchronisation (reduce_sorted).
 template <int RB, class KT>
 int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, int nbits, KT **sorted) {
     constexpr double KB = sizeof(KT);
     constexpr uint64_t T = os_tile<KT>();
-    constexpr uint64_t HCHUNK = 1u << 16;  // keys per histogram CTA
     constexpr int NB = 1 << RB;
     OsPasses ps{};
     ps.n = (nbits + RB - 1) / RB;
@@ -1672,35 +1714,45 @@ int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, i
         ps.shift[p] = sh;
         sh += ps.width[p];
     }
-    std::vector<OsTile> td;
-    std::vector<OsChunk> ch;
-    uint64_t start = 0;
-    for (uint32_t sgi = 0; sgi < (uint32_t)segs.size(); sgi++) {
-        const uint64_t sz = segs[sgi];
-        for (uint64_t t = 0; t * T < sz; t++)
-            td.push_back({start + t * T, start, (uint32_t)std::min<uint64_t>(T, sz - t * T), (uint32_t)t, sgi,
-                          (uint32_t)sz});
-        for (uint64_t c = 0; c < sz; c += HCHUNK)
-            ch.push_back({start + c, (uint32_t)std::min<uint64_t>(HCHUNK, sz - c), sgi});
-        start += sz;
+    // segment tables: first key, first tile and first histogram chunk of
+    // each segment (a few KB, through a pinned buffer: the previous sort's
+    // copy finished at its reduction's synchronisation)
+    const uint32_t nseg = (uint32_t)segs.size();
+    const size_t tab = (nseg + 1) * (8ull + 4 + 4);
+    CK(ctx->h_segs.ensure(tab));
+    CK(ctx->os_segs.ensure(tab));
+    auto *key0 = ctx->h_segs.as<unsigned long long>();
+    auto *tile0 = reinterpret_cast<uint32_t *>(key0 + nseg + 1);
+    uint32_t *chunk0 = tile0 + nseg + 1;
+    uint64_t ntiles = 0, nchunks = 0, start = 0;
+    for (uint32_t i = 0; i <= nseg; i++) {
+        key0[i] = start;
+        tile0[i] = (uint32_t)ntiles;
+        chunk0[i] = (uint32_t)nchunks;
+        if (i == nseg) break;
+        ntiles += (segs[i] + T - 1) / T;
+        nchunks += (segs[i] + OS_HCHUNK - 1) / OS_HCHUNK;
+        start += segs[i];
     }
     KT *src = ctx->keysA.as<KT>(), *dst = ctx->keysB.as<KT>();
     *sorted = src;
-    const uint64_t ntiles = td.size();
     if (!ntiles) return GKC_OK;
+    if (ntiles > UINT32_MAX || nchunks > INT32_MAX) return ctx->fail(GKC_ELIMIT, "radix sort: too many tiles");
     const uint64_t nhist = segs.size() * (uint64_t)ps.n * NB;
-    CK(ctx->tiles.ensure(ntiles * sizeof(OsTile)));
-    CK(ctx->os_chunks.ensure(ch.size() * sizeof(OsChunk)));
     CK(ctx->os_hist.ensure(nhist * 4));
     CK(ctx->os_status.ensure(ntiles * NB * 4));
     CK(ctx->os_ctr.ensure(64 * 4));
     CK(ctx->part_err.ensure(64));
-    CK(cudaMemcpyAsync(ctx->tiles.p, td.data(), ntiles * sizeof(OsTile), cudaMemcpyHostToDevice, ctx->s));
-    CK(cudaMemcpyAsync(ctx->os_chunks.p, ch.data(), ch.size() * sizeof(OsChunk), cudaMemcpyHostToDevice, ctx->s));
+    CK(cudaMemcpyAsync(ctx->os_segs.p, ctx->h_segs.p, tab, cudaMemcpyHostToDevice, ctx->s));
     CK(cudaMemsetAsync(ctx->os_hist.p, 0, nhist * 4, ctx->s));
     CK(cudaMemsetAsync(ctx->os_status.p, 0, ntiles * NB * 4, ctx->s));
     CK(cudaMemsetAsync(ctx->os_ctr.p, 0, 64 * 4, ctx->s));
     CK(cudaMemsetAsync(ctx->part_err.p, 0, 16, ctx->s));
+    OsSegs sg;
+    sg.key0 = ctx->os_segs.as<unsigned long long>();
+    sg.tile0 = reinterpret_cast<const uint32_t *>(sg.key0 + nseg + 1);
+    sg.chunk0 = sg.tile0 + nseg + 1;
+    sg.nseg = nseg;
     const size_t hsm = (size_t)ps.n * NB * 4;
     {
         static bool attr = false;  // per template instance
@@ -1717,8 +1769,8 @@ int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, i
     }
     {
         KScope ks(ctx, GKC_K_RADIX_HIST, KB * n + 4.0 * nhist);
-        os_hist_kernel<RB, KT><<<(unsigned)ch.size(), OS_THREADS, hsm, ctx->s>>>(
-            src, ctx->os_chunks.as<OsChunk>(), ps, ctx->os_hist.as<uint32_t>());
+        os_hist_kernel<RB, KT><<<(unsigned)nchunks, OS_THREADS, hsm, ctx->s>>>(src, sg, ps,
+                                                                              ctx->os_hist.as<uint32_t>());
         LAUNCHED();
     }
     {
@@ -1735,7 +1787,7 @@ int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, i
         OsPassParams q;
         q.in = src;
         q.out = dst;
-        q.tiles = ctx->tiles.as<OsTile>();
+        q.seg = sg;
         q.ntiles = (uint32_t)ntiles;
         q.status = ctx->os_status.as<uint32_t>();
         q.gbase = ctx->os_hist.as<uint32_t>();
@@ -1754,12 +1806,6 @@ int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, i
         }
         std::swap(src, dst);
     }
-    uint32_t e[4] = {0, 0, 0, 0};
-    CK(cudaMemcpyAsync(e, ctx->part_err.p, 16, cudaMemcpyDeviceToHost, ctx->s));
-    CK(cudaStreamSynchronize(ctx->s));
-    if (e[0] & ERR_LOOKBACK)
-        return ctx->fail(GKC_EINTERNAL, "radix sort: a look-back wait ran out (tile %u of %llu, %u of its segment, "
-                                        "digit slot %u)", e[1], (unsigned long long)ntiles, e[3], e[2]);
     *sorted = src;
     return GKC_OK;
 }
@@ -1783,7 +1829,7 @@ int sort_and_reduce_rb(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t
         const int rc = onesweep_sort<RB, KT>(ctx, segs, n, nbits, &sorted);
         if (rc != GKC_OK) return rc;
         CK(cudaEventRecord(ctx->e3, ctx->s));
-        return reduce_sorted<KT>(ctx, sorted, n, cmin, cmax, sort_ms);
+        return reduce_sorted<KT>(ctx, sorted, n, cmin, cmax, sort_ms, n ? ctx->part_err.as<uint32_t>() : nullptr);
     }
     constexpr int RB8 = RB > 8 ? 8 : RB;  // the three-kernel sort keeps per-warp u32 counters of 2^RB digits
     // tiles
@@ -1864,7 +1910,9 @@ int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     if (!budget) {
         size_t fr = 0, tot = 0;
         CK(cudaMemGetInfo(&fr, &tot));
-        budget = std::max<uint64_t>(1ull << 20, (uint64_t)(fr * 0.5) / (5 * sizeof(KT)));
+        // per key of a group: two key buffers, the look-back statuses, and at
+        // worst (every key distinct) a run head and an output entry each
+        budget = std::max<uint64_t>(1ull << 20, (uint64_t)(fr * 0.8) / (4 * sizeof(KT) + 16));
     }
     CK(ctx->segoff.ensure(P * 8));
     CK(ctx->segcur.ensure(P * 8));

@@ -40,6 +40,26 @@ def _mem_available() -> int:
     return 0
 
 
+def _device_count_sum(c: KmerCounter, piece: int = 1 << 28) -> int:
+    """Sum of the last result's counts, read from device memory in pieces
+    through a pinned host buffer (the result can be tens of GB)."""
+    import ctypes
+
+    import torch
+    kp, cp, n = c.result_device()
+    cudart = ctypes.CDLL("libcudart.so.12")  # device pointers are shared through the primary context
+    buf = torch.empty(min(n, piece) or 1, dtype=torch.int32, pin_memory=True)
+    total = 0
+    for i in range(0, n, piece):
+        m = min(piece, n - i)
+        rc = cudart.cudaMemcpy(ctypes.c_void_p(buf.data_ptr()), ctypes.c_void_p(cp + 4 * i), ctypes.c_size_t(4 * m),
+                               2)  # cudaMemcpyDeviceToHost
+        if rc != 0:
+            raise RuntimeError(f"cudaMemcpy failed ({rc})")
+        total += int(buf[:m].numpy().view(np.uint32).sum(dtype=np.uint64))
+    return total
+
+
 def stream_count(workload: str = "human_3g", scale: float = 1.0, batch_gb: float = 1.0, order: str = "learned",
                  k: int = 31, p: int = 11, partitions: int = 512, cmin: int = 2, spill: bool = True,
                  device: int = 0, threads: int = 0) -> dict:
@@ -119,12 +139,19 @@ def stream_count(workload: str = "human_3g", scale: float = 1.0, batch_gb: float
         tm = c.timings()
         ks = {cls: round(v[0] / 1e3, 4) for cls, v in c.kernel_stats(reset=True).items() if v[1]}
         c.set_profiling(False)
+        sum_kept = _device_count_sum(c) if cmin == 2 else None
     out.update({"bases": bases, "store_bytes": int(pb.sum()), "superkmers": int(ps.sum()),
                 "kmer_instances": int(pk.sum()), "maxmean_kmers": float(pk.max() / pk.mean()),
                 "maxmean_bytes": float(pb.max() / pb.mean()), "kept": kept, "distinct": distinct,
                 "phase1_s": t_add, "phase2_s": t_count, "phase2_kernel_s": tm["phase2_kernel_ms"] / 1e3,
                 "phase2_stage_s": tm["phase2_stage_ms"] / 1e3, "phase2_groups": tm["phase2_groups"],
                 "phase2_kernel_classes_s": ks,
+                # threshold >= 2 with no upper bound: every distinct k-mer not
+                # kept occurs once, so the kept counts plus the singletons
+                # must add up to the k-mer instances
+                "instances_check": None if sum_kept is None else {
+                    "kept_count_sum": sum_kept, "singletons": distinct - kept,
+                    "equal": sum_kept + (distinct - kept) == int(pk.sum())},
                 "gbps_incl_pinning": bases / (t_add + t_count + pin["s"]) / 1e9,
                 "gbps": bases / (t_add + t_count) / 1e9,
                 "batch_latency_ms": {"p50": float(np.percentile(lat, 50)), "max": float(np.max(lat))} if lat else None,
