@@ -14,7 +14,8 @@
 //                    (tile ids from an atomic counter, so every tile before
 //                    it is already running), ranks them by digit in shared
 //                    memory (per-warp digit counters and __match_any_sync,
-//                    stable), publishes its per-digit counts, and reads the
+//                    stable; a chain of one ballot per digit bit measured
+//                    slower), publishes its per-digit counts, and reads the
 //                    earlier tiles' counts of its segment back to its own
 //                    offsets (decoupled look-back: each tile publishes its
 //                    count first and its inclusive prefix once known, and a

@@ -250,6 +250,9 @@ struct gkc_ctx {
     // spilled chunks: two device staging slots, copied to the host arena on
     // their own stream so the next batch's phase 1 overlaps the copy
     cudaStream_t ss = nullptr;
+    // a spilled store's staged ranges get their index entries rebuilt here,
+    // beside the copy stream's next copies
+    cudaStream_t rs = nullptr;
     cudaEvent_t spill_ready = nullptr, spill_done[2] = {nullptr, nullptr};
     int spill_slot = 0;
 
@@ -392,6 +395,7 @@ struct gkc_ctx {
         if (own_s) cudaStreamDestroy(own_s);
         if (cs) cudaStreamDestroy(cs);
         if (ss) cudaStreamDestroy(ss);
+        if (rs) cudaStreamDestroy(rs);
     }
     static void delete_chunk(StoreChunk *c) {
         c->release();
@@ -712,27 +716,46 @@ int spill_chunk(gkc_ctx *ctx, StoreChunk *c) {
 // rebuilt from the bytes by the .skm parse (skm_load.cu) under the context's
 // order, to pi / pk (one per superkmer of the range, in byte order; the
 // order of a partition's entries does not matter to any reader).
-int stage_spilled(gkc_ctx *ctx, StoreChunk *c, uint32_t p0, uint32_t p1, uint8_t *pb, uint64_t *pi, uint32_t *pk,
-                  cudaStream_t st) {
-    const uint64_t b0 = c->byte_off[p0], b1 = c->byte_off[p1], s0 = c->skm_off[p0], s1 = c->skm_off[p1];
-    const uint64_t n = b1 - b0, nskm = s1 - s0;
-    CK(cudaMemcpyAsync(pb, c->bytes + b0, n, cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(pb + n, 0, 32, st));
-    if (!nskm) return GKC_OK;
-    const uint32_t np = p1 - p0;
+// Scratch of the index rebuild for a staged range of n bytes, nskm
+// superkmers and np partitions.  A staging loop sizes it for its largest
+// range first, so that no buffer grows (cudaFree waits for the device) while
+// the staging overlaps the counting.
+int stage_scratch(gkc_ctx *ctx, uint64_t n, uint64_t nskm, uint32_t np) {
     const uint64_t ntiles = (n + gkc::SL_TILE - 1) / gkc::SL_TILE;
     CK(ctx->sk_po.ensure((np + 1) * 8ull));
-    CK(ctx->sk_tiles.ensure(ntiles * sizeof(gkc::SlT)));
-    CK(ctx->sk_state.ensure(ntiles));
-    CK(ctx->sk_tstarts.ensure(ntiles * 8));
+    CK(ctx->sk_tiles.ensure(std::max<uint64_t>(ntiles, 1) * sizeof(gkc::SlT)));
+    CK(ctx->sk_state.ensure(std::max<uint64_t>(ntiles, 1)));
+    CK(ctx->sk_tstarts.ensure(std::max<uint64_t>(ntiles, 1) * 8));
     CK(ctx->sk_res.ensure(64));
-    CK(ctx->sk_starts.ensure(nskm * 8));
-    CK(ctx->sk_k32.ensure(nskm * 4));
-    // the partition offsets, rebased to the staged range (a pageable copy: the
-    // call returns once the source is consumed)
-    std::vector<unsigned long long> po(np + 1);
-    for (uint32_t j = 0; j <= np; j++) po[j] = c->byte_off[p0 + j] - b0;
-    CK(cudaMemcpyAsync(ctx->sk_po.p, po.data(), (np + 1) * 8ull, cudaMemcpyHostToDevice, st));
+    CK(ctx->sk_starts.ensure(std::max<uint64_t>(nskm, 1) * 8));
+    CK(ctx->sk_k32.ensure(std::max<uint64_t>(nskm, 1) * 4));
+    return GKC_OK;
+}
+
+// Stages partitions [p0, p1) of spilled chunk c back to the device: the
+// superkmer bytes to pb (copy, on stream st), then their index entries to pi
+// and minimizer keys to pk (rebuild).  STAGE_BOTH does both on st; a staging
+// loop may issue every copy first and the rebuilds on another stream.
+enum { STAGE_COPY = 1, STAGE_REBUILD = 2, STAGE_BOTH = 3 };
+
+int stage_spilled(gkc_ctx *ctx, StoreChunk *c, uint32_t p0, uint32_t p1, uint8_t *pb, uint64_t *pi, uint32_t *pk,
+                  cudaStream_t st, int what = STAGE_BOTH) {
+    const uint64_t b0 = c->byte_off[p0], b1 = c->byte_off[p1], s0 = c->skm_off[p0], s1 = c->skm_off[p1];
+    const uint64_t n = b1 - b0, nskm = s1 - s0;
+    if (what & STAGE_COPY) {
+        CK(cudaMemcpyAsync(pb, c->bytes + b0, n, cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(pb + n, 0, 32, st));
+    }
+    if (!(what & STAGE_REBUILD) || !nskm) return GKC_OK;
+    const uint32_t np = p1 - p0;
+    const uint64_t ntiles = (n + gkc::SL_TILE - 1) / gkc::SL_TILE;
+    RET(stage_scratch(ctx, n, nskm, np));
+    // the partition offsets, rebased to the staged range, from the chunk's
+    // device copy (no host copy: a pageable one may wait for the stream)
+    CK(cudaMemcpyAsync(ctx->sk_po.p, c->d_byte_off.as<unsigned long long>() + p0, (np + 1) * 8ull,
+                       cudaMemcpyDeviceToDevice, st));
+    gkc::rebase_offsets_kernel<<<1, 256, 0, st>>>(ctx->sk_po.as<uint64_t>(), np + 1, b0);
+    LAUNCHED();
     CK(cudaMemsetAsync(ctx->sk_res.p, 0, 64, st));
     gkc::SlParams a;
     a.bytes = pb;
@@ -998,7 +1021,8 @@ int phase1_finish(gkc_ctx *ctx, std::vector<uint64_t> *redo) {
 // by the chunk's own partition offsets (spilled chunks are staged into `arena`
 // at *arena_used and the pointers rebased).
 int chunk_range(gkc_ctx *ctx, StoreChunk *c, uint32_t p0, uint32_t p1, DevBuf &arena, uint64_t *arena_used,
-                const uint8_t **bytes, const uint64_t **idx, const uint32_t **keys, cudaStream_t st = nullptr) {
+                const uint8_t **bytes, const uint64_t **idx, const uint32_t **keys, cudaStream_t st = nullptr,
+                int what = STAGE_BOTH) {
     if (!st) st = ctx->s;
     if (!c->on_host) {
         *bytes = c->bytes;
@@ -1017,7 +1041,7 @@ int chunk_range(gkc_ctx *ctx, StoreChunk *c, uint32_t p0, uint32_t p1, DevBuf &a
     uint8_t *pb = base;
     uint64_t *pi = reinterpret_cast<uint64_t *>(base + nbb);
     uint32_t *pk = reinterpret_cast<uint32_t *>(base + nbb + nib);
-    RET(stage_spilled(ctx, c, p0, p1, pb, pi, pk, st));
+    RET(stage_spilled(ctx, c, p0, p1, pb, pi, pk, st, what));
     *arena_used += need;
     // the kernels index with the chunk's absolute offsets: rebase
     *bytes = pb - b0;
@@ -1392,19 +1416,29 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     std::vector<const uint64_t *> cis[2];
     std::vector<const uint32_t *> cks[2];
     cudaEvent_t staged[2] = {nullptr, nullptr}, freed[2] = {nullptr, nullptr}, st0[2] = {nullptr, nullptr};
+    cudaEvent_t copied[2] = {nullptr, nullptr};
     long staged_g[2] = {-1, -1};
     struct EvBack {  // the events go back to the pool on every exit
         gkc_ctx *c;
-        cudaEvent_t *e[3];
+        cudaEvent_t *e[4];
         ~EvBack() {
             for (auto *a : e)
                 for (int i = 0; i < 2; i++)
                     if (a[i]) c->evpool.push_back(a[i]);
         }
-    } evback{ctx, {staged, freed, st0}};
+    } evback{ctx, {staged, freed, st0, copied}};
     if (spilled) {
         uint64_t mx = 0;
         for (const auto &g : grps) mx = std::max<uint64_t>(mx, g.gb);
+        uint64_t mn = 0, ms = 0;  // largest staged range of one chunk
+        uint32_t mp = 0;
+        for (const auto &g : grps)
+            for (auto *c : ctx->store) {
+                mn = std::max<uint64_t>(mn, c->byte_off[g.p1] - c->byte_off[g.p0]);
+                ms = std::max<uint64_t>(ms, c->skm_off[g.p1] - c->skm_off[g.p0]);
+                mp = std::max<uint32_t>(mp, g.p1 - g.p0);
+            }
+        RET(stage_scratch(ctx, mn, ms, mp));
         for (int i = 0; i < 2; i++) {
             // each chunk's range adds at most 32 + 3 x 15 bytes of padding
             CK(arena[i]->ensure(mx + 96 * nst + 64));
@@ -1414,9 +1448,12 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
             staged[i] = ctx->take_event();
             freed[i] = ctx->take_event();
             st0[i] = ctx->take_event();
+            copied[i] = ctx->take_event();
             CK(cudaEventRecord(freed[i], ctx->s));
         }
     }
+    // a group's copies go back to back on the copy stream; its index
+    // rebuilds follow on the rebuild stream, beside the next group's copies
     auto stage = [&](size_t gi) -> int {
         const int sl = (int)(gi & 1);
         uint64_t used = 0;
@@ -1424,8 +1461,14 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         CK(cudaEventRecord(st0[sl], ctx->cs));
         for (size_t j = 0; j < nst; j++)
             RET(chunk_range(ctx, ctx->store[j], grps[gi].p0, grps[gi].p1, *arena[sl], &used, &cbs[sl][j],
-                            &cis[sl][j], &cks[sl][j], ctx->cs));
-        CK(cudaEventRecord(staged[sl], ctx->cs));
+                            &cis[sl][j], &cks[sl][j], ctx->cs, STAGE_COPY));
+        CK(cudaEventRecord(copied[sl], ctx->cs));
+        CK(cudaStreamWaitEvent(ctx->rs, copied[sl], 0));
+        used = 0;
+        for (size_t j = 0; j < nst; j++)
+            RET(chunk_range(ctx, ctx->store[j], grps[gi].p0, grps[gi].p1, *arena[sl], &used, &cbs[sl][j],
+                            &cis[sl][j], &cks[sl][j], ctx->rs, STAGE_REBUILD));
+        CK(cudaEventRecord(staged[sl], ctx->rs));
         staged_g[sl] = (long)gi;
         return GKC_OK;
     };
@@ -2069,7 +2112,8 @@ int gkc_create(int device, const gkc_options *opt, gkc_ctx **out) {
     ctx->sms = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&ctx->own_s, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->cs, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->ss, cudaStreamNonBlocking) != cudaSuccess)
+        cudaStreamCreateWithFlags(&ctx->ss, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->rs, cudaStreamNonBlocking) != cudaSuccess)
         return cleanup(GKC_ECUDA);
     cudaEvent_t *sevs[] = {&ctx->spill_ready, &ctx->spill_done[0], &ctx->spill_done[1]};
     for (auto *e : sevs)
