@@ -65,12 +65,17 @@ WORKLOAD_DESC = {
     "mixed_100m": "100 Mbp genome; 80% bases from 150 bp reads (0.3%), 20% log-normal long reads (5%)",
 }
 
-# DRAM bytes (read + write) per read base of the phase-1 kernels, from one ncu
+# DRAM bytes (read + write) per read base of a kernel class, from one ncu
 # capture of the current kernels on a 0.05-scale case of the named workload
-# (profiles/phase1_kernels_skewed_small.md, learned order, 256 MiB batches);
-# the roofline's `traffic` scales them to the bases of one launch.  Keyed by
-# (workload, order, kernel class).
-TRAFFIC_PER_BASE: dict = {}
+# (profiles/phase1_and_counter_skewed_small.md, learned order, 256 MiB
+# batches): find_superkmers from a full 256 MiB batch (682 MB / 268.4M bases),
+# hash_insert (bucket_count_kernel) from its one launch over the whole case
+# (846 MB / 300M bases).  The roofline's `traffic` scales them to the bases of
+# one launch.  Keyed by (workload, order, kernel class).
+TRAFFIC_PER_BASE: dict = {
+    ("skewed_200m", "learned", "find_superkmers"): (301.616384e6 + 380.149e6) / 268435456,
+    ("skewed_200m", "learned", "hash_insert"): (739.905536e6 + 105.852e6) / 300e6,
+}
 
 
 def peaks():
@@ -598,7 +603,7 @@ def main():
                 "frac": achieved / hbm, "peak_source": src,
                 "traffic": tpb * launch_bases if tpb else None,
                 "traffic_source": ("ncu dram__bytes_read+write per base of the same kernel "
-                                   "(profiles/phase1_kernels_skewed_small.md), scaled to the launch's bases")
+                                   "(profiles/phase1_and_counter_skewed_small.md), scaled to the launch's bases")
                 if tpb else "no ncu capture of this kernel on this workload and order",
                 "bytes_per_launch": kb / max(kl, 1), "launch_ms": per_launch_s * 1e3, "classes": classes}
 

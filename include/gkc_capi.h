@@ -249,13 +249,14 @@ int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint
                    uint64_t *n_out, uint64_t *n_distinct);
 
 /* Statistics of the last gkc_add_reads (phase 1) and gkc_count (phase 2)
- * calls (n <= 8 entries): times[0..3] = device milliseconds (CUDA events) of
+ * calls (n <= 9 entries): times[0..3] = device milliseconds (CUDA events) of
  * phase 1, its superkmer search, phase 2, and phase 2's counting kernels;
  * times[4] = sub-buckets of the hash counter, times[5] = those re-split by
- * k-mer hash (their distinct k-mers overflowed shared memory, or they held
- * more than 65536 k-mer instances); hash counter only: times[6] = device
- * milliseconds of staging spilled chunks back, times[7] = partition groups
- * counted. */
+ * k-mer hash (they held more than 65536 k-mer instances, or their distinct
+ * k-mers overflowed shared memory twice); hash counter only: times[6] =
+ * device milliseconds of staging spilled chunks back, times[7] = partition
+ * groups counted, times[8] = sub-buckets that overflowed the first table and
+ * were counted by the second pass (16384 slots). */
 int gkc_last_timings(gkc_ctx *ctx, double *times, int n);
 
 /* Number of kernels this context launched since creation. */
@@ -269,7 +270,7 @@ int gkc_set_stream(gkc_ctx *ctx, void *stream);
 enum {
     GKC_K_FIND_SUPERKMERS = 0,  /* phase 1: minimizers + superkmer records */
     GKC_K_SCATTER = 1,          /* phase 1: records -> partition bytes     */
-    GKC_K_HASH_INSERT = 2,      /* phase 2 hash: decode + insert           */
+    GKC_K_HASH_INSERT = 2,      /* phase 2 hash: sub-bucket decode + count */
     GKC_K_HASH_COLLECT = 3,     /* phase 2 hash: threshold + clear table   */
     GKC_K_SORT_EXTRACT = 4,     /* phase 2 sort: decode -> key buffer      */
     GKC_K_RADIX_HIST = 5,       /* phase 2 sort: tile digit histograms     */
@@ -277,7 +278,9 @@ enum {
     GKC_K_SCAN = 7,             /* device-wide scans                       */
     GKC_K_RLE = 8,              /* run-length encoding + threshold         */
     GKC_K_BUCKET_SPLIT = 9,     /* phase 2 hash: superkmers -> sub-buckets */
-    GKC_K_CLASSES = 10
+    GKC_K_HASH_RECORDS = 10,    /* phase 2 hash: heavy / overflowed sub-   */
+                                /* buckets through k-mer records           */
+    GKC_K_CLASSES = 11
 };
 
 /* With profiling on, every kernel launch is bracketed by CUDA events on the

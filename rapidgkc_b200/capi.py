@@ -38,7 +38,7 @@ EXPORTS = (
     "gkc_init", "gkc_skmgen_batch", "gkc_count_partition", "gkc_set_order_lut", "gkc_shutdown",
 )
 KERNEL_CLASSES = ("find_superkmers", "scatter_superkmers", "hash_insert", "hash_collect", "sort_extract",
-                  "radix_hist", "radix_scatter", "scan", "rle", "bucket_split")
+                  "radix_hist", "radix_scatter", "scan", "rle", "bucket_split", "hash_records")
 
 
 class Options(C.Structure):
@@ -438,11 +438,11 @@ class KmerCounter:
         return lut
 
     def timings(self):
-        t = (C.c_double * 8)()
-        self._check(self._L.gkc_last_timings(self._h, t, 8))
+        t = (C.c_double * 9)()
+        self._check(self._L.gkc_last_timings(self._h, t, 9))
         return {"phase1_ms": t[0], "phase1_search_ms": t[1], "phase2_ms": t[2], "phase2_kernel_ms": t[3],
                 "sub_buckets": int(t[4]), "overflowed_sub_buckets": int(t[5]), "phase2_stage_ms": t[6],
-                "phase2_groups": int(t[7])}
+                "phase2_groups": int(t[7]), "second_pass_sub_buckets": int(t[8])}
 
     def kernel_launches(self) -> int:
         return int(self._L.gkc_kernel_launches(self._h))

@@ -3,7 +3,7 @@
 // Every partition p of the store is split into 2^s_p sub-buckets by a hash of
 // the superkmers' minimizer keys.  A canonical k-mer has one minimizer, so all
 // its occurrences land in one sub-bucket, and a sub-bucket can be counted on
-// its own.  s_p is chosen from partition p's k-mer count (about 16k instances
+// its own.  s_p is chosen from partition p's k-mer count (about 8k instances
 // per sub-bucket), so that a sub-bucket's distinct k-mers fit an
 // open-addressing table in one CTA's shared memory however skewed the
 // partitions are:
@@ -144,7 +144,7 @@ constexpr int BS_THREADS = 512;
 constexpr int BS_PER_CTA = 8192;   // superkmers per split CTA
 constexpr int BS_MAX_PARTS = 4;    // partitions a split CTA aggregates in shared memory
 constexpr int BS_SLOTS = 4096;     // shared-memory sub-bucket counters per split CTA
-constexpr int BS_LOG_LIMIT = 14;   // at most 16384 sub-buckets per partition
+constexpr int BS_LOG_LIMIT = 16;   // at most 65536 sub-buckets per partition
 constexpr size_t BS_SMEM = (size_t)BS_SLOTS * 12;  // dynamic shared memory
 
 // One store chunk's part of a split launch.
@@ -286,6 +286,7 @@ struct BCountParams {
     const unsigned long long *bucket_kmers;  // [nb] k-mer instances per sub-bucket
     uint64_t heavy_kmers;         // larger sub-buckets are listed, not counted
     uint32_t b0;                  // first sub-bucket of this launch
+    const uint32_t *ids;          // or, when not null: CTA i counts sub-bucket ids[i]
     int k;
     uint32_t cmin, cmax;
     uint64_t *out_k;
@@ -377,7 +378,7 @@ bucket_count_kernel(BCountParams a) {
     __shared__ uint32_t ws[BC_THREADS / 32];
     __shared__ volatile uint32_t over;
     __shared__ unsigned long long base_s;
-    const uint32_t b = a.b0 + blockIdx.x;
+    const uint32_t b = a.ids ? a.ids[blockIdx.x] : a.b0 + blockIdx.x;
     const uint64_t e0 = a.bucket_off[b], e1 = a.bucket_off[b + 1];
     if (e0 == e1) return;
     if (a.bucket_kmers[b] > a.heavy_kmers) {

@@ -293,7 +293,7 @@ struct gkc_ctx {
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
     std::string err;
     uint64_t launches = 0;
-    double times[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // see gkc_last_timings
+    double times[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // see gkc_last_timings
 
     // phase 1 buffers
     DevBuf reads[2], offs[2];
@@ -337,6 +337,8 @@ struct gkc_ctx {
     // shared-memory bucket counter
     DevBuf bk_skms, bk_kmers, bk_off, bk_cur, bk_entries, bk_failed, bk_arena, bk_part, bk_desc;
     DevBuf bk_arena2;  // second staging arena: a spilled store's next group is staged beside the current one
+    DevBuf bk_ids2, bk_failed2;  // the second counting pass: its sub-buckets and those that failed again
+    PinBuf h_ids2;
     DevBuf r_work, r_count, r_off, r_cur, r_recs, r_failed;  // record sub-buckets
     DevBuf r_stage, r_winst, r_woff, r_wrec;                  // per-work-item record segments
     uint64_t fallback_buckets = 0;  // sub-buckets counted through the L2 table
@@ -380,10 +382,10 @@ struct gkc_ctx {
                         &mlp_w, &mlp_s, &mlp_scalar, &fx_text, &fx_tiles, &fx_state, &fx_kept,
                         &fx_reads, &fx_res, &fx_out, &fx_offs, &sk_tiles, &sk_state, &sk_tstarts, &sk_res,
                         &sk_starts, &sk_k32, &hpc_tiles, &hpc_tbase, &hpc_reads, &hpc_offs, &os_status, &os_hist,
-                        &os_segs, &os_ctr};
+                        &os_segs, &os_ctr, &bk_ids2, &bk_failed2};
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work,
-                        &h_desc, &h_cur, &h_segs};
+                        &h_desc, &h_cur, &h_segs, &h_ids2};
         for (auto *p : ps) p->release();
         arena.release();
         cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_ready[0], buf_ready[1], spill_ready,
@@ -1100,9 +1102,11 @@ int count_buckets_l2(gkc_ctx *ctx, const std::vector<uint32_t> &ids, const std::
     return GKC_OK;
 }
 
-constexpr int BC_TS = 8192;  // shared-memory table slots per CTA (96 KB)
-// sub-buckets of more k-mer instances go to the record split (about 4x the
-// 16k instances a sub-bucket is sized for)
+constexpr int BC_TS = 8192;    // shared-memory table slots per CTA (96 KB)
+constexpr int BC_TS2 = 16384;  // second pass over the sub-buckets that overflowed (192 KB, one CTA per SM)
+// sub-buckets of more k-mer instances go to the record split (8x the 8k
+// instances a sub-bucket is sized for: only a minimizer that dominates its
+// sub-bucket, as in a low-complexity run, makes one this large)
 constexpr uint64_t BC_HEAVY_KMERS = 65536;
 
 // Counts the minimizer sub-buckets `ids` that overflowed shared memory or are
@@ -1146,7 +1150,7 @@ int count_buckets_records_slice(gkc_ctx *ctx, const std::vector<uint32_t> &ids, 
     CK(cudaMemsetAsync(ctx->r_failed.p, 0, 4, ctx->s));
     auto *sc = ctx->scal.as<unsigned long long>();
     {
-        KScope ks(ctx, GKC_K_SCAN, 16.0 * (double)ents + 4.0 * nw);
+        KScope ks(ctx, GKC_K_HASH_RECORDS, 16.0 * (double)ents + 4.0 * nw);
         work_inst_kernel<<<(nw + 7) / 8, 256, 0, ctx->s>>>(ctx->bk_entries.as<BEntry>(), ctx->r_work.as<RWork>(),
                                                             nw, ctx->r_winst.as<uint32_t>());
         LAUNCHED();
@@ -1163,7 +1167,7 @@ int count_buckets_records_slice(gkc_ctx *ctx, const std::vector<uint32_t> &ids, 
         ap.wrec = ctx->r_wrec.as<uint32_t>();
         ap.rcount = ctx->r_count.as<uint32_t>();
         CK(cudaFuncSetAttribute(rec_agg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RA_SMEM));
-        KScope ks(ctx, GKC_K_HASH_INSERT, 16.0 * inst);
+        KScope ks(ctx, GKC_K_HASH_RECORDS, 16.0 * inst);
         rec_agg_kernel<<<nw, RSP_THREADS, RA_SMEM, ctx->s>>>(ap);
         LAUNCHED();
     }
@@ -1178,7 +1182,7 @@ int count_buckets_records_slice(gkc_ctx *ctx, const std::vector<uint32_t> &ids, 
         rp.stage = ctx->r_stage.as<KRec>();
         rp.rcursor = ctx->r_cur.as<unsigned long long>();
         rp.recs = ctx->r_recs.as<KRec>();
-        KScope ks(ctx, GKC_K_SCAN, 32.0 * inst);
+        KScope ks(ctx, GKC_K_HASH_RECORDS, 32.0 * inst);
         rec_scatter_kernel<<<nw, RSP_THREADS, 0, ctx->s>>>(rp);
         LAUNCHED();
     }
@@ -1203,7 +1207,7 @@ int count_buckets_records_slice(gkc_ctx *ctx, const std::vector<uint32_t> &ids, 
     cp.err = reinterpret_cast<uint32_t *>(sc + 2);
     CK(cudaFuncSetAttribute(rec_count_kernel<BC_TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, BC_TS * 12));
     {
-        KScope ks(ctx, GKC_K_HASH_COLLECT, 16.0 * nrec);
+        KScope ks(ctx, GKC_K_HASH_RECORDS, 16.0 * nrec);
         rec_count_kernel<BC_TS><<<(unsigned)nwin, BC_THREADS, BC_TS * 12, ctx->s>>>(cp);
         LAUNCHED();
     }
@@ -1320,14 +1324,18 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     }
     uint64_t N = 0, NS = 0;
     for (uint32_t p = 0; p < P; p++) N += np[p], NS += nsp[p];
-    // sub-buckets of partition p: 2^s_p of about 16k k-mer instances each, so
-    // that a sub-bucket's distinct k-mers (a fraction of its instances) fit
-    // the table
+    // sub-buckets of partition p: 2^s_p of about 8k k-mer instances each (4k
+    // to 8k), so that a sub-bucket's distinct k-mers (a fraction of its
+    // instances) fit the table.  A sub-bucket that outgrows it goes to the
+    // record path, which costs several times its decode: halving the target
+    // from 16k cut phase 2 by a third on bacterial_100m (60 -> 40 ms per
+    // 3 Gbp) and by 3% on skewed_200m, where doubling it cost 26%.
+    constexpr uint64_t SUB_BUCKET_KMERS = 8192;
     std::vector<uint32_t> slog(2 * P);  // [0, P) s_p, [P, 2P) first sub-bucket of p
     uint64_t NB = 0;
     for (uint32_t p = 0; p < P; p++) {
         uint32_t sl = 0;
-        while (!ctx->opt.hash_l2_only && sl < (uint32_t)BS_LOG_LIMIT && np[p] > (16384ull << sl)) sl++;
+        while (!ctx->opt.hash_l2_only && sl < (uint32_t)BS_LOG_LIMIT && np[p] > (SUB_BUCKET_KMERS << sl)) sl++;
         slog[p] = sl;
         slog[P + p] = (uint32_t)NB;
         NB += 1ull << sl;
@@ -1335,6 +1343,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     auto bbase = [&](uint32_t p) -> uint64_t { return p < P ? slog[P + p] : NB; };
     ctx->times[4] = (double)NB;
     ctx->times[5] = 0;
+    ctx->times[8] = 0;
     float stage_ms = 0;  // host-to-device staging of spilled chunks
     uint64_t groups = 0;
     // output capacity, grown per group from the kept k-mers per instance of
@@ -1550,6 +1559,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         bp.bucket_kmers = ctx->bk_kmers.as<unsigned long long>();
         bp.heavy_kmers = BC_HEAVY_KMERS;
         bp.b0 = (uint32_t)bbase(p0);
+        bp.ids = nullptr;
         bp.k = ctx->opt.k;
         bp.cmin = cmin;
         bp.cmax = cmax;
@@ -1595,6 +1605,41 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         if (ctx->opt.hash_l2_only)  // every non-empty sub-bucket (one per partition)
             for (uint64_t b = bbase(p0); b < bbase(p1); b++)
                 if (off[b + 1] > off[b]) ids.push_back(b);
+        if (!ids.empty() && !ctx->opt.hash_l2_only) {
+            // Second pass: a sub-bucket that outgrew the 8192-slot table (not a
+            // heavy one) is counted again with 16384 slots; only heavy
+            // sub-buckets and those that overflow again take the record path,
+            // whose records cost several times the decode.
+            std::vector<uint32_t> heavy, over;
+            for (uint32_t b : ids) (ctx->h_km.as<uint64_t>()[b] > BC_HEAVY_KMERS ? heavy : over).push_back(b);
+            if (!over.empty()) {
+                const uint32_t no = (uint32_t)over.size();
+                CK(ctx->h_ids2.ensure((no + 1) * 4ull));
+                CK(ctx->bk_ids2.ensure(no * 4ull));
+                CK(ctx->bk_failed2.ensure((no + 1) * 4ull));
+                std::memcpy(ctx->h_ids2.p, over.data(), no * 4ull);
+                CK(cudaMemcpyAsync(ctx->bk_ids2.p, ctx->h_ids2.p, no * 4ull, cudaMemcpyHostToDevice, ctx->s));
+                CK(cudaMemsetAsync(ctx->bk_failed2.p, 0, 4, ctx->s));
+                CK(cudaFuncSetAttribute(bucket_count_kernel<BC_TS2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        BC_TS2 * 12));
+                bp.ids = ctx->bk_ids2.as<uint32_t>();
+                bp.failed = ctx->bk_failed2.as<uint32_t>();
+                bp.out_cap = ctx->out_cap;
+                {
+                    uint64_t ob = 0;
+                    for (uint32_t b : over) ob += 16 * (off[b + 1] - off[b]);
+                    KScope ks(ctx, GKC_K_HASH_INSERT, (double)ob);
+                    bucket_count_kernel<BC_TS2><<<no, BC_THREADS, BC_TS2 * 12, ctx->s>>>(bp);
+                    LAUNCHED();
+                }
+                CK(cudaMemcpyAsync(ctx->h_ids2.p, ctx->bk_failed2.p, (no + 1) * 4ull, cudaMemcpyDeviceToHost, ctx->s));
+                CK(cudaStreamSynchronize(ctx->s));
+                const uint32_t nf2 = std::min<uint32_t>(ctx->h_ids2.as<uint32_t>()[0], no);
+                ctx->times[8] += (double)(no - nf2);
+                heavy.insert(heavy.end(), ctx->h_ids2.as<uint32_t>() + 1, ctx->h_ids2.as<uint32_t>() + 1 + nf2);
+            }
+            ids.swap(heavy);
+        }
         if (!ids.empty()) {
             if (ctx->opt.hash_l2_only) {
                 RET(count_buckets_l2(ctx, ids, off, cmin, cmax));
@@ -3150,7 +3195,7 @@ int gkc_kernel_stats(gkc_ctx *ctx, double *ms, uint64_t *launches, double *bytes
 
 int gkc_last_timings(gkc_ctx *ctx, double *t, int n) {
     if (!ctx || !t) return GKC_EINVAL;
-    for (int i = 0; i < n && i < 8; i++) t[i] = ctx->times[i];
+    for (int i = 0; i < n && i < 9; i++) t[i] = ctx->times[i];
     return GKC_OK;
 }
 

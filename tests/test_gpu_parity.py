@@ -326,6 +326,34 @@ def test_heavy_and_overflowing_sub_buckets(oracle, record_slice, monkeypatch):
     assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
 
 
+def test_second_pass_counts_a_moderately_overflowing_sub_bucket(oracle):
+    """One minimizer made the preferred one for 250 reads adds ~5k distinct
+    k-mers to its sub-bucket (about 4-8k instances of other minimizers):
+    more than the first 8192-slot table holds, well within the second pass's
+    16384 slots.  It is counted there, not by the record split, with the
+    oracle's multiset."""
+    k, p, P = 31, 11, 4
+    r = np.random.default_rng(33)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    rnd = lambda n: bytes(acgt[r.integers(0, 4, n)])
+    X = b"CTTGACCGTAG"
+    parts = [rnd(70) + X + rnd(69) for _ in range(250)] + [rnd(150) for _ in range(3000)]
+    reads, offs = csr(parts)
+    code = lambda s: int("".join(str("ACGT".index(chr(ch))) for ch in s), 4)
+    lut = r.permutation(4 ** p).astype(np.uint32)
+    j = int(np.nonzero(lut == 0)[0][0])
+    lut[j], lut[code(X)] = lut[code(X)], 0
+    ko, co, do, _ = oracle.count_reads(reads, offs, k, p, P)
+    ko, co = sorted_table(ko, co)
+    with counter(k, p, P, "hash") as c:
+        c.set_order(lut)
+        n, d = c.count_reads(reads, offs)
+        km, ct = sorted_table(*c.result())
+        t = c.timings()
+    assert t["second_pass_sub_buckets"] >= 1 and t["overflowed_sub_buckets"] == 0
+    assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
+
+
 @pytest.mark.parametrize("kind", ["hash", "sort", "hash_redo", "hash_spill", "hash_spill_redo"])
 def test_count_partitions_subsets(oracle, kind, monkeypatch):
     """Counting a store in disjoint partition subsets (as the reference's
