@@ -544,6 +544,12 @@ def main():
     if "mix" in runs and "learned" in runs:
         orders["speedup_learned_vs_mix"] = runs["learned"]["gbps"] / runs["mix"]["gbps"]
 
+    # the hash counter's context is done: its pooled device memory goes back
+    # before the sort counter runs, so the sort's partition groups are sized
+    # as in a count of its own
+    c.close()
+    torch.cuda.empty_cache()
+
     # ---- counting phase against byte models ----
     hbm, src = peaks()
     N, S = main_run["kmer_instances"], main_run["store_bytes"]
@@ -661,7 +667,6 @@ def main():
             line["cpu_baseline"] = cpu_baseline(args, threads_all, samples)
         except Exception as ex:  # the reference library is test infrastructure; report why it is absent
             line["cpu_baseline"] = {"value": None, "unavailable": f"{type(ex).__name__}: {ex}"}
-    c.close()
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:

@@ -278,8 +278,9 @@ enum {
     GKC_K_SCAN = 7,             /* device-wide scans                       */
     GKC_K_RLE = 8,              /* run-length encoding + threshold         */
     GKC_K_BUCKET_SPLIT = 9,     /* phase 2 hash: superkmers -> sub-buckets */
-    GKC_K_HASH_RECORDS = 10,    /* phase 2 hash: heavy / overflowed sub-   */
-                                /* buckets through k-mer records           */
+    GKC_K_HASH_RECORDS = 10,    /* phase 2 hash: overflowed sub-buckets    */
+                                /* (second pass, 16384 slots) and heavy    */
+                                /* ones (k-mer records)                    */
     GKC_K_CLASSES = 11
 };
 

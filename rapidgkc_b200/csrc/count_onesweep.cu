@@ -82,6 +82,25 @@ struct OsTile {
     uint32_t seg_n;      // keys in the segment
 };
 
+// The descriptor of every pass tile (T keys), written once per sort: a pass
+// CTA then reads its next tile's descriptor with one load, issued while it
+// works on the current tile.
+template <int T>
+__global__ void os_tiles_kernel(OsSegs sg, uint32_t ntiles, OsTile *tiles) {
+    const uint32_t tile = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tile >= ntiles) return;
+    const uint32_t s = os_seg_of(sg.tile0, sg.nseg, tile);
+    const uint64_t s0 = sg.key0[s], sn = sg.key0[s + 1] - s0;
+    OsTile td;
+    td.t = tile - sg.tile0[s];
+    td.seg = s;
+    td.seg_start = s0;
+    td.seg_n = (uint32_t)sn;
+    td.start = s0 + (uint64_t)td.t * T;
+    td.n = (uint32_t)(sn - (uint64_t)td.t * T < (uint64_t)T ? sn - (uint64_t)td.t * T : (uint64_t)T);
+    tiles[tile] = td;
+}
+
 struct OsPasses {
     int n;                        // passes
     int shift[OS_MAX_PASSES];     // lowest bit of each pass's digit
@@ -163,7 +182,7 @@ __device__ __forceinline__ void os_store_status(uint32_t *p, uint32_t v) {
 struct OsPassParams {
     const void *in;
     void *out;
-    OsSegs seg;
+    const OsTile *tiles;
     uint32_t ntiles;
     uint32_t *status;         // [ntiles][NB]
     const uint32_t *gbase;    // [nseg][npass][NB] digit starts in the segment
@@ -181,14 +200,27 @@ template <class KT> constexpr int os_min_ctas() { return sizeof(KT) == 16 ? 4 : 
 struct OsShared {
     uint32_t ws[32];
     OsTile td;
+    __align__(16) OsTile td_next;  // the next tile's descriptor, fetched by cp.async
     uint32_t tile;
     uint32_t lb_fail;  // a look-back of this tile gave up: its keys are not written
 };
 
-// One tile of a pass.  WHOLE: the tile holds os_tile<KT>() keys (every tile
-// but a segment's last), so no key needs a bounds check.
-template <int RB, class KT, bool WHOLE>
-__device__ __forceinline__ void os_pass_tile(const OsPassParams &a, OsShared &sh) {
+// Thread 0 fetches a tile descriptor (32 bytes) into shared memory without
+// waiting for it; os_desc_wait makes the copy complete.
+__device__ __forceinline__ void os_desc_fetch(OsTile *dst, const OsTile *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d + 16), "l"(reinterpret_cast<const char *>(src) + 16)
+                 : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void os_desc_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// One tile of a pass.  (A bounds-check-free body for full tiles measured no
+// faster: with its loads unconditional the compiler holds all of them at
+// once and spills under the three-CTA register budget.)
+template <int RB, class KT>
+__device__ __forceinline__ void os_pass_tile(const OsPassParams &a, OsShared &sh, uint32_t next) {
     constexpr int NB = 1 << RB;
     constexpr int ITEMS = os_items<KT>();
     constexpr int T = os_tile<KT>();
@@ -211,7 +243,7 @@ __device__ __forceinline__ void os_pass_tile(const OsPassParams &a, OsShared &sh
     // this many tiles per L2 round trip; tiles start in order, so the tile
     // before is usually already inclusive or nearly so
     constexpr int LB_ROWS = BPT >= 4 ? 1 : 4 / BPT;
-    auto has = [&](uint32_t j) { return WHOLE || j < td.n; };
+    auto has = [&](uint32_t j) { return j < td.n; };
 
     // ---- load (all loads in flight first), then rank; warp w owns keys
     //      [w * 32 * ITEMS, (w + 1) * 32 * ITEMS) ----
@@ -236,6 +268,9 @@ __device__ __forceinline__ void os_pass_tile(const OsPassParams &a, OsShared &sh
         if (valid && (grp & lt) == 0) wcnt[warp * NB + dig] = (uint16_t)(pre + __popc(grp));
         __syncwarp();
     }
+    // thread 0: the next tile's descriptor, needed only at the next tile's
+    // start (its id came back from the atomic long ago)
+    if (threadIdx.x == 0 && next < a.ntiles) os_desc_fetch(&sh.td_next, a.tiles + next);
     __syncthreads();
     // ---- per digit: exclusive prefix over warps, tile count, published at once ----
     uint32_t *st = a.status + (uint64_t)tile * NB;
@@ -401,36 +436,28 @@ os_pass_kernel(OsPassParams a) {
     extern __shared__ __align__(16) unsigned char os_smem[];
     uint16_t *wcnt = reinterpret_cast<uint16_t *>(os_smem);
     __shared__ OsShared sh;
-    // The next tile's id is taken while the current tile runs, so the atomic's
-    // round trip is off the critical path.  A CTA's next tile is always later
+    // The next tile's id is taken while the current tile runs, and its
+    // descriptor read once the id is back, so neither round trip is on the
+    // critical path.  A CTA's next tile is always later
     // than its current one, so the earliest unfinished tile is always running
     // and every look-back ends.
-    uint32_t next = 0;
-    if (threadIdx.x == 0) next = atomicAdd(a.tile_ctr, 1u);
+    uint32_t next = 0;  // thread 0: the next tile
+    if (threadIdx.x == 0) {
+        next = atomicAdd(a.tile_ctr, 1u);
+        if (next < a.ntiles) os_desc_fetch(&sh.td_next, a.tiles + next);
+    }
     for (;;) {
         if (threadIdx.x == 0) {
-            const uint32_t tile = next;
-            if (tile < a.ntiles) next = atomicAdd(a.tile_ctr, 1u);
-            sh.tile = tile;
+            os_desc_wait();
+            sh.tile = next;
+            sh.td = sh.td_next;
             sh.lb_fail = 0;
-            if (tile < a.ntiles) {
-                const uint32_t s = os_seg_of(a.seg.tile0, a.seg.nseg, tile);
-                const uint64_t s0 = a.seg.key0[s], sn = a.seg.key0[s + 1] - s0;
-                OsTile td;
-                td.t = tile - a.seg.tile0[s];
-                td.seg = s;
-                td.seg_start = s0;
-                td.seg_n = (uint32_t)sn;
-                td.start = s0 + (uint64_t)td.t * T;
-                td.n = (uint32_t)(sn - (uint64_t)td.t * T < (uint64_t)T ? sn - (uint64_t)td.t * T : (uint64_t)T);
-                sh.td = td;
-            }
+            if (next < a.ntiles) next = atomicAdd(a.tile_ctr, 1u);
         }
         for (int i = threadIdx.x; i < OS_WARPS * NB / 2; i += OS_THREADS) reinterpret_cast<uint32_t *>(wcnt)[i] = 0;
         __syncthreads();
         if (sh.tile >= a.ntiles) break;
-        if (sh.td.n == (uint32_t)T) os_pass_tile<RB, KT, true>(a, sh);
-        else os_pass_tile<RB, KT, false>(a, sh);
+        os_pass_tile<RB, KT>(a, sh, next);
         __syncthreads();  // the staging area is cleared for the next tile
     }
 }

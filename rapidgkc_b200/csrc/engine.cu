@@ -1628,7 +1628,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
                 {
                     uint64_t ob = 0;
                     for (uint32_t b : over) ob += 16 * (off[b + 1] - off[b]);
-                    KScope ks(ctx, GKC_K_HASH_INSERT, (double)ob);
+                    KScope ks(ctx, GKC_K_HASH_RECORDS, (double)ob);
                     bucket_count_kernel<BC_TS2><<<no, BC_THREADS, BC_TS2 * 12, ctx->s>>>(bp);
                     LAUNCHED();
                 }
@@ -1829,6 +1829,7 @@ int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, i
     const uint64_t nhist = segs.size() * (uint64_t)ps.n * NB;
     CK(ctx->os_hist.ensure(nhist * 4));
     CK(ctx->os_status.ensure(ntiles * NB * 4));
+    CK(ctx->tiles.ensure(ntiles * sizeof(OsTile)));
     CK(ctx->os_ctr.ensure(64 * 4));
     CK(ctx->part_err.ensure(64));
     CK(cudaMemcpyAsync(ctx->os_segs.p, ctx->h_segs.p, tab, cudaMemcpyHostToDevice, ctx->s));
@@ -1862,8 +1863,11 @@ int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, i
         LAUNCHED();
     }
     {
-        KScope ks(ctx, GKC_K_SCAN, 8.0 * nhist);
+        KScope ks(ctx, GKC_K_SCAN, 8.0 * nhist + 32.0 * ntiles);
         os_scan_kernel<RB><<<(unsigned)(segs.size() * ps.n), 1024, 0, ctx->s>>>(ctx->os_hist.as<uint32_t>());
+        LAUNCHED();
+        os_tiles_kernel<(int)T><<<(unsigned)((ntiles + 255) / 256), 256, 0, ctx->s>>>(sg, (uint32_t)ntiles,
+                                                                                     ctx->tiles.as<OsTile>());
         LAUNCHED();
     }
     int per_sm = 0;
@@ -1875,7 +1879,7 @@ int onesweep_sort(gkc_ctx *ctx, const std::vector<uint64_t> &segs, uint64_t n, i
         OsPassParams q;
         q.in = src;
         q.out = dst;
-        q.seg = sg;
+        q.tiles = ctx->tiles.as<OsTile>();
         q.ntiles = (uint32_t)ntiles;
         q.status = ctx->os_status.as<uint32_t>();
         q.gbase = ctx->os_hist.as<uint32_t>();

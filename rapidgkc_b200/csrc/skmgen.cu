@@ -218,8 +218,11 @@ constexpr int P1_INF = 0x7FFFFFFF;
 // a later lane (a suffix minimum over lanes), in a later strip (published per
 // warp), or past the tile (the owning warp scans the staged halo, then global
 // memory).  Each lane then writes its records.
+// Four CTAs per SM for k <= 32 (64 registers; a few bytes spill) hide the
+// order table's L2 latency better than two (111 registers): 55.4 -> 43.7 ms
+// per 6 Gbp; three for k > 32, whose wider windows spill more at 64.
 template <bool LUT, bool KW>
-__global__ void __launch_bounds__(P1_THREADS)
+__global__ void __launch_bounds__(P1_THREADS, KW ? 3 : 4)
 find_superkmers_kernel(P1Params a) {
     extern __shared__ uint32_t hist[];  // [3P]: bytes, superkmers, k-mers per partition
     __shared__ P1Smem sm;
