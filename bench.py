@@ -18,7 +18,9 @@ Reported (one JSON line on rank 0):
              ranks), with the learned minimizer order (rapidgkc_b200/orders,
              trained on skewed genomes of other seeds; --order picks another)
   e2e        the same count through the C ABI from pinned host reads to host
-             (k-mer, count) arrays, copies inside the timed region
+             (k-mer, count) arrays, copies inside the timed region (the library
+             packs every other host batch to 2-bit codes on the host's threads
+             before copying it; h2d bytes are those it copied)
   orders     default (value order), mix (the learned order's pseudo-random
              bulk order with no network levels) and learned: each timed on the
              device and end to end, with max/mean partition load in k-mers
@@ -488,7 +490,7 @@ def main():
             lats.clear()
             ems, no = timed(step_batched, args.steps)
             e2e_by_order[nm] = {"value": bases * world / (ems / 1e3) / 1e9, "unit": "Gbp/s",
-                                "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)),
+                                "h2d_bytes_per_step": c.timings()["h2d_bytes"],
                                 "d2h_bytes_per_step": int((8 * kw + 4) * (xinfo.get("local_kept", no)
                                                                           if exchange else no)),
                                 "ms_per_step": ems, "path": "gkc_add_reads_batches + gkc_count + gkc_result"}
@@ -518,11 +520,12 @@ def main():
                 step_host()
             ems, no = timed(step_host, args.steps)
             e2e_by_order[nm] = {"value": bases * world / (ems / 1e3) / 1e9, "unit": "Gbp/s",
-                                "h2d_bytes_per_step": int(len(reads) + 8 * len(offs)),
+                                "h2d_bytes_per_step": c.timings()["h2d_bytes"],
                                 "d2h_bytes_per_step": int((8 * kw + 4) * (xinfo.get("local_kept", no)
                                                                           if exchange else no)),
                                 "ms_per_step": ems,
-                                "path": "gkc_count_reads (host reads, host result arrays)"}
+                                "path": "gkc_count_reads (host reads, host result arrays; every other host "
+                                        "batch packed to 2-bit codes on the host's threads before its copy)"}
     e2e = e2e_by_order.get(args.order)
 
     orders = {nm: {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()

@@ -249,14 +249,16 @@ int gkc_count_keys(gkc_ctx *ctx, const uint64_t *keys, uint64_t n, int mem, uint
                    uint64_t *n_out, uint64_t *n_distinct);
 
 /* Statistics of the last gkc_add_reads (phase 1) and gkc_count (phase 2)
- * calls (n <= 9 entries): times[0..3] = device milliseconds (CUDA events) of
+ * calls (n <= 10 entries): times[0..3] = device milliseconds (CUDA events) of
  * phase 1, its superkmer search, phase 2, and phase 2's counting kernels;
  * times[4] = sub-buckets of the hash counter, times[5] = those re-split by
  * k-mer hash (they held more than 65536 k-mer instances, or their distinct
  * k-mers overflowed shared memory twice); hash counter only: times[6] =
  * device milliseconds of staging spilled chunks back, times[7] = partition
  * groups counted, times[8] = sub-buckets that overflowed the first table and
- * were counted by the second pass (16384 slots). */
+ * were counted by the second pass (16384 slots); times[9] = bytes the last
+ * gkc_add_reads copied from host to device (host batches: read bases, half of
+ * the batches packed to 2-bit words, and offsets). */
 int gkc_last_timings(gkc_ctx *ctx, double *times, int n);
 
 /* Number of kernels this context launched since creation. */
@@ -293,6 +295,17 @@ enum {
  * inside a graph.  Arrays of n <= GKC_K_CLASSES entries; any may be NULL. */
 int gkc_set_profiling(gkc_ctx *ctx, int on);
 int gkc_kernel_stats(gkc_ctx *ctx, double *ms, uint64_t *launches, double *bytes, int n, int reset);
+
+/* No counterpart in the reference (its host passes ASCII to the device,
+ * gpu_skmgen.cu:573-574).  Packs n ASCII bases into 2-bit codes, 16 to a
+ * word, base 16w + t in bits 31-2t..30-2t of words[w], with the device's base
+ * map (A/C/G/T in either case -> 0..3, every other byte -> 0); positions past
+ * n in the last word are 0.  words holds (n + 15) / 16 entries.  Host memory
+ * only; runs on the library's pool of host threads.  This is the form in which
+ * gkc_add_reads and gkc_count_reads copy host batches to the device (a
+ * quarter of the ASCII bytes), except with homopolymer compression on, whose
+ * kernels read ASCII. */
+int gkc_pack_bases(const char *bases, uint64_t n, uint32_t *words);
 
 /* ---- learned minimizer order ------------------------------------------
  * No counterpart in the reference: its order is fixed (value order with the

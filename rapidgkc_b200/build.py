@@ -40,10 +40,13 @@ def _csrc(*names):
 def build_cuda(ptxas: bool = False, force: bool = False) -> str:
     out = os.path.join(PKG, "librapidgkc_b200.so")
     srcs = [os.path.join(CSRC, n) for n in sorted(os.listdir(CSRC)) if n.endswith((".cu", ".cuh"))]
-    srcs += [os.path.join(ROOT, "include", "gkc_capi.h")]
+    srcs += [os.path.join(CSRC, "pack_host.cpp"), os.path.join(ROOT, "include", "gkc_capi.h")]
     if force or ptxas or _stale(out, srcs):
+        # engine.cu includes the other .cu files; pack_host.cpp is host code
+        # (its AVX2 path is chosen at run time)
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
-               "-Xcompiler", "-fPIC", "-shared", "-o", out, os.path.join(CSRC, "engine.cu")]
+               "-Xcompiler", "-fPIC", "-shared", "-o", out, os.path.join(CSRC, "engine.cu"),
+               os.path.join(CSRC, "pack_host.cpp")]
         if ptxas:
             cmd.insert(1, "-Xptxas=-v")
         _run(cmd)

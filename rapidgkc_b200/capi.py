@@ -34,7 +34,7 @@ EXPORTS = (
     "gkc_count", "gkc_count_partitions", "gkc_result", "gkc_result_device", "gkc_count_reads", "gkc_count_keys",
     "gkc_last_timings", "gkc_kernel_launches", "gkc_set_stream", "gkc_set_profiling", "gkc_kernel_stats",
     "gkc_mlp_param_count", "gkc_minimizer_loads", "gkc_mlp_grad", "gkc_mlp_train", "gkc_mlp_scores",
-    "gkc_mlp_order", "gkc_count_keys_noalloc",
+    "gkc_mlp_order", "gkc_count_keys_noalloc", "gkc_pack_bases",
     "gkc_init", "gkc_skmgen_batch", "gkc_count_partition", "gkc_set_order_lut", "gkc_shutdown",
 )
 KERNEL_CLASSES = ("find_superkmers", "scatter_superkmers", "hash_insert", "hash_collect", "sort_extract",
@@ -120,6 +120,7 @@ def load_library(path: str = LIB_PATH):
     L.gkc_mlp_scores.argtypes = [vp, vp, vp, i32]
     L.gkc_mlp_order.argtypes = [vp, vp, u64, vp]
     L.gkc_count_keys_noalloc.argtypes = [vp, u64, u32, u32, vp, vp, u64, C.POINTER(u64), C.POINTER(u64), vp]
+    L.gkc_pack_bases.argtypes = [vp, u64, vp]
     L.gkc_init.argtypes = [i32, C.POINTER(Options), C.POINTER(vp)]
     L.gkc_skmgen_batch.argtypes = [vp, vp, vp, u64, i32, i32, i32, vp, i32, vp, vp, vp]
     L.gkc_count_partition.argtypes = [vp, i32, u32, u32, vp, vp, u64, i32, C.POINTER(u64), C.POINTER(u64)]
@@ -146,6 +147,19 @@ def _ptr(a):
             raise ValueError("tensors must be contiguous")
         return C.c_void_p(a.data_ptr()), MEM_DEVICE if a.is_cuda else MEM_HOST
     raise TypeError(f"unsupported buffer type {type(a)!r}")
+
+
+def pack_bases(bases) -> np.ndarray:
+    """ASCII bases (a uint8 array or bytes) -> uint32 words of 16 2-bit codes,
+    first base highest, with the device's base map (gkc_pack_bases; host
+    memory, the library's host threads)."""
+    b = np.frombuffer(bases, np.uint8) if isinstance(bases, (bytes, bytearray)) else np.ascontiguousarray(bases,
+                                                                                                        np.uint8)
+    out = np.zeros(max(1, (len(b) + 15) // 16), np.uint32)
+    rc = load_library().gkc_pack_bases(b.ctypes.data if len(b) else None, len(b), out.ctypes.data)
+    if rc != 0:
+        raise GkcError(rc, "gkc_pack_bases")
+    return out[:(len(b) + 15) // 16]
 
 
 class KmerCounter:
@@ -438,11 +452,11 @@ class KmerCounter:
         return lut
 
     def timings(self):
-        t = (C.c_double * 9)()
-        self._check(self._L.gkc_last_timings(self._h, t, 9))
+        t = (C.c_double * 10)()
+        self._check(self._L.gkc_last_timings(self._h, t, 10))
         return {"phase1_ms": t[0], "phase1_search_ms": t[1], "phase2_ms": t[2], "phase2_kernel_ms": t[3],
                 "sub_buckets": int(t[4]), "overflowed_sub_buckets": int(t[5]), "phase2_stage_ms": t[6],
-                "phase2_groups": int(t[7]), "second_pass_sub_buckets": int(t[8])}
+                "phase2_groups": int(t[7]), "second_pass_sub_buckets": int(t[8]), "h2d_bytes": int(t[9])}
 
     def kernel_launches(self) -> int:
         return int(self._L.gkc_kernel_launches(self._h))

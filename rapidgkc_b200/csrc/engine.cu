@@ -37,6 +37,11 @@
 
 using namespace gkc;
 
+namespace gkc_host {
+// pack_host.cpp: n ASCII bases -> nwords 2-bit words on the host's threads
+void pack_bases(const uint8_t *src, uint64_t n, uint32_t *words, uint64_t nwords);
+}  // namespace gkc_host
+
 namespace {
 
 struct DevBuf {
@@ -293,11 +298,14 @@ struct gkc_ctx {
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
     std::string err;
     uint64_t launches = 0;
-    double times[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // see gkc_last_timings
+    double times[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // see gkc_last_timings
 
     // phase 1 buffers
     DevBuf reads[2], offs[2];
     PinBuf offs_pin[2];
+    PinBuf pk_host[2];                   // host batches packed to 2-bit words (pinned), one per slot
+    uint64_t h2d_bytes = 0;              // bytes the last gkc_add_reads copied host to device
+    const uint32_t *p1_packed = nullptr;  // the batch in phase 1 as packed words (device), or null: ASCII
     cudaEvent_t buf_free[2] = {nullptr, nullptr}, buf_ready[2] = {nullptr, nullptr};
     DevBuf cta_hist, cta_base;  // phase 1: per-CTA partition counts and base offsets
     DevBuf records, region_count, hist, flags, cursors, part_off, tile_read, codes;
@@ -384,7 +392,7 @@ struct gkc_ctx {
                         &sk_starts, &sk_k32, &hpc_tiles, &hpc_tbase, &hpc_reads, &hpc_offs, &os_status, &os_hist,
                         &os_segs, &os_ctr, &bk_ids2, &bk_failed2};
         for (auto *d : ds) d->release();
-        PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work,
+        PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &pk_host[0], &pk_host[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work,
                         &h_desc, &h_cur, &h_segs, &h_ids2};
         for (auto *p : ps) p->release();
         arena.release();
@@ -598,7 +606,7 @@ int launch_find(gkc_ctx *ctx, const P1Plan &pl, const uint8_t *d_reads, const ui
                 uint64_t total, uint64_t cap, uint32_t *flags) {
     const uint32_t P = (uint32_t)ctx->opt.partitions;
     auto *hist = ctx->hist.as<unsigned long long>();
-    CK(cudaMemsetAsync(ctx->codes.as<uint32_t>() + pl.ntiles * P1_TILE_WORDS, 0, 16, ctx->s));
+    if (!ctx->p1_packed) CK(cudaMemsetAsync(ctx->codes.as<uint32_t>() + pl.ntiles * P1_TILE_WORDS, 0, 16, ctx->s));
     {
         uint32_t g = (uint32_t)std::min<uint64_t>((pl.ntiles + 255) / 256, (uint64_t)ctx->sms * 8);
         tile_reads_kernel<<<g, 256, 0, ctx->s>>>(d_offs, (int64_t)n_reads, pl.ntiles, ctx->tile_read.as<int64_t>());
@@ -608,6 +616,7 @@ int launch_find(gkc_ctx *ctx, const P1Plan &pl, const uint8_t *d_reads, const ui
     CK(cudaMemsetAsync(flags, 0, 4, ctx->s));
     P1Params a;
     a.reads = d_reads;
+    a.packed = ctx->p1_packed;
     a.offs = d_offs;
     a.n_reads = (int64_t)n_reads;
     a.total = total;
@@ -627,8 +636,9 @@ int launch_find(gkc_ctx *ctx, const P1Plan &pl, const uint8_t *d_reads, const ui
     a.part_kmers = hist + 2 * P;
     a.cta_hist = ctx->cta_hist.as<uint32_t>();
     a.err = flags;
-    // reads + offsets in, 2-bit codes out (records are added by the caller)
-    KScope ks(ctx, GKC_K_FIND_SUPERKMERS, 1.25 * (double)total + 8.0 * (n_reads + 1));
+    // reads (ASCII in, 2-bit codes out; or packed words in) + offsets (records
+    // are added by the caller)
+    KScope ks(ctx, GKC_K_FIND_SUPERKMERS, (ctx->p1_packed ? 0.25 : 1.25) * (double)total + 8.0 * (n_reads + 1));
     pl.kfind<<<pl.grid, P1_THREADS, pl.dyn, ctx->s>>>(a);
     LAUNCHED();
     return GKC_OK;
@@ -646,7 +656,7 @@ int launch_scatter(gkc_ctx *ctx, const P1Plan &pl, StoreChunk *c, uint64_t total
         LAUNCHED();
     }
     P2Params b;
-    b.codes = ctx->codes.as<uint32_t>();
+    b.codes = ctx->p1_packed ? ctx->p1_packed : ctx->codes.as<uint32_t>();
     b.records = ctx->records.as<SkmRecord>();
     b.region_cap = (uint32_t)cap;
     b.region_count = ctx->region_count.as<uint32_t>();
@@ -2254,8 +2264,16 @@ int hpc_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, uint
 // Phase 1 over host batches: the copy of batch i+1 (copy stream, two device
 // slots) overlaps phase 1 of batch i; no batch waits for the host (phase1_async)
 // unless the store spills (phase1_exact).
+// Host batches.  Every other batch crosses PCIe packed into 2-bit words (a
+// quarter of the ASCII bytes; gkc_pack_bases, on the host's threads), the
+// others as ASCII: the host's threads pack one batch while the copy engine
+// moves the next, so both host-memory readers work at once (packing every
+// batch left the copy engine idle and the threads the bound).  With
+// homopolymer compression every batch goes as ASCII (its kernels read it).
+// Batch i + 1 is prepared and copied while phase 1 of batch i runs.
 int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, const std::vector<ReadBatch> &batches) {
     const bool exact = ctx->opt.spill_host;
+    const bool pack = !ctx->opt.hpc;
     const size_t nbat = batches.size();
     uint64_t max_b = 0, max_r = 0;
     for (const auto &b : batches) {
@@ -2263,23 +2281,43 @@ int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, cons
         max_r = std::max<uint64_t>(max_r, b.r1 - b.r0);
     }
     CK(cudaStreamSynchronize(ctx->s));  // the slots may be reallocated below
+    // packed words of a batch, and 4 zero words after them (the scatter reads
+    // a code window one word past a superkmer's last base)
+    const uint64_t max_w = (max_b + 15) / 16 + 4;
     for (int slot = 0; slot < 2; slot++) {
-        CK(ctx->reads[slot].ensure(max_b + 64));
+        CK(ctx->reads[slot].ensure(std::max<uint64_t>(max_b + 64, pack ? max_w * 4 : 0)));
         CK(ctx->offs[slot].ensure((max_r + 1) * 8));
+        if (pack) CK(ctx->pk_host[slot].ensure(max_w * 4));
     }
     while (ctx->batch_ev.size() < 2 * nbat) {
         cudaEvent_t ev;
         CK(cudaEventCreate(&ev));
         ctx->batch_ev.push_back(ev);
     }
+    auto packed = [&](size_t bi) { return pack && (bi & 1); };
     auto stage = [&](size_t bi, cudaStream_t st) -> int {
         const int slot = (int)(bi & 1);
         const ReadBatch &b = batches[bi];
         const uint64_t base = offs[b.r0], nb = offs[b.r1] - base, nr = b.r1 - b.r0;
-        CK(cudaStreamWaitEvent(st, ctx->buf_free[slot], 0));
-        CK(cudaEventRecord(ctx->batch_ev[2 * bi], st));  // the batch starts with its copy
-        CK(cudaMemcpyAsync(ctx->reads[slot].p, reads + base, nb, cudaMemcpyHostToDevice, st));
+        if (packed(bi)) {
+            // the slot's pinned words are rewritten once their last copy is done
+            CK(cudaEventSynchronize(ctx->buf_ready[slot]));
+            const uint64_t nw = (nb + 15) / 16;
+            uint32_t *hw = ctx->pk_host[slot].as<uint32_t>();
+            gkc_host::pack_bases(reinterpret_cast<const uint8_t *>(reads) + base, nb, hw, nw);
+            std::memset(hw + nw, 0, 16);
+            CK(cudaStreamWaitEvent(st, ctx->buf_free[slot], 0));
+            CK(cudaEventRecord(ctx->batch_ev[2 * bi], st));  // the batch starts with its copy
+            CK(cudaMemcpyAsync(ctx->reads[slot].p, hw, (nw + 4) * 4, cudaMemcpyHostToDevice, st));
+            ctx->h2d_bytes += (nw + 4) * 4;
+        } else {
+            CK(cudaStreamWaitEvent(st, ctx->buf_free[slot], 0));
+            CK(cudaEventRecord(ctx->batch_ev[2 * bi], st));  // the batch starts with its copy
+            CK(cudaMemcpyAsync(ctx->reads[slot].p, reads + base, nb, cudaMemcpyHostToDevice, st));
+            ctx->h2d_bytes += nb;
+        }
         CK(cudaMemcpyAsync(ctx->offs[slot].p, offs + b.r0, (nr + 1) * 8, cudaMemcpyHostToDevice, st));
+        ctx->h2d_bytes += (nr + 1) * 8;
         CK(cudaEventRecord(ctx->buf_ready[slot], st));
         return GKC_OK;
     };
@@ -2295,13 +2333,18 @@ int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, cons
             const uint8_t *hr = ctx->hpc_reads.as<uint8_t>();
             uint64_t *ho = ctx->hpc_offs.as<uint64_t>();
             rc = sync_exact ? phase1_exact(ctx, hr, ho, nr, kept) : phase1_async(ctx, hr, ho, nr, kept, 0, bi);
-        } else if (sync_exact) {
-            const uint32_t g = (uint32_t)std::min<uint64_t>((nr + 256) / 256, (uint64_t)ctx->sms * 8);
-            rebase_offsets_kernel<<<g, 256, 0, ctx->s>>>(ctx->offs[slot].as<uint64_t>(), nr + 1, base);
-            LAUNCHED();
-            rc = phase1_exact(ctx, ctx->reads[slot].as<uint8_t>(), ctx->offs[slot].as<uint64_t>(), nr, nb);
         } else {
-            rc = phase1_async(ctx, ctx->reads[slot].as<uint8_t>(), ctx->offs[slot].as<uint64_t>(), nr, nb, base, bi);
+            ctx->p1_packed = packed(bi) ? ctx->reads[slot].as<uint32_t>() : nullptr;
+            if (sync_exact) {
+                const uint32_t g = (uint32_t)std::min<uint64_t>((nr + 256) / 256, (uint64_t)ctx->sms * 8);
+                rebase_offsets_kernel<<<g, 256, 0, ctx->s>>>(ctx->offs[slot].as<uint64_t>(), nr + 1, base);
+                LAUNCHED();
+                rc = phase1_exact(ctx, ctx->reads[slot].as<uint8_t>(), ctx->offs[slot].as<uint64_t>(), nr, nb);
+            } else {
+                rc = phase1_async(ctx, ctx->reads[slot].as<uint8_t>(), ctx->offs[slot].as<uint64_t>(), nr, nb,
+                                  base, bi);
+            }
+            ctx->p1_packed = nullptr;
         }
         CK(cudaEventRecord(ctx->buf_free[slot], ctx->s));
         CK(cudaEventRecord(ctx->batch_ev[2 * bi + 1], ctx->s));
@@ -2309,10 +2352,12 @@ int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, cons
     };
     CK(cudaEventRecord(ctx->buf_free[0], ctx->s));
     CK(cudaEventRecord(ctx->buf_free[1], ctx->s));
+    // batch i's phase 1 is queued before batch i + 1 is staged, so that the
+    // device works while the host packs
     int rc = nbat ? stage(0, ctx->cs) : GKC_OK;
     for (size_t bi = 0; rc == GKC_OK && bi < nbat; bi++) {
-        if (bi + 1 < nbat) rc = stage(bi + 1, ctx->cs);
-        if (rc == GKC_OK) rc = run(bi, exact);
+        rc = run(bi, exact);
+        if (rc == GKC_OK && bi + 1 < nbat) rc = stage(bi + 1, ctx->cs);
     }
     CK(cudaStreamSynchronize(ctx->s));
     if (rc != GKC_OK) return rc;
@@ -2473,6 +2518,7 @@ int gkc_add_reads(gkc_ctx *ctx, const char *reads, const uint64_t *offs, uint64_
     for (char c : ctx->counted)
         if (c) return ctx->fail(GKC_ESTATE, "the store is partly counted; clear it before adding reads");
     ctx->times[0] = ctx->times[1] = 0;
+    ctx->h2d_bytes = 0;
     ctx->batch_ms.clear();
     if (n_reads == 0) return GKC_OK;
     if (mem == GKC_MEM_DEVICE) {
@@ -2539,6 +2585,7 @@ int gkc_add_reads_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs,
     for (char c : ctx->counted)
         if (c) return ctx->fail(GKC_ESTATE, "the store is partly counted; clear it before adding reads");
     ctx->times[0] = ctx->times[1] = 0;
+    ctx->h2d_bytes = 0;
     ctx->batch_ms.clear();
     std::vector<ReadBatch> batches;
     uint64_t r = 0;
@@ -2905,6 +2952,12 @@ int gkc_store_append(gkc_ctx *ctx, int p0, int p1, const uint8_t *bytes, const u
     return GKC_OK;
 }
 
+int gkc_pack_bases(const char *bases, uint64_t n, uint32_t *words) {
+    if ((!bases || !words) && n) return GKC_EINVAL;
+    gkc_host::pack_bases(reinterpret_cast<const uint8_t *>(bases), n, words, (n + 15) / 16);
+    return GKC_OK;
+}
+
 int gkc_reserve_host(gkc_ctx *ctx, uint64_t bytes, uint64_t *pinned) {
     if (!ctx) return GKC_EINVAL;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return GKC_ECUDA;
@@ -3199,7 +3252,8 @@ int gkc_kernel_stats(gkc_ctx *ctx, double *ms, uint64_t *launches, double *bytes
 
 int gkc_last_timings(gkc_ctx *ctx, double *t, int n) {
     if (!ctx || !t) return GKC_EINVAL;
-    for (int i = 0; i < n && i < 9; i++) t[i] = ctx->times[i];
+    ctx->times[9] = (double)ctx->h2d_bytes;
+    for (int i = 0; i < n && i < 10; i++) t[i] = ctx->times[i];
     return GKC_OK;
 }
 

@@ -58,7 +58,10 @@ constexpr int P1_CODE_WORDS = P1_STAGE / 16 + 2;      // 16 bases per word
 constexpr int P1_BM_WORDS = P1_STAGE / 32 + 2;        // 32 positions per word
 
 struct P1Params {
-    const uint8_t *reads;      // concatenated ASCII bases
+    const uint8_t *reads;      // concatenated ASCII bases, or
+    const uint32_t *packed;    // (when not null) the same bases as 2-bit codes, 16 to a word
+                               // (first base highest: the words staged below); then they
+                               // are also the batch's codes, and `codes` is not written
     const uint64_t *offs;      // n_reads+1 read offsets
     int64_t n_reads;
     uint64_t total;            // offs[n_reads]
@@ -122,6 +125,11 @@ __device__ __forceinline__ uint32_t pmer_key(uint32_t v, int p, uint32_t pmask) 
     return mm_valid(v, p) ? v : pmask;
 }
 
+// 2-bit code of base q of the batch, from the ASCII or the packed words.
+__device__ __forceinline__ uint32_t base_code(const P1Params &a, uint64_t q) {
+    return a.packed ? (__ldg(a.packed + (q >> 4)) >> (30 - 2 * (uint32_t)(q & 15))) & 3u : code1(a.reads[q]);
+}
+
 // Minimizer key of k-mer q computed directly from global memory (used only
 // for superkmers that run past the staged halo).
 template <bool LUT>
@@ -129,7 +137,7 @@ __device__ uint32_t kmer_key_global(const P1Params &a, uint64_t q) {
     const uint32_t pmask = 0xFFFFFFFFu >> (32 - 2 * a.p);
     uint32_t f = 0, best = 0xFFFFFFFFu;
     for (int j = 0; j < a.k; j++) {
-        f = ((f << 2) | code1(a.reads[q + j])) & pmask;
+        f = ((f << 2) | base_code(a, q + j)) & pmask;
         if (j >= a.p - 1) {
             uint32_t m;
             if (LUT) {
@@ -256,7 +264,9 @@ find_superkmers_kernel(P1Params a) {
         for (int i = threadIdx.x; i < P1_CODE_WORDS; i += blockDim.x) {
             int64_t q = sbeg + 16 * (int64_t)i;
             uint32_t word = 0;
-            if (q >= 0 && q + 16 <= (int64_t)a.total && a.vec_ok) {
+            if (a.packed) {  // q is a multiple of 16: one word (0 past the batch's end)
+                if (q >= 0 && q < (int64_t)a.total) word = __ldg(a.packed + (q >> 4));
+            } else if (q >= 0 && q + 16 <= (int64_t)a.total && a.vec_ok) {
                 uint4 v = __ldg(reinterpret_cast<const uint4 *>(a.reads + q));
                 word = (pack4(codes4(v.x)) << 24) | (pack4(codes4(v.y)) << 16) |
                        (pack4(codes4(v.z)) << 8) | pack4(codes4(v.w));
@@ -269,7 +279,7 @@ find_superkmers_kernel(P1Params a) {
             }
             sm.codes[i] = word;
             if (!LUT) sm.rcodes[P1_CODE_WORDS - 1 - i] = rc16(word);
-            if (i >= 2 && i < 2 + P1_TILE_WORDS) a.codes[tile * P1_TILE_WORDS + (i - 2)] = word;
+            if (!a.packed && i >= 2 && i < 2 + P1_TILE_WORDS) a.codes[tile * P1_TILE_WORDS + (i - 2)] = word;
         }
         for (int i = threadIdx.x; i < P1_BM_WORDS; i += blockDim.x) sm.bm[i] = 0;
         if (threadIdx.x == 0) sm.rs0 = a.offs[r0];
