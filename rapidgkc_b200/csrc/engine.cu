@@ -588,7 +588,7 @@ int p1_plan(gkc_ctx *ctx, uint64_t total, P1Plan *pl) {
     pl->tiles_per_cta = (pl->ntiles + pl->grid - 1) / pl->grid;
     pl->cap = std::min<uint64_t>(pl->tiles_per_cta * P1_TILE / 4 + 4096, UINT32_MAX);  // records per CTA
     pl->cap_max = pl->tiles_per_cta * P1_TILE + 64;
-    const size_t dyn2 = 2ull * P * (sizeof(unsigned long long) + sizeof(uint32_t));
+    const size_t dyn2 = p2_smem(P);
     CK(cudaFuncSetAttribute(scatter_superkmers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn2));
     // per-context buffers every batch of this size needs
     CK(ctx->region_count.ensure(pl->grid * sizeof(uint32_t)));
@@ -669,7 +669,7 @@ int launch_scatter(gkc_ctx *ctx, const P1Plan &pl, StoreChunk *c, uint64_t total
     b.bytes = c->bytes;
     b.idx = c->idx;
     b.keys = c->keys;
-    const size_t dyn2 = 2ull * P * (sizeof(unsigned long long) + sizeof(uint32_t));
+    const size_t dyn2 = p2_smem(P);
     // records (16 B) and codes in; superkmer bytes, index (8 B) and keys (4 B) out
     KScope ks(ctx, GKC_K_SCATTER, 28.0 * nskm_hint + 0.25 * (double)total + nbytes_hint);
     scatter_superkmers_kernel<<<pl.grid, P2_THREADS, dyn2, ctx->s>>>(b);

@@ -644,112 +644,195 @@ struct P2Params {
     uint32_t *keys;  // minimizer key of each superkmer, indexed like idx
 };
 
-// One thread per record at a time; 1024-thread CTAs timed faster than
-// 256 x 6 or 512 x 3 with their register caps.
+// 1024-thread CTAs.  A CTA's records are taken in chunks of P2_CHUNK, each
+// put in partition order first (a counting sort in shared memory), so that a
+// warp's 32 records fall into a few runs of one partition each: a run
+// reserves its bytes and index slots with one atomic, and its superkmers
+// leave as contiguous, mostly whole sectors.  In record order every record of
+// a warp went to another partition's write front (296-592 CTAs x P fronts),
+// and partial sectors were completed by read-modify-write in DRAM.
 constexpr int P2_THREADS = 1024;
+constexpr int P2_CHUNK = 8192;  // records per chunk (8 per thread)
 
-__global__ void __launch_bounds__(P2_THREADS)
+// Dynamic shared memory of the scatter: CTA bases (2P u64), cursors (2P),
+// chunk counts and starts (P each), the chunk order (u16 per record).
+__host__ __device__ inline size_t p2_smem(uint32_t P) {
+    return 2ull * P * 8 + 2ull * P * 4 + 2ull * P * 4 + (size_t)P2_CHUNK * 2;
+}
+
+__global__ void __launch_bounds__(P2_THREADS, 2)
 scatter_superkmers_kernel(P2Params a) {
-    extern __shared__ unsigned long long sbase[];  // [2P] CTA bases in each partition
-    uint32_t *lcnt = reinterpret_cast<uint32_t *>(sbase + 2 * a.P);  // [2P] CTA-local cursors
+    extern __shared__ unsigned long long sbase[];                    // [2P] CTA bases in each partition
+    uint32_t *lcnt = reinterpret_cast<uint32_t *>(sbase + 2 * a.P);  // [2P] CTA-local cursors (bytes, superkmers)
+    uint32_t *ccnt = lcnt + 2 * a.P;                                 // [P] records of the chunk per partition
+    uint32_t *cstart = ccnt + a.P;                                   // [P] their first place in chunk order
+    uint16_t *order = reinterpret_cast<uint16_t *>(cstart + a.P);    // [P2_CHUNK] chunk records by partition
+    __shared__ uint32_t ws[P2_THREADS / 32];
     if (*a.flags & (ERR_RECORD_OVERFLOW | ERR_CAPACITY)) return;  // the batch is redone
     const uint32_t n = a.region_count[blockIdx.x] < a.region_cap ? a.region_count[blockIdx.x] : a.region_cap;
     const SkmRecord *rec = a.records + (uint64_t)blockIdx.x * a.region_cap;
     // this CTA's ranges, laid out by cta_offsets_kernel from the find kernel's
-    // per-CTA counts: one pass over the records
+    // per-CTA counts
     const unsigned long long *cb = a.cta_base + (uint64_t)blockIdx.x * 2 * a.P;
     for (uint32_t i = threadIdx.x; i < 2 * a.P; i += blockDim.x) {
         sbase[i] = cb[i];
         lcnt[i] = 0;
     }
-    __syncthreads();
-    // Warps take 32 records at a time.  Each lane sets up its own record
-    // (destination, code slot, headers); then the warp writes the records'
-    // destination words cooperatively, one aligned 4-byte word per lane per
-    // step (no lane waits for a longer superkmer, and consecutive lanes
-    // write consecutive words).
     const int lane = threadIdx.x & 31;
-    const uint32_t nwarps = blockDim.x >> 5;
-    for (uint32_t base = (threadIdx.x >> 5) * 32; base < n; base += nwarps * 32) {
-        const uint32_t i = base + lane;
-        const bool has = i < n;
-        uint64_t dst = 0, pos = 0;
-        uint32_t nb = 0, rlim = 0, hdr = 0, nw = 0;
-        if (has) {
-            const SkmRecord r = rec[i];
-            const uint32_t part = fastmod(~r.key, a.pmod, a.P);
-            const uint32_t phase = rec_phase(r.pos), tail = rec_tail(r.pos);
-            nb = skm_nbytes(phase, r.len, a.k);
-            const uint32_t ob = atomicAdd(&lcnt[part], nb);
-            const uint32_t os = atomicAdd(&lcnt[a.P + part], 1u);
-            const uint64_t pbase = sbase[part] - a.part_byte_off[part];  // this CTA's range in the partition
-            dst = reinterpret_cast<uint64_t>(a.bytes + sbase[part] + ob);
-            pos = rec_base(r.pos) - phase;              // first code slot of the first byte
-            rlim = phase + r.len + (uint32_t)a.k - 1 + tail;  // read bases used, from pos
-            hdr = (3 - phase) | (((phase + r.len + (uint32_t)a.k - 1) % 3) << 2);  // first, last byte headers
-            nw = (uint32_t)((((dst + nb + 3) & ~3ull) - (dst & ~3ull)) >> 2);
-            a.idx[sbase[a.P + part] + os] = idx_pack(pbase + ob, r.len);
-            a.keys[sbase[a.P + part] + os] = r.key;
-        }
-        uint32_t incl = nw;
+    const unsigned lanes_le = 0xFFFFFFFFu >> (31 - lane);
+    constexpr int PER = P2_CHUNK / P2_THREADS;
+    for (uint32_t c0 = 0; c0 < n; c0 += P2_CHUNK) {
+        const uint32_t m = n - c0 < (uint32_t)P2_CHUNK ? n - c0 : (uint32_t)P2_CHUNK;
+        for (uint32_t i = threadIdx.x; i < a.P; i += blockDim.x) ccnt[i] = 0;
+        __syncthreads();
+        // ---- the chunk's records counted per partition (rank within it) ----
+        uint32_t pr[PER];  // partition << 16 | rank (ranks < P2_CHUNK)
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(FULL, incl, d);
-            if (lane >= d) incl += y;
-        }
-        const uint32_t total = __shfl_sync(FULL, incl, 31), excl = incl - nw;
-        for (uint32_t c0 = 0; c0 < total; c0 += 32) {
-            const uint32_t gi = c0 + lane;
-            int own = 0;  // the last lane whose first word index is <= gi
-#pragma unroll
-            for (int st = 16; st; st >>= 1) {
-                const int cand = own + st;
-                if (__shfl_sync(FULL, excl, cand) <= gi) own = cand;
+        for (int t = 0; t < PER; t++) {
+            const uint32_t j = threadIdx.x + t * P2_THREADS;
+            pr[t] = 0;
+            if (j < m) {
+                const uint32_t part = fastmod(~rec[c0 + j].key, a.pmod, a.P);
+                pr[t] = (part << 16) | atomicAdd(&ccnt[part], 1u);
             }
-            const uint32_t s = gi - __shfl_sync(FULL, excl, own);
-            const uint64_t odst = __shfl_sync(FULL, dst, own), opos = __shfl_sync(FULL, pos, own);
-            const uint32_t onb = __shfl_sync(FULL, nb, own), olim = __shfl_sync(FULL, rlim, own);
-            const uint32_t ohdr = __shfl_sync(FULL, hdr, own);
-            if (gi >= total) continue;
-            const uint64_t A = (odst & ~3ull) + 4ull * s;    // this lane's destination word
-            const int b0 = (int)((int64_t)A - (int64_t)odst);  // superkmer byte at A (may be < 0)
-            auto codes_at = [&](uint64_t q) -> uint64_t {   // base q in bits 63-62, >= 17 bases
-                const uint64_t wi = q >> 4;
-                return (((uint64_t)__ldg(a.codes + wi) << 32) | __ldg(a.codes + wi + 1)) << (2 * (uint32_t)(q & 15));
-            };
-            if (b0 >= 1 && b0 + 4 < (int)onb) {
-                // interior: 12 bases -> 4 bytes of 6 code bits + header 3 (little-endian)
-                const uint32_t x = (uint32_t)(codes_at(opos + 3ull * (uint32_t)b0) >> 40);
-                *reinterpret_cast<uint32_t *>(A) = (x >> 18) | (((x >> 12) & 63u) << 8) | (((x >> 6) & 63u) << 16) |
-                                                   ((x & 63u) << 24) | 0xC0C0C0C0u;
-            } else {
-                // first or last word: byte by byte, only the superkmer's bytes
-                uint32_t word = 0, nvalid = 0;
-                for (int j = 0; j < 4; j++) {
-                    const int bb = b0 + j;
-                    if (bb < 0 || bb >= (int)onb) continue;
-                    const uint32_t q = 3u * (uint32_t)bb;  // slot of byte bb, from opos
-                    uint32_t v = (uint32_t)(codes_at(opos + q) >> 58), h = 3;
-                    if (bb == (int)onb - 1) {
-                        const uint32_t keep = olim > q ? (olim - q < 3 ? olim - q : 3u) : 0u;
-                        v &= ~((1u << (6 - 2 * keep)) - 1) & 63u;
-                        h = ohdr >> 2;
-                    } else if (bb == 0) {
-                        h = ohdr & 3;
-                    }
-                    word |= (v | (h << 6)) << (8 * j);
-                    nvalid++;
+        }
+        __syncthreads();
+        // ---- each partition's first place in chunk order ----
+        {
+            const uint32_t per = (a.P + P2_THREADS - 1) / P2_THREADS, p0 = threadIdx.x * per;
+            uint32_t sum = 0, tot;
+            for (uint32_t p = p0; p < p0 + per && p < a.P; p++) sum += ccnt[p];
+            uint32_t pre = block_exclusive_scan<P2_THREADS>(sum, &tot, ws);
+            for (uint32_t p = p0; p < p0 + per && p < a.P; p++) {
+                cstart[p] = pre;
+                pre += ccnt[p];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const uint32_t j = threadIdx.x + t * P2_THREADS;
+            if (j < m) order[cstart[pr[t] >> 16] + (pr[t] & 0xFFFFu)] = (uint16_t)j;
+        }
+        __syncthreads();
+        // ---- warps take 32 records in partition order at a time.  Each lane
+        //      sets up its own record (destination, code slot, headers); the
+        //      lanes of one partition form a run that reserves its bytes and
+        //      index slots with one atomic.  Then the warp writes the records'
+        //      destination words cooperatively, one aligned 4-byte word per
+        //      lane per step (no lane waits for a longer superkmer, and
+        //      consecutive lanes write consecutive words). ----
+        const uint32_t nwarps = blockDim.x >> 5;
+        for (uint32_t base = (threadIdx.x >> 5) * 32; base < m; base += nwarps * 32) {
+            const uint32_t i = base + lane;
+            const bool has = i < m;
+            SkmRecord r;
+            r.pos = 0;
+            r.len = 0;
+            r.key = 0;
+            uint32_t part = 0xFFFFFFFFu, nb = 0;
+            if (has) {
+                r = rec[c0 + order[i]];
+                part = fastmod(~r.key, a.pmod, a.P);
+                nb = skm_nbytes(rec_phase(r.pos), r.len, a.k);
+            }
+            // runs of one partition: heads, inclusive byte prefix, run bounds
+            const uint32_t prev = __shfl_up_sync(FULL, part, 1);
+            const unsigned heads = __ballot_sync(FULL, lane == 0 || prev != part);
+            uint32_t incl = nb;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL, incl, d);
+                if (lane >= d) incl += y;
+            }
+            const int hs = 31 - __clz(heads & lanes_le);                   // this run's first lane
+            const unsigned later = heads & ~lanes_le;                      // heads after this lane
+            const int he = later ? __ffs(later) - 2 : 31;                  // this run's last lane
+            const uint32_t excl_s = __shfl_sync(FULL, incl - nb, hs);      // bytes before the run
+            const uint32_t run_bytes = __shfl_sync(FULL, incl, he) - excl_s;
+            uint32_t rb = 0, rs = 0;
+            if (has && lane == hs) {
+                rb = atomicAdd(&lcnt[part], run_bytes);
+                rs = atomicAdd(&lcnt[a.P + part], (uint32_t)(he - hs + 1));
+            }
+            rb = __shfl_sync(FULL, rb, hs);
+            rs = __shfl_sync(FULL, rs, hs);
+            uint64_t dst = 0, pos = 0;
+            uint32_t rlim = 0, hdr = 0, nw = 0;
+            if (has) {
+                const uint32_t phase = rec_phase(r.pos), tail = rec_tail(r.pos);
+                const uint32_t ob = rb + (incl - nb - excl_s);
+                const uint32_t os = rs + (uint32_t)(lane - hs);
+                const uint64_t pbase = sbase[part] - a.part_byte_off[part];  // this CTA's range in the partition
+                dst = reinterpret_cast<uint64_t>(a.bytes + sbase[part] + ob);
+                pos = rec_base(r.pos) - phase;              // first code slot of the first byte
+                rlim = phase + r.len + (uint32_t)a.k - 1 + tail;  // read bases used, from pos
+                hdr = (3 - phase) | (((phase + r.len + (uint32_t)a.k - 1) % 3) << 2);  // first, last byte headers
+                nw = (uint32_t)((((dst + nb + 3) & ~3ull) - (dst & ~3ull)) >> 2);
+                a.idx[sbase[a.P + part] + os] = idx_pack(pbase + ob, r.len);
+                a.keys[sbase[a.P + part] + os] = r.key;
+            }
+            uint32_t wincl = nw;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL, wincl, d);
+                if (lane >= d) wincl += y;
+            }
+            const uint32_t total = __shfl_sync(FULL, wincl, 31), excl = wincl - nw;
+            for (uint32_t w0 = 0; w0 < total; w0 += 32) {
+                const uint32_t gi = w0 + lane;
+                int own = 0;  // the last lane whose first word index is <= gi
+#pragma unroll
+                for (int st = 16; st; st >>= 1) {
+                    const int cand = own + st;
+                    if (__shfl_sync(FULL, excl, cand) <= gi) own = cand;
                 }
-                if (nvalid == 4) {
-                    *reinterpret_cast<uint32_t *>(A) = word;
+                const uint32_t sw = gi - __shfl_sync(FULL, excl, own);
+                const uint64_t odst = __shfl_sync(FULL, dst, own), opos = __shfl_sync(FULL, pos, own);
+                const uint32_t onb = __shfl_sync(FULL, nb, own), olim = __shfl_sync(FULL, rlim, own);
+                const uint32_t ohdr = __shfl_sync(FULL, hdr, own);
+                if (gi >= total) continue;
+                const uint64_t A = (odst & ~3ull) + 4ull * sw;   // this lane's destination word
+                const int b0 = (int)((int64_t)A - (int64_t)odst);  // superkmer byte at A (may be < 0)
+                auto codes_at = [&](uint64_t q) -> uint64_t {   // base q in bits 63-62, >= 17 bases
+                    const uint64_t wi = q >> 4;
+                    return (((uint64_t)__ldg(a.codes + wi) << 32) | __ldg(a.codes + wi + 1)) << (2 * (uint32_t)(q & 15));
+                };
+                if (b0 >= 1 && b0 + 4 < (int)onb) {
+                    // interior: 12 bases -> 4 bytes of 6 code bits + header 3 (little-endian)
+                    const uint32_t x = (uint32_t)(codes_at(opos + 3ull * (uint32_t)b0) >> 40);
+                    *reinterpret_cast<uint32_t *>(A) = (x >> 18) | (((x >> 12) & 63u) << 8) | (((x >> 6) & 63u) << 16) |
+                                                       ((x & 63u) << 24) | 0xC0C0C0C0u;
                 } else {
+                    // first or last word: byte by byte, only the superkmer's bytes
+                    uint32_t word = 0, nvalid = 0;
                     for (int j = 0; j < 4; j++) {
                         const int bb = b0 + j;
-                        if (bb >= 0 && bb < (int)onb) reinterpret_cast<uint8_t *>(A)[j] = (uint8_t)(word >> (8 * j));
+                        if (bb < 0 || bb >= (int)onb) continue;
+                        const uint32_t q = 3u * (uint32_t)bb;  // slot of byte bb, from opos
+                        uint32_t v = (uint32_t)(codes_at(opos + q) >> 58), h = 3;
+                        if (bb == (int)onb - 1) {
+                            const uint32_t keep = olim > q ? (olim - q < 3 ? olim - q : 3u) : 0u;
+                            v &= ~((1u << (6 - 2 * keep)) - 1) & 63u;
+                            h = ohdr >> 2;
+                        } else if (bb == 0) {
+                            h = ohdr & 3;
+                        }
+                        word |= (v | (h << 6)) << (8 * j);
+                        nvalid++;
+                    }
+                    if (nvalid == 4) {
+                        *reinterpret_cast<uint32_t *>(A) = word;
+                    } else {
+                        for (int j = 0; j < 4; j++) {
+                            const int bb = b0 + j;
+                            if (bb >= 0 && bb < (int)onb) reinterpret_cast<uint8_t *>(A)[j] = (uint8_t)(word >> (8 * j));
+                        }
                     }
                 }
             }
         }
+        __syncthreads();  // ccnt, cstart and order are reused by the next chunk
     }
 }
 
