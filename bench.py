@@ -70,13 +70,13 @@ WORKLOAD_DESC = {
 # DRAM bytes (read + write) per read base of a kernel class, from one ncu
 # capture of the current kernels on a 0.05-scale case of the named workload
 # (profiles/phase1_and_counter_skewed_small.md, learned order, 256 MiB
-# batches): find_superkmers from a full 256 MiB batch (682 MB / 268.4M bases),
+# batches): find_superkmers from a full 256 MiB batch (686 MB / 268.4M bases),
 # hash_insert (bucket_count_kernel) from its one launch over the whole case
 # (846 MB / 300M bases).  The roofline's `traffic` scales them to the bases of
 # one launch.  Keyed by (workload, order, kernel class).
 TRAFFIC_PER_BASE: dict = {
-    ("skewed_200m", "learned", "find_superkmers"): (301.616384e6 + 380.149e6) / 268435456,
-    ("skewed_200m", "learned", "hash_insert"): (739.905536e6 + 105.852e6) / 300e6,
+    ("skewed_200m", "learned", "find_superkmers"): (301.380352e6 + 384.318208e6) / 268435456,
+    ("skewed_200m", "learned", "hash_insert"): (739.846144e6 + 105.991424e6) / 300e6,
 }
 
 
