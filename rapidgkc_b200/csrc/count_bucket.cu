@@ -111,11 +111,16 @@ __device__ __forceinline__ void warp_kmer_runs(const BEntry *ent, uint64_t b, ui
         const uint64_t w0 = w[0], w1 = w[1], w2 = w[2];
         const uint64_t lo = sh ? (w0 >> sh) | (w1 << (64 - sh)) : w0;  // bytes 0..7
         const uint64_t hi = sh ? (w1 >> sh) | (w2 << (64 - sh)) : w1;  // bytes 8..15
-        // 48 bases, slot 0 in bits 95-94
-        const unsigned __int128 v = ((unsigned __int128)pack6x8(lo) << 48) | pack6x8(hi);
-        uint64_t x = (uint64_t)(v >> (96 - 2 * (s + (uint32_t)k))) & mask;
+        // 48 bases, slot 0 first: A holds slots 0-23 (48 bits), B slots 24-47.
+        // The 96-bit value A:B shifted right by d is, in its low 64 bits (all
+        // that the masks below keep), (A << (48 - d)) | (B >> d) for d <= 48
+        // and A >> (d - 48) beyond: 64-bit shifts, no 128-bit one.
+        const uint64_t A = pack6x8(lo), B = pack6x8(hi);
+        auto shr96 = [&](uint32_t dd) -> uint64_t { return dd <= 48 ? (A << (48 - dd)) | (B >> dd) : A >> (dd - 48); };
+        const uint32_t d = 96 - 2 * (s + (uint32_t)k);  // 30..34 for k = 31
+        uint64_t x = shr96(d) & mask;
         // the quad's KQ-1 entering bases (slots s+k .. s+k+KQ-2), the last in bits 1-0
-        const uint32_t nxt = (uint32_t)(v >> (96 - 2 * (s + (uint32_t)k + KQ - 1)));
+        const uint32_t nxt = (uint32_t)shr96(d - 2 * (KQ - 1));
         uint64_t r = rc64(x, k);
         uint64_t last = x < r ? x : r;
         uint32_t run = 1;
