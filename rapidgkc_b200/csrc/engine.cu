@@ -28,6 +28,7 @@
 #include "count_records.cu"
 #include "count_sort.cu"
 #include "count_onesweep.cu"
+#include "count_wide.cu"
 #include "order_mlp.cu"
 #include "skmgen.cu"
 #include "store_pack.cu"
@@ -2082,6 +2083,256 @@ int count_sort(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     return GKC_OK;
 }
 
+// Hash counter for k of 33 to 64 (u128 keys, count_wide.cu) over the
+// partitions `want` (null: all) of a device-resident store, in groups of
+// partitions whose sub-bucket entries fit a fifth of free memory.  Per group:
+// the split (count_bucket.cu, key-independent), a 4096-slot count per
+// sub-bucket of about 4k instances, a second pass with 8192 slots over the
+// sub-buckets that overflowed, and the radix sort for the rest (heavy
+// sub-buckets and those that overflowed twice), whose k-mer instances are
+// extracted into the key buffer.  A spilled store is counted by the sort
+// counter.
+int count_hash_wide(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<char> *want) {
+    for (auto *c : ctx->store)
+        if (c->on_host) return count_sort<u128>(ctx, cmin, cmax, want);
+    const uint32_t P = (uint32_t)ctx->opt.partitions;
+    const int k = ctx->opt.k;
+    std::vector<uint64_t> np(P, 0), nsp(P, 0);
+    for (auto *c : ctx->store)
+        for (uint32_t p = 0; p < P; p++) {
+            np[p] += c->kmers[p];
+            nsp[p] += c->skm_off[p + 1] - c->skm_off[p];
+        }
+    // sub-buckets of about 4k instances (2k to 4k): the table holds 4096 keys
+    constexpr uint64_t SUB_BUCKET_KMERS_WIDE = 4096;
+    constexpr uint64_t HEAVY_WIDE = 32768;  // larger sub-buckets go to the radix sort at once
+    constexpr int TS1 = 4096, TS2 = 8192;
+    std::vector<uint32_t> slog(2 * P);
+    uint64_t NB = 0;
+    for (uint32_t p = 0; p < P; p++) {
+        uint32_t sl = 0;
+        while (sl < (uint32_t)BS_LOG_LIMIT && np[p] > (SUB_BUCKET_KMERS_WIDE << sl)) sl++;
+        slog[p] = sl;
+        slog[P + p] = (uint32_t)NB;
+        NB += 1ull << sl;
+    }
+    auto bbase = [&](uint32_t p) -> uint64_t { return p < P ? slog[P + p] : NB; };
+    ctx->times[4] = (double)NB;
+    ctx->times[5] = 0;
+    ctx->times[6] = 0;
+    ctx->times[8] = 0;
+    size_t free0 = 0, tot0 = 0;
+    CK(cudaMemGetInfo(&free0, &tot0));
+    ctx->free_hint = free0;
+    CK(ctx->bk_skms.ensure(NB * 4));
+    CK(ctx->bk_kmers.ensure(NB * 8));
+    CK(ctx->bk_off.ensure((NB + 1) * 8));
+    CK(ctx->bk_cur.ensure(NB * 8));
+    CK(ctx->bk_failed.ensure((NB + 1) * 4));
+    CK(ctx->bk_part.ensure(2ull * P * 4));
+    CK(cudaMemcpyAsync(ctx->bk_part.p, slog.data(), 2ull * P * 4, cudaMemcpyHostToDevice, ctx->s));
+    CK(ctx->scal.ensure(64));
+    CK(ctx->h_scal.ensure(64));
+    CK(ctx->h_ids.ensure((NB + 1) * 4));
+    CK(ctx->h_off.ensure((NB + 1) * 8));
+    CK(ctx->h_km.ensure(NB * 8));
+    auto *sc = ctx->scal.as<unsigned long long>();  // [0] output cursor, [1] distinct, [2] errors
+    CK(cudaFuncSetAttribute(bucket_count_wide_kernel<TS1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS1 * 24));
+    CK(cudaFuncSetAttribute(bucket_count_wide_kernel<TS2>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS2 * 24));
+    CK(cudaFuncSetAttribute(bucket_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BS_SMEM));
+    const uint64_t budget = std::max<uint64_t>(1ull << 26, (uint64_t)(free0 * 0.2));  // entry bytes per group
+    uint64_t distinct_dev = 0;
+    float acc_ms = 0;
+    uint64_t groups = 0;
+    for (uint32_t p0 = 0; p0 < P;) {
+        if (want && !(*want)[p0]) {
+            p0++;
+            continue;
+        }
+        uint32_t p1 = p0;
+        uint64_t gs = 0, gN = 0;
+        while (p1 < P && (!want || (*want)[p1]) && (p1 == p0 || 16 * (gs + nsp[p1]) <= budget)) {
+            gs += nsp[p1];
+            gN += np[p1];
+            p1++;
+        }
+        if (!gs) {
+            p0 = p1;
+            continue;
+        }
+        groups++;
+        const uint64_t out_used = ctx->n_out;
+        // room for every k-mer of the group that can pass the threshold
+        RET(ensure_out(ctx, out_used + gN / std::max<uint32_t>(cmin, 1) + 1024, out_used));
+        for (int attempt = 0;; attempt++) {
+            CK(ctx->bk_entries.ensure(gs * sizeof(BEntry)));
+            CK(cudaMemsetAsync(ctx->bk_skms.p, 0, NB * 4, ctx->s));
+            CK(cudaMemsetAsync(ctx->bk_kmers.p, 0, NB * 8, ctx->s));
+            // the device cursor starts at this group's output; the stream is idle here
+            // (the previous group ended with a wait), so the pinned words are free
+            const unsigned long long start[3] = {out_used, 0, 0};
+            std::memcpy(ctx->h_scal.p, start, 24);
+            CK(cudaMemcpyAsync(sc, ctx->h_scal.p, 24, cudaMemcpyHostToDevice, ctx->s));
+            CK(cudaEventRecord(ctx->e2, ctx->s));
+            // the split of every chunk's part of the group (device chunks: their own pointers)
+            std::vector<BSChunk> bsc;
+            uint32_t ncta = 0;
+            for (StoreChunk *c : ctx->store) {
+                const uint64_t i0 = c->skm_off[p0], i1 = c->skm_off[p1];
+                if (i1 == i0) continue;
+                bsc.push_back({c->idx, c->keys, c->bytes, i0, i1, c->d_skm_off.as<unsigned long long>(),
+                               c->d_byte_off.as<unsigned long long>(), ncta});
+                ncta += (uint32_t)((i1 - i0 + BS_PER_CTA - 1) / BS_PER_CTA);
+            }
+            CK(ctx->h_desc.ensure(bsc.size() * sizeof(BSChunk)));
+            CK(ctx->bk_desc.ensure(bsc.size() * sizeof(BSChunk)));
+            std::memcpy(ctx->h_desc.p, bsc.data(), bsc.size() * sizeof(BSChunk));
+            CK(cudaMemcpyAsync(ctx->bk_desc.p, ctx->h_desc.p, bsc.size() * sizeof(BSChunk), cudaMemcpyHostToDevice,
+                               ctx->s));
+            for (int pass = 0; pass < 2; pass++) {
+                if (pass == 1) {
+                    RET(scan_u32(ctx, ctx->bk_skms.as<uint32_t>(), NB, ctx->bk_off.as<uint64_t>(),
+                                 ctx->bk_off.as<unsigned long long>() + NB));
+                    CK(cudaMemcpyAsync(ctx->bk_cur.p, ctx->bk_off.p, NB * 8, cudaMemcpyDeviceToDevice, ctx->s));
+                }
+                BSplitParams sp;
+                sp.chunks = ctx->bk_desc.as<BSChunk>();
+                sp.nchunks = (uint32_t)bsc.size();
+                sp.P = P;
+                sp.part_slog = ctx->bk_part.as<uint32_t>();
+                sp.part_bbase = ctx->bk_part.as<uint32_t>() + P;
+                sp.bucket_skms = ctx->bk_skms.as<uint32_t>();
+                sp.bucket_kmers = ctx->bk_kmers.as<unsigned long long>();
+                sp.bucket_cursor = ctx->bk_cur.as<unsigned long long>();
+                sp.entries = ctx->bk_entries.as<BEntry>();
+                sp.pass = pass;
+                KScope ks(ctx, GKC_K_BUCKET_SPLIT, pass ? 28.0 * gs : 12.0 * gs);
+                bucket_split_kernel<<<ncta, BS_THREADS, BS_SMEM, ctx->s>>>(sp);
+                LAUNCHED();
+            }
+            BCountParams bp;
+            bp.entries = ctx->bk_entries.as<BEntry>();
+            bp.bucket_off = ctx->bk_off.as<uint64_t>();
+            bp.bucket_kmers = ctx->bk_kmers.as<unsigned long long>();
+            bp.heavy_kmers = HEAVY_WIDE;
+            bp.b0 = (uint32_t)bbase(p0);
+            bp.ids = nullptr;
+            bp.k = k;
+            bp.cmin = cmin;
+            bp.cmax = cmax;
+            bp.out_k = ctx->out_k.as<uint64_t>();
+            bp.out_c = ctx->out_c.as<uint32_t>();
+            bp.out_cursor = sc;
+            bp.out_cap = ctx->out_cap;
+            bp.distinct = sc + 1;
+            bp.failed = ctx->bk_failed.as<uint32_t>();
+            bp.err = reinterpret_cast<uint32_t *>(sc + 2);
+            CK(cudaMemsetAsync(ctx->bk_failed.p, 0, 4, ctx->s));
+            {
+                uint64_t gbytes = 0;
+                for (StoreChunk *c : ctx->store) gbytes += c->byte_off[p1] - c->byte_off[p0];
+                KScope ks(ctx, GKC_K_HASH_INSERT, (double)gbytes + 16.0 * gs);
+                bucket_count_wide_kernel<TS1><<<(unsigned)(bbase(p1) - bbase(p0)), BC_THREADS, TS1 * 24, ctx->s>>>(bp);
+                LAUNCHED();
+            }
+            CK(cudaMemcpyAsync(ctx->h_ids.p, ctx->bk_failed.p, (NB + 1) * 4, cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaMemcpyAsync(ctx->h_off.p, ctx->bk_off.p, (NB + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaMemcpyAsync(ctx->h_km.p, ctx->bk_kmers.p, NB * 8, cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaStreamSynchronize(ctx->s));
+            const uint32_t nfail = std::min<uint32_t>(ctx->h_ids.as<uint32_t>()[0], (uint32_t)NB);
+            const uint64_t *hkm = ctx->h_km.as<uint64_t>(), *hoff = ctx->h_off.as<uint64_t>();
+            std::vector<uint32_t> rest, over;
+            for (uint32_t i = 0; i < nfail; i++) {
+                const uint32_t b = ctx->h_ids.as<uint32_t>()[1 + i];
+                (hkm[b] > HEAVY_WIDE ? rest : over).push_back(b);
+            }
+            if (!over.empty()) {  // second pass: 8192 slots, one CTA per SM
+                const uint32_t no = (uint32_t)over.size();
+                CK(ctx->h_ids2.ensure((no + 1) * 4ull));
+                CK(ctx->bk_ids2.ensure(no * 4ull));
+                CK(ctx->bk_failed2.ensure((no + 1) * 4ull));
+                std::memcpy(ctx->h_ids2.p, over.data(), no * 4ull);
+                CK(cudaMemcpyAsync(ctx->bk_ids2.p, ctx->h_ids2.p, no * 4ull, cudaMemcpyHostToDevice, ctx->s));
+                CK(cudaMemsetAsync(ctx->bk_failed2.p, 0, 4, ctx->s));
+                bp.ids = ctx->bk_ids2.as<uint32_t>();
+                bp.failed = ctx->bk_failed2.as<uint32_t>();
+                {
+                    uint64_t ob = 0;
+                    for (uint32_t b : over) ob += 16 * (hoff[b + 1] - hoff[b]);
+                    KScope ks(ctx, GKC_K_HASH_RECORDS, (double)ob);
+                    bucket_count_wide_kernel<TS2><<<no, BC_THREADS, TS2 * 24, ctx->s>>>(bp);
+                    LAUNCHED();
+                }
+                CK(cudaMemcpyAsync(ctx->h_ids2.p, ctx->bk_failed2.p, (no + 1) * 4ull, cudaMemcpyDeviceToHost, ctx->s));
+                CK(cudaStreamSynchronize(ctx->s));
+                const uint32_t nf2 = std::min<uint32_t>(ctx->h_ids2.as<uint32_t>()[0], no);
+                ctx->times[8] += (double)(no - nf2);
+                rest.insert(rest.end(), ctx->h_ids2.as<uint32_t>() + 1, ctx->h_ids2.as<uint32_t>() + 1 + nf2);
+            }
+            unsigned long long hg[3];
+            CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
+            CK(cudaStreamSynchronize(ctx->s));
+            std::memcpy(hg, ctx->h_scal.p, 24);
+            if ((uint32_t)hg[2] & ERR_OUTPUT_FULL) {  // count the group again with room for all of it
+                if (attempt >= 2) return ctx->fail(GKC_EINTERNAL, "output capacity exceeded");
+                RET(ensure_out(ctx, hg[0] + hg[0] / 16 + 1024, out_used));
+                continue;
+            }
+            ctx->n_out = hg[0];
+            distinct_dev += hg[1];
+            float ms = 0;
+            CK(cudaEventRecord(ctx->e3, ctx->s));
+            CK(cudaEventSynchronize(ctx->e3));
+            CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
+            acc_ms += ms;
+            // the rest by the radix sort: their instances extracted, sorted,
+            // run-length reduced and thresholded after this group's output
+            if (!rest.empty()) {
+                ctx->times[5] += (double)rest.size();
+                std::vector<unsigned long long> koff(rest.size());
+                uint64_t n = 0;
+                for (size_t i = 0; i < rest.size(); i++) {
+                    koff[i] = n;
+                    n += hkm[rest[i]];
+                }
+                const uint32_t nr = (uint32_t)rest.size();
+                CK(ctx->keysA.ensure(n * sizeof(u128)));
+                CK(ctx->keysB.ensure(n * sizeof(u128)));
+                CK(ctx->bk_ids2.ensure(nr * 4ull));
+                CK(ctx->h_ids2.ensure(nr * 4ull + nr * 8ull));
+                CK(ctx->r_off.ensure(nr * 8ull));
+                std::memcpy(ctx->h_ids2.p, rest.data(), nr * 4ull);
+                std::memcpy(ctx->h_ids2.as<uint8_t>() + nr * 4ull, koff.data(), nr * 8ull);
+                CK(cudaMemcpyAsync(ctx->bk_ids2.p, ctx->h_ids2.p, nr * 4ull, cudaMemcpyHostToDevice, ctx->s));
+                CK(cudaMemcpyAsync(ctx->r_off.p, ctx->h_ids2.as<uint8_t>() + nr * 4ull, nr * 8ull,
+                                   cudaMemcpyHostToDevice, ctx->s));
+                BExtractParams xp;
+                xp.entries = ctx->bk_entries.as<BEntry>();
+                xp.bucket_off = ctx->bk_off.as<uint64_t>();
+                xp.ids = ctx->bk_ids2.as<uint32_t>();
+                xp.key_off = ctx->r_off.as<unsigned long long>();
+                xp.k = k;
+                xp.keys = ctx->keysA.as<u128>();
+                {
+                    KScope ks(ctx, GKC_K_SORT_EXTRACT, 16.0 * n);
+                    bucket_extract_wide_kernel<<<nr, BC_THREADS, 0, ctx->s>>>(xp);
+                    LAUNCHED();
+                }
+                float sort_ms = 0;  // appends at ctx->n_out, adds its distinct k-mers to ctx->n_distinct
+                RET(sort_and_reduce<u128>(ctx, std::vector<uint64_t>{n}, n, 2 * k, cmin, cmax, &sort_ms));
+                acc_ms += sort_ms;
+            }
+            break;
+        }
+        p0 = p1;
+    }
+    ctx->n_distinct += distinct_dev;
+    ctx->times[3] = acc_ms;
+    ctx->times[7] = (double)groups;
+    return GKC_OK;
+}
+
+
 // Makes the rank table `ranks` (device, 4^p) the context's order: phase 1
 // reads its canonical form.
 int install_order(gkc_ctx *ctx, const uint32_t *ranks) {
@@ -2996,7 +3247,8 @@ int count_store(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<ch
     CK(cudaEventRecord(t0, ctx->s));
     // k > 32: u128 keys, sort counter only
     ctx->res_kw = ctx->opt.k > 32 ? 2 : 1;
-    int rc = ctx->opt.k > 32                         ? count_sort<u128>(ctx, cmin, cmax, want)
+    int rc = ctx->opt.k > 32 ? (ctx->opt.counter == GKC_COUNTER_HASH ? count_hash_wide(ctx, cmin, cmax, want)
+                                                                     : count_sort<u128>(ctx, cmin, cmax, want))
              : ctx->opt.counter == GKC_COUNTER_HASH ? count_hash(ctx, cmin, cmax, want)
                                                     : count_sort<uint64_t>(ctx, cmin, cmax, want);
     cudaEventRecord(t1, ctx->s);

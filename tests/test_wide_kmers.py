@@ -68,8 +68,8 @@ def test_wide_long_and_low_complexity_reads(oracle, k, p):
 
 def test_wide_device_input_batches_spill_and_learned_order(oracle):
     """Device input cut into many batches, a spilled store, and a learned
-    order all give the default order's table (the hash setting counts with
-    the sort counter for k > 32)."""
+    order all give the default order's table; so does the 128-bit hash
+    counter, and the sort counter that a spilled store falls back to."""
     import torch
     k, p, P = 51, 11, 64
     reads, offs = random_reads(12, 40_000, 2500, (40, 600), 0.005)
@@ -78,6 +78,7 @@ def test_wide_device_input_batches_spill_and_learned_order(oracle):
     lut = np.random.default_rng(13).permutation(4 ** p).astype(np.uint32)
     pbl, psl, pkl, _, _ = oracle.skmgen(reads, offs, k, p, P, lut)
     runs = [dict(batch_bases=20_000), dict(batch_bases=50_000, spill_host=True), dict(kind="hash"),
+            dict(kind="hash", batch_bases=50_000, spill_host=True),
             dict(order=True), dict(group_keys=5000), dict(sort_seg_max=1000), dict(radix_bits=8)]
     for kw in runs:
         order = kw.pop("order", False)
