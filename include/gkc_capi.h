@@ -63,8 +63,8 @@ typedef struct gkc_ctx gkc_ctx;
 typedef struct gkc_options {
     int k;                  /* k-mer length, p <= k <= 64 (reference -k, utilities.hpp:187); k   */
                             /* > 32 is the reference's 128-bit LONGERKMER build (types.h:34-35,  */
-                            /* utilities.hpp:280-281): k-mers take two words and are counted by  */
-                            /* the sort counter whatever `counter` says                          */
+                            /* utilities.hpp:280-281): k-mers take two words; either counter     */
+                            /* counts them (hash: 16-byte keys in the sub-bucket tables)         */
     int p;                  /* minimizer length, 3 <= p <= 16 (reference -p, utilities.hpp:188)   */
     int partitions;         /* superkmer partitions, 1..4096 (reference -skm, utilities.hpp:189)  */
     int counter;            /* GKC_COUNTER_SORT or GKC_COUNTER_HASH                               */

@@ -167,8 +167,9 @@ class KmerCounter:
     k [-k], p [-p], partitions [-skm], counter 'hash' or 'sort'.
 
     k <= 32 gives uint64 k-mers.  32 < k <= 64 (the reference's 128-bit
-    LONGERKMER build) counts with the sort counter and gives k-mers as (n, 2)
-    uint64 arrays of (low word, high word), ordered as 128-bit values."""
+    LONGERKMER build) gives k-mers as (n, 2) uint64 arrays of (low word, high
+    word); the sort counter orders them as 128-bit values within a partition,
+    the hash counter leaves them unordered, as it does for k <= 32."""
 
     def __init__(self, k: int = 31, p: int = 11, partitions: int = 512, counter: str = "hash",
                  device: int = 0, radix_bits: int = 0, table_slots: float = 0.35,

@@ -14,8 +14,9 @@
 //   count    one CTA per sub-bucket: warps take groups of 32 superkmers from
 //            a shared-memory counter (groups differ in k-mers, so a fixed
 //            round robin left warps idle at the barrier), decode them 32 quads
-//            of consecutive k-mers at a time (warp_kmer_runs below), merge equal
-//            neighbouring k-mers into runs, and add the runs to a shared-memory table with
+//            of up to four consecutive k-mers at a time (warp_kmer_runs
+//            below), merge equal neighbouring k-mers into runs, and add the
+//            runs to a shared-memory table with
 //            shared-memory atomics; then the k-mers whose count lies in
 //            [cmin, cmax] are written with one global atomic per CTA.  A
 //            sub-bucket whose distinct k-mers outgrow the table is abandoned
@@ -61,15 +62,60 @@ __device__ __forceinline__ uint64_t pack6x8(uint64_t le) {
 
 constexpr int KQ = 4;  // k-mers per lane per step (a quad)
 
+// Calls f(key, run) for the canonical k-mers of quad qi of a superkmer (first
+// byte p, pad bases of padding, len k-mers), equal consecutive k-mers merged
+// into runs.  A quad is up to KQ consecutive k-mers.  Its first k-mer is
+// decoded from a 48-base window (16 bytes from three aligned 8-byte loads;
+// store buffers carry 32 bytes of padding); the others roll in one base each,
+// forward and reverse complement.  f must not use warp collectives.
+template <class F>
+__device__ __forceinline__ void quad_runs(const uint8_t *p, uint32_t pad, uint32_t len, uint32_t qi, int k,
+                                          uint64_t mask, F &&f) {
+    const uint32_t j0 = KQ * qi;
+    const uint32_t nk = len - j0 < (uint32_t)KQ ? len - j0 : (uint32_t)KQ;
+    const uint32_t u = pad + j0, bi = u / 3, s = u - 3 * bi;
+    const uintptr_t addr = (uintptr_t)p + bi;
+    const uint64_t *w = reinterpret_cast<const uint64_t *>(addr & ~(uintptr_t)7);
+    const uint32_t sh = 8 * (uint32_t)(addr & 7);
+    const uint64_t w0 = w[0], w1 = w[1], w2 = w[2];
+    const uint64_t lo = sh ? (w0 >> sh) | (w1 << (64 - sh)) : w0;  // bytes 0..7
+    const uint64_t hi = sh ? (w1 >> sh) | (w2 << (64 - sh)) : w1;  // bytes 8..15
+    // 48 bases, slot 0 first: A holds slots 0-23 (48 bits), B slots 24-47.
+    // The 96-bit value A:B shifted right by d is, in its low 64 bits (all
+    // that the masks below keep), (A << (48 - d)) | (B >> d) for d <= 48
+    // and A >> (d - 48) beyond: 64-bit shifts, no 128-bit one.
+    const uint64_t A = pack6x8(lo), B = pack6x8(hi);
+    auto shr96 = [&](uint32_t dd) -> uint64_t { return dd <= 48 ? (A << (48 - dd)) | (B >> dd) : A >> (dd - 48); };
+    const uint32_t d = 96 - 2 * (s + (uint32_t)k);  // 30..34 for k = 31
+    uint64_t x = shr96(d) & mask;
+    // the quad's KQ-1 entering bases (slots s+k .. s+k+KQ-2), the last in bits 1-0
+    const uint32_t nxt = (uint32_t)shr96(d - 2 * (KQ - 1));
+    uint64_t r = rc64(x, k);
+    uint64_t last = x < r ? x : r;
+    uint32_t run = 1;
+#pragma unroll
+    for (uint32_t t = 1; t < (uint32_t)KQ; t++) {
+        if (t >= nk) break;
+        const uint32_t bt = (nxt >> (2 * (KQ - 1 - t))) & 3u;  // the entering base
+        x = ((x << 2) | bt) & mask;
+        r = (r >> 2) | ((uint64_t)(3u - bt) << (2 * k - 2));
+        const uint64_t key = x < r ? x : r;
+        if (key == last) {
+            run++;
+        } else {
+            f(last, run);
+            last = key;
+            run = 1;
+        }
+    }
+    f(last, run);
+}
+
 // Calls f(key, run) for every canonical k-mer of the entries ent[b .. b+32)
 // of a warp (entry b + lane exists when b + lane < end), equal consecutive
-// k-mers merged into runs.  Work is split into quads, up to KQ consecutive
-// k-mers of one superkmer; a warp step gives each lane one quad (a shuffle
-// prefix sum and owner search over the 32 entries).  The first k-mer of a
-// quad is decoded from a 48-base window (16 bytes from three aligned 8-byte
-// loads; store buffers carry 32 bytes of padding); the others roll in one
-// base each, forward and reverse complement.  Must be called by the whole
-// warp; f is called by single lanes and must not use warp collectives.
+// k-mers merged into runs (quad_runs).  A warp step gives each lane one quad
+// (a shuffle prefix sum and owner search over the 32 entries).  Must be
+// called by the whole warp; f is called by single lanes.
 template <class F>
 __device__ __forceinline__ void warp_kmer_runs(const BEntry *ent, uint64_t b, uint64_t end, int k, uint64_t mask,
                                                F &&f) {
@@ -102,44 +148,7 @@ __device__ __forceinline__ void warp_kmer_runs(const BEntry *ent, uint64_t b, ui
         const uint64_t po = __shfl_sync(FULL, pv, own);
         const uint32_t opad = __shfl_sync(FULL, pad, own), olen = __shfl_sync(FULL, en.len, own);
         if (g >= total) continue;
-        const uint32_t j0 = KQ * qi;
-        const uint32_t nk = olen - j0 < (uint32_t)KQ ? olen - j0 : (uint32_t)KQ;
-        const uint32_t u = opad + j0, bi = u / 3, s = u - 3 * bi;
-        const uintptr_t addr = (uintptr_t)po + bi;
-        const uint64_t *w = reinterpret_cast<const uint64_t *>(addr & ~(uintptr_t)7);
-        const uint32_t sh = 8 * (uint32_t)(addr & 7);
-        const uint64_t w0 = w[0], w1 = w[1], w2 = w[2];
-        const uint64_t lo = sh ? (w0 >> sh) | (w1 << (64 - sh)) : w0;  // bytes 0..7
-        const uint64_t hi = sh ? (w1 >> sh) | (w2 << (64 - sh)) : w1;  // bytes 8..15
-        // 48 bases, slot 0 first: A holds slots 0-23 (48 bits), B slots 24-47.
-        // The 96-bit value A:B shifted right by d is, in its low 64 bits (all
-        // that the masks below keep), (A << (48 - d)) | (B >> d) for d <= 48
-        // and A >> (d - 48) beyond: 64-bit shifts, no 128-bit one.
-        const uint64_t A = pack6x8(lo), B = pack6x8(hi);
-        auto shr96 = [&](uint32_t dd) -> uint64_t { return dd <= 48 ? (A << (48 - dd)) | (B >> dd) : A >> (dd - 48); };
-        const uint32_t d = 96 - 2 * (s + (uint32_t)k);  // 30..34 for k = 31
-        uint64_t x = shr96(d) & mask;
-        // the quad's KQ-1 entering bases (slots s+k .. s+k+KQ-2), the last in bits 1-0
-        const uint32_t nxt = (uint32_t)shr96(d - 2 * (KQ - 1));
-        uint64_t r = rc64(x, k);
-        uint64_t last = x < r ? x : r;
-        uint32_t run = 1;
-#pragma unroll
-        for (uint32_t t = 1; t < (uint32_t)KQ; t++) {
-            if (t >= nk) break;
-            const uint32_t bt = (nxt >> (2 * (KQ - 1 - t))) & 3u;  // the entering base
-            x = ((x << 2) | bt) & mask;
-            r = (r >> 2) | ((uint64_t)(3u - bt) << (2 * k - 2));
-            const uint64_t key = x < r ? x : r;
-            if (key == last) {
-                run++;
-            } else {
-                f(last, run);
-                last = key;
-                run = 1;
-            }
-        }
-        f(last, run);
+        quad_runs(reinterpret_cast<const uint8_t *>(po), opad, olen, qi, k, mask, f);
     }
 }
 
@@ -301,7 +310,96 @@ struct BCountParams {
     unsigned long long *distinct;
     uint32_t *failed;             // [1 + nb]: count, then the abandoned sub-buckets
     uint32_t *err;
+    // 128-bit counter only: when not null, CTA i counts piece (piece[2i] of
+    // piece[2i+1]) of sub-bucket ids[i] (wide_piece) and lists i, not the
+    // sub-bucket, when it fails
+    const uint32_t *piece = nullptr;
 };
+
+// Quads of a sub-bucket spread evenly over a CTA (the 128-bit counter,
+// count_wide.cu).  The entries are taken in chunks of QS_CH (one per thread):
+// a block scan of their quad counts gives each entry its first quad, and
+// warps claim the chunk's 32-quad steps one at a time from a shared counter.
+// A lane finds its quad's entry in a window of 32 entries from the owner of
+// the step's first quad (two ballots over the chunk; every entry has at least
+// one quad, so the window covers the step).  At large k a sub-bucket of about
+// 4k instances holds only about 150 superkmers, so groups of 32 entries per
+// warp (bucket_count_kernel) left most warps at the barrier: 96.8 -> 40.0 ms
+// for the 128-bit counter on 3 Gbp at k = 63.  With the short superkmers of
+// k <= 32 the groups balance well enough, and their cheaper steps win
+// (29.8 vs 32.7 ms on 3 Gbp at k = 31).
+constexpr int QS_CH = BC_THREADS;
+constexpr int QS_STRIDE = QS_CH / 32;
+static_assert(QS_CH == 32 * QS_STRIDE && QS_STRIDE <= 32, "chunk search in two ballots");
+constexpr uint32_t QS_LEN_MASK = 0x3FFFFFFFu;  // ql: k-mers in bits 0-29, padding bases in 30-31
+
+struct QStage {
+    uint32_t qx[QS_CH + 32];  // first quad of each entry of the chunk; UINT32_MAX past its end
+    const uint8_t *qp[QS_CH];  // first byte of each entry
+    uint32_t ql[QS_CH];       // k-mers | padding << 30
+    uint32_t next;            // the next step to claim
+};
+
+// Calls q(p, pad, len, qi) for every quad qi of every entry of ent[e0, e1)
+// (entries of fewer than 2^30 k-mers).  Must be called by the whole CTA of
+// NT == QS_CH threads; it starts and ends with a barrier's worth of
+// synchronisation (the block scan and a final __syncthreads), so shared state
+// written before it is visible to q and everything q wrote is visible after
+// it.  A warp stops taking steps once *over is set.
+template <int NT, class QF>
+__device__ __forceinline__ void cta_quads(const BEntry *ent, uint64_t e0, uint64_t e1, QStage &qs, uint32_t *ws,
+                                          volatile uint32_t *over, QF &&q) {
+    static_assert(NT == QS_CH, "one entry per thread per chunk");
+    constexpr int NW = NT / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (uint64_t c0 = e0; c0 < e1; c0 += QS_CH) {
+        const uint32_t n = (uint32_t)(e1 - c0 < (uint64_t)QS_CH ? e1 - c0 : (uint64_t)QS_CH);
+        uint32_t nq = 0;
+        if (threadIdx.x < n) {
+            const BEntry en = ent[c0 + threadIdx.x];
+            const uint32_t pad = 3u - (en.ptr[0] >> 6);
+            nq = en.len ? (en.len + KQ - 1) / KQ : 1u;  // an empty entry keeps one (skipped) quad
+            qs.qp[threadIdx.x] = en.ptr;
+            qs.ql[threadIdx.x] = (en.len & QS_LEN_MASK) | (pad << 30);
+        }
+        uint32_t nquads;
+        const uint32_t ex = block_exclusive_scan<NT>(nq, &nquads, ws);
+        qs.qx[threadIdx.x] = threadIdx.x < n ? ex : 0xFFFFFFFFu;
+        if (threadIdx.x < 32) qs.qx[QS_CH + threadIdx.x] = 0xFFFFFFFFu;
+        if (threadIdx.x == 0) qs.next = NW;
+        __syncthreads();
+        const uint32_t S = (nquads + 31) / 32;
+        // steps are claimed one at a time from a shared counter (warp w starts at step w)
+        uint32_t s = warp;
+        while (s < S) {
+            if (__any_sync(FULL, *over != 0)) break;  // a warp vote: the warp leaves together
+            // c: the owner of quad 32 s, the last entry whose first quad is <= 32 s
+            // (qx[0] = 0, so both ballots have lane 0 set)
+            const uint32_t t0 = 32 * s;
+            uint32_t m = __ballot_sync(FULL, qs.qx[lane * QS_STRIDE] <= t0);
+            uint32_t c = (31 - __clz(m)) * QS_STRIDE;
+            m = __ballot_sync(FULL, lane < QS_STRIDE && qs.qx[c + lane] <= t0);
+            c += 31 - __clz(m);
+            const uint32_t v = qs.qx[c + lane];  // c < n, so c + lane < QS_CH + 32
+            const uint32_t g = t0 + lane;
+            int own = 0;  // the last window entry whose first quad is <= g
+#pragma unroll
+            for (int st = 16; st; st >>= 1) {
+                const int cand = own + st;
+                if (__shfl_sync(FULL, v, cand) <= g) own = cand;
+            }
+            const uint32_t first = __shfl_sync(FULL, v, own);
+            uint32_t nx = 0;
+            if (lane == 0) nx = atomicAdd(&qs.next, 1u);
+            if (g < nquads) {
+                const uint32_t l = qs.ql[c + own];
+                if (l & QS_LEN_MASK) q(qs.qp[c + own], l >> 30, l & QS_LEN_MASK, g - first);
+            }
+            s = __shfl_sync(FULL, nx, 0);
+        }
+        __syncthreads();
+    }
+}
 
 // Shared-memory table insert (multiplicative hash on the top bits).  A probe
 // sequence longer than SM_MAX_PROBE (the table is nearly full) raises *over

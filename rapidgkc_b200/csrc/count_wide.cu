@@ -32,12 +32,60 @@ __device__ __forceinline__ u128 rc128(u128 v, int k) {
 
 __device__ __forceinline__ u128 kmask128(int k) { return k >= 64 ? ~(u128)0 : (((u128)1 << (2 * k)) - 1); }
 
+// quad_runs (count_bucket.cu) for 33 <= k <= 64: calls f(key, run) for the
+// canonical k-mers of quad qi of a superkmer (first byte p, pad bases of
+// padding, len k-mers), equal consecutive k-mers merged into runs.  The
+// quad's first k-mer is taken from a 72-base window: 24 bytes from four
+// aligned 8-byte loads (store buffers carry 32 bytes of padding) as three
+// 48-bit fields A (slots 0-23), B (24-47) and C (48-71).  f must not use
+// warp collectives.
+template <class F>
+__device__ __forceinline__ void quad_runs_wide(const uint8_t *p, uint32_t pad, uint32_t len, uint32_t qi, int k,
+                                               u128 mask, F &&f) {
+    const uint32_t j0 = KQ * qi;
+    const uint32_t nk = len - j0 < (uint32_t)KQ ? len - j0 : (uint32_t)KQ;
+    const uint32_t u = pad + j0, bi = u / 3, s = u - 3 * bi;
+    const uintptr_t addr = (uintptr_t)p + bi;
+    const uint64_t *w = reinterpret_cast<const uint64_t *>(addr & ~(uintptr_t)7);
+    const uint32_t sh = 8 * (uint32_t)(addr & 7);
+    const uint64_t w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
+    auto fs = [&](uint64_t x, uint64_t y) -> uint64_t { return sh ? (x >> sh) | (y << (64 - sh)) : x; };
+    const uint64_t A = pack6x8(fs(w0, w1)), B = pack6x8(fs(w1, w2)), C = pack6x8(fs(w2, w3));
+    // the 144-bit A:B:C shifted right by d, low 128 bits (6 <= d <= 78 here)
+    auto shr144 = [&](uint32_t d) -> u128 {
+        u128 r = (u128)A << (96 - d);
+        r |= d <= 48 ? ((u128)B << (48 - d)) : (u128)(B >> (d - 48));
+        if (d < 48) r |= (u128)(C >> d);
+        return r;
+    };
+    const uint32_t d = 144 - 2 * (s + (uint32_t)k);
+    u128 x = shr144(d) & mask;
+    // the quad's KQ-1 entering bases (slots s+k .. s+k+KQ-2), the last in bits 1-0
+    const uint32_t nxt = (uint32_t)shr144(d - 2 * (KQ - 1));
+    u128 r = rc128(x, k);
+    u128 last = x < r ? x : r;
+    uint32_t run = 1;
+#pragma unroll
+    for (uint32_t t = 1; t < (uint32_t)KQ; t++) {
+        if (t >= nk) break;
+        const uint32_t bt = (nxt >> (2 * (KQ - 1 - t))) & 3u;  // the entering base
+        x = ((x << 2) | bt) & mask;
+        r = (r >> 2) | ((u128)(3u - bt) << (2 * k - 2));
+        const u128 key = x < r ? x : r;
+        if (key == last) {
+            run++;
+        } else {
+            f(last, run);
+            last = key;
+            run = 1;
+        }
+    }
+    f(last, run);
+}
+
 // warp_kmer_runs (count_bucket.cu) for 33 <= k <= 64: calls f(key, run) for
-// every canonical k-mer of the entries ent[b .. b+32) of a warp, equal
-// consecutive k-mers merged into runs.  A quad's first k-mer is taken from a
-// 72-base window: 24 bytes from four aligned 8-byte loads (store buffers
-// carry 32 bytes of padding) as three 48-bit fields A (slots 0-23), B (24-47)
-// and C (48-71).  Must be called by the whole warp; f is called by single
+// every canonical k-mer of the entries ent[b .. b+32) of a warp, by
+// quad_runs_wide.  Must be called by the whole warp; f is called by single
 // lanes and must not use warp collectives.
 template <class F>
 __device__ __forceinline__ void warp_kmer_runs_wide(const BEntry *ent, uint64_t b, uint64_t end, int k, u128 mask,
@@ -71,45 +119,7 @@ __device__ __forceinline__ void warp_kmer_runs_wide(const BEntry *ent, uint64_t 
         const uint64_t po = __shfl_sync(FULL, pv, own);
         const uint32_t opad = __shfl_sync(FULL, pad, own), olen = __shfl_sync(FULL, en.len, own);
         if (g >= total) continue;
-        const uint32_t j0 = KQ * qi;
-        const uint32_t nk = olen - j0 < (uint32_t)KQ ? olen - j0 : (uint32_t)KQ;
-        const uint32_t u = opad + j0, bi = u / 3, s = u - 3 * bi;
-        const uintptr_t addr = (uintptr_t)po + bi;
-        const uint64_t *w = reinterpret_cast<const uint64_t *>(addr & ~(uintptr_t)7);
-        const uint32_t sh = 8 * (uint32_t)(addr & 7);
-        const uint64_t w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
-        auto fs = [&](uint64_t x, uint64_t y) -> uint64_t { return sh ? (x >> sh) | (y << (64 - sh)) : x; };
-        const uint64_t A = pack6x8(fs(w0, w1)), B = pack6x8(fs(w1, w2)), C = pack6x8(fs(w2, w3));
-        // the 144-bit A:B:C shifted right by d, low 128 bits (6 <= d <= 78 here)
-        auto shr144 = [&](uint32_t d) -> u128 {
-            u128 r = (u128)A << (96 - d);
-            r |= d <= 48 ? ((u128)B << (48 - d)) : (u128)(B >> (d - 48));
-            if (d < 48) r |= (u128)(C >> d);
-            return r;
-        };
-        const uint32_t d = 144 - 2 * (s + (uint32_t)k);
-        u128 x = shr144(d) & mask;
-        // the quad's KQ-1 entering bases (slots s+k .. s+k+KQ-2), the last in bits 1-0
-        const uint32_t nxt = (uint32_t)shr144(d - 2 * (KQ - 1));
-        u128 r = rc128(x, k);
-        u128 last = x < r ? x : r;
-        uint32_t run = 1;
-#pragma unroll
-        for (uint32_t t = 1; t < (uint32_t)KQ; t++) {
-            if (t >= nk) break;
-            const uint32_t bt = (nxt >> (2 * (KQ - 1 - t))) & 3u;  // the entering base
-            x = ((x << 2) | bt) & mask;
-            r = (r >> 2) | ((u128)(3u - bt) << (2 * k - 2));
-            const u128 key = x < r ? x : r;
-            if (key == last) {
-                run++;
-            } else {
-                f(last, run);
-                last = key;
-                run = 1;
-            }
-        }
-        f(last, run);
+        quad_runs_wide(reinterpret_cast<const uint8_t *>(po), opad, olen, qi, k, mask, f);
     }
 }
 
@@ -135,6 +145,18 @@ __device__ __forceinline__ WideTable wide_table(unsigned long long *smem) {
 }
 
 constexpr uint32_t WIDE_MAX_WAIT = 1u << 20;  // polls of a slot being written before giving up
+
+// The piece of n (n >= 1) that a key belongs to when a sub-bucket is counted
+// in n pieces by key hash: [0, n), from the top 32 bits of a mix of the key
+// that is independent of the table's slot hash.  Piece r of n is exactly
+// pieces 2r and 2r + 1 of 2n, so a piece that overflows splits in two.
+__device__ __forceinline__ uint32_t wide_piece(u128 key, uint32_t n) {
+    uint64_t x = (uint64_t)key ^ ((uint64_t)(key >> 64) * 0xC2B2AE3D27D4EB4Full);
+    x ^= x >> 33;
+    x *= 0xFF51AFD7ED558CCDull;
+    x ^= x >> 29;
+    return (uint32_t)(((x >> 32) * (uint64_t)n) >> 32);
+}
 
 template <int TS>
 __device__ __forceinline__ void wide_add(const WideTable &t, volatile uint32_t *over, u128 key, uint32_t c) {
@@ -184,14 +206,16 @@ bucket_count_wide_kernel(BCountParams a) {
     __shared__ uint32_t ws[BC_THREADS / 32];
     __shared__ volatile uint32_t over;
     __shared__ unsigned long long base_s;
-    __shared__ uint32_t next_grp;
+    __shared__ QStage qs;
     const uint32_t b = a.ids ? a.ids[blockIdx.x] : a.b0 + blockIdx.x;
+    const uint32_t pr = a.piece ? a.piece[2 * blockIdx.x] : 0u, pn = a.piece ? a.piece[2 * blockIdx.x + 1] : 1u;
+    const uint32_t fail_id = a.piece ? blockIdx.x : b;
     const uint64_t e0 = a.bucket_off[b], e1 = a.bucket_off[b + 1];
     if (e0 == e1) return;
     if (a.bucket_kmers[b] > a.heavy_kmers) {
         if (threadIdx.x == 0) {
             const uint32_t i = atomicAdd(a.failed, 1u);
-            a.failed[1 + i] = b;
+            a.failed[1 + i] = fail_id;
         }
         return;
     }
@@ -199,26 +223,19 @@ bucket_count_wide_kernel(BCountParams a) {
         t.st[x] = 0;
         t.cnt[x] = 0;
     }
-    if (threadIdx.x == 0) {
-        over = 0;
-        next_grp = BC_THREADS / 32;
-    }
+    if (threadIdx.x == 0) over = 0;
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const u128 mask = kmask128(a.k);
-    for (uint64_t bb = e0 + (uint64_t)warp * 32; bb < e1;) {
-        if (__any_sync(FULL, over != 0)) break;  // a warp vote: the warp leaves together
-        warp_kmer_runs_wide(a.entries, bb, e1, a.k, mask,
-                            [&](u128 key, uint32_t run) { wide_add<TS>(t, &over, key, run); });
-        uint32_t g = 0;
-        if (lane == 0) g = atomicAdd(&next_grp, 1u);
-        bb = e0 + 32ull * __shfl_sync(FULL, g, 0);
-    }
-    __syncthreads();
+    cta_quads<BC_THREADS>(a.entries, e0, e1, qs, ws, &over, [&](const uint8_t *p, uint32_t pad, uint32_t len,
+                                                                uint32_t qi) {
+        quad_runs_wide(p, pad, len, qi, a.k, mask, [&](u128 key, uint32_t run) {
+            if (pn == 1u || wide_piece(key, pn) == pr) wide_add<TS>(t, &over, key, run);
+        });
+    });
     if (over) {
         if (threadIdx.x == 0) {
             const uint32_t i = atomicAdd(a.failed, 1u);
-            a.failed[1 + i] = b;
+            a.failed[1 + i] = fail_id;
         }
         return;
     }
@@ -258,32 +275,57 @@ bucket_count_wide_kernel(BCountParams a) {
     }
 }
 
-// The k-mer instances of listed sub-buckets (CTA i: ids[i]) written to keys
-// from key_off[i] on, one key per instance (runs expanded), in any order:
-// the radix sort that counts them does not care.
+// The k-mer instances of listed pieces of sub-buckets written to keys, one
+// key per instance (runs expanded), in any order: the radix sort that counts
+// them does not care.  Work item i covers the entries [range[2i],
+// range[2i+1]) of one sub-bucket and keeps the keys of piece piece[2i] of
+// piece[2i+1] (wide_piece); a large sub-bucket is cut into many items, so
+// that one low-complexity run does not hold a single CTA.  Its keys go to
+// keys from key_off[i] on; with keys null, the item's instances are only
+// counted, into counts[i].
 struct BExtractParams {
     const BEntry *entries;
-    const uint64_t *bucket_off;
-    const uint32_t *ids;
+    const unsigned long long *range;
+    const uint32_t *piece;
     const unsigned long long *key_off;
     int k;
     u128 *keys;
+    unsigned long long *counts;
 };
 
 __global__ void __launch_bounds__(BC_THREADS) bucket_extract_wide_kernel(BExtractParams a) {
+    __shared__ QStage qs;
+    __shared__ uint32_t ws[BC_THREADS / 32];
+    __shared__ volatile uint32_t never;  // cta_quads' stop flag: extraction does not stop
     __shared__ unsigned long long cur;
-    const uint32_t b = a.ids[blockIdx.x];
-    const uint64_t e0 = a.bucket_off[b], e1 = a.bucket_off[b + 1];
-    if (threadIdx.x == 0) cur = 0;
+    const uint32_t pr = a.piece[2 * blockIdx.x], pn = a.piece[2 * blockIdx.x + 1];
+    const uint64_t e0 = a.range[2 * blockIdx.x], e1 = a.range[2 * blockIdx.x + 1];
+    if (threadIdx.x == 0) {
+        cur = 0;
+        never = 0;
+    }
     __syncthreads();
-    u128 *out = a.keys + a.key_off[blockIdx.x];
+    const bool write = a.keys != nullptr;
+    u128 *out = write ? a.keys + a.key_off[blockIdx.x] : nullptr;
     const u128 mask = kmask128(a.k);
-    const uint64_t step = (uint64_t)(BC_THREADS / 32) * 32;
-    for (uint64_t bb = e0 + (uint64_t)(threadIdx.x >> 5) * 32; bb < e1; bb += step)
-        warp_kmer_runs_wide(a.entries, bb, e1, a.k, mask, [&](u128 key, uint32_t run) {
+    uint32_t mine = 0;  // count mode: this thread's instances
+    cta_quads<BC_THREADS>(a.entries, e0, e1, qs, ws, &never, [&](const uint8_t *p, uint32_t pad, uint32_t len,
+                                                                  uint32_t qi) {
+        quad_runs_wide(p, pad, len, qi, a.k, mask, [&](u128 key, uint32_t run) {
+            if (pn != 1u && wide_piece(key, pn) != pr) return;
+            if (!write) {
+                mine += run;
+                return;
+            }
             const unsigned long long o = atomicAdd(&cur, (unsigned long long)run);
             for (uint32_t r = 0; r < run; r++) out[o + r] = key;
         });
+    });
+    if (!write) {
+        if (mine) atomicAdd(&cur, (unsigned long long)mine);
+        __syncthreads();
+        if (threadIdx.x == 0) a.counts[blockIdx.x] = cur;
+    }
 }
 
 }  // namespace gkc

@@ -347,6 +347,7 @@ struct gkc_ctx {
     DevBuf bk_skms, bk_kmers, bk_off, bk_cur, bk_entries, bk_failed, bk_arena, bk_part, bk_desc;
     DevBuf bk_arena2;  // second staging arena: a spilled store's next group is staged beside the current one
     DevBuf bk_ids2, bk_failed2;  // the second counting pass: its sub-buckets and those that failed again
+    DevBuf bk_piece;             // 128-bit counter: (piece, pieces) of each second-pass CTA
     PinBuf h_ids2;
     DevBuf r_work, r_count, r_off, r_cur, r_recs, r_failed;  // record sub-buckets
     DevBuf r_stage, r_winst, r_woff, r_wrec;                  // per-work-item record segments
@@ -391,7 +392,7 @@ struct gkc_ctx {
                         &mlp_w, &mlp_s, &mlp_scalar, &fx_text, &fx_tiles, &fx_state, &fx_kept,
                         &fx_reads, &fx_res, &fx_out, &fx_offs, &sk_tiles, &sk_state, &sk_tstarts, &sk_res,
                         &sk_starts, &sk_k32, &hpc_tiles, &hpc_tbase, &hpc_reads, &hpc_offs, &os_status, &os_hist,
-                        &os_segs, &os_ctr, &bk_ids2, &bk_failed2};
+                        &os_segs, &os_ctr, &bk_ids2, &bk_failed2, &bk_piece};
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &pk_host[0], &pk_host[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work,
                         &h_desc, &h_cur, &h_segs, &h_ids2};
@@ -2107,6 +2108,14 @@ int count_hash_wide(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vecto
     constexpr uint64_t SUB_BUCKET_KMERS_WIDE = 4096;
     constexpr uint64_t HEAVY_WIDE = 32768;  // larger sub-buckets go to the radix sort at once
     constexpr int TS1 = 4096, TS2 = 8192;
+    // pieces of a failed sub-bucket: each sized for WIDE_PIECE_KEYS distinct
+    // keys at 0.3 distinct per instance, at most WIDE_MAX_PIECES of them and
+    // WIDE_PIECE_WORK instances decoded over all of them (each piece decodes
+    // the whole sub-bucket); beyond that, and for sub-buckets of more than
+    // WIDE_SPLIT_MAX instances, the radix sort
+    constexpr uint64_t WIDE_PIECE_KEYS = 6144, WIDE_MAX_PIECES = 64, WIDE_PIECE_WORK = 1ull << 22,
+                       WIDE_SPLIT_MAX = 1ull << 20;
+    constexpr uint64_t WIDE_EXTRACT_KMERS = 1ull << 16;  // instances per extraction work item
     std::vector<uint32_t> slog(2 * P);
     uint64_t NB = 0;
     for (uint32_t p = 0; p < P; p++) {
@@ -2241,34 +2250,75 @@ int count_hash_wide(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vecto
             CK(cudaStreamSynchronize(ctx->s));
             const uint32_t nfail = std::min<uint32_t>(ctx->h_ids.as<uint32_t>()[0], (uint32_t)NB);
             const uint64_t *hkm = ctx->h_km.as<uint64_t>(), *hoff = ctx->h_off.as<uint64_t>();
-            std::vector<uint32_t> rest, over;
+            // the failed sub-buckets in pieces by key hash (wide_piece): pb the
+            // sub-bucket, pp its (piece, pieces); pieces that stay too large go
+            // to the radix sort (sb, sp)
+            std::vector<uint32_t> pb, pp, sb, sp;
             for (uint32_t i = 0; i < nfail; i++) {
                 const uint32_t b = ctx->h_ids.as<uint32_t>()[1 + i];
-                (hkm[b] > HEAVY_WIDE ? rest : over).push_back(b);
+                const uint64_t m = hkm[b];
+                const uint64_t n0 = std::max<uint64_t>(1, (m * 3 / 10 + WIDE_PIECE_KEYS - 1) / WIDE_PIECE_KEYS);
+                const bool split = m <= WIDE_SPLIT_MAX && n0 <= WIDE_MAX_PIECES && n0 * m <= WIDE_PIECE_WORK;
+                for (uint32_t r = 0; r < (split ? n0 : 1u); r++) {
+                    (split ? pb : sb).push_back(b);
+                    (split ? pp : sp).push_back(r);
+                    (split ? pp : sp).push_back(split ? (uint32_t)n0 : 1u);
+                }
             }
-            if (!over.empty()) {  // second pass: 8192 slots, one CTA per SM
-                const uint32_t no = (uint32_t)over.size();
-                CK(ctx->h_ids2.ensure((no + 1) * 4ull));
-                CK(ctx->bk_ids2.ensure(no * 4ull));
-                CK(ctx->bk_failed2.ensure((no + 1) * 4ull));
-                std::memcpy(ctx->h_ids2.p, over.data(), no * 4ull);
-                CK(cudaMemcpyAsync(ctx->bk_ids2.p, ctx->h_ids2.p, no * 4ull, cudaMemcpyHostToDevice, ctx->s));
+            auto put_pieces = [&](const std::vector<uint32_t> &ib, const std::vector<uint32_t> &ip) -> int {
+                const size_t np = ib.size();
+                CK(ctx->h_ids2.ensure(np * 12 + 8 * (np + 1)));
+                CK(ctx->bk_ids2.ensure(np * 4));
+                CK(ctx->bk_piece.ensure(np * 8));
+                std::memcpy(ctx->h_ids2.p, ib.data(), np * 4);
+                std::memcpy(ctx->h_ids2.as<uint8_t>() + np * 4, ip.data(), np * 8);
+                CK(cudaMemcpyAsync(ctx->bk_ids2.p, ctx->h_ids2.p, np * 4, cudaMemcpyHostToDevice, ctx->s));
+                CK(cudaMemcpyAsync(ctx->bk_piece.p, ctx->h_ids2.as<uint8_t>() + np * 4, np * 8, cudaMemcpyHostToDevice,
+                                   ctx->s));
+                return GKC_OK;
+            };
+            // second pass, level by level: 8192 slots, one CTA per SM; a piece
+            // that overflows splits in two at the next level
+            while (!pb.empty()) {
+                const uint32_t np = (uint32_t)pb.size();
+                RET(put_pieces(pb, pp));
+                CK(ctx->bk_failed2.ensure((np + 1) * 4ull));
                 CK(cudaMemsetAsync(ctx->bk_failed2.p, 0, 4, ctx->s));
                 bp.ids = ctx->bk_ids2.as<uint32_t>();
+                bp.piece = ctx->bk_piece.as<uint32_t>();
                 bp.failed = ctx->bk_failed2.as<uint32_t>();
+                bp.heavy_kmers = UINT64_MAX;
                 {
                     uint64_t ob = 0;
-                    for (uint32_t b : over) ob += 16 * (hoff[b + 1] - hoff[b]);
+                    for (uint32_t b : pb) ob += 16 * (hoff[b + 1] - hoff[b]);
                     KScope ks(ctx, GKC_K_HASH_RECORDS, (double)ob);
-                    bucket_count_wide_kernel<TS2><<<no, BC_THREADS, TS2 * 24, ctx->s>>>(bp);
+                    bucket_count_wide_kernel<TS2><<<np, BC_THREADS, TS2 * 24, ctx->s>>>(bp);
                     LAUNCHED();
                 }
-                CK(cudaMemcpyAsync(ctx->h_ids2.p, ctx->bk_failed2.p, (no + 1) * 4ull, cudaMemcpyDeviceToHost, ctx->s));
+                uint32_t *hf = reinterpret_cast<uint32_t *>(ctx->h_ids2.as<uint8_t>() + np * 12);
+                CK(cudaMemcpyAsync(hf, ctx->bk_failed2.p, (np + 1) * 4ull, cudaMemcpyDeviceToHost, ctx->s));
                 CK(cudaStreamSynchronize(ctx->s));
-                const uint32_t nf2 = std::min<uint32_t>(ctx->h_ids2.as<uint32_t>()[0], no);
-                ctx->times[8] += (double)(no - nf2);
-                rest.insert(rest.end(), ctx->h_ids2.as<uint32_t>() + 1, ctx->h_ids2.as<uint32_t>() + 1 + nf2);
+                const uint32_t nf2 = std::min<uint32_t>(hf[0], np);
+                ctx->times[8] += (double)(np - nf2);
+                std::vector<uint32_t> nb, npp;
+                for (uint32_t i = 0; i < nf2; i++) {
+                    const uint32_t j = hf[1 + i], b = pb[j], r = pp[2 * j], n = pp[2 * j + 1];
+                    if (2ull * n <= WIDE_MAX_PIECES && 2ull * n * hkm[b] <= WIDE_PIECE_WORK) {
+                        for (uint32_t h = 0; h < 2; h++) {
+                            nb.push_back(b);
+                            npp.push_back(2 * r + h);
+                            npp.push_back(2 * n);
+                        }
+                    } else {
+                        sb.push_back(b);
+                        sp.push_back(r);
+                        sp.push_back(n);
+                    }
+                }
+                pb.swap(nb);
+                pp.swap(npp);
             }
+            bp.piece = nullptr;
             unsigned long long hg[3];
             CK(cudaMemcpyAsync(ctx->h_scal.p, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
             CK(cudaStreamSynchronize(ctx->s));
@@ -2285,37 +2335,69 @@ int count_hash_wide(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vecto
             CK(cudaEventSynchronize(ctx->e3));
             CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
             acc_ms += ms;
-            // the rest by the radix sort: their instances extracted, sorted,
-            // run-length reduced and thresholded after this group's output
-            if (!rest.empty()) {
-                ctx->times[5] += (double)rest.size();
-                std::vector<unsigned long long> koff(rest.size());
-                uint64_t n = 0;
-                for (size_t i = 0; i < rest.size(); i++) {
-                    koff[i] = n;
-                    n += hkm[rest[i]];
+            // the rest by the radix sort: the k-mer instances of those pieces
+            // counted, extracted, sorted, run-length reduced and thresholded
+            // after this group's output
+            if (!sb.empty()) {
+                ctx->times[5] += (double)sb.size();
+                // work items of about WIDE_EXTRACT_KMERS instances: entry ranges of one piece
+                std::vector<unsigned long long> wr;
+                std::vector<uint32_t> wp;
+                uint64_t ib = 0;
+                for (size_t j = 0; j < sb.size(); j++) {
+                    const uint32_t b = sb[j];
+                    const uint64_t ne = hoff[b + 1] - hoff[b];
+                    const uint64_t per = std::max<uint64_t>(1, hkm[b] / std::max<uint64_t>(ne, 1));
+                    const uint64_t w = std::max<uint64_t>(32, WIDE_EXTRACT_KMERS / per);
+                    ib += 16 * ne;
+                    for (uint64_t c = hoff[b]; c < hoff[b + 1]; c += w) {
+                        wr.push_back(c);
+                        wr.push_back(std::min<uint64_t>(c + w, hoff[b + 1]));
+                        wp.push_back(sp[2 * j]);
+                        wp.push_back(sp[2 * j + 1]);
+                    }
                 }
-                const uint32_t nr = (uint32_t)rest.size();
-                CK(ctx->keysA.ensure(n * sizeof(u128)));
-                CK(ctx->keysB.ensure(n * sizeof(u128)));
-                CK(ctx->bk_ids2.ensure(nr * 4ull));
-                CK(ctx->h_ids2.ensure(nr * 4ull + nr * 8ull));
-                CK(ctx->r_off.ensure(nr * 8ull));
-                std::memcpy(ctx->h_ids2.p, rest.data(), nr * 4ull);
-                std::memcpy(ctx->h_ids2.as<uint8_t>() + nr * 4ull, koff.data(), nr * 8ull);
-                CK(cudaMemcpyAsync(ctx->bk_ids2.p, ctx->h_ids2.p, nr * 4ull, cudaMemcpyHostToDevice, ctx->s));
-                CK(cudaMemcpyAsync(ctx->r_off.p, ctx->h_ids2.as<uint8_t>() + nr * 4ull, nr * 8ull,
-                                   cudaMemcpyHostToDevice, ctx->s));
+                const uint32_t nw = (uint32_t)(wr.size() / 2);
+                // pinned: [ranges 16 B][pieces 8 B][counts, then offsets 8 B] per item
+                CK(ctx->h_ids2.ensure(nw * 32ull));
+                CK(ctx->bk_piece.ensure(nw * 8ull));
+                CK(ctx->r_work.ensure(nw * 16ull));
+                CK(ctx->r_off.ensure(nw * 8ull));
+                uint8_t *hb = ctx->h_ids2.as<uint8_t>();
+                std::memcpy(hb, wr.data(), nw * 16ull);
+                std::memcpy(hb + nw * 16ull, wp.data(), nw * 8ull);
+                CK(cudaMemcpyAsync(ctx->r_work.p, hb, nw * 16ull, cudaMemcpyHostToDevice, ctx->s));
+                CK(cudaMemcpyAsync(ctx->bk_piece.p, hb + nw * 16ull, nw * 8ull, cudaMemcpyHostToDevice, ctx->s));
                 BExtractParams xp;
                 xp.entries = ctx->bk_entries.as<BEntry>();
-                xp.bucket_off = ctx->bk_off.as<uint64_t>();
-                xp.ids = ctx->bk_ids2.as<uint32_t>();
-                xp.key_off = ctx->r_off.as<unsigned long long>();
+                xp.range = ctx->r_work.as<unsigned long long>();
+                xp.piece = ctx->bk_piece.as<uint32_t>();
+                xp.key_off = nullptr;
                 xp.k = k;
+                xp.keys = nullptr;
+                xp.counts = ctx->r_off.as<unsigned long long>();
+                {
+                    KScope ks(ctx, GKC_K_SORT_EXTRACT, (double)ib);
+                    bucket_extract_wide_kernel<<<nw, BC_THREADS, 0, ctx->s>>>(xp);  // instances per item
+                    LAUNCHED();
+                }
+                unsigned long long *hc = reinterpret_cast<unsigned long long *>(hb + nw * 24ull);
+                CK(cudaMemcpyAsync(hc, ctx->r_off.p, nw * 8ull, cudaMemcpyDeviceToHost, ctx->s));
+                CK(cudaStreamSynchronize(ctx->s));
+                uint64_t n = 0;
+                for (uint32_t i = 0; i < nw; i++) {
+                    const unsigned long long c = hc[i];
+                    hc[i] = n;
+                    n += c;
+                }
+                CK(cudaMemcpyAsync(ctx->r_off.p, hc, nw * 8ull, cudaMemcpyHostToDevice, ctx->s));
+                CK(ctx->keysA.ensure(n * sizeof(u128)));
+                CK(ctx->keysB.ensure(n * sizeof(u128)));
+                xp.key_off = ctx->r_off.as<unsigned long long>();
                 xp.keys = ctx->keysA.as<u128>();
                 {
-                    KScope ks(ctx, GKC_K_SORT_EXTRACT, 16.0 * n);
-                    bucket_extract_wide_kernel<<<nr, BC_THREADS, 0, ctx->s>>>(xp);
+                    KScope ks(ctx, GKC_K_SORT_EXTRACT, (double)ib + 16.0 * n);
+                    bucket_extract_wide_kernel<<<nw, BC_THREADS, 0, ctx->s>>>(xp);
                     LAUNCHED();
                 }
                 float sort_ms = 0;  // appends at ctx->n_out, adds its distinct k-mers to ctx->n_distinct
@@ -3245,7 +3327,7 @@ int count_store(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<ch
     CK(cudaEventCreate(&t0));
     CK(cudaEventCreate(&t1));
     CK(cudaEventRecord(t0, ctx->s));
-    // k > 32: u128 keys, sort counter only
+    // k > 32: u128 keys (the hash counter's 128-bit tables, or the sort counter)
     ctx->res_kw = ctx->opt.k > 32 ? 2 : 1;
     int rc = ctx->opt.k > 32 ? (ctx->opt.counter == GKC_COUNTER_HASH ? count_hash_wide(ctx, cmin, cmax, want)
                                                                      : count_sort<u128>(ctx, cmin, cmax, want))

@@ -32,12 +32,13 @@ def test_wide_hash_matches_oracle(oracle, k, p, P, seed, cmin):
 
 @pytest.mark.parametrize("k,p", [(45, 11), (64, 11)])
 def test_wide_hash_low_complexity_takes_the_sort(oracle, k, p):
-    """Poly-A and (AT)n runs make sub-buckets of more than 32768 instances:
-    they are extracted and counted by the 128-bit radix sort, beside the
-    hash counter's own sub-buckets."""
+    """A poly-A read of 1.1 Mbp makes a sub-bucket of more than 2^20
+    instances: it is extracted and counted by the 128-bit radix sort, beside
+    the hash counter's own sub-buckets; (AT)n and (CAG)n runs make heavy
+    sub-buckets that are counted in pieces."""
     r = np.random.default_rng(11)
     rnd = lambda n: bytes(np.frombuffer(b"ACGT", np.uint8)[r.integers(0, 4, n)])
-    parts = [rnd(20_000), b"A" * 40_000, rnd(100) + b"A" * 3000 + rnd(100), b"AT" * 25_000,
+    parts = [rnd(20_000), b"A" * 1_100_000, rnd(100) + b"A" * 3000 + rnd(100), b"AT" * 25_000,
              rnd(k), rnd(k - 1), rnd(k + 1), b"", rnd(2047), rnd(8193), b"CAG" * 1000 + rnd(3000),
              b"ACGTNACGTN" * 40, rnd(300).lower()]
     reads, offs = csr(parts)
@@ -52,17 +53,21 @@ def test_wide_hash_low_complexity_takes_the_sort(oracle, k, p):
     assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
 
 
-def test_wide_hash_overflowing_sub_bucket(oracle):
-    """A minimizer made the preferred one for 150 reads adds ~5k distinct
-    k-mers to its sub-bucket: more than the 4096-slot table holds.  It is
-    counted by the second pass or, failing that, the radix sort; either way
-    the oracle's multiset."""
+@pytest.mark.parametrize("n_x,route", [(150, "one"), (600, "split"), (6000, "sort")])
+def test_wide_hash_overflowing_sub_bucket(oracle, n_x, route):
+    """A minimizer X made the preferred one for n_x reads of 150 bases: each
+    read adds the 35 k-mers that contain X to X's sub-bucket, all distinct.
+    150 reads (5k keys) overflow the 4096-slot table and fit the second
+    pass's 8192; 600 (21k) are counted in two key-hash pieces that overflow
+    and split into four; 6000 (210k) in pieces whose split would decode more
+    than the limit, so those pieces go to the radix sort, with the key filter.
+    Every route gives the oracle's multiset."""
     k, p, P = 45, 11, 4
     r = np.random.default_rng(41)
     acgt = np.frombuffer(b"ACGT", np.uint8)
     rnd = lambda n: bytes(acgt[r.integers(0, 4, n)])
     X = b"CTTGACCGTAG"
-    parts = [rnd(70) + X + rnd(69) for _ in range(150)] + [rnd(150) for _ in range(3000)]
+    parts = [rnd(70) + X + rnd(69) for _ in range(n_x)] + [rnd(150) for _ in range(3000)]
     reads, offs = csr(parts)
     code = lambda s: int("".join(str("ACGT".index(chr(ch))) for ch in s), 4)
     lut = r.permutation(4 ** p).astype(np.uint32)
@@ -75,7 +80,12 @@ def test_wide_hash_overflowing_sub_bucket(oracle):
         n, d = c.count_reads(reads, offs)
         km, ct = sorted_table(*c.result())
         t = c.timings()
-    assert t["second_pass_sub_buckets"] + t["overflowed_sub_buckets"] >= 1
+    if route == "one":
+        assert t["second_pass_sub_buckets"] >= 1 and t["overflowed_sub_buckets"] == 0
+    elif route == "split":
+        assert t["second_pass_sub_buckets"] >= 4 and t["overflowed_sub_buckets"] == 0
+    else:
+        assert t["overflowed_sub_buckets"] >= 2
     assert d == do and np.array_equal(km, ko) and np.array_equal(ct, co)
 
 
