@@ -406,11 +406,12 @@ __device__ __forceinline__ void cta_quads(const BEntry *ent, uint64_t e0, uint64
 // instead of inserting; the caller then abandons the table.
 constexpr uint32_t SM_MAX_PROBE = 128;
 
+// TS need not be a power of two: the slot is the top 32 bits of the hash
+// scaled to [0, TS) (for TS = 2^L, its top L bits), and probes wrap at TS.
 template <int TS>
 __device__ __forceinline__ void smem_add(unsigned long long *tk, uint32_t *tc, volatile uint32_t *over,
                                          uint64_t key, uint32_t c) {
-    constexpr int LOG = __builtin_ctz(TS);
-    uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (64 - LOG));
+    uint32_t h = (uint32_t)((((key * 0x9E3779B97F4A7C15ull) >> 32) * (uint64_t)TS) >> 32);
     for (uint32_t pr = 0; pr < SM_MAX_PROBE; pr++) {
         unsigned long long cur = tk[h];
         if (cur == key) {
@@ -424,7 +425,7 @@ __device__ __forceinline__ void smem_add(unsigned long long *tk, uint32_t *tc, v
                 return;
             }
         }
-        h = (h + 1) & (TS - 1);
+        h = h + 1 == (uint32_t)TS ? 0u : h + 1;
     }
     *over = 1;
 }
@@ -439,6 +440,7 @@ __device__ __forceinline__ void smem_collect(const unsigned long long *tk, const
                                              unsigned long long *base_s) {
     // thread i owns slots i, i + NT, i + 2 NT, ...: conflict-free loads (the
     // output order inside a table does not matter)
+    static_assert(TS % NT == 0, "whole slots per thread");
     constexpr int PER = TS / NT;
     uint32_t keep = 0, occ = 0;
 #pragma unroll
@@ -473,8 +475,12 @@ __device__ __forceinline__ void smem_collect(const unsigned long long *tk, const
     }
 }
 
+// CTAs per SM that a table of TS slots (12 bytes each) allows in 228 KB of
+// shared memory, as the launch bound's minimum.
+constexpr int bc_min_ctas(int ts) { return ts <= 4096 ? 4 : ts <= 6144 ? 3 : ts <= 8192 ? 2 : 1; }
+
 template <int TS>
-__global__ void __launch_bounds__(BC_THREADS)
+__global__ void __launch_bounds__(BC_THREADS, bc_min_ctas(TS))
 bucket_count_kernel(BCountParams a) {
     extern __shared__ unsigned long long tk[];             // [TS] keys
     uint32_t *tc = reinterpret_cast<uint32_t *>(tk + TS);  // [TS] counts

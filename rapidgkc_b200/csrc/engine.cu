@@ -1621,7 +1621,10 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
             // Second pass: a sub-bucket that outgrew the 8192-slot table (not a
             // heavy one) is counted again with 16384 slots; only heavy
             // sub-buckets and those that overflow again take the record path,
-            // whose records cost several times the decode.
+            // whose records cost several times the decode.  (A first pass of
+            // 6144 slots at three CTAs per SM inserted 14% faster, but sent so
+            // many more sub-buckets of high-error reads to the later passes
+            // that mixed long reads lost 25%.)
             std::vector<uint32_t> heavy, over;
             for (uint32_t b : ids) (ctx->h_km.as<uint64_t>()[b] > BC_HEAVY_KMERS ? heavy : over).push_back(b);
             if (!over.empty()) {
@@ -1648,8 +1651,9 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
                 CK(cudaStreamSynchronize(ctx->s));
                 const uint32_t nf2 = std::min<uint32_t>(ctx->h_ids2.as<uint32_t>()[0], no);
                 ctx->times[8] += (double)(no - nf2);
-                heavy.insert(heavy.end(), ctx->h_ids2.as<uint32_t>() + 1, ctx->h_ids2.as<uint32_t>() + 1 + nf2);
+                over.assign(ctx->h_ids2.as<uint32_t>() + 1, ctx->h_ids2.as<uint32_t>() + 1 + nf2);
             }
+            heavy.insert(heavy.end(), over.begin(), over.end());
             ids.swap(heavy);
         }
         if (!ids.empty()) {
