@@ -529,6 +529,136 @@ bucket_count_kernel(BCountParams a) {
                                  a.err, ws, &base_s);
 }
 
+// smem_add that also lists each slot it claims in tl (nl counts them), so
+// that the table can be collected and cleared by its occupied slots alone.
+template <int TS>
+__device__ __forceinline__ void smem_add_listed(unsigned long long *tk, uint32_t *tc, uint16_t *tl, uint32_t *nl,
+                                                volatile uint32_t *over, uint64_t key, uint32_t c) {
+    uint32_t h = (uint32_t)((((key * 0x9E3779B97F4A7C15ull) >> 32) * (uint64_t)TS) >> 32);
+    for (uint32_t pr = 0; pr < SM_MAX_PROBE; pr++) {
+        unsigned long long cur = tk[h];
+        if (cur == key) {
+            atomicAdd(&tc[h], c);
+            return;
+        }
+        if (cur == EMPTY_KEY) {
+            unsigned long long old = atomicCAS(&tk[h], (unsigned long long)EMPTY_KEY, (unsigned long long)key);
+            if (old == EMPTY_KEY) {
+                tl[atomicAdd(nl, 1u)] = (uint16_t)h;
+                atomicAdd(&tc[h], c);
+                return;
+            }
+            if (old == key) {
+                atomicAdd(&tc[h], c);
+                return;
+            }
+        }
+        h = h + 1 == (uint32_t)TS ? 0u : h + 1;
+    }
+    *over = 1;
+}
+
+// The first pass of the sub-bucket counter as a persistent kernel: each CTA
+// clears its table once, then takes sub-buckets b0 + i (i from the counter
+// *next, below nb) one after another.  A sub-bucket is counted as in
+// bucket_count_kernel, but every claimed slot is listed, and the table is
+// collected and cleared through that list: a sub-bucket of 8k instances holds
+// about 1-2k distinct k-mers, so clearing and scanning all 8192 slots for
+// each of a million sub-buckets cost more than its decode (11.5 of the
+// 50 ms the launch took on 6 Gbp).  TS <= 65536 (u16 slot list).
+template <int TS>
+__global__ void __launch_bounds__(BC_THREADS, bc_min_ctas(TS))
+bucket_count_persistent_kernel(BCountParams a, uint32_t nb, uint32_t *next) {
+    static_assert(TS <= 65536, "u16 slot list");
+    extern __shared__ unsigned long long tk[];             // [TS] keys
+    uint32_t *tc = reinterpret_cast<uint32_t *>(tk + TS);  // [TS] counts
+    uint16_t *tl = reinterpret_cast<uint16_t *>(tc + TS);  // [TS] claimed slots
+    __shared__ uint32_t ws[BC_THREADS / 32];
+    __shared__ volatile uint32_t over;
+    __shared__ unsigned long long base_s;
+    __shared__ uint32_t next_grp, cur_i, nl;
+    for (int t = threadIdx.x; t < TS; t += BC_THREADS) {
+        tk[t] = EMPTY_KEY;
+        tc[t] = 0;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t mask = kmask(a.k);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            cur_i = atomicAdd(next, 1u);
+            over = 0;
+            nl = 0;
+            next_grp = BC_THREADS / 32;
+        }
+        __syncthreads();  // also orders the previous sub-bucket's clearing before this one's inserts
+        const uint32_t i = cur_i;
+        if (i >= nb) break;
+        const uint32_t b = a.b0 + i;
+        const uint64_t e0 = a.bucket_off[b], e1 = a.bucket_off[b + 1];
+        if (e0 != e1 && a.bucket_kmers[b] > a.heavy_kmers) {
+            if (threadIdx.x == 0) {
+                const uint32_t f = atomicAdd(a.failed, 1u);
+                a.failed[1 + f] = b;
+            }
+        } else if (e0 != e1) {
+            for (uint64_t bb = e0 + (uint64_t)warp * 32; bb < e1;) {
+                if (__any_sync(FULL, over != 0)) break;  // a warp vote: the warp leaves together
+                warp_kmer_runs(a.entries, bb, e1, a.k, mask, [&](uint64_t key, uint32_t run) {
+                    smem_add_listed<TS>(tk, tc, tl, &nl, &over, key, run);
+                });
+                uint32_t g = 0;
+                if (lane == 0) g = atomicAdd(&next_grp, 1u);
+                bb = e0 + 32ull * __shfl_sync(FULL, g, 0);
+            }
+            __syncthreads();
+            const uint32_t n = nl;  // <= TS: a slot is claimed once
+            if (over) {
+                if (threadIdx.x == 0) {
+                    const uint32_t f = atomicAdd(a.failed, 1u);
+                    a.failed[1 + f] = b;
+                }
+                for (uint32_t j = threadIdx.x; j < n; j += BC_THREADS) {
+                    const uint32_t sl = tl[j];
+                    tk[sl] = EMPTY_KEY;
+                    tc[sl] = 0;
+                }
+            } else {
+                // collect through the list (thread t takes entries t, t + NT, ...
+                // in both loops, so its prefix offsets line up), clearing as it goes
+                uint32_t keep = 0;
+                for (uint32_t j = threadIdx.x; j < n; j += BC_THREADS) {
+                    const uint32_t c = tc[tl[j]];
+                    keep += (c >= a.cmin && c <= a.cmax);
+                }
+                uint32_t tot;
+                const uint32_t pre = block_exclusive_scan<BC_THREADS>(keep, &tot, ws);
+                if (threadIdx.x == 0) {
+                    base_s = tot ? atomicAdd(a.out_cursor, (unsigned long long)tot) : 0ull;
+                    if (n) atomicAdd(a.distinct, (unsigned long long)n);
+                }
+                __syncthreads();
+                uint64_t o = base_s + pre;
+                for (uint32_t j = threadIdx.x; j < n; j += BC_THREADS) {
+                    const uint32_t sl = tl[j];
+                    const uint32_t c = tc[sl];
+                    if (c >= a.cmin && c <= a.cmax) {
+                        if (o < a.out_cap) {
+                            a.out_k[o] = tk[sl];
+                            a.out_c[o] = c;
+                        } else {
+                            atomicOr(a.err, ERR_OUTPUT_FULL);
+                        }
+                        o++;
+                    }
+                    tk[sl] = EMPTY_KEY;
+                    tc[sl] = 0;
+                }
+            }
+        }
+        __syncthreads();  // cur_i, nl and the list are rewritten at the top
+    }
+}
+
 // L2-table insert of one sub-bucket's entries (hash_l2_only mode).
 __global__ void __launch_bounds__(H_THREADS)
 hash_insert_entries_kernel(const BEntry *ent, uint64_t n, int k, HSlot *tab, uint64_t tmask, uint32_t *err) {

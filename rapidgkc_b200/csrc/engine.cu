@@ -348,6 +348,7 @@ struct gkc_ctx {
     DevBuf bk_arena2;  // second staging arena: a spilled store's next group is staged beside the current one
     DevBuf bk_ids2, bk_failed2;  // the second counting pass: its sub-buckets and those that failed again
     DevBuf bk_piece;             // 128-bit counter: (piece, pieces) of each second-pass CTA
+    DevBuf bk_next;              // the persistent first pass's sub-bucket counter
     PinBuf h_ids2;
     DevBuf r_work, r_count, r_off, r_cur, r_recs, r_failed;  // record sub-buckets
     DevBuf r_stage, r_winst, r_woff, r_wrec;                  // per-work-item record segments
@@ -392,7 +393,7 @@ struct gkc_ctx {
                         &mlp_w, &mlp_s, &mlp_scalar, &fx_text, &fx_tiles, &fx_state, &fx_kept,
                         &fx_reads, &fx_res, &fx_out, &fx_offs, &sk_tiles, &sk_state, &sk_tstarts, &sk_res,
                         &sk_starts, &sk_k32, &hpc_tiles, &hpc_tbase, &hpc_reads, &hpc_offs, &os_status, &os_hist,
-                        &os_segs, &os_ctr, &bk_ids2, &bk_failed2, &bk_piece};
+                        &os_segs, &os_ctr, &bk_ids2, &bk_failed2, &bk_piece, &bk_next};
         for (auto *d : ds) d->release();
         PinBuf *ps[] = {&offs_pin[0], &offs_pin[1], &pk_host[0], &pk_host[1], &h_hist, &h_flags, &h_scal, &h_off, &h_km, &h_ids, &h_work,
                         &h_desc, &h_cur, &h_segs, &h_ids2};
@@ -1390,8 +1391,14 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     CK(cudaMemsetAsync(ctx->scal.p, 0, 64, ctx->s));
     auto *sc = ctx->scal.as<unsigned long long>();
     CK(cudaMemcpyAsync(sc, &ctx->n_out, 8, cudaMemcpyHostToDevice, ctx->s));
-    CK(cudaFuncSetAttribute(bucket_count_kernel<BC_TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            BC_TS * 12));
+    CK(cudaFuncSetAttribute(bucket_count_persistent_kernel<BC_TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            BC_TS * 14));
+    CK(cudaFuncSetAttribute(bucket_count_persistent_kernel<BC_TS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                            cudaSharedmemCarveoutMaxShared));
+    int bc_per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bc_per_sm, bucket_count_persistent_kernel<BC_TS>, BC_THREADS,
+                                                     BC_TS * 14));
+    CK(ctx->bk_next.ensure(8));
     CK(cudaFuncSetAttribute(bucket_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BS_SMEM));
     // groups of partitions
     // a spilled store holds two staging arenas (this group's and the next's)
@@ -1585,8 +1592,13 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         if (!ctx->opt.hash_l2_only) {
             uint64_t gbytes = 0;
             for (uint32_t p = p0; p < p1; p++) gbytes += nbp[p];
+            const uint32_t nbg = (uint32_t)(bbase(p1) - bbase(p0));
+            const uint32_t grid =
+                std::max<uint32_t>(1, std::min<uint32_t>(nbg, (uint32_t)(ctx->sms * std::max(bc_per_sm, 1))));
+            CK(cudaMemsetAsync(ctx->bk_next.p, 0, 4, ctx->s));
             KScope ks(ctx, GKC_K_HASH_INSERT, (double)gbytes + 16.0 * gs);
-            bucket_count_kernel<BC_TS><<<(unsigned)(bbase(p1) - bbase(p0)), BC_THREADS, BC_TS * 12, ctx->s>>>(bp);
+            bucket_count_persistent_kernel<BC_TS><<<grid, BC_THREADS, BC_TS * 14, ctx->s>>>(bp, nbg,
+                                                                                           ctx->bk_next.as<uint32_t>());
             LAUNCHED();
         }
         CK(cudaEventRecord(ctx->e3, ctx->s));
