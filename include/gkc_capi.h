@@ -370,8 +370,7 @@ int gkc_mlp_order(gkc_ctx *ctx, const float *params, uint64_t heavy, uint32_t *l
  *                waits for the stream before it returns
  * Runs on the current CUDA device.  The first call on a device (and the first
  * after the device's context is reset, e.g. by cudaDeviceReset) looks up the
- * scratch's address (cudaGetSymbolAddress); make that first call before any
- * stream capture begins.  All calls on one device share the one scratch
+ * scratch's address (cudaGetSymbolAddress).  All calls on one device share the one scratch
  * table and it keeps the last call's contents (each call clears it first),
  * so two calls in flight at the same time (other host threads, other
  * streams) race and give wrong results: the caller serialises them.
