@@ -302,12 +302,16 @@ struct gkc_ctx {
     double times[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // see gkc_last_timings
 
     // phase 1 buffers
-    DevBuf reads[2], offs[2];
+    // host batches: NSLOT device slots, so a batch's copy does not wait for the
+    // phase 1 of the batch before it in the same slot
+    static constexpr int NSLOT = 3;
+    DevBuf reads[NSLOT], offs[NSLOT];
     PinBuf offs_pin[2];
     PinBuf pk_host[2];                   // host batches packed to 2-bit words (pinned), one per slot
     uint64_t h2d_bytes = 0;              // bytes the last gkc_add_reads copied host to device
     const uint32_t *p1_packed = nullptr;  // the batch in phase 1 as packed words (device), or null: ASCII
-    cudaEvent_t buf_free[2] = {nullptr, nullptr}, buf_ready[2] = {nullptr, nullptr};
+    cudaEvent_t buf_free[NSLOT] = {}, buf_ready[NSLOT] = {};
+    cudaEvent_t pk_copied[2] = {nullptr, nullptr};  // the last copy from pk_host[i] is done
     DevBuf cta_hist, cta_base;  // phase 1: per-CTA partition counts and base offsets
     DevBuf records, region_count, hist, flags, cursors, part_off, tile_read, codes;
     PinBuf h_hist, h_flags;
@@ -380,7 +384,7 @@ struct gkc_ctx {
         for (auto *c : pool) delete_chunk(c);
         store.clear();
         pool.clear();
-        DevBuf *ds[] = {&reads[0], &reads[1], &offs[0], &offs[1], &records, &region_count, &cta_hist, &cta_base,
+        DevBuf *ds[] = {&reads[0], &reads[1], &reads[2], &offs[0], &offs[1], &offs[2], &records, &region_count, &cta_hist, &cta_base,
                         &hist, &flags,
                         &cursors, &part_off, &tile_read, &codes, &lut, &table, &out_k, &out_c, &keysA, &keysB, &tiles,
                         &counts, &offsets, &blocksums, &heads_pos, &heads_key, &tilecnt, &tileoff, &segoff,
@@ -399,8 +403,8 @@ struct gkc_ctx {
                         &h_desc, &h_cur, &h_segs, &h_ids2};
         for (auto *p : ps) p->release();
         arena.release();
-        cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_ready[0], buf_ready[1], spill_ready,
-                             spill_done[0], spill_done[1]};
+        cudaEvent_t evs[] = {e0, e1, e2, e3, buf_free[0], buf_free[1], buf_free[2], buf_ready[0], buf_ready[1], buf_ready[2], spill_ready,
+                             spill_done[0], spill_done[1], pk_copied[0], pk_copied[1]};
         for (auto e : evs) if (e) cudaEventDestroy(e);
         for (auto e : batch_ev) cudaEventDestroy(e);
         prof_flush();
@@ -519,7 +523,8 @@ int ensure_table(gkc_ctx *ctx, uint64_t C) {
 // the output fails; the buffers are allocated again when next needed.
 void trim_scratch(gkc_ctx *ctx) {
     cudaStreamSynchronize(ctx->s);
-    DevBuf *ds[] = {&ctx->reads[0], &ctx->reads[1], &ctx->offs[0], &ctx->offs[1], &ctx->records, &ctx->codes,
+    DevBuf *ds[] = {&ctx->reads[0], &ctx->reads[1], &ctx->reads[2], &ctx->offs[0], &ctx->offs[1], &ctx->offs[2],
+                    &ctx->records, &ctx->codes,
                     &ctx->tile_read, &ctx->cta_hist, &ctx->cta_base, &ctx->spill_bytes[0], &ctx->spill_bytes[1],
                     &ctx->spill_idx[0], &ctx->spill_idx[1], &ctx->spill_keys[0], &ctx->spill_keys[1],
                     &ctx->stage_bytes, &ctx->stage_idx, &ctx->stage_keys, &ctx->r_work, &ctx->r_count, &ctx->r_off,
@@ -2530,9 +2535,12 @@ int gkc_create(int device, const gkc_options *opt, gkc_ctx **out) {
     cudaEvent_t *evs[] = {&ctx->e0, &ctx->e1, &ctx->e2, &ctx->e3};
     for (auto *e : evs)
         if (cudaEventCreate(e) != cudaSuccess) return cleanup(GKC_ECUDA);
-    for (int i = 0; i < 2; i++)
+    for (int i = 0; i < gkc_ctx::NSLOT; i++)
         if (cudaEventCreateWithFlags(&ctx->buf_free[i], cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&ctx->buf_ready[i], cudaEventDisableTiming) != cudaSuccess)
+            return cleanup(GKC_ECUDA);
+    for (int i = 0; i < 2; i++)
+        if (cudaEventCreateWithFlags(&ctx->pk_copied[i], cudaEventDisableTiming) != cudaSuccess)
             return cleanup(GKC_ECUDA);
     *out = ctx;
     return GKC_OK;
@@ -2610,16 +2618,18 @@ int hpc_batch(gkc_ctx *ctx, const uint8_t *d_reads, const uint64_t *d_offs, uint
     return GKC_OK;
 }
 
-// Phase 1 over host batches: the copy of batch i+1 (copy stream, two device
+// Phase 1 over host batches: the copy of batch i+1 (copy stream, three device
 // slots) overlaps phase 1 of batch i; no batch waits for the host (phase1_async)
 // unless the store spills (phase1_exact).
 // Host batches.  Every other batch crosses PCIe packed into 2-bit words (a
 // quarter of the ASCII bytes; gkc_pack_bases, on the host's threads), the
 // others as ASCII: the host's threads pack one batch while the copy engine
 // moves the next, so both host-memory readers work at once (packing every
-// batch left the copy engine idle and the threads the bound).  With
-// homopolymer compression every batch goes as ASCII (its kernels read it).
-// Batch i + 1 is prepared and copied while phase 1 of batch i runs.
+// batch left the copy engine idle and the threads the bound).  Packed
+// batches alternate between two pinned buffers, so the host packs the next
+// one while the last one's copy is still in flight.  With homopolymer
+// compression every batch goes as ASCII (its kernels read it).  Batch i + 1
+// is prepared and copied while phase 1 of batch i runs.
 int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, const std::vector<ReadBatch> &batches) {
     const bool exact = ctx->opt.spill_host;
     const bool pack = !ctx->opt.hpc;
@@ -2633,11 +2643,12 @@ int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, cons
     // packed words of a batch, and 4 zero words after them (the scatter reads
     // a code window one word past a superkmer's last base)
     const uint64_t max_w = (max_b + 15) / 16 + 4;
-    for (int slot = 0; slot < 2; slot++) {
+    for (int slot = 0; slot < gkc_ctx::NSLOT; slot++) {
         CK(ctx->reads[slot].ensure(std::max<uint64_t>(max_b + 64, pack ? max_w * 4 : 0)));
         CK(ctx->offs[slot].ensure((max_r + 1) * 8));
-        if (pack) CK(ctx->pk_host[slot].ensure(max_w * 4));
     }
+    if (pack)
+        for (int pb = 0; pb < 2; pb++) CK(ctx->pk_host[pb].ensure(max_w * 4));
     while (ctx->batch_ev.size() < 2 * nbat) {
         cudaEvent_t ev;
         CK(cudaEventCreate(&ev));
@@ -2645,19 +2656,21 @@ int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, cons
     }
     auto packed = [&](size_t bi) { return pack && (bi & 1); };
     auto stage = [&](size_t bi, cudaStream_t st) -> int {
-        const int slot = (int)(bi & 1);
+        const int slot = (int)(bi % gkc_ctx::NSLOT);
         const ReadBatch &b = batches[bi];
         const uint64_t base = offs[b.r0], nb = offs[b.r1] - base, nr = b.r1 - b.r0;
         if (packed(bi)) {
-            // the slot's pinned words are rewritten once their last copy is done
-            CK(cudaEventSynchronize(ctx->buf_ready[slot]));
+            // pinned buffer pb's words are rewritten once their last copy is done
+            const int pb = (int)((bi >> 1) & 1);
+            CK(cudaEventSynchronize(ctx->pk_copied[pb]));
             const uint64_t nw = (nb + 15) / 16;
-            uint32_t *hw = ctx->pk_host[slot].as<uint32_t>();
+            uint32_t *hw = ctx->pk_host[pb].as<uint32_t>();
             gkc_host::pack_bases(reinterpret_cast<const uint8_t *>(reads) + base, nb, hw, nw);
             std::memset(hw + nw, 0, 16);
             CK(cudaStreamWaitEvent(st, ctx->buf_free[slot], 0));
             CK(cudaEventRecord(ctx->batch_ev[2 * bi], st));  // the batch starts with its copy
             CK(cudaMemcpyAsync(ctx->reads[slot].p, hw, (nw + 4) * 4, cudaMemcpyHostToDevice, st));
+            CK(cudaEventRecord(ctx->pk_copied[pb], st));
             ctx->h2d_bytes += (nw + 4) * 4;
         } else {
             CK(cudaStreamWaitEvent(st, ctx->buf_free[slot], 0));
@@ -2671,7 +2684,7 @@ int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, cons
         return GKC_OK;
     };
     auto run = [&](size_t bi, bool sync_exact) -> int {
-        const int slot = (int)(bi & 1);
+        const int slot = (int)(bi % gkc_ctx::NSLOT);
         const ReadBatch &b = batches[bi];
         const uint64_t base = offs[b.r0], nb = offs[b.r1] - base, nr = b.r1 - b.r0;
         CK(cudaStreamWaitEvent(ctx->s, ctx->buf_ready[slot], 0));
@@ -2699,8 +2712,7 @@ int add_host_batches(gkc_ctx *ctx, const char *reads, const uint64_t *offs, cons
         CK(cudaEventRecord(ctx->batch_ev[2 * bi + 1], ctx->s));
         return rc;
     };
-    CK(cudaEventRecord(ctx->buf_free[0], ctx->s));
-    CK(cudaEventRecord(ctx->buf_free[1], ctx->s));
+    for (int slot = 0; slot < gkc_ctx::NSLOT; slot++) CK(cudaEventRecord(ctx->buf_free[slot], ctx->s));
     // batch i's phase 1 is queued before batch i + 1 is staged, so that the
     // device works while the host packs
     int rc = nbat ? stage(0, ctx->cs) : GKC_OK;
