@@ -1408,14 +1408,18 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
     // groups of partitions
     // a spilled store holds two staging arenas (this group's and the next's)
     uint64_t budget = spilled ? std::max<uint64_t>(1ull << 26, (uint64_t)(free0 * 0.1)) : ~0ull;
-    // streamed output: about four groups, so that each group's output is
-    // copied to the host while the next one counts
+    // streamed output: groups of 1/2, 1/4, 1/8 and 1/16 of the store, then
+    // the rest, so that each group's output is copied to the host while the
+    // next one counts (a group's copy takes about 0.4 of its counting time)
+    // and only the last, small group's copy is exposed
     const bool stream_out = ctx->stream_k && ctx->stream_c;
-    if (stream_out) {
-        uint64_t tot = 0;
-        for (uint32_t p = 0; p < P; p++) tot += nbp[p] + 28 * nsp[p];
-        budget = std::min<uint64_t>(budget, std::max<uint64_t>(tot / 4 + 1, 1ull << 20));
-    }
+    uint64_t stream_tot = 0;
+    if (stream_out)
+        for (uint32_t p = 0; p < P; p++) stream_tot += nbp[p] + 12 * nsp[p];  // as a group's gb counts
+    auto group_budget = [&](size_t g) -> uint64_t {
+        if (!stream_out) return budget;
+        return std::min<uint64_t>(budget, (stream_tot >> (std::min<size_t>(g, 3) + 1)) + 1);
+    };
     float acc_ms = 0;
     // the groups of partitions, formed up front
     struct Grp {
@@ -1430,8 +1434,9 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         }
         uint32_t q1 = q0;
         uint64_t gb = 0, gs = 0;
+        const uint64_t gbud = group_budget(grps.size());
         while (q1 < P && (!want || (*want)[q1]) &&
-               (q1 == q0 || gb + nbp[q1] + 12 * nsp[q1] + 16 * nsp[q1] <= budget)) {
+               (q1 == q0 || gb + nbp[q1] + 12 * nsp[q1] + 16 * nsp[q1] <= gbud)) {
             gb += nbp[q1] + 12 * nsp[q1];
             gs += nsp[q1];
             q1++;
@@ -1505,6 +1510,9 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         staged_g[sl] = (long)gi;
         return GKC_OK;
     };
+    // host copies of the sub-bucket offsets and k-mer counts, filled group by
+    // group over each group's own range of sub-buckets
+    std::vector<uint64_t> off(NB + 1), km(NB);
     for (size_t gi = 0; gi < grps.size();) {
         const uint32_t p0 = grps[gi].p0, p1 = grps[gi].p1;
         const uint64_t gs = grps[gi].gs;
@@ -1608,27 +1616,30 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
         }
         CK(cudaEventRecord(ctx->e3, ctx->s));
         // one host round trip: the failed sub-buckets, the sub-bucket offsets and
-        // k-mer counts the record path needs for them, and the output cursor
-        // (pinned buffers: pageable copies stage through the driver and stall
-        // with the host's load; every wait is a chance to catch such a stall)
+        // k-mer counts the record path needs for them (this group's range of
+        // sub-buckets only), and the output cursor (pinned buffers: pageable
+        // copies stage through the driver and stall with the host's load;
+        // every wait is a chance to catch such a stall)
+        const uint64_t gb0 = bbase(p0), gb1 = bbase(p1);
         CK(ctx->h_ids.ensure((NB + 1) * 4));
         CK(ctx->h_off.ensure((NB + 1) * 8));
         CK(ctx->h_km.ensure(NB * 8));
         CK(ctx->h_cur.ensure(32));
-        CK(cudaMemcpyAsync(ctx->h_ids.p, ctx->bk_failed.p, (NB + 1) * 4, cudaMemcpyDeviceToHost, ctx->s));
-        CK(cudaMemcpyAsync(ctx->h_off.p, ctx->bk_off.p, (NB + 1) * 8, cudaMemcpyDeviceToHost, ctx->s));
-        CK(cudaMemcpyAsync(ctx->h_km.p, ctx->bk_kmers.p, NB * 8, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(ctx->h_ids.p, ctx->bk_failed.p, (gb1 - gb0 + 1) * 4, cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(ctx->h_off.as<uint64_t>() + gb0, ctx->bk_off.as<uint64_t>() + gb0, (gb1 - gb0 + 1) * 8,
+                           cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaMemcpyAsync(ctx->h_km.as<uint64_t>() + gb0, ctx->bk_kmers.as<uint64_t>() + gb0, (gb1 - gb0) * 8,
+                           cudaMemcpyDeviceToHost, ctx->s));
         CK(cudaMemcpyAsync(ctx->h_cur.p, sc, 24, cudaMemcpyDeviceToHost, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
-        const uint32_t nfail = std::min<uint32_t>(ctx->h_ids.as<uint32_t>()[0], (uint32_t)NB);
+        const uint32_t nfail = std::min<uint32_t>(ctx->h_ids.as<uint32_t>()[0], (uint32_t)(gb1 - gb0));
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ctx->e2, ctx->e3));
         acc_ms += ms;
         groups++;
         std::vector<uint32_t> ids;
-        std::vector<uint64_t> off;
-        if (nfail || ctx->opt.hash_l2_only) {
-            off.assign(ctx->h_off.as<uint64_t>(), ctx->h_off.as<uint64_t>() + NB + 1);
+        if (nfail || ctx->opt.hash_l2_only) {  // this group's sub-bucket offsets: off[gb0 .. gb1]
+            std::copy(ctx->h_off.as<uint64_t>() + gb0, ctx->h_off.as<uint64_t>() + gb1 + 1, off.begin() + gb0);
             if (nfail) ids.assign(ctx->h_ids.as<uint32_t>() + 1, ctx->h_ids.as<uint32_t>() + 1 + nfail);
         }
         if (ctx->opt.hash_l2_only)  // every non-empty sub-bucket (one per partition)
@@ -1679,7 +1690,7 @@ int count_hash(gkc_ctx *ctx, uint32_t cmin, uint32_t cmax, const std::vector<cha
             } else {
                 ctx->fallback_buckets += ids.size();
                 ctx->times[5] += (double)ids.size();
-                std::vector<uint64_t> km(ctx->h_km.as<uint64_t>(), ctx->h_km.as<uint64_t>() + NB);
+                std::copy(ctx->h_km.as<uint64_t>() + gb0, ctx->h_km.as<uint64_t>() + gb1, km.begin() + gb0);
                 RET(count_buckets_records(ctx, ids, off, km, cmin, cmax));
             }
         }

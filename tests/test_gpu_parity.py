@@ -224,9 +224,10 @@ def test_retries_spill_and_groups(oracle):
 
 @pytest.mark.parametrize("pinned,redo", [(True, False), (False, False), (True, True)])
 def test_host_output_streamed_by_groups(oracle, pinned, redo, monkeypatch):
-    """count_reads into host arrays: the hash counter counts in about four
-    partition groups and copies each group's k-mers out while the next group
-    counts (forced output overflows redo every group before its copy)."""
+    """count_reads into host arrays: the hash counter counts in partition
+    groups of halving size (1/2, 1/4, 1/8, 1/16 of the store, then the rest)
+    and copies each group's k-mers out while the next group counts (forced
+    output overflows redo every group before its copy)."""
     import torch
     if redo:
         monkeypatch.setenv("GKC_OUT_ESTIMATE", "1")
