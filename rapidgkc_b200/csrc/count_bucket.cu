@@ -566,6 +566,8 @@ __device__ __forceinline__ void smem_add_listed(unsigned long long *tk, uint32_t
 // about 1-2k distinct k-mers, so clearing and scanning all 8192 slots for
 // each of a million sub-buckets cost more than its decode (11.5 of the
 // 50 ms the launch took on 6 Gbp).  TS <= 65536 (u16 slot list).
+constexpr int BC_TAIL = 256;  // entries at a sub-bucket's end handed out in groups of 16
+
 template <int TS>
 __global__ void __launch_bounds__(BC_THREADS, bc_min_ctas(TS))
 bucket_count_persistent_kernel(BCountParams a, uint32_t nb, uint32_t *next) {
@@ -601,14 +603,21 @@ bucket_count_persistent_kernel(BCountParams a, uint32_t nb, uint32_t *next) {
                 a.failed[1 + f] = b;
             }
         } else if (e0 != e1) {
-            for (uint64_t bb = e0 + (uint64_t)warp * 32; bb < e1;) {
+            // group g: 32 entries, except the sub-bucket's last BC_TAIL entries,
+            // which go in groups of 16 so that the warps finish close together
+            const uint64_t E = e1 - e0, tail = E < (uint64_t)BC_TAIL ? E : (uint64_t)BC_TAIL;
+            const uint64_t head = E - tail, nbig = (head + 31) / 32;
+            for (uint64_t g = warp;;) {
+                const uint64_t g0 = g < nbig ? 32 * g : head + 16 * (g - nbig);
+                if (g0 >= E) break;
+                const uint64_t g1 = g < nbig ? (32 * g + 32 < head ? 32 * g + 32 : head) : (g0 + 16 < E ? g0 + 16 : E);
                 if (__any_sync(FULL, over != 0)) break;  // a warp vote: the warp leaves together
-                warp_kmer_runs(a.entries, bb, e1, a.k, mask, [&](uint64_t key, uint32_t run) {
+                warp_kmer_runs(a.entries, e0 + g0, e0 + g1, a.k, mask, [&](uint64_t key, uint32_t run) {
                     smem_add_listed<TS>(tk, tc, tl, &nl, &over, key, run);
                 });
-                uint32_t g = 0;
-                if (lane == 0) g = atomicAdd(&next_grp, 1u);
-                bb = e0 + 32ull * __shfl_sync(FULL, g, 0);
+                uint32_t gn = 0;
+                if (lane == 0) gn = atomicAdd(&next_grp, 1u);
+                g = __shfl_sync(FULL, gn, 0);
             }
             __syncthreads();
             const uint32_t n = nl;  // <= TS: a slot is claimed once
