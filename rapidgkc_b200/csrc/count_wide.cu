@@ -4,7 +4,7 @@
 // significant position, masked to 2k bits, canonical min(x, revcomp(x)),
 // gpu_kmercounting.cu:63-74).  The reference counts these with its sort path
 // only; here they take the same sub-bucket scheme as the 64-bit counter
-// (count_bucket.cu), with three differences:
+// (count_bucket.cu), with four differences:
 //   * a lane's quad of k-mers is decoded from a 72-base window (24 bytes,
 //     three 48-bit fields) instead of 48 bases;
 //   * the shared-memory table holds 16-byte keys, which no atomic claims in
@@ -12,9 +12,14 @@
 //     being written -> ready) and its key is compared only once ready;
 //     4096 slots in 96 KB (8192 in the second pass), so sub-buckets are
 //     sized at about 4k instances;
-//   * sub-buckets that overflow the second pass too, and heavy ones, are not
-//     split into records: their k-mer instances are extracted into the key
-//     buffer and counted by the 128-bit radix sort (count_onesweep.cu).
+//   * a sub-bucket's quads are spread over the whole CTA (cta_quads): at
+//     large k a sub-bucket holds few, long superkmers;
+//   * sub-buckets that overflow, and heavy ones, are not split into records:
+//     they are counted in pieces by a hash of the key (wide_piece), each
+//     piece one CTA that decodes the whole sub-bucket and inserts its own
+//     keys; a piece that overflows splits in two, and pieces past the decode
+//     limit have their instances extracted into the key buffer and counted by
+//     the 128-bit radix sort (count_onesweep.cu).
 // Included by engine.cu after count_bucket.cu.
 
 namespace gkc {
